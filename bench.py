@@ -1,0 +1,406 @@
+"""Throughput of the TDMD force + integration path on B200.
+
+Workload: 32x32x32 Cu FCC = 131,072 atoms (a = 3.615 A, +-0.01 A seeded
+jitter, 300 K Maxwell-Boltzmann), analytic EAM tabulated as setfl splines
+(Nr = Nrho = 2000, smoothly cut over 4.5-5.0 A), dt = 1 fs, skin 0.3 A,
+neighbor rebuild every 10 steps, NVE -- mixed precision is the headline,
+the plain FP64 path is measured in the same run.
+
+One bench step = one FastPipelineScheduler::run_until window of 10 MD steps
+(one neighbor rebuild + 10 force evaluations), i.e. 1,310,720 atom-steps.
+L2 is flushed (256 MiB write) before every bench step, outside its timing.
+
+  value     atom-steps/s, device time (CUDA events on the scheduler's stream
+            around each window), inputs resident in HBM
+  e2e       same metric through the C ABI with host buffers: upload (pinned
+            host -> device) + run_until(10) + download (device -> pinned host)
+            per step, wall clock
+  roofline  dominant kernel (EAM force pass, mixed) vs the measured HBM copy
+            bandwidth, algorithmic bytes from the gather model
+  cpu_baseline  the reference's CPU path (oracle/_ref, compiled from its
+            sources; else the oracle port), 1 thread, a bounded sample
+
+`--impl reference` runs only the reference CPU path on the same workload.
+Multi-GPU (torchrun): replicas only -- every rank runs its own system, the
+value is the sum over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WINDOW = 10            # MD steps per bench step (= rebuild interval)
+NCELL = 32             # 32^3 FCC cells = 131,072 atoms
+SKIN = 0.3
+DT = 0.001
+METRIC = "atom-steps/s (EAM 131k atoms) mixed vs FP64 on 1 B200 at force rel err <=1e-5"
+
+
+# ---------------------------------------------------------------------------
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = max(smax, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def workload(seed=4321):
+    from tdmd_claude_b200 import workloads as W
+    return W.fcc_system(NCELL, 3.615, 300.0, seed), W.cu_eam_tables()
+
+
+def make_eam(t):
+    from tdmd_claude_b200 import EamAlloy
+    return EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+
+
+def make_sched(sysm, eam, precision, **kw):
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, make_config
+    s = FastPipelineScheduler(Box.make(sysm.lo, sysm.hi), sysm.n, eam,
+                              make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW,
+                                          precision=precision, **kw))
+    s.upload(sysm.positions, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+    return s
+
+
+def mean_neighbors(sysm, cutoff):
+    """Mean full-list length K of the built list (for the roofline bytes)."""
+    import torch
+
+    from tdmd_claude_b200 import Box, DeviceNeighborList
+    d = torch.as_tensor(sysm.positions, dtype=torch.float64, device="cuda")
+    nl = DeviceNeighborList()
+    nl.build(d, sysm.n, Box.make(sysm.lo, sysm.hi), cutoff, SKIN)
+    c, _, _ = nl.host_csr()
+    # interacting pairs (r < rc) for reference
+    return float(c.mean())
+
+
+def timed_windows(sched, steps, warmup, flush, torch, dist=None):
+    """Device ms per window (L2 flushed before each), max over ranks."""
+    stream = torch.cuda.ExternalStream(sched.stream())
+    step = sched.current_step()
+    for _ in range(warmup):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        step += WINDOW
+        sched.run_until(step)
+    l0 = sched.stats().kernel_launches
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ms = []
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)
+        step += WINDOW
+        sched.run_until(step)
+        ms.append(sched.last_window_ms())
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    wall = time.perf_counter() - t0
+    launches = sched.stats().kernel_launches - l0
+    total = float(np.sum(ms))
+    if dist is not None:
+        t = torch.tensor([total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    return total, wall, launches, ms
+
+
+def e2e_windows(sysm, eam, steps, warmup, torch):
+    """upload (pinned host) + run_until(WINDOW) + download (pinned host), wall."""
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, make_config
+    s = FastPipelineScheduler(Box.make(sysm.lo, sysm.hi), sysm.n, eam,
+                              make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW,
+                                          precision="mixed"))
+    n = sysm.n
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h_pos, h_vel = pin(sysm.positions), pin(sysm.velocities)
+    h_typ, h_ids, h_m = pin(sysm.types), pin(sysm.ids), pin(sysm.masses)
+    o_pos = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    o_vel = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    o_frc = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    h2d = h_pos.nbytes + h_vel.nbytes + h_typ.nbytes + h_ids.nbytes + h_m.nbytes
+    d2h = o_pos.nbytes + o_vel.nbytes + o_frc.nbytes
+
+    def one():
+        s.upload_ptrs(h_pos.data_ptr(), h_vel.data_ptr(), 0, h_typ.data_ptr(), h_ids.data_ptr(),
+                      h_m.data_ptr(), sysm.masses.size)
+        s.run_until(WINDOW)
+        s.download_ptrs(o_pos.data_ptr(), o_vel.data_ptr(), o_frc.data_ptr())
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    s.close()
+    return wall, h2d, d2h
+
+
+def cpu_baseline_sample(sysm, t, nsteps):
+    """The reference CPU path (or the oracle port) on the same system, 1 thread."""
+    from oracle import oracle as O
+    pos = sysm.positions.copy()
+    vel = sysm.velocities.copy()
+    frc = np.zeros_like(pos)
+    lo, hi = np.array(sysm.lo), np.array(sysm.hi)
+    R = O.ref()
+    if R is not None:
+        from tdmd_claude_b200 import io as TIO
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "cu.eam.alloy")
+            TIO.write_setfl(p, t)
+            h = R.ref_eam_load(p.encode())
+            import ctypes as C
+            pe = C.c_double()
+            sec = R.ref_run_cpu(h, 0, 0, 0, 0, pos.reshape(-1), vel.reshape(-1), frc.reshape(-1),
+                                sysm.types, sysm.masses, 1, sysm.n, lo, hi, np.ones(3, np.int32),
+                                DT, SKIN, WINDOW, nsteps, C.byref(pe))
+            R.ref_eam_free(h)
+        kind = "reference"
+    else:
+        oe = O.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+        t0 = time.perf_counter()
+        O.md_run(pos, vel, sysm.types, sysm.masses, sysm.lo, sysm.hi, DT, SKIN, WINDOW, [nsteps],
+                 eam=oe)
+        sec = time.perf_counter() - t0
+        kind = "port"
+    return sec, kind
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sysm, t = workload()
+    warm = max(1, min(args.warmup, 2))
+    cpu_baseline_sample(sysm, t, warm)          # warm caches/pages (untimed)
+    sec, kind = cpu_baseline_sample(sysm, t, args.steps)
+    value = sysm.n * args.steps / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "atom-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "eam_cu_fcc_131072", "atoms": sysm.n, "precision": "fp64 (CPU)",
+                   "dt_fs": 1.0, "skin": SKIN, "rebuild_every": WINDOW,
+                   "step": "one MD timestep of the whole system"},
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": 1, "kind": kind,
+                         "sample": f"{args.steps} MD steps of the 131,072-atom EAM system "
+                                   "(single-threaded reference CPU loop, rebuild every 10)"},
+        "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=10, help="reference CPU sample size")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = env_rank()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as D
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = D
+
+    sysm, t = workload(seed=4321 + rank)
+    eam = make_eam(t)
+    K = mean_neighbors(sysm, t.cutoff)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    # Force accuracy of the mixed path vs FP64 on the same state.
+    s64 = make_sched(sysm, eam, "fp64")
+    s32 = make_sched(sysm, eam, "mixed")
+    s64.run_until(0)
+    s32.run_until(0)
+    f64 = s64.download().forces
+    f32 = s32.download().forces.astype(np.float64)
+    rel_err = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
+
+    # Headline: mixed.
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_mixed, wall_mixed, launches, per = timed_windows(s32, args.steps, args.warmup, flush, torch,
+                                                        dist)
+    clk = clocks.stop()
+    # Plain FP64 path, same protocol.
+    ms_fp64, _, _, _ = timed_windows(s64, args.steps, args.warmup, flush, torch, dist)
+
+    units = world * sysm.n * WINDOW * args.steps
+    value = units / (ms_mixed * 1e-3)
+    value64 = units / (ms_fp64 * 1e-3)
+
+    # Per-kernel times (events around each phase, same windows, no graphs).
+    s32.set_profiling(True)
+    timed_windows(s32, max(5, args.steps // 3), 1, flush, torch, None)
+    kt = s32.kernel_times()
+    s32.set_profiling(False)
+    s64.set_profiling(True)
+    timed_windows(s64, max(5, args.steps // 3), 1, flush, torch, None)
+    kt64 = s64.kernel_times()
+    s64.set_profiling(False)
+
+    hbm, peak_kind = measured_peaks()
+    force_bytes = sysm.n * (48 + 24 * K)          # gather model, mixed force pass
+    dens_bytes = sysm.n * (40 + 20 * K)
+    force_ms = kt["force"][0]
+    achieved = force_bytes / (force_ms * 1e-3) / 1e9 if force_ms > 0 else None
+    traffic = None
+    prof_json = os.path.join(ROOT, "profiles", "eam_force_mixed_131k.json")
+    if os.path.exists(prof_json):
+        with open(prof_json) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    e2e_wall, h2d, d2h = (None, 0, 0)
+    if rank == 0 or world > 1:
+        e2e_wall, h2d, d2h = e2e_windows(sysm, eam, max(3, args.steps // 3), 2, torch)
+    e2e_steps = max(3, args.steps // 3)
+    e2e_value = sysm.n * WINDOW * e2e_steps / e2e_wall * world
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sec, kind = cpu_baseline_sample(sysm, t, args.cpu_steps)
+        cpu = {"value": sysm.n * args.cpu_steps / sec, "unit": "atom-steps/s", "cores": 1,
+               "kind": kind,
+               "sample": f"{args.cpu_steps} MD steps (rebuild every 10) of the same 131,072-atom "
+                         "EAM system, single-threaded reference CPU loop"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_mixed / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {
+                "workload": "eam_cu_fcc_131072", "atoms": sysm.n, "precision": "mixed",
+                "potential": "analytic Cu EAM as setfl splines, Nr=Nrho=2000, cut 4.5-5.0 A",
+                "dt_fs": 1.0, "skin": SKIN, "rebuild_every": WINDOW,
+                "md_steps_per_bench_step": WINDOW, "parallelism": f"replicas x{world}",
+                "l2": "flushed (256 MiB write) before every bench step, outside its timing",
+                "mean_neighbors_K": K,
+                "fp64": {"value": value64, "ms_per_step": ms_fp64 / args.steps},
+                "mixed_over_fp64": value / value64,
+                "force_rel_rms_err_mixed_vs_fp64": rel_err,
+                "wall_s_timed_region": wall_mixed,
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                         "kernel": "k_eam_force<GeoQ> (mixed)", "peak_source": peak_kind,
+                         "bytes_per_launch": force_bytes, "ms_per_launch": force_ms,
+                         "model": "gather model n*(48+24K) B, K = mean full-list length"},
+            "kernel_ms": {"mixed": kt, "fp64": kt64,
+                          "density_bytes_per_launch": dens_bytes},
+            "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "timing": "wall clock per step"},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    for s in (s32, s64):
+        s.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

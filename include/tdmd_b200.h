@@ -1,0 +1,305 @@
+/*
+ * tdmd_b200.h -- C ABI of the B200-native TDMD force + integration path.
+ *
+ * Plain C: pointers, sizes, opaque handles and int status codes.  No CUDA or
+ * torch types appear in a signature; CUDA streams travel as `void*`
+ * (a cudaStream_t, NULL = legacy default stream) and device arrays as typed
+ * pointers.  Every call returns TDMD_OK (0) or a tdmd_status code and leaves
+ * a message for tdmd_last_error() (thread-local).
+ *
+ * Each entry point names the reference interface it replaces
+ * (tdmd_Claude, path:line).  The header-only C++ layer in tdmd_b200.hpp puts
+ * the reference's class and function names back on top of these calls.
+ *
+ * Array layouts follow the reference's role types (src/core/types.hpp:63-79):
+ *   positions, velocities : double[3*n]  (Vec3D, AoS)
+ *   forces                : double[3*n] (FP64) or float[3*n] (mixed), AoS
+ *   types                 : int32[n], 1-based
+ *   ids                   : int32[n]
+ *   masses                : double[ntypes+1], indexed by the 1-based type
+ */
+#ifndef TDMD_B200_H
+#define TDMD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TDMD_B200_ABI_VERSION 1
+
+typedef enum tdmd_status {
+  TDMD_OK = 0,
+  TDMD_ERR_INVALID_ARGUMENT = 1,
+  TDMD_ERR_CUDA = 2,
+  TDMD_ERR_OUT_OF_MEMORY = 3,
+  TDMD_ERR_PARSE = 4,          /* malformed setfl / data input            */
+  TDMD_ERR_STATE = 5,          /* call order (e.g. run_until before upload) */
+  TDMD_ERR_NLIST_OVERFLOW = 6, /* neighbor capacity exceeded, retry failed  */
+  TDMD_ERR_TIMEOUT = 7,        /* a bounded device-side wait gave up        */
+  TDMD_ERR_UNSUPPORTED = 8
+} tdmd_status;
+
+/* Arithmetic of the force path.  FP64: everything double (the reference's
+ * TDMD_PRECISION=fp64 build).  MIXED: pair distances, splines and forces in
+ * FP32 with compensated FP32 per-atom accumulation; positions, velocities,
+ * energies, virial and the thermostat chain in FP64. */
+typedef enum tdmd_precision { TDMD_FP64 = 0, TDMD_MIXED = 1 } tdmd_precision;
+
+/* PotentialKind, src/scheduler/fast_pipeline_scheduler.cuh:36-39 */
+typedef enum tdmd_potential_kind { TDMD_POT_MORSE = 0, TDMD_POT_EAM = 1 } tdmd_potential_kind;
+
+/* Box, src/core/box.hpp:17-26 (orthorhombic, periodic flags per axis). */
+typedef struct tdmd_box {
+  double lo[3];
+  double hi[3];
+  int32_t periodic[3];
+} tdmd_box;
+
+/* MorseParams, src/potentials/device_morse.cuh:14-20 */
+typedef struct tdmd_morse_params {
+  double d;
+  double alpha;
+  double r0;
+  double rc;
+  double rc_sq;
+} tdmd_morse_params;
+
+/* FastPipelineConfig, src/scheduler/fast_pipeline_scheduler.cuh:42-46, plus
+ * the precision chosen per scheduler at run time (the reference fixes it at
+ * compile time), the CUDA-graph switch, NVT and adaptive-dt settings
+ * (PipelineConfig, src/scheduler/pipeline_scheduler.cuh:26-45). */
+typedef struct tdmd_fast_pipeline_config {
+  double dt;              /* ps, default 0.001                               */
+  double r_skin;          /* A, default 1.0                                  */
+  int32_t rebuild_every;  /* default 10                                      */
+  int32_t precision;      /* tdmd_precision                                  */
+  int32_t use_graphs;     /* capture rebuild windows as CUDA graphs (1)      */
+  int32_t lanes_per_atom; /* 0 = autotuned choice, else 1,2,4,8,16 or 32     */
+  /* NVT (Nose-Hoover chain) -- enabled when t_target > 0. */
+  double t_target;        /* K                                               */
+  double t_period;        /* ps                                              */
+  int32_t nhc_length;     /* chain length                                    */
+  /* Adaptive dt: dt = clamp(c2*rc/vmax, dt_min, dt_max) at each step start. */
+  int32_t adaptive_dt;
+  double dt_min;
+  double dt_max;
+  double c2;
+  /* Energy log: every `energy_every` steps (0 = off) the step's potential
+   * energy, kinetic energy (integer time) and virial are reduced on the
+   * device (FP64) into a log read by tdmd_sched_energy_log. */
+  int32_t energy_every;
+  int32_t energy_log_capacity;
+} tdmd_fast_pipeline_config;
+
+/* FastPipelineStats, src/scheduler/fast_pipeline_scheduler.cuh:49-53, plus
+ * graph and neighbor-capacity counters. */
+typedef struct tdmd_fast_pipeline_stats {
+  int64_t ticks;
+  int64_t kernel_launches; /* kernels enqueued (graph nodes counted per replay) */
+  int64_t rebuilds;
+  int64_t graph_launches;
+  int64_t nlist_retries;   /* windows re-run after a capacity overflow        */
+  int64_t nlist_capacity;  /* neighbor slots per atom currently allocated     */
+} tdmd_fast_pipeline_stats;
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                   */
+/* ------------------------------------------------------------------------ */
+const char* tdmd_last_error(void);
+int32_t tdmd_abi_version(void);
+/* Copies `bytes` between any two host/device pointers (cudaMemcpyDefault)
+ * on `stream` and waits for it.  Lets FFI callers read back the device
+ * arrays the list/force entry points fill (no reference counterpart: the
+ * reference's DeviceBuffer::copy_to_host, src/core/device_buffer.cuh:80-95,
+ * is a member of its RAII buffer). */
+int32_t tdmd_copy(void* dst, const void* src, size_t bytes, void* stream);
+/* Fills cfg with the reference defaults (dt 0.001, skin 1.0, rebuild 10,
+ * FP64, graphs on, NVE, no energy log). */
+void tdmd_fast_pipeline_config_default(tdmd_fast_pipeline_config* cfg);
+
+/* ------------------------------------------------------------------------ */
+/* EAM/alloy tables -- EamAlloy, src/potentials/eam_alloy.hpp:47-93          */
+/* ------------------------------------------------------------------------ */
+typedef struct tdmd_eam tdmd_eam;
+
+/* EamAlloy::read_setfl, src/potentials/eam_alloy.cpp:90-192. */
+int32_t tdmd_eam_read_setfl(const char* path, tdmd_eam** out);
+/* Same tables from raw setfl arrays: F[ntypes*nrho], rho[ntypes*nr],
+ * rphi[npairs*nr] (r*phi(r), pairs i<=j in setfl order). */
+int32_t tdmd_eam_create(int32_t ntypes, int32_t nrho, double drho, int32_t nr, double dr,
+                        double cutoff, const double* F, const double* rho, const double* rphi,
+                        tdmd_eam** out);
+int32_t tdmd_eam_destroy(tdmd_eam* eam);
+/* cutoff(), ntypes(); table sizes. */
+int32_t tdmd_eam_info(const tdmd_eam* eam, int32_t* ntypes, int32_t* nrho, double* drho,
+                      int32_t* nr, double* dr, double* cutoff);
+/* Packed a|b|c|d coefficients of one spline (kind 0 = F, 1 = rho, 2 = phi),
+ * SplineTable::build_splines, eam_alloy.cpp:19-50.  out holds 4*(n-1). */
+int32_t tdmd_eam_coeffs(const tdmd_eam* eam, int32_t kind, int32_t index, double* out);
+
+/* ------------------------------------------------------------------------ */
+/* Cell list -- DeviceCellList, src/domain/device_cell_list.cuh:16           */
+/* ------------------------------------------------------------------------ */
+typedef struct tdmd_cell_list tdmd_cell_list;
+int32_t tdmd_cell_list_create(tdmd_cell_list** out);
+int32_t tdmd_cell_list_destroy(tdmd_cell_list* cl);
+/* DeviceCellList::build, device_cell_list.cu:59-150: counting sort of the
+ * atoms into nc = max(3, floor(L/r_list)) cells per axis, atoms ID-ascending
+ * within each cell.  d_positions: double[3*n] on the device. */
+int32_t tdmd_cell_list_build(tdmd_cell_list* cl, const double* d_positions, int64_t natoms,
+                             const tdmd_box* box, double r_list, void* stream);
+/* Device pointers: cell_atoms[n], cell_offsets[ncells], cell_counts[ncells],
+ * atom_cells[n]; grid dims nc[3]. */
+int32_t tdmd_cell_list_get(const tdmd_cell_list* cl, const int32_t** cell_atoms,
+                           const int32_t** cell_offsets, const int32_t** cell_counts,
+                           const int32_t** atom_cells, int32_t nc[3]);
+
+/* ------------------------------------------------------------------------ */
+/* Neighbor list -- DeviceNeighborList, device_neighbor_list.cuh:20-65       */
+/* ------------------------------------------------------------------------ */
+typedef struct tdmd_nlist tdmd_nlist;
+int32_t tdmd_nlist_create(tdmd_nlist** out);
+int32_t tdmd_nlist_destroy(tdmd_nlist* nl);
+/* DeviceNeighborList::build, device_neighbor_list.cu:158-278: full list
+ * (both i->j and j->i), dense CSR.  Per-atom order is the reference's
+ * ID-ordered-scatter order: stencil dz,dy,dx in -1..1, atoms of each cell
+ * ID-ascending; pairs kept when the FP64 min-image r^2 < (r_cut+r_skin)^2. */
+int32_t tdmd_nlist_build(tdmd_nlist* nl, const double* d_positions, int64_t natoms,
+                         const tdmd_box* box, double r_cut, double r_skin, void* stream);
+/* d_neighbors(), d_counts(), d_offsets(), max_neighbors(), plus total. */
+int32_t tdmd_nlist_get(const tdmd_nlist* nl, const int32_t** d_neighbors,
+                       const int32_t** d_offsets, const int32_t** d_counts,
+                       int32_t* max_neighbors, int64_t* total_pairs);
+
+/* ------------------------------------------------------------------------ */
+/* Forces on caller-owned device arrays                                      */
+/* ------------------------------------------------------------------------ */
+/* compute_morse_gpu, src/potentials/device_morse.cuh:37-41.  Forces are
+ * STORED (not accumulated); d_energy (nullable) is ACCUMULATED (+=) with the
+ * potential energy in FP64; d_virial (nullable, 6 doubles xx,yy,zz,xy,xz,yz)
+ * is accumulated likewise.  precision selects double or float d_forces.
+ * Energies are reduced in a fixed order (no atomics). */
+int32_t tdmd_morse_compute(const double* d_positions, void* d_forces, int32_t precision,
+                           const int32_t* d_neighbors, const int32_t* d_offsets,
+                           const int32_t* d_counts, int32_t natoms, const tdmd_box* box,
+                           const tdmd_morse_params* params, double* d_energy, double* d_virial,
+                           void* stream);
+
+/* DeviceEam, src/potentials/device_eam.cuh:26-75: device copy of the
+ * tables plus rho/fp scratch. */
+typedef struct tdmd_device_eam tdmd_device_eam;
+/* DeviceEam::upload_tables, device_eam.cu:282-340. */
+int32_t tdmd_device_eam_create(const tdmd_eam* eam, tdmd_device_eam** out);
+int32_t tdmd_device_eam_destroy(tdmd_device_eam* de);
+/* DeviceEam::compute, device_eam.cu:342-420: density -> embedding -> force.
+ * Same store/accumulate contract as tdmd_morse_compute.  d_rho / d_fp
+ * (nullable, double[n]) receive the per-atom density and F'(rho). */
+int32_t tdmd_device_eam_compute(tdmd_device_eam* de, const double* d_positions, void* d_forces,
+                                int32_t precision, const int32_t* d_types,
+                                const int32_t* d_neighbors, const int32_t* d_offsets,
+                                const int32_t* d_counts, int32_t natoms, const tdmd_box* box,
+                                double* d_energy, double* d_virial, double* d_rho, double* d_fp,
+                                void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Integrator -- src/integrator/device_velocity_verlet.cuh:13-59             */
+/* force_precision says whether d_forces is double or float.                 */
+/* ------------------------------------------------------------------------ */
+int32_t tdmd_vv_half_kick(double* d_velocities, const void* d_forces, int32_t force_precision,
+                          const int32_t* d_types, const double* d_masses, int32_t natoms,
+                          double dt, void* stream);
+int32_t tdmd_vv_drift(double* d_positions, const double* d_velocities, int32_t natoms, double dt,
+                      const tdmd_box* box, void* stream);
+/* full_kick = 0: device_fused_half_kick_drift; 1: device_fused_full_kick_drift. */
+int32_t tdmd_vv_fused_kick_drift(double* d_velocities, double* d_positions, const void* d_forces,
+                                 int32_t force_precision, const int32_t* d_types,
+                                 const double* d_masses, int32_t natoms, double dt,
+                                 const tdmd_box* box, int32_t full_kick, void* stream);
+int32_t tdmd_vv_zero_forces(void* d_forces, int32_t force_precision, int32_t natoms,
+                            void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Reductions + thermostat -- src/integrator/device_nose_hoover.cuh:26-88    */
+/* All reductions are FP64, fixed-order (bit-reproducible), no atomics.      */
+/* ------------------------------------------------------------------------ */
+/* device_compute_ke: writes the result to *h_ke (host) after a stream sync. */
+int32_t tdmd_reduce_ke(const double* d_velocities, const int32_t* d_types,
+                       const double* d_masses, int32_t natoms, double* h_ke, void* stream);
+/* device_compute_vmax: sqrt(max |v|^2). */
+int32_t tdmd_reduce_vmax(const double* d_velocities, int32_t natoms, double* h_vmax,
+                         void* stream);
+/* device_scale_velocities. */
+int32_t tdmd_scale_velocities(double* d_velocities, int32_t natoms, double factor, void* stream);
+
+/* NoseHooverChain (host object), device_nose_hoover.cu:187-289. */
+typedef struct tdmd_nhc tdmd_nhc;
+int32_t tdmd_nhc_create(double t_target, double t_period, int32_t chain_length, double dt,
+                        int32_t n_dof, tdmd_nhc** out);
+int32_t tdmd_nhc_destroy(tdmd_nhc* nhc);
+int32_t tdmd_nhc_half_step(tdmd_nhc* nhc, double ke_current, double* scale);
+/* state out: eta[M], eta_v[M], eta_m[M]. */
+int32_t tdmd_nhc_state(const tdmd_nhc* nhc, double* eta, double* eta_v, double* eta_m);
+
+/* ------------------------------------------------------------------------ */
+/* FastPipelineScheduler, src/scheduler/fast_pipeline_scheduler.cuh:76-192  */
+/* ------------------------------------------------------------------------ */
+typedef struct tdmd_sched tdmd_sched;
+/* ctor (Box, natoms, MorseParams, FastPipelineConfig), .cu:15-26 */
+int32_t tdmd_sched_create_morse(const tdmd_box* box, int32_t natoms,
+                                const tdmd_morse_params* params,
+                                const tdmd_fast_pipeline_config* cfg, tdmd_sched** out);
+/* ctor (Box, natoms, EamAlloy, FastPipelineConfig), .cu:27-40 */
+int32_t tdmd_sched_create_eam(const tdmd_box* box, int32_t natoms, const tdmd_eam* eam,
+                              const tdmd_fast_pipeline_config* cfg, tdmd_sched** out);
+int32_t tdmd_sched_destroy(tdmd_sched* s);
+/* upload(), .cu:49-73.  forces may be NULL (zeros); its element type follows
+ * the scheduler's precision.  Resets the step counter. */
+int32_t tdmd_sched_upload(tdmd_sched* s, const double* positions, const double* velocities,
+                          const void* forces, const int32_t* types, const int32_t* ids,
+                          const double* masses, int32_t n_types);
+/* run_until(), .cu:195-223: run_until(0) computes the initial forces only;
+ * velocities are at integer time on return. */
+int32_t tdmd_sched_run_until(tdmd_sched* s, int32_t target_step);
+/* download(), .cu:75-85.  Any output pointer may be NULL. */
+int32_t tdmd_sched_download(const tdmd_sched* s, double* positions, double* velocities,
+                            void* forces, int32_t* types, int32_t* ids, int32_t natoms);
+int32_t tdmd_sched_stats(const tdmd_sched* s, tdmd_fast_pipeline_stats* out);
+int32_t tdmd_sched_current_step(const tdmd_sched* s, int32_t* step);
+int32_t tdmd_sched_potential_kind(const tdmd_sched* s, int32_t* kind);
+int32_t tdmd_sched_interaction_cutoff(const tdmd_sched* s, double* cutoff);
+/* Potential energy, kinetic energy and virial (FP64) of the current state.
+ * Runs an energy pass on the device; no state changes. */
+int32_t tdmd_sched_energies(tdmd_sched* s, double* pe, double* ke, double* virial6);
+/* Energy log (tdmd_fast_pipeline_config.energy_every): copies up to `cap`
+ * records of 9 doubles {step, pe, ke, vxx, vyy, vzz, vxy, vxz, vyz}; *count
+ * gets the number of records written since upload. */
+int32_t tdmd_sched_energy_log(const tdmd_sched* s, double* records, int32_t cap, int32_t* count);
+/* Current dt (adaptive) and NHC chain state (eta[M], eta_v[M]). */
+int32_t tdmd_sched_thermostat_state(const tdmd_sched* s, double* dt, double* eta,
+                                    double* eta_v);
+/* Device pointers of the scheduler's state (for zero-copy callers):
+ * positions as double4[n] {x,y,z,type}, velocities double[3n], forces
+ * (double or float)[3n]; valid until the next upload/destroy. */
+int32_t tdmd_sched_device_state(tdmd_sched* s, void** d_pos4, double** d_vel, void** d_forces);
+/* Per-kernel timing (no reference counterpart; the reference profiles only
+ * from outside with nsys/ncu).  While on, windows run without graph replay
+ * and CUDA events on the scheduler's stream bracket each phase; averages in
+ * ms per launch for the phases {kick+drift, neighbor rebuild, EAM density,
+ * force, other} go to avg_ms[0..4], launch counts to counts[0..4]. */
+int32_t tdmd_sched_set_profiling(tdmd_sched* s, int32_t on);
+int32_t tdmd_sched_kernel_times(const tdmd_sched* s, double* avg_ms, int64_t* counts,
+                                int32_t ncat);
+/* Device time (ms) of the last run_until window: CUDA events recorded on the
+ * scheduler's stream before its first and after its last enqueued kernel. */
+int32_t tdmd_sched_last_window_ms(const tdmd_sched* s, double* ms);
+/* The stream the scheduler enqueues on (a cudaStream_t). */
+int32_t tdmd_sched_stream(const tdmd_sched* s, void** stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* TDMD_B200_H */

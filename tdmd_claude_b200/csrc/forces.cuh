@@ -1,0 +1,458 @@
+// forces.cuh -- Morse and three-pass EAM force kernels (sm_100a), shared by
+// the free-function C ABI (reference array layouts) and the scheduler
+// (its own layouts).
+//
+// Reference kernels (tdmd_Claude): morse_force_kernel
+// (src/potentials/device_morse.cu:32-132), eam_density_kernel /
+// eam_embedding_kernel / eam_force_kernel (src/potentials/device_eam.cu:
+// 72-278), spline_eval / spline_eval_deriv (device_eam.cu:41-66).
+//
+// Design (B200):
+//  * LPA lanes per atom (1..32, a template parameter the autotuner picks):
+//    the lanes of a group stride through the atom's neighbor row and merge
+//    their partial sums with xor-shuffles; no atomics anywhere.
+//  * Geometry policies: FP64 positions (double4 records or the reference's
+//    Vec3D AoS, min-image in double), the reference's mixed trick (double
+//    subtract, cast to float), or fixed-point int32 positions whose wrapped
+//    difference IS the minimum image (scheduler's mixed path, 16-byte
+//    gathers, no FP64 ops per pair).
+//  * Mixed precision: FP32 distances/splines/forces, compensated FP32
+//    (TwoSum) per-atom sums; energies and virial always accumulate in FP64.
+//  * Energy/virial (template EV): per-block FP64 partials reduced later in a
+//    fixed order by k_reduce_partials.
+//  * EAM splines: rows of (a,b,c,d) per interval, all r-splines of one
+//    interval contiguous (density of each type, then phi of each pair), so a
+//    pair's lookups share one 32-byte sector for a single-type alloy.  The
+//    embedding F(rho) is always evaluated in FP64 (one lookup per atom).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace tdmd_b200 {
+
+constexpr int kEvStride = 8;  // doubles per block partial: e, w[6], pad
+
+// --------------------------------------------------------------------------
+// Neighbor rows: padded (row = i*cap) or dense CSR (row = row_off[i]).
+// --------------------------------------------------------------------------
+struct NbrView {
+  const int* nbr;
+  const int* row_off;  // nullable
+  const int* cnt;
+  int cap;
+  __device__ __forceinline__ long long row(int i) const {
+    return row_off ? static_cast<long long>(__ldg(row_off + i)) : static_cast<long long>(i) * cap;
+  }
+  __device__ __forceinline__ int count(int i) const {
+    const int c = __ldg(cnt + i);
+    return row_off ? c : (c < cap ? c : cap);
+  }
+};
+
+// --------------------------------------------------------------------------
+// Geometry policies: own(i) loads atom i once; delta(own, j) returns
+// r_i - r_j after the minimum image, in the policy's arithmetic type T.
+// --------------------------------------------------------------------------
+struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
+  using T = double;
+  using Own = double3;
+  const double4* p;
+  double L[3], halfL[3];
+  int per[3];
+  __device__ __forceinline__ double3 load(int i) const {
+    const double2* q = reinterpret_cast<const double2*>(p + i);
+    const double2 a = __ldg(q);
+    const double b = __ldg(reinterpret_cast<const double*>(q + 1));
+    return make_double3(a.x, a.y, b);
+  }
+  __device__ __forceinline__ Own own(int i) const { return load(i); }
+  __device__ __forceinline__ void delta(const Own& o, int j, T& dx, T& dy, T& dz) const {
+    const double3 q = load(j);
+    dx = min_image1(o.x - q.x, L[0], halfL[0], per[0]);
+    dy = min_image1(o.y - q.y, L[1], halfL[1], per[1]);
+    dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
+  }
+};
+
+struct GeoAoS64 {  // FP64, reference Vec3D AoS
+  using T = double;
+  using Own = double3;
+  const double* p;
+  double L[3], halfL[3];
+  int per[3];
+  __device__ __forceinline__ double3 load(int i) const {
+    const double* q = p + 3ll * i;
+    return make_double3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+  }
+  __device__ __forceinline__ Own own(int i) const { return load(i); }
+  __device__ __forceinline__ void delta(const Own& o, int j, T& dx, T& dy, T& dz) const {
+    const double3 q = load(j);
+    dx = min_image1(o.x - q.x, L[0], halfL[0], per[0]);
+    dy = min_image1(o.y - q.y, L[1], halfL[1], per[1]);
+    dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
+  }
+};
+
+struct GeoAoS32 {  // mixed, reference layout: double subtract, cast, float min-image
+  using T = float;
+  using Own = double3;
+  const double* p;
+  float L[3], halfL[3];
+  int per[3];
+  __device__ __forceinline__ double3 load(int i) const {
+    const double* q = p + 3ll * i;
+    return make_double3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+  }
+  __device__ __forceinline__ Own own(int i) const { return load(i); }
+  __device__ __forceinline__ void delta(const Own& o, int j, T& dx, T& dy, T& dz) const {
+    const double3 q = load(j);
+    dx = min_image1(static_cast<float>(o.x - q.x), L[0], halfL[0], per[0]);
+    dy = min_image1(static_cast<float>(o.y - q.y), L[1], halfL[1], per[1]);
+    dz = min_image1(static_cast<float>(o.z - q.z), L[2], halfL[2], per[2]);
+  }
+};
+
+struct GeoQ {  // mixed, scheduler layout: fixed-point int4 {qx,qy,qz,type}
+  using T = float;
+  using Own = int4;
+  const int4* q;
+  float s[3];
+  __device__ __forceinline__ Own own(int i) const { return __ldg(q + i); }
+  __device__ __forceinline__ void delta(const Own& o, int j, T& dx, T& dy, T& dz) const {
+    const int4 b = __ldg(q + j);
+    dx = __fmul_rn(__int2float_rn(o.x - b.x), s[0]);
+    dy = __fmul_rn(__int2float_rn(o.y - b.y), s[1]);
+    dz = __fmul_rn(__int2float_rn(o.z - b.z), s[2]);
+  }
+};
+
+// --------------------------------------------------------------------------
+// Accumulators: plain double (FP64) or compensated float (mixed).
+// --------------------------------------------------------------------------
+template <class T>
+struct Acc;
+template <>
+struct Acc<double> {
+  double s = 0.0;
+  __device__ __forceinline__ void add(double x) { s += x; }
+  __device__ __forceinline__ void shfl_merge(int o) { s += __shfl_xor_sync(0xffffffffu, s, o); }
+  __device__ __forceinline__ double value() const { return s; }
+};
+template <>
+struct Acc<float> {
+  CSum cs;
+  __device__ __forceinline__ void add(float x) { cs.add(x); }
+  __device__ __forceinline__ void shfl_merge(int o) {
+    const float os = __shfl_xor_sync(0xffffffffu, cs.s, o);
+    const float oc = __shfl_xor_sync(0xffffffffu, cs.c, o);
+    cs.merge(os, oc);
+  }
+  __device__ __forceinline__ double value() const {
+    return static_cast<double>(cs.s) + static_cast<double>(cs.c);
+  }
+};
+
+__device__ __forceinline__ double mul_rn(double a, double b) { return a * b; }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+// Force output: AoS float3 or double3.
+template <class F>
+struct ForceOut {
+  F* f;
+  __device__ __forceinline__ void store(int i, double x, double y, double z) const {
+    f[3ll * i] = static_cast<F>(x);
+    f[3ll * i + 1] = static_cast<F>(y);
+    f[3ll * i + 2] = static_cast<F>(z);
+  }
+};
+
+// Per-block FP64 energy/virial partials (thread 0 writes 8 doubles).
+__device__ __forceinline__ void write_ev_partials(double e, const double (&w)[6],
+                                                  double* __restrict__ partials) {
+  __shared__ double red[32 * 7];
+  double v[7] = {e, w[0], w[1], w[2], w[3], w[4], w[5]};
+  block_sum<7>(v, red);
+  if (threadIdx.x == 0) {
+    double* o = partials + static_cast<long long>(blockIdx.x) * kEvStride;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) o[k] = v[k];
+    o[7] = 0.0;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Morse, MorsePair::compute (src/potentials/morse.hpp:37-55) on the full
+// list: F_i = sum_j fpair(r_ij) (r_i - r_j), energy 1/2 U per listed pair.
+// --------------------------------------------------------------------------
+template <class T>
+struct MorseP {
+  T d, alpha, r0, rc_sq;
+};
+
+template <class Geo, int LPA, bool EV, class F>
+__global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
+                                               MorseP<typename Geo::T> mp, ForceOut<F> out,
+                                               double* __restrict__ partials) {
+  using T = typename Geo::T;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = tid / LPA;
+  const int sub = tid % LPA;
+  const bool active = i < n;
+  Acc<T> fx, fy, fz;
+  double pe = 0.0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  if (active) {
+    const typename Geo::Own o = g.own(i);
+    const long long row = nl.row(i);
+    const int c = nl.count(i);
+    for (int k = sub; k < c; k += LPA) {
+      const int j = __ldg(nl.nbr + row + k);
+      T dx, dy, dz;
+      g.delta(o, j, dx, dy, dz);
+      const T r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < mp.rc_sq) {
+        const T r = sqrt(r2);
+        const T ex = exp(-mp.alpha * (r - mp.r0));
+        const T ome = T(1) - ex;
+        const T dudr = T(2) * mp.d * mp.alpha * ome * ex;
+        const T fpair = -dudr / r;
+        fx.add(mul_rn(fpair, dx));
+        fy.add(mul_rn(fpair, dy));
+        fz.add(mul_rn(fpair, dz));
+        if (EV) {
+          pe += 0.5 * static_cast<double>(mp.d * (ome * ome - T(1)));
+          const double hf = 0.5 * static_cast<double>(fpair);
+          const double ddx = dx, ddy = dy, ddz = dz;
+          w[0] += hf * ddx * ddx;
+          w[1] += hf * ddy * ddy;
+          w[2] += hf * ddz * ddz;
+          w[3] += hf * ddx * ddy;
+          w[4] += hf * ddx * ddz;
+          w[5] += hf * ddy * ddz;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = LPA / 2; o > 0; o >>= 1) {
+    fx.shfl_merge(o);
+    fy.shfl_merge(o);
+    fz.shfl_merge(o);
+  }
+  if (active && sub == 0) out.store(i, fx.value(), fy.value(), fz.value());
+  if (EV) write_ev_partials(pe, w, partials);
+}
+
+// --------------------------------------------------------------------------
+// EAM tables on the device.
+// --------------------------------------------------------------------------
+template <class T>
+struct V4;
+template <>
+struct V4<double> {
+  using type = double4;
+};
+template <>
+struct V4<float> {
+  using type = float4;
+};
+
+template <class T>
+struct EamDev {
+  const typename V4<T>::type* rtab;  // [(nr-1) * S], S = ntypes + npairs
+  const double4* ftab;               // [ntypes * (nrho-1)], FP64 always
+  int ntypes, S, nr, nrho;
+  T dr, inv_dr, rc_sq;
+  double drho;
+};
+
+__device__ __forceinline__ int phi_slot(int ti, int tj, int nt) {
+  if (ti > tj) {
+    const int t = ti;
+    ti = tj;
+    tj = t;
+  }
+  return nt + ti * nt - ti * (ti + 1) / 2 + tj;
+}
+
+// Interval index and offset, SplineTable::eval (eam_alloy.cpp:52-61):
+// idx = int((r - rmin)/dr) clamped to [0, n-2], dx = r - idx*dr (rmin = 0).
+__device__ __forceinline__ int spline_idx(double r, double dr, double /*inv*/, int n,
+                                          double& dx) {
+  int idx = static_cast<int>(r / dr);
+  idx = idx < 0 ? 0 : (idx > n - 2 ? n - 2 : idx);
+  dx = r - static_cast<double>(idx) * dr;
+  return idx;
+}
+__device__ __forceinline__ int spline_idx(float r, float dr, float inv_dr, int n, float& dx) {
+  int idx = static_cast<int>(r * inv_dr);
+  idx = idx < 0 ? 0 : (idx > n - 2 ? n - 2 : idx);
+  dx = fmaf(-static_cast<float>(idx), dr, r);
+  return idx;
+}
+
+template <class C, class T>
+__device__ __forceinline__ T spl_val(const C& c, T dx) {
+  return c.x + dx * (c.y + dx * (c.z + dx * c.w));
+}
+template <class C, class T>
+__device__ __forceinline__ T spl_der(const C& c, T dx) {
+  return c.y + dx * (T(2) * c.z + dx * T(3) * c.w);
+}
+
+template <class T>
+__device__ __forceinline__ typename V4<T>::type ldv4(const typename V4<T>::type* p);
+template <>
+__device__ __forceinline__ double4 ldv4<double>(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  const double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+template <>
+__device__ __forceinline__ float4 ldv4<float>(const float4* p) {
+  return __ldg(p);
+}
+
+// Embedding F(rho), F'(rho) in FP64 (SplineTable eval/eval_deriv on F).
+__device__ __forceinline__ void embed_eval(const double4* ftab, int nrho, double drho, int t,
+                                           double rho, double& F, double& dF) {
+  double dx;
+  const int idx = spline_idx(rho, drho, 0.0, nrho, dx);
+  const double4 c = ldv4<double>(ftab + static_cast<long long>(t) * (nrho - 1) + idx);
+  F = spl_val(c, dx);
+  dF = spl_der(c, dx);
+}
+
+// Pass 1 (+ fused pass 2): rho_i = sum_j f_tj(r_ij); then fp_i = F'(rho_i)
+// and, with EV, the embedding energy F(rho_i) into the block partials.
+// types == nullptr means a single-type alloy.
+template <class Geo, int LPA, bool EV, class FP>
+__global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
+                                                     EamDev<typename Geo::T> e,
+                                                     const int* __restrict__ types,
+                                                     FP* __restrict__ fp_out,
+                                                     double* __restrict__ rho_out,
+                                                     double* __restrict__ fpd_out,
+                                                     double* __restrict__ partials) {
+  using T = typename Geo::T;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = tid / LPA;
+  const int sub = tid % LPA;
+  const bool active = i < n;
+  Acc<T> rho;
+  if (active) {
+    const typename Geo::Own o = g.own(i);
+    const long long row = nl.row(i);
+    const int c = nl.count(i);
+    for (int k = sub; k < c; k += LPA) {
+      const int j = __ldg(nl.nbr + row + k);
+      T dx, dy, dz;
+      g.delta(o, j, dx, dy, dz);
+      const T r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < e.rc_sq) {
+        const T r = sqrt(r2);
+        T sx;
+        const int idx = spline_idx(r, e.dr, e.inv_dr, e.nr, sx);
+        const int tj = types ? __ldg(types + j) - 1 : 0;
+        const auto cf = ldv4<T>(e.rtab + static_cast<long long>(idx) * e.S + tj);
+        rho.add(spl_val(cf, sx));
+      }
+    }
+  }
+#pragma unroll
+  for (int o = LPA / 2; o > 0; o >>= 1) rho.shfl_merge(o);
+  double Fi = 0.0;
+  if (active && sub == 0) {
+    const double rh = rho.value();
+    const int ti = types ? __ldg(types + i) - 1 : 0;
+    double dF;
+    embed_eval(e.ftab, e.nrho, e.drho, ti, rh, Fi, dF);
+    fp_out[i] = static_cast<FP>(dF);
+    if (rho_out) rho_out[i] = rh;
+    if (fpd_out) fpd_out[i] = dF;
+  }
+  if (EV) {
+    const double w[6] = {0, 0, 0, 0, 0, 0};
+    write_ev_partials(Fi, w, partials);
+  }
+}
+
+// Pass 3: f_ij = -(phi' + fp_i rho'_tj + fp_j rho'_ti)/r * (r_i - r_j).
+template <class Geo, int LPA, bool EV, class FP, class F>
+__global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
+                                                   EamDev<typename Geo::T> e,
+                                                   const int* __restrict__ types,
+                                                   const FP* __restrict__ fp, ForceOut<F> out,
+                                                   double* __restrict__ partials) {
+  using T = typename Geo::T;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = tid / LPA;
+  const int sub = tid % LPA;
+  const bool active = i < n;
+  Acc<T> fx, fy, fz;
+  double pe = 0.0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  if (active) {
+    const typename Geo::Own o = g.own(i);
+    const long long row = nl.row(i);
+    const int c = nl.count(i);
+    const int ti = types ? __ldg(types + i) - 1 : 0;
+    const T fpi = static_cast<T>(__ldg(fp + i));
+    for (int k = sub; k < c; k += LPA) {
+      const int j = __ldg(nl.nbr + row + k);
+      T dx, dy, dz;
+      g.delta(o, j, dx, dy, dz);
+      const T r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < e.rc_sq) {
+        const T r = sqrt(r2);
+        T sx;
+        const int idx = spline_idx(r, e.dr, e.inv_dr, e.nr, sx);
+        const int tj = types ? __ldg(types + j) - 1 : 0;
+        const auto* rowp = e.rtab + static_cast<long long>(idx) * e.S;
+        const auto cphi = ldv4<T>(rowp + (types ? phi_slot(ti, tj, e.ntypes) : 1));
+        const auto crj = ldv4<T>(rowp + tj);
+        const T drj = spl_der(crj, sx);
+        T dri = drj;
+        if (types && tj != ti) dri = spl_der(ldv4<T>(rowp + ti), sx);
+        const T fpj = static_cast<T>(__ldg(fp + j));
+        const T fpair = -(spl_der(cphi, sx) + fpi * drj + fpj * dri) / r;
+        fx.add(mul_rn(fpair, dx));
+        fy.add(mul_rn(fpair, dy));
+        fz.add(mul_rn(fpair, dz));
+        if (EV) {
+          pe += 0.5 * static_cast<double>(spl_val(cphi, sx));
+          const double hf = 0.5 * static_cast<double>(fpair);
+          const double ddx = dx, ddy = dy, ddz = dz;
+          w[0] += hf * ddx * ddx;
+          w[1] += hf * ddy * ddy;
+          w[2] += hf * ddz * ddz;
+          w[3] += hf * ddx * ddy;
+          w[4] += hf * ddx * ddz;
+          w[5] += hf * ddy * ddz;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = LPA / 2; o > 0; o >>= 1) {
+    fx.shfl_merge(o);
+    fy.shfl_merge(o);
+    fz.shfl_merge(o);
+  }
+  if (active && sub == 0) out.store(i, fx.value(), fy.value(), fz.value());
+  if (EV) write_ev_partials(pe, w, partials);
+}
+
+// Sums nblk partial records (kEvStride doubles each) in block order and
+// ADDS them to energy[0] / virial[0..5] (either may be null).
+__global__ void k_reduce_partials(const double* __restrict__ partials, int nblk,
+                                  double* __restrict__ energy, double* __restrict__ virial);
+
+// Launch helpers (forces.cu).  `ev` non-null => energy/virial partials are
+// written there (nblocks * kEvStride doubles) -- see ev_blocks().
+int force_blocks(long long n, int lpa);
+
+}  // namespace tdmd_b200

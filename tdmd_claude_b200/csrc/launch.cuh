@@ -1,0 +1,89 @@
+// launch.cuh -- host-side launchers of the force kernels: runtime LPA
+// (lanes per atom) and energy/virial flags dispatched onto the template
+// instantiations in forces.cuh.
+#pragma once
+
+#include "common.cuh"
+#include "forces.cuh"
+
+namespace tdmd_b200 {
+
+constexpr int kForceThreads = 256;
+
+int force_blocks(long long n, int lpa);
+int default_lpa(long long n);
+
+#define TDMD_LPA_DISPATCH(lpa, ...)                              \
+  switch (lpa) {                                                  \
+    case 1: { constexpr int L = 1; __VA_ARGS__; } break;          \
+    case 2: { constexpr int L = 2; __VA_ARGS__; } break;          \
+    case 4: { constexpr int L = 4; __VA_ARGS__; } break;          \
+    case 8: { constexpr int L = 8; __VA_ARGS__; } break;          \
+    case 16: { constexpr int L = 16; __VA_ARGS__; } break;        \
+    case 32: { constexpr int L = 32; __VA_ARGS__; } break;        \
+    default: throw Error{TDMD_ERR_INVALID_ARGUMENT, "lanes per atom must be 1,2,4,8,16,32"}; \
+  }
+
+// Morse forces; with ev, per-block partials (force_blocks records).
+template <class Geo, class F>
+void launch_morse(const Geo& g, const NbrView& nl, int n, const MorseP<typename Geo::T>& mp,
+                  F* forces, bool ev, double* partials, int lpa, cudaStream_t s) {
+  const int nblk = force_blocks(n, lpa);
+  TDMD_LPA_DISPATCH(lpa, {
+    if (ev)
+      k_morse<Geo, L, true, F><<<nblk, kForceThreads, 0, s>>>(g, nl, n, mp, ForceOut<F>{forces},
+                                                              partials);
+    else
+      k_morse<Geo, L, false, F><<<nblk, kForceThreads, 0, s>>>(g, nl, n, mp, ForceOut<F>{forces},
+                                                               nullptr);
+  });
+  TDMD_LAUNCH_CHECK();
+}
+
+// Density(+embedding) then force.  With ev, the density pass writes records
+// [0, nblk) and the force pass [nblk, 2*nblk) of `partials`.
+template <class Geo, class FP, class F>
+void launch_eam_density(const Geo& g, const NbrView& nl, int n,
+                        const EamDev<typename Geo::T>& e, const int* types, FP* fp,
+                        double* rho_out, double* fpd_out, bool ev, double* partials, int lpa,
+                        cudaStream_t s) {
+  const int nblk = force_blocks(n, lpa);
+  TDMD_LPA_DISPATCH(lpa, {
+    if (ev)
+      k_eam_density<Geo, L, true, FP><<<nblk, kForceThreads, 0, s>>>(g, nl, n, e, types, fp,
+                                                                     rho_out, fpd_out, partials);
+    else
+      k_eam_density<Geo, L, false, FP><<<nblk, kForceThreads, 0, s>>>(g, nl, n, e, types, fp,
+                                                                      rho_out, fpd_out, nullptr);
+  });
+  TDMD_LAUNCH_CHECK();
+}
+
+template <class Geo, class FP, class F>
+void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typename Geo::T>& e,
+                      const int* types, const FP* fp, F* forces, bool ev, double* partials,
+                      int lpa, cudaStream_t s) {
+  const int nblk = force_blocks(n, lpa);
+  TDMD_LPA_DISPATCH(lpa, {
+    if (ev)
+      k_eam_force<Geo, L, true, FP, F><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, e, types, fp, ForceOut<F>{forces}, partials);
+    else
+      k_eam_force<Geo, L, false, FP, F><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
+  });
+  TDMD_LAUNCH_CHECK();
+}
+
+template <class Geo, class FP, class F>
+void launch_eam(const Geo& g, const NbrView& nl, int n, const EamDev<typename Geo::T>& e,
+                const int* types, FP* fp, double* rho_out, double* fpd_out, F* forces, bool ev,
+                double* partials, int lpa, cudaStream_t s) {
+  const int nblk = force_blocks(n, lpa);
+  launch_eam_density<Geo, FP, F>(g, nl, n, e, types, fp, rho_out, fpd_out, ev, partials, lpa, s);
+  launch_eam_force<Geo, FP, F>(g, nl, n, e, types, fp, forces, ev,
+                               ev ? partials + static_cast<long long>(nblk) * kEvStride : nullptr,
+                               lpa, s);
+}
+
+}  // namespace tdmd_b200

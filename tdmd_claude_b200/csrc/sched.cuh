@@ -1,0 +1,195 @@
+// sched.cuh -- the scheduler object behind tdmd_sched (scheduler.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <list>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "buffers.cuh"
+#include "common.cuh"
+#include "eam_tables.cuh"
+#include "forces.cuh"
+#include "integrate.cuh"
+
+namespace tdmd_b200 {
+
+// Device control block: everything the step kernels decide on the device.
+struct SchedCtl {
+  double dt;      // current time step (adaptive dt writes it)
+  double scale;   // pending NHC velocity scale, applied by the next kick
+  double ke;      // last reduced kinetic energy (after the thermostat)
+  double ev[8];   // energy pass sums: pe, virial xx,yy,zz,xy,xz,yz
+  double eta[kMaxChain], eta_v[kMaxChain], eta_m[kMaxChain];
+  long long step;  // device step counter (kick-drift increments it)
+  int status[4];   // [0] neighbor overflow flag, [1] max neighbor count
+  int log_count;
+  int pad;
+};
+
+struct CtlParams {
+  int M;
+  int n_dof;
+  double t_target, t_period, dt_nhc;
+  int adaptive;
+  double c2, rc, dt_min, dt_max;
+  int nvt;
+};
+
+struct StepPlan {
+  bool first;    // first step of the run_until window
+  bool last;     // last step of the window
+  bool rebuild;  // neighbor rebuild after this step's drift
+  bool ev;       // energy-log step
+};
+
+enum ProfCat : int {
+  kProfKickDrift = 0,
+  kProfRebuild = 1,
+  kProfDensity = 2,  // EAM density + embedding
+  kProfForce = 3,    // Morse or EAM force pass
+  kProfOther = 4,    // closing kicks, reductions, control
+  kProfCount = 5
+};
+
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+  long long kernels = 0;
+};
+
+class Scheduler {
+ public:
+  Scheduler(const tdmd_box& box, int natoms, const tdmd_fast_pipeline_config& cfg);
+  ~Scheduler();
+  Scheduler(const Scheduler&) = delete;
+  Scheduler& operator=(const Scheduler&) = delete;
+
+  void set_morse(const tdmd_morse_params& p);
+  void set_eam(const tdmd_eam& e);
+  void upload(const double* x, const double* v, const void* f, const int* types, const int* ids,
+              const double* masses, int n_types);
+  void download(double* x, double* v, void* f, int* types, int* ids, int natoms) const;
+  void run_until(int target);
+  void energies(double* pe, double* ke, double* virial6);
+  void energy_log(double* rec, int cap, int* count) const;
+  void thermostat_state(double* dt, double* eta, double* eta_v) const;
+  void stats(tdmd_fast_pipeline_stats* o) const;
+  int current_step() const { return step_; }
+  int potential_kind() const { return kind_; }
+  double interaction_cutoff() const { return cutoff_; }
+  cudaStream_t stream() const { return stream_; }
+  // Per-kernel timing with CUDA events on the scheduler's stream (disables
+  // graph replay while on).  Categories: see ProfCat.
+  void set_profiling(bool on);
+  // Device time of the last run_until window (events on the stream around
+  // its enqueued work), ms.
+  double last_window_ms() const { return last_window_ms_; }
+  void kernel_times(double* avg_ms, long long* counts, int ncat) const;
+  void device_state(void** pos4, double** vel, void** forces) {
+    if (pos4) *pos4 = pos4_.data();
+    if (vel) *vel = vel_.data();
+    if (forces)
+      *forces = mixed_ ? static_cast<void*>(f32_.data()) : static_cast<void*>(f64_.data());
+  }
+
+ private:
+  void finish_setup();
+  void size_neighbor_list();
+  void grow_capacity(int max_count);
+  void initial_forces();
+  void enqueue_rebuild();
+  void enqueue_force(bool ev);
+  template <class F>
+  void enqueue_kick_drift_t(F* f, bool full, bool scale);
+  void enqueue_kick_drift(bool full, bool scale);
+  template <class F>
+  void enqueue_half_kick_t(F* f, bool ke);
+  void enqueue_half_kick(bool ke);
+  CtlParams ctl_params() const;
+  void enqueue_control(int mode);
+  void enqueue_ke_pre();
+  void enqueue_log_nve();
+  void enqueue_apply_scale();
+  void enqueue_step(const StepPlan& st);
+  void enqueue_finalize();
+  void run_segment(const std::vector<StepPlan>& seg, bool finalize);
+  std::vector<StepPlan> plan_steps(int target, int* since_out) const;
+  void snapshot();
+  void restore();
+  void clear_graphs();
+  void prof_begin(int cat);
+  void prof_end(int cat);
+  void prof_collect();
+  int* ctl_status() const {
+    return reinterpret_cast<int*>(reinterpret_cast<char*>(ctl_.data()) +
+                                  offsetof(SchedCtl, status));
+  }
+  double* ctl_ev() const {
+    return reinterpret_cast<double*>(reinterpret_cast<char*>(ctl_.data()) +
+                                     offsetof(SchedCtl, ev));
+  }
+
+  tdmd_box hbox_;
+  DevBox box_{};
+  int n_;
+  tdmd_fast_pipeline_config cfg_;
+  int kind_ = -1;
+  double cutoff_ = 0.0;
+  bool mixed_ = false, nvt_ = false, thermo_ = false;
+  int lpa_ = 8;
+  MorseP<double> m64_{};
+  MorseP<float> m32_{};
+  std::unique_ptr<EamDevTables> eam_;
+
+  // State (device layouts).
+  DevArray<double4> pos4_;
+  DevArray<int4> q_;
+  DevArray<double> vel_;
+  DevArray<double> f64_;
+  DevArray<float> f32_;
+  DevArray<int> types_, ids_;
+  DevArray<double> masses_;
+  mutable DevArray<double> stage_;
+  int n_types_ = 0;
+
+  // Neighbor list: padded rows of cap_ entries.
+  CellListDev cl_;
+  DevArray<int> nbr_, cnt_;
+  int cap_ = 0;
+
+  // Scratch.
+  DevArray<float> fp32_;
+  DevArray<double> fp64_;
+  DevArray<double> ev_part_, ke_part_;
+  DevArray<SchedCtl> ctl_, snap_ctl_;
+  DevArray<double> log_;
+  int log_cap_ = 0;
+
+  // Snapshot for the overflow retry.
+  DevArray<double4> snap_pos4_;
+  DevArray<int4> snap_q_;
+  DevArray<double> snap_vel_, snap_f64_;
+  DevArray<float> snap_f32_;
+
+  cudaStream_t stream_ = nullptr;
+  std::map<std::vector<int>, GraphEntry> graphs_;
+  std::list<std::vector<int>> graph_lru_;
+
+  cudaEvent_t win_ev_[2] = {nullptr, nullptr};
+  double last_window_ms_ = 0.0;
+  bool profiling_ = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending_;
+  std::vector<cudaEvent_t> prof_pool_;
+  cudaEvent_t prof_open_ = nullptr;
+  double prof_ms_[kProfCount] = {0, 0, 0, 0, 0};
+  long long prof_n_[kProfCount] = {0, 0, 0, 0, 0};
+
+  bool uploaded_ = false, initialized_ = false;
+  int step_ = 0, since_rebuild_ = 0;
+  long long ticks_ = 0, launches_ = 0, rebuilds_ = 0, graph_launches_ = 0, retries_ = 0;
+};
+
+}  // namespace tdmd_b200

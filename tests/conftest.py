@@ -1,0 +1,66 @@
+"""Shared fixtures.  `-m gpu` tests need a CUDA device and the in-tree
+libtdmd_b200.so; everything else runs on the CPU."""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+REF_TREE = os.environ.get("TDMD_REFERENCE_TREE", "/root/reference")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built library")
+    config.addinivalue_line("markers", "slow: long-running")
+
+
+def golden(name: str) -> dict:
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import oracle as O
+    O.lib()
+    return O
+
+
+@pytest.fixture(scope="session")
+def ref_lib(oracle):
+    """The reference's own CPU path (skips where it was not built)."""
+    R = oracle.ref()
+    if R is None:
+        pytest.skip("reference CPU path not built (oracle/_ref)")
+    return R
+
+
+def reference_file(rel: str) -> str:
+    p = os.path.join(REF_TREE, rel)
+    if not os.path.exists(p):
+        pytest.skip(f"reference file {rel} not available here")
+    return p
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from tdmd_claude_b200 import _lib
+    _lib.lib()
+    return torch
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))

@@ -1,0 +1,261 @@
+"""FastPipelineScheduler on the GPU vs the oracle's restatement of the
+reference scheduler loop (oracle.md_run), through the C ABI."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+
+def _wrap_diff(a, b, L):
+    d = a - b
+    return d - np.round(d / L) * L
+
+
+def _c0():
+    g = golden("ref_morse_256.json")
+    return (np.array(g["positions"]), np.array(g["velocities"]), np.array(g["masses"]), g["lo"],
+            g["hi"], g["morse"], g["skin"])
+
+
+def _sched_morse(pos, vel, masses, lo, hi, morse, skin, **cfg):
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, MorseParams, make_config
+    s = FastPipelineScheduler(Box.make(lo, hi), len(pos), MorseParams.make(*morse),
+                              make_config(r_skin=skin, **cfg))
+    s.upload(pos, vel, None, np.ones(len(pos), np.int32), None, masses)
+    return s
+
+
+@pytest.mark.parametrize("use_graphs", [True, False])
+def test_morse_fp64_trajectory_matches_oracle(cuda, oracle, use_graphs):
+    pos, vel, masses, lo, hi, morse, skin = _c0()
+    s = _sched_morse(pos, vel, masses, lo, hi, morse, skin, use_graphs=use_graphs)
+    windows = [1, 10, 25, 60, 100]
+    for w in windows:
+        s.run_until(w)
+    st = s.download()
+    r = oracle.md_run(pos, vel, np.ones(256, np.int32), masses, lo, hi, 0.001, skin, 10, windows,
+                      morse=morse)
+    L = np.array(hi) - np.array(lo)
+    assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 1e-10
+    assert np.abs(st.velocities - r["vel"]).max() < 1e-9
+    assert rel_rms(st.forces, r["forces"]) < 1e-9
+    assert s.current_step() == 100
+    # reference md100 (CPU driver loop) stays within rounding of this path
+    g = golden("ref_morse_256.json")
+    assert np.abs(_wrap_diff(st.positions, np.array(g["md100"]["positions"]), L)).max() < 1e-10
+
+
+def test_run_until_zero_computes_initial_forces_only(cuda, oracle):
+    pos, vel, masses, lo, hi, morse, skin = _c0()
+    s = _sched_morse(pos, vel, masses, lo, hi, morse, skin)
+    s.run_until(0)
+    st = s.download()
+    assert np.array_equal(st.positions, pos)
+    assert np.array_equal(st.velocities, vel)
+    pe, fo, _ = oracle.morse_forces(pos, lo, hi, *morse, skin)
+    assert rel_rms(st.forces, fo) < 1e-10
+    assert s.stats().rebuilds == 1 and s.current_step() == 0
+
+
+def test_one_step_windows_equal_unfused_verlet(cuda, oracle):
+    """run_until one step at a time == plain half-kick/drift/force/half-kick."""
+    pos, vel, masses, lo, hi, morse, skin = _c0()
+    s = _sched_morse(pos, vel, masses, lo, hi, morse, skin)
+    for k in range(1, 21):
+        s.run_until(k)
+    st = s.download()
+    r = oracle.md_run(pos, vel, np.ones(256, np.int32), masses, lo, hi, 0.001, skin, 10,
+                      list(range(1, 21)), morse=morse)
+    L = np.array(hi) - np.array(lo)
+    assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 1e-11
+    assert np.abs(st.velocities - r["vel"]).max() < 1e-10
+
+
+def test_mixed_morse_cross_precision(cuda, oracle):
+    """VerifyLab cross-precision-ab: mixed vs FP64 after 100 steps,
+    |dx| < 5e-4 A and |dF| < 2e-2 eV/A."""
+    pos, vel, masses, lo, hi, morse, skin = _c0()
+    s = _sched_morse(pos, vel, masses, lo, hi, morse, skin, precision="mixed")
+    s.run_until(100)
+    st = s.download()
+    r = oracle.md_run(pos, vel, np.ones(256, np.int32), masses, lo, hi, 0.001, skin, 10, [100],
+                      morse=morse)
+    L = np.array(hi) - np.array(lo)
+    assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 5e-4
+    assert np.abs(st.forces - r["forces"]).max() < 2e-2
+    assert st.forces.dtype == np.float32
+
+
+def _eam_setup(precision, ncell=6, **cfg):
+    from tdmd_claude_b200 import Box, EamAlloy, FastPipelineScheduler, make_config
+    from tdmd_claude_b200 import workloads as W
+    t = W.cu_eam_tables()
+    sysm = W.fcc_system(ncell, 3.615, 300.0, seed=21)
+    eam = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    s = FastPipelineScheduler(Box.make(sysm.lo, sysm.hi), sysm.n, eam,
+                              make_config(r_skin=0.3, precision=precision, **cfg))
+    s.upload(sysm.positions, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+    return s, sysm, t
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_eam_trajectory_matches_oracle(cuda, oracle, precision):
+    s, sysm, t = _eam_setup(precision)
+    s.run_until(50)
+    st = s.download()
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    r = oracle.md_run(sysm.positions, sysm.velocities, sysm.types, sysm.masses, sysm.lo, sysm.hi,
+                      0.001, 0.3, 10, [50], eam=oe)
+    L = np.array(sysm.hi) - np.array(sysm.lo)
+    if precision == "fp64":
+        assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 1e-10
+        assert rel_rms(st.forces, r["forces"]) < 1e-9
+    else:
+        assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 5e-4
+        assert rel_rms(st.forces, r["forces"]) < 1e-4
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_energies_and_virial(cuda, oracle, precision):
+    s, sysm, t = _eam_setup(precision)
+    s.run_until(7)
+    pe, ke, w = s.energies()
+    st = s.download()
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    r = oe.forces(st.positions, sysm.types, sysm.lo, sysm.hi, 0.3)
+    ke_o = oracle.kinetic_energy(st.velocities, sysm.types, sysm.masses)
+    tol = 1e-10 if precision == "fp64" else 1e-6
+    assert abs(pe - r["pe"]) / abs(r["pe"]) < tol
+    assert abs(ke - ke_o) / ke_o < 1e-12
+    assert np.abs(w - r["virial"]).max() / np.abs(r["virial"]).max() < tol
+
+
+def test_nve_energy_log_and_drift(cuda):
+    """Device energy log: total energy conserved over 2000 steps (smoothly cut
+    EAM), and each record matches an on-demand energy evaluation."""
+    s, sysm, t = _eam_setup("fp64", ncell=5, energy_every=10, energy_log_capacity=400)
+    s.run_until(2000)
+    log = s.energy_log()
+    assert log.shape[0] == 200
+    assert np.array_equal(log[:, 0], np.arange(10, 2001, 10))
+    etot = log[:, 1] + log[:, 2]
+    drift = abs(etot[-1] - etot[0]) / sysm.n
+    assert drift < 1e-5           # eV/atom over 2 ps
+    pe, ke, _ = s.energies()
+    assert abs(log[-1, 1] - pe) < 1e-9 * abs(pe)
+    assert abs(log[-1, 2] - ke) < 1e-9 * abs(ke)
+
+
+def test_nvt_matches_oracle_composition(cuda, oracle):
+    """NHC chain 3, tau 0.1 ps at 600 K on the EAM system: trajectory equals
+    the oracle composition of NoseHooverChain + VV (pipeline_scheduler order)."""
+    s, sysm, t = _eam_setup("fp64", ncell=4, t_target=600.0, t_period=0.1, nhc_length=3)
+    s.run_until(30)
+    s.run_until(60)
+    st = s.download()
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    r = oracle.md_run(sysm.positions, sysm.velocities, sysm.types, sysm.masses, sysm.lo, sysm.hi,
+                      0.001, 0.3, 10, [30, 60], eam=oe, nhc=(600.0, 0.1, 3))
+    L = np.array(sysm.hi) - np.array(sysm.lo)
+    assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 1e-10
+    assert np.abs(st.velocities - r["vel"]).max() < 1e-9
+
+
+def test_nvt_temperature_control(cuda):
+    """test_nvt_thermostat.cu:105-167: <T> within 15 % of the target."""
+    from tdmd_claude_b200.workloads import KB
+    s, sysm, t = _eam_setup("mixed", ncell=5, t_target=500.0, t_period=0.05, nhc_length=3,
+                            energy_every=10, energy_log_capacity=1000)
+    s.run_until(4000)
+    log = s.energy_log()
+    T = 2.0 * log[:, 2] / ((3 * sysm.n - 3) * KB)
+    tmean = T[len(T) // 2:].mean()
+    assert abs(tmean - 500.0) / 500.0 < 0.15
+
+
+def test_adaptive_dt_matches_oracle(cuda, oracle):
+    pos, vel, masses, lo, hi, morse, skin = _c0()
+    s = _sched_morse(pos, vel * 8.0, masses, lo, hi, morse, skin, adaptive_dt=True, dt_min=1e-4,
+                     dt_max=0.002, c2=0.05)
+    s.run_until(40)
+    st = s.download()
+    dt, _, _ = s.thermostat_state()
+    r = oracle.md_run(pos, vel * 8.0, np.ones(256, np.int32), masses, lo, hi, 0.001, skin, 10,
+                      [40], morse=morse, adaptive=(1e-4, 0.002, 0.05), record=True)
+    L = np.array(hi) - np.array(lo)
+    assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 1e-9
+    assert 1e-4 <= dt <= 0.002
+
+
+def test_kernel_launch_accounting(cuda):
+    """Morse NVE, one window without rebuild: 1 (initial force) + 2 per step
+    + 1 closing half kick, plus the initial list build (6 kernels)."""
+    pos, vel, masses, lo, hi, morse, skin = _c0()
+    s = _sched_morse(pos, vel, masses, lo, hi, morse, skin, use_graphs=False)
+    s.run_until(5)
+    st = s.stats()
+    assert st.kernel_launches == 6 + 1 + 2 * 5 + 1
+    assert st.ticks == 5 and st.rebuilds == 1
+
+
+def test_graph_replay_equals_direct_launches(cuda):
+    pos, vel, masses, lo, hi, morse, skin = _c0()
+    a = _sched_morse(pos, vel, masses, lo, hi, morse, skin, use_graphs=True)
+    b = _sched_morse(pos, vel, masses, lo, hi, morse, skin, use_graphs=False)
+    for w in (10, 20, 30, 45, 90):
+        a.run_until(w)
+        b.run_until(w)
+    sa, sb = a.download(), b.download()
+    assert np.array_equal(sa.positions, sb.positions)
+    assert np.array_equal(sa.velocities, sb.velocities)
+    assert a.stats().graph_launches > 0 and b.stats().graph_launches == 0
+
+
+def test_deterministic_replay(cuda):
+    s1, _, _ = _eam_setup("mixed", ncell=5)
+    s2, _, _ = _eam_setup("mixed", ncell=5)
+    s1.run_until(100)
+    s2.run_until(100)
+    a, b = s1.download(), s2.download()
+    assert np.array_equal(a.positions, b.positions)
+    assert np.array_equal(a.forces, b.forces)
+
+
+def test_neighbor_overflow_retry(cuda, oracle):
+    """Squeezing a gas into a dense cluster overflows the padded rows: the
+    window is re-run with a larger capacity and still matches the oracle."""
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, MorseParams, make_config
+    rng = np.random.default_rng(3)
+    L = 30.0
+    n = 300
+    pos = rng.uniform(0, L, size=(n, 3))
+    centre = np.array([15.0, 15.0, 15.0])
+    vel = (centre - pos) * 1.0           # all atoms drift to the centre
+    masses = np.array([1.0, 63.546])
+    morse = (0.01, 1.0, 3.0, 5.0)
+    s = FastPipelineScheduler(Box.make((0, 0, 0), (L, L, L)), n, MorseParams.make(*morse),
+                              make_config(r_skin=1.0, rebuild_every=5, dt=0.002))
+    s.upload(pos, vel, None, np.ones(n, np.int32), None, masses)
+    s.run_until(200)
+    st = s.download()
+    assert s.stats().nlist_retries >= 1
+    r = oracle.md_run(pos, vel, np.ones(n, np.int32), masses, (0, 0, 0), (L, L, L), 0.002, 1.0, 5,
+                      [200], morse=morse)
+    assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 1e-8
+
+
+def test_upload_rejects_bad_types(cuda):
+    from tdmd_claude_b200 import TdmdError
+    pos, vel, masses, lo, hi, morse, skin = _c0()
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, MorseParams, make_config
+    s = FastPipelineScheduler(Box.make(lo, hi), 256, MorseParams.make(*morse), make_config())
+    bad = np.ones(256, np.int32)
+    bad[3] = 7
+    with pytest.raises(TdmdError):
+        s.upload(pos, vel, None, bad, None, masses)
+    with pytest.raises(TdmdError):
+        s.run_until(3)     # nothing uploaded
