@@ -285,6 +285,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=10, help="reference CPU sample size")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only the mixed timed windows (for profiler captures); no JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
@@ -315,6 +317,12 @@ def main():
     f64 = s64.download().forces
     f32 = s32.download().forces.astype(np.float64)
     rel_err = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
+
+    if args.kernels_only:
+        timed_windows(s32, args.steps, args.warmup, flush, torch, dist)
+        for s in (s32, s64):
+            s.close()
+        return
 
     # Headline: mixed.
     clocks = ClockSampler(local)

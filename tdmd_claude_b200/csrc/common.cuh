@@ -73,6 +73,7 @@ struct DevBox {
   double qlo[3];     // fixed-point origin (lo on periodic axes)
   double qinv[3];    // 2^32 / Lq  (fixed-point encode)
   float qscale[3];   // Lq / 2^32  (fixed-point decode, FP32)
+  double qstep[3];   // Lq / 2^32  (fixed-point decode, FP64)
   int nc[3];
   int periodic[3];
 };

@@ -51,6 +51,7 @@ DevBox make_devbox(const tdmd_box& b, double r_list) {
     d.qlo[a] = d.periodic[a] ? b.lo[a] : b.lo[a] - 1.5 * L;
     d.qinv[a] = 4294967296.0 / Lq;
     d.qscale[a] = static_cast<float>(Lq / 4294967296.0);
+    d.qstep[a] = Lq / 4294967296.0;
   }
   return d;
 }

@@ -216,10 +216,10 @@ void EamDevTables::upload(const tdmd_eam& e, cudaStream_t stream) {
   ntypes = nt;
   cutoff = e.cutoff;
   d64 = EamDev<double>{rtab64.data(), ftab.data(), nt, S, e.nr, e.nrho, e.dr, 1.0 / e.dr,
-                       e.cutoff * e.cutoff, e.drho};
+                       e.cutoff * e.cutoff, e.drho, e.dr};
   d32 = EamDev<float>{rtab32.data(), ftab.data(), nt, S, e.nr, e.nrho,
                       static_cast<float>(e.dr), static_cast<float>(1.0 / e.dr),
-                      static_cast<float>(e.cutoff * e.cutoff), e.drho};
+                      static_cast<float>(e.cutoff * e.cutoff), e.drho, e.dr};
 }
 
 // --------------------------------------------------------------------------
@@ -381,16 +381,13 @@ int32_t tdmd_morse_compute(const double* d_positions, void* d_forces, int32_t pr
     if (precision == TDMD_FP64) {
       GeoAoS64 g{d_positions, {b.L[0], b.L[1], b.L[2]}, {b.halfL[0], b.halfL[1], b.halfL[2]},
                  {b.periodic[0], b.periodic[1], b.periodic[2]}};
-      MorseP<double> mp{params->d, params->alpha, params->r0, params->rc_sq};
+      MorseP<double> mp{params->d, params->alpha, params->r0, params->rc_sq, params->r0};
       launch_morse(g, nl, natoms, mp, static_cast<double*>(d_forces), ev, part.p, lpa, s);
     } else {
       TDMD_REQUIRE(precision == TDMD_MIXED, "unknown precision");
-      GeoAoS32 g{d_positions,
-                 {float(b.L[0]), float(b.L[1]), float(b.L[2])},
-                 {float(0.5 * b.L[0]), float(0.5 * b.L[1]), float(0.5 * b.L[2])},
-                 {b.periodic[0], b.periodic[1], b.periodic[2]}};
+      const GeoAoS32 g = make_geo_aos32(d_positions, b);
       MorseP<float> mp{float(params->d), float(params->alpha), float(params->r0),
-                       float(params->rc_sq)};
+                       float(params->rc_sq), params->r0};
       launch_morse(g, nl, natoms, mp, static_cast<float*>(d_forces), ev, part.p, lpa, s);
     }
     if (ev) {
@@ -449,10 +446,7 @@ int32_t tdmd_device_eam_compute(tdmd_device_eam* de, const double* d_positions, 
     } else {
       TDMD_REQUIRE(precision == TDMD_MIXED, "unknown precision");
       de->fp32.reserve(static_cast<size_t>(natoms));
-      GeoAoS32 g{d_positions,
-                 {float(b.L[0]), float(b.L[1]), float(b.L[2])},
-                 {float(0.5 * b.L[0]), float(0.5 * b.L[1]), float(0.5 * b.L[2])},
-                 {b.periodic[0], b.periodic[1], b.periodic[2]}};
+      const GeoAoS32 g = make_geo_aos32(d_positions, b);
       launch_eam(g, nl, natoms, de->tabs.d32, types, de->fp32.data(), d_rho, d_fp,
                  static_cast<float*>(d_forces), ev, part.p, lpa, s);
     }

@@ -53,12 +53,25 @@ struct NbrView {
 };
 
 // --------------------------------------------------------------------------
-// Geometry policies: own(i) loads atom i once; delta(own, j) returns
-// r_i - r_j after the minimum image, in the policy's arithmetic type T.
+// Geometry policies.  own(i) loads atom i once; pair(own, j, p) fills p with
+// r_i - r_j after the minimum image and r^2 in the policy's arithmetic type
+// T; radius(p, r, rd) gives |r_i - r_j| as T (for 1/r and cut tests) and as
+// an FP64 value rd that the spline offset and the Morse exponent use.
+// In FP32, r itself carries an absolute error of ~ulp(r) = 2.4e-7 A at
+// r ~ 2.5 A, which moves the spline argument and, through the large pair
+// forces that cancel in each atom's net force, dominates the mixed-precision
+// force error; rd removes that term.
 // --------------------------------------------------------------------------
+template <class T>
+struct PairD {
+  T dx, dy, dz, r2;
+  double r2d;  // precise r^2 (A^2); equals r2 on FP64 geometries
+};
+
 struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
   using T = double;
   using Own = double3;
+  using Pair = PairD<double>;
   const double4* p;
   double L[3], halfL[3];
   int per[3];
@@ -69,17 +82,23 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
     return make_double3(a.x, a.y, b);
   }
   __device__ __forceinline__ Own own(int i) const { return load(i); }
-  __device__ __forceinline__ void delta(const Own& o, int j, T& dx, T& dy, T& dz) const {
+  __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
     const double3 q = load(j);
-    dx = min_image1(o.x - q.x, L[0], halfL[0], per[0]);
-    dy = min_image1(o.y - q.y, L[1], halfL[1], per[1]);
-    dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
+    pr.dx = min_image1(o.x - q.x, L[0], halfL[0], per[0]);
+    pr.dy = min_image1(o.y - q.y, L[1], halfL[1], per[1]);
+    pr.dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
+    pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
+  }
+  __device__ __forceinline__ void radius(const Pair& pr, T& r, double& rd) const {
+    r = sqrt(pr.r2);
+    rd = r;
   }
 };
 
 struct GeoAoS64 {  // FP64, reference Vec3D AoS
   using T = double;
   using Own = double3;
+  using Pair = PairD<double>;
   const double* p;
   double L[3], halfL[3];
   int per[3];
@@ -88,46 +107,105 @@ struct GeoAoS64 {  // FP64, reference Vec3D AoS
     return make_double3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
   }
   __device__ __forceinline__ Own own(int i) const { return load(i); }
-  __device__ __forceinline__ void delta(const Own& o, int j, T& dx, T& dy, T& dz) const {
+  __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
     const double3 q = load(j);
-    dx = min_image1(o.x - q.x, L[0], halfL[0], per[0]);
-    dy = min_image1(o.y - q.y, L[1], halfL[1], per[1]);
-    dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
+    pr.dx = min_image1(o.x - q.x, L[0], halfL[0], per[0]);
+    pr.dy = min_image1(o.y - q.y, L[1], halfL[1], per[1]);
+    pr.dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
+    pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
+  }
+  __device__ __forceinline__ void radius(const Pair& pr, T& r, double& rd) const {
+    r = sqrt(pr.r2);
+    rd = r;
   }
 };
 
-struct GeoAoS32 {  // mixed, reference layout: double subtract, cast, float min-image
+// Mixed on the reference layout (free functions): the delta is formed in
+// FP64 and min-imaged there, then cast to FP32 (the reference's
+// relative-coordinate form, device_morse.cu:58-73, without its FP32
+// min-image step).
+struct GeoAoS32 {
   using T = float;
   using Own = double3;
+  using Pair = PairD<float>;
   const double* p;
-  float L[3], halfL[3];
+  double L[3], halfL[3];
   int per[3];
   __device__ __forceinline__ double3 load(int i) const {
     const double* q = p + 3ll * i;
     return make_double3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
   }
   __device__ __forceinline__ Own own(int i) const { return load(i); }
-  __device__ __forceinline__ void delta(const Own& o, int j, T& dx, T& dy, T& dz) const {
+  __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
     const double3 q = load(j);
-    dx = min_image1(static_cast<float>(o.x - q.x), L[0], halfL[0], per[0]);
-    dy = min_image1(static_cast<float>(o.y - q.y), L[1], halfL[1], per[1]);
-    dz = min_image1(static_cast<float>(o.z - q.z), L[2], halfL[2], per[2]);
+    const double x = min_image1(o.x - q.x, L[0], halfL[0], per[0]);
+    const double y = min_image1(o.y - q.y, L[1], halfL[1], per[1]);
+    const double z = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
+    pr.dx = static_cast<float>(x);
+    pr.dy = static_cast<float>(y);
+    pr.dz = static_cast<float>(z);
+    pr.r2d = x * x + y * y + z * z;
+    pr.r2 = static_cast<float>(pr.r2d);
+  }
+  __device__ __forceinline__ void radius(const Pair& pr, T& r, double& rd) const {
+    r = sqrtf(pr.r2);
+    // one Newton step from the FP32 root: rd = r + (r2d - r^2) / (2 r)
+    rd = static_cast<double>(r) +
+         static_cast<double>(static_cast<float>(fma(-static_cast<double>(r), r, pr.r2d)) *
+                             (0.5f / r));
   }
 };
 
-struct GeoQ {  // mixed, scheduler layout: fixed-point int4 {qx,qy,qz,type}
+// Mixed, scheduler layout: fixed-point int4 {qx,qy,qz,type}.  The wrapped
+// int32 difference is the exact minimum-image delta in units of L/2^32;
+// FP32 components come from one conversion each, the precise r^2 from the
+// exact integers in FP64.
+struct PairQ {
+  float dx, dy, dz, r2;
+  int ix, iy, iz;
+};
+
+struct GeoQ {
   using T = float;
   using Own = int4;
+  using Pair = PairQ;
   const int4* q;
   float s[3];
+  double s2[3];  // (Lq/2^32)^2 per axis
   __device__ __forceinline__ Own own(int i) const { return __ldg(q + i); }
-  __device__ __forceinline__ void delta(const Own& o, int j, T& dx, T& dy, T& dz) const {
+  __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
     const int4 b = __ldg(q + j);
-    dx = __fmul_rn(__int2float_rn(o.x - b.x), s[0]);
-    dy = __fmul_rn(__int2float_rn(o.y - b.y), s[1]);
-    dz = __fmul_rn(__int2float_rn(o.z - b.z), s[2]);
+    pr.ix = o.x - b.x;
+    pr.iy = o.y - b.y;
+    pr.iz = o.z - b.z;
+    pr.dx = __fmul_rn(__int2float_rn(pr.ix), s[0]);
+    pr.dy = __fmul_rn(__int2float_rn(pr.iy), s[1]);
+    pr.dz = __fmul_rn(__int2float_rn(pr.iz), s[2]);
+    pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
+  }
+  // Only pairs inside the cutoff pay for the FP64 refinement.
+  __device__ __forceinline__ void radius(const Pair& pr, T& r, double& rd) const {
+    const double x = pr.ix, y = pr.iy, z = pr.iz;
+    const double r2d = x * x * s2[0] + y * y * s2[1] + z * z * s2[2];
+    r = sqrtf(pr.r2);
+    rd = static_cast<double>(r) +
+         static_cast<double>(static_cast<float>(fma(-static_cast<double>(r), r, r2d)) *
+                             (0.5f / r));
   }
 };
+
+__host__ inline GeoQ make_geoq(const int4* q, const DevBox& b) {
+  return GeoQ{q,
+              {b.qscale[0], b.qscale[1], b.qscale[2]},
+              {b.qstep[0] * b.qstep[0], b.qstep[1] * b.qstep[1], b.qstep[2] * b.qstep[2]}};
+}
+
+__host__ inline GeoAoS32 make_geo_aos32(const double* p, const DevBox& b) {
+  return GeoAoS32{p,
+                  {b.L[0], b.L[1], b.L[2]},
+                  {b.halfL[0], b.halfL[1], b.halfL[2]},
+                  {b.periodic[0], b.periodic[1], b.periodic[2]}};
+}
 
 // --------------------------------------------------------------------------
 // Accumulators: plain double (FP64) or compensated float (mixed).
@@ -190,6 +268,7 @@ __device__ __forceinline__ void write_ev_partials(double e, const double (&w)[6]
 template <class T>
 struct MorseP {
   T d, alpha, r0, rc_sq;
+  double r0d;
 };
 
 template <class Geo, int LPA, bool EV, class F>
@@ -210,12 +289,14 @@ __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
     const int c = nl.count(i);
     for (int k = sub; k < c; k += LPA) {
       const int j = __ldg(nl.nbr + row + k);
-      T dx, dy, dz;
-      g.delta(o, j, dx, dy, dz);
-      const T r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 < mp.rc_sq) {
-        const T r = sqrt(r2);
-        const T ex = exp(-mp.alpha * (r - mp.r0));
+      typename Geo::Pair pr;
+      g.pair(o, j, pr);
+      if (pr.r2 < mp.rc_sq) {
+        T r;
+        double rd;
+        g.radius(pr, r, rd);
+        const T dx = pr.dx, dy = pr.dy, dz = pr.dz;
+        const T ex = exp(-mp.alpha * static_cast<T>(rd - mp.r0d));
         const T ome = T(1) - ex;
         const T dudr = T(2) * mp.d * mp.alpha * ome * ex;
         const T fpair = -dudr / r;
@@ -267,6 +348,7 @@ struct EamDev {
   int ntypes, S, nr, nrho;
   T dr, inv_dr, rc_sq;
   double drho;
+  double dr_d;
 };
 
 __device__ __forceinline__ int phi_slot(int ti, int tj, int nt) {
@@ -291,6 +373,21 @@ __device__ __forceinline__ int spline_idx(float r, float dr, float inv_dr, int n
   int idx = static_cast<int>(r * inv_dr);
   idx = idx < 0 ? 0 : (idx > n - 2 ? n - 2 : idx);
   dx = fmaf(-static_cast<float>(idx), dr, r);
+  return idx;
+}
+
+// Interval of r (index from r in T) and the offset from the FP64 radius.
+__device__ __forceinline__ int spline_at(double r, double rd, double dr, double inv, int n,
+                                         double dr_d, double& sx) {
+  (void)rd;
+  (void)dr_d;
+  return spline_idx(r, dr, inv, n, sx);
+}
+__device__ __forceinline__ int spline_at(float r, double rd, float /*dr*/, float inv_dr, int n,
+                                         double dr_d, float& sx) {
+  int idx = static_cast<int>(r * inv_dr);
+  idx = idx < 0 ? 0 : (idx > n - 2 ? n - 2 : idx);
+  sx = static_cast<float>(fma(-static_cast<double>(idx), dr_d, rd));
   return idx;
 }
 
@@ -349,13 +446,13 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
     const int c = nl.count(i);
     for (int k = sub; k < c; k += LPA) {
       const int j = __ldg(nl.nbr + row + k);
-      T dx, dy, dz;
-      g.delta(o, j, dx, dy, dz);
-      const T r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 < e.rc_sq) {
-        const T r = sqrt(r2);
-        T sx;
-        const int idx = spline_idx(r, e.dr, e.inv_dr, e.nr, sx);
+      typename Geo::Pair pr;
+      g.pair(o, j, pr);
+      if (pr.r2 < e.rc_sq) {
+        T r, sx;
+        double rd;
+        g.radius(pr, r, rd);
+        const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
         const int tj = types ? __ldg(types + j) - 1 : 0;
         const auto cf = ldv4<T>(e.rtab + static_cast<long long>(idx) * e.S + tj);
         rho.add(spl_val(cf, sx));
@@ -403,13 +500,14 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
     const T fpi = static_cast<T>(__ldg(fp + i));
     for (int k = sub; k < c; k += LPA) {
       const int j = __ldg(nl.nbr + row + k);
-      T dx, dy, dz;
-      g.delta(o, j, dx, dy, dz);
-      const T r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 < e.rc_sq) {
-        const T r = sqrt(r2);
-        T sx;
-        const int idx = spline_idx(r, e.dr, e.inv_dr, e.nr, sx);
+      typename Geo::Pair pr;
+      g.pair(o, j, pr);
+      if (pr.r2 < e.rc_sq) {
+        T r, sx;
+        double rd;
+        g.radius(pr, r, rd);
+        const T dx = pr.dx, dy = pr.dy, dz = pr.dz;
+        const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
         const int tj = types ? __ldg(types + j) - 1 : 0;
         const auto* rowp = e.rtab + static_cast<long long>(idx) * e.S;
         const auto cphi = ldv4<T>(rowp + (types ? phi_slot(ti, tj, e.ntypes) : 1));

@@ -12,14 +12,17 @@
 //    scan, atomic scatter and a per-cell sort that restores ID order -- so the
 //    result is deterministic with no host round trip (the reference copies the
 //    counts to the host and scans there).
-//  * list build: one warp per atom.  The 27-cell stencil is walked as 9 rows
-//    of 3 x-adjacent cells; the lanes take 32 candidates at a time, test
-//    r^2 < (rc+skin)^2 in FP64 with explicit round-to-nearest ops (no FMA
-//    contraction, so r^2 matches the CPU reference bit for bit), and a
+//  * list build: one CTA per cell stages the 27-cell candidate tile in shared
+//    memory as fixed-point records; warps sweep it 32 candidates at a time
+//    with an FP32 filter and fall back to the reference's exact FP64
+//    expression (round-to-nearest ops, no FMA contraction) only within 1e-5
+//    of r_list^2, so the lists match the CPU reference bit for bit; a
 //    ballot/popc compaction writes accepted neighbors in stencil order.  One
 //    pass: rows are padded to a fixed capacity and an overflow flag replaces
 //    the reference's count pass + 8-byte D2H sync.
+#include <algorithm>
 #include <climits>
+#include <cmath>
 
 #include "buffers.cuh"
 #include "common.cuh"
@@ -68,93 +71,165 @@ __global__ void k_scatter_atoms(const int* __restrict__ atom_cell, int n,
   cell_atoms[slot] = i;
 }
 
-// Restores ID-ascending order inside each cell (insertion sort; cells hold
-// a few tens of atoms).  One thread per cell.
+// Restores ID-ascending order inside each cell: one warp per cell, rank
+// sort through shuffles for cells of up to 32 atoms (a lane's rank is the
+// number of smaller ids), lane-0 insertion sort beyond that.
 __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __restrict__ cell_count,
                              int ncells, int* __restrict__ cell_atoms) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncells) return;
+  const long long gw = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= ncells) return;  // uniform per warp
+  const int c = static_cast<int>(gw);
   int* a = cell_atoms + cell_start[c];
   const int m = cell_count[c];
-  for (int k = 1; k < m; ++k) {
-    const int v = a[k];
-    int j = k - 1;
-    while (j >= 0 && a[j] > v) {
-      a[j + 1] = a[j];
-      --j;
+  if (m <= 32) {
+    const int v = lane < m ? a[lane] : INT_MAX;
+    int rank = 0;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) rank += __shfl_sync(0xffffffffu, v, k) < v ? 1 : 0;
+    if (lane < m) a[rank] = v;
+    return;
+  }
+  if (lane == 0) {
+    for (int k = 1; k < m; ++k) {
+      const int v = a[k];
+      int j = k - 1;
+      while (j >= 0 && a[j] > v) {
+        a[j + 1] = a[j];
+        --j;
+      }
+      a[j + 1] = v;
     }
-    a[j + 1] = v;
   }
 }
 
-// Warp per atom.  See the file comment for the scheme.
+// --------------------------------------------------------------------------
+// Row build, one CTA per cell.  The 27 stencil cells (dz, dy, dx in -1..1,
+// wrapped) are concatenated in stencil order; their atoms (ID order within
+// each cell) become candidate records {qx, qy, qz, j} with fixed-point
+// coordinates, staged in shared memory when they fit (kStageCap records),
+// read through L1 otherwise.  Each warp takes center-cell atoms in turn and
+// sweeps the candidates 32 at a time:
+//   * FP32 filter: r^2 from the exact int32 differences; a candidate whose
+//     r^2 lies outside the band rl^2 (1 -+ eps) is decided by it.  The FP32
+//     r^2 is within ~5e-7 relative of the FP64 one, plus the fixed-point
+//     quantisation (one unit L/2^32 per component: 2 sqrt(3) rl L/2^32 in
+//     r^2); eps = 1e-5 + 8 (L/2^32)/rl covers both with a wide margin, so
+//     the decision equals the FP64 one;
+//   * otherwise the reference expression decides: delta = r_j - r_i in FP64,
+//     minimum image, (x*x + y*y) + z*z with round-to-nearest ops, < rl^2.
+// Accepted candidates are compacted with ballot/popc in candidate order, so
+// every row is the reference's per-atom list, bit for bit.
+// --------------------------------------------------------------------------
+constexpr int kRowThreads = 128;
+constexpr int kStageCap = 1536;  // staged candidate records (24 KiB)
+
 template <class Load>
-__global__ void __launch_bounds__(256) k_build_rows(
-    Load pos, int n, DevBox b, const int* __restrict__ atom_cell,
-    const int* __restrict__ cell_start, const int* __restrict__ cell_count,
-    const int* __restrict__ cell_atoms, double rl2, int* __restrict__ nbr,
+__global__ void __launch_bounds__(kRowThreads) k_build_cells(
+    Load pos, DevBox b, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
+    const int* __restrict__ cell_atoms, double rl2, float lo_f, float hi_f, int* __restrict__ nbr,
     const int* __restrict__ row_off, int cap, int* __restrict__ counts,
     int* __restrict__ status) {
-  const int lane = threadIdx.x & 31;
-  const long long gw = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  if (gw >= n) return;  // uniform per warp
-  const int i = static_cast<int>(gw);
-  const double3 pi = pos(i);
+  __shared__ int4 stage[kStageCap];
+  __shared__ int s_start[27], s_pre[28];
+  const int c = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int ncx = b.nc[0], ncy = b.nc[1], ncz = b.nc[2];
   const int ncxy = ncx * ncy;
-  const int ci = atom_cell[i];
-  const int iz = ci / ncxy;
-  const int iy = (ci - iz * ncxy) / ncx;
-  const int ix = ci - iz * ncxy - iy * ncx;
-  const long long base = row_off ? static_cast<long long>(row_off[i])
-                                 : static_cast<long long>(i) * cap;
-  const int limit = row_off ? INT_MAX : cap;
-  const int xm = wrap_cell(ix - 1, ncx), xp = wrap_cell(ix + 1, ncx);
+  const int iz = c / ncxy, iy = (c - iz * ncxy) / ncx, ix = c - iz * ncxy - iy * ncx;
+  if (threadIdx.x < 32) {
+    int cnt = 0, st = 0;
+    if (lane < 27) {
+      const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dx = lane % 3 - 1;
+      const int nb_c = wrap_cell(iz + dz, ncz) * ncxy + wrap_cell(iy + dy, ncy) * ncx +
+                       wrap_cell(ix + dx, ncx);
+      st = cell_start[nb_c];
+      cnt = cell_count[nb_c];
+      s_start[lane] = st;
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane < 27) s_pre[lane + 1] = incl;
+    if (lane == 0) s_pre[0] = 0;
+  }
+  __syncthreads();
+  const int total = s_pre[27];
+  const bool staged = total <= kStageCap;
+  // Candidate record k: cell t with s_pre[t] <= k < s_pre[t+1].
+  auto fetch = [&](int k) -> int4 {
+    int lo = 0, hi = 27;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s_pre[mid] <= k) lo = mid; else hi = mid;
+    }
+    const int j = __ldg(cell_atoms + s_start[lo] + (k - s_pre[lo]));
+    const double3 p = pos(j);
+    return make_int4(encode_q(p.x, b.qlo[0], b.qinv[0]), encode_q(p.y, b.qlo[1], b.qinv[1]),
+                     encode_q(p.z, b.qlo[2], b.qinv[2]), j);
+  };
+  if (staged) {
+    for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = fetch(k);
+  }
+  __syncthreads();
+  // The center cell is stencil slot 13.
+  const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];
+  const float s0 = b.qscale[0], s1 = b.qscale[1], s2 = b.qscale[2];
   const unsigned lt_mask = (1u << lane) - 1u;
-  int cnt = 0;
-  for (int dz = -1; dz <= 1; ++dz) {
-    const int cz = wrap_cell(iz + dz, ncz);
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int row = cz * ncxy + wrap_cell(iy + dy, ncy) * ncx;
-      const int c0 = row + xm, c1 = row + ix, c2 = row + xp;
-      const int s0 = cell_start[c0], n0 = cell_count[c0];
-      const int s1 = cell_start[c1], n1 = cell_count[c1];
-      const int s2 = cell_start[c2], n2 = cell_count[c2];
-      const int n01 = n0 + n1;
-      const int T = n01 + n2;
-      for (int k0 = 0; k0 < T; k0 += 32) {
-        const int k = k0 + lane;
-        bool pred = false;
-        int j = -1;
-        if (k < T) {
-          const int slot = k < n0 ? s0 + k : (k < n01 ? s1 + (k - n0) : s2 + (k - n01));
-          j = cell_atoms[slot];
-          if (j != i) {
+  for (int a = warp; a < ncen; a += kRowThreads / 32) {
+    const int4 ci = staged ? stage[c0 + a] : fetch(c0 + a);
+    const int i = ci.w;
+    const long long base = row_off ? static_cast<long long>(row_off[i])
+                                   : static_cast<long long>(i) * cap;
+    const int limit = row_off ? INT_MAX : cap;
+    double3 pi = make_double3(0, 0, 0);
+    bool have_pi = false;
+    int cnt = 0;
+    for (int k0 = 0; k0 < total; k0 += 32) {
+      const int k = k0 + lane;
+      bool pred = false;
+      int j = -1;
+      if (k < total) {
+        const int4 cj = staged ? stage[k] : fetch(k);
+        j = cj.w;
+        if (j != i) {
+          const float fx = __fmul_rn(__int2float_rn(cj.x - ci.x), s0);
+          const float fy = __fmul_rn(__int2float_rn(cj.y - ci.y), s1);
+          const float fz = __fmul_rn(__int2float_rn(cj.z - ci.z), s2);
+          const float r2f = fx * fx + fy * fy + fz * fz;
+          if (r2f < lo_f) {
+            pred = true;
+          } else if (r2f <= hi_f) {
+            if (!have_pi) {
+              pi = pos(i);
+              have_pi = true;
+            }
             const double3 pj = pos(j);
-            // delta = r_j - r_i, minimum image, r^2 = (x*x + y*y) + z*z,
-            // all round-to-nearest: NeighborList::build, neighbor_list.cpp:57-63.
-            double dx = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
-            double dy2 = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
-            double dz2 = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
+            const double dx = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
+            const double dy = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
+            const double dz = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
             const double r2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy2, dy2)), __dmul_rn(dz2, dz2));
+                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
             pred = r2 < rl2;
           }
         }
-        const unsigned m = __ballot_sync(0xffffffffu, pred);
-        if (pred && nbr) {
-          const int p = cnt + __popc(m & lt_mask);
-          if (p < limit) nbr[base + p] = j;
-        }
-        cnt += __popc(m);
       }
+      const unsigned m = __ballot_sync(0xffffffffu, pred);
+      if (pred && nbr) {
+        const int p = cnt + __popc(m & lt_mask);
+        if (p < limit) nbr[base + p] = j;
+      }
+      cnt += __popc(m);
     }
-  }
-  if (lane == 0) {
-    counts[i] = cnt;
-    if (status) {
-      if (!row_off && cnt > cap) atomicOr(&status[0], 1);
-      atomicMax(&status[1], cnt);
+    if (lane == 0) {
+      counts[i] = cnt;
+      if (status) {
+        if (!row_off && cnt > cap) atomicOr(&status[0], 1);
+        atomicMax(&status[1], cnt);
+      }
     }
   }
 }
@@ -195,10 +270,10 @@ void build_cell_list(CellListDev& cl, const void* d_pos, PosLayout layout, long 
   k_scatter_atoms<<<nb, 256, 0, stream>>>(cl.atom_cell.data(), static_cast<int>(n),
                                           cl.cursor.data(), cl.cell_atoms.data());
   TDMD_LAUNCH_CHECK();
-  k_sort_cells<<<ceil_div(ncells, 128), 128, 0, stream>>>(cl.cell_start.data(),
-                                                          cl.cell_count.data(),
-                                                          static_cast<int>(ncells),
-                                                          cl.cell_atoms.data());
+  k_sort_cells<<<ceil_div(ncells * 32, 256), 256, 0, stream>>>(cl.cell_start.data(),
+                                                                cl.cell_count.data(),
+                                                                static_cast<int>(ncells),
+                                                                cl.cell_atoms.data());
   TDMD_LAUNCH_CHECK();
 }
 
@@ -207,19 +282,22 @@ void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout lay
                          const int* row_off, int cap, int* counts, int* status,
                          cudaStream_t stream) {
   if (n == 0) return;
-  const int threads = 256;
-  const long long blocks = (n * 32 + threads - 1) / threads;
-  TDMD_REQUIRE(blocks < INT_MAX, "too many atoms for the list build grid");
+  // Band of the FP32 filter (see k_build_cells).
+  const double step = std::max(box.qstep[0], std::max(box.qstep[1], box.qstep[2]));
+  const double rl = std::sqrt(r_list_sq);
+  const double eps = 1e-5 + 8.0 * step / (rl > 0.0 ? rl : 1.0);
+  const float lo_f = static_cast<float>(r_list_sq * (1.0 - eps));
+  const float hi_f = static_cast<float>(r_list_sq * (1.0 + eps));
   if (layout == PosLayout::AoS3)
-    k_build_rows<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(
-        LoadAoS3{static_cast<const double*>(d_pos)}, static_cast<int>(n), box,
-        cl.atom_cell.data(), cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(),
-        r_list_sq, nbr, row_off, cap, counts, status);
+    k_build_cells<<<cl.ncells, kRowThreads, 0, stream>>>(
+        LoadAoS3{static_cast<const double*>(d_pos)}, box, cl.cell_start.data(),
+        cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq, lo_f, hi_f, nbr, row_off, cap,
+        counts, status);
   else
-    k_build_rows<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(
-        LoadD4{static_cast<const double4*>(d_pos)}, static_cast<int>(n), box,
-        cl.atom_cell.data(), cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(),
-        r_list_sq, nbr, row_off, cap, counts, status);
+    k_build_cells<<<cl.ncells, kRowThreads, 0, stream>>>(
+        LoadD4{static_cast<const double4*>(d_pos)}, box, cl.cell_start.data(),
+        cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq, lo_f, hi_f, nbr, row_off, cap,
+        counts, status);
   TDMD_LAUNCH_CHECK();
 }
 

@@ -350,9 +350,9 @@ void Scheduler::set_morse(const tdmd_morse_params& p) {
   kind_ = TDMD_POT_MORSE;
   cutoff_ = p.rc;
   const double rc_sq = p.rc_sq > 0.0 ? p.rc_sq : p.rc * p.rc;
-  m64_ = MorseP<double>{p.d, p.alpha, p.r0, rc_sq};
+  m64_ = MorseP<double>{p.d, p.alpha, p.r0, rc_sq, p.r0};
   m32_ = MorseP<float>{static_cast<float>(p.d), static_cast<float>(p.alpha),
-                       static_cast<float>(p.r0), static_cast<float>(rc_sq)};
+                       static_cast<float>(p.r0), static_cast<float>(rc_sq), p.r0};
   finish_setup();
 }
 
@@ -507,7 +507,7 @@ void Scheduler::enqueue_rebuild() {
   build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl * rl, nbr_.data(), nullptr,
                       cap_, cnt_.data(), ctl_status(), s);
   prof_end(kProfRebuild);
-  launches_ += cl_.ncells > 8192 ? 8 : 6;  // bin, scan(1|3), scatter, sort, rows
+  launches_ += cell_list_kernels() + 1;  // cell list + row build
   ++rebuilds_;
 }
 
@@ -520,7 +520,7 @@ void Scheduler::enqueue_force(bool ev) {
   if (kind_ == TDMD_POT_MORSE) {
     prof_begin(kProfForce);
     if (mixed_) {
-      GeoQ g{q_.data(), {box_.qscale[0], box_.qscale[1], box_.qscale[2]}};
+      const GeoQ g = make_geoq(q_.data(), box_);
       launch_morse(g, nl, n_, m32_, f32_.data(), ev, part, lpa_, s);
     } else {
       GeoD4 g{pos4_.data(), {box_.L[0], box_.L[1], box_.L[2]},
@@ -534,7 +534,7 @@ void Scheduler::enqueue_force(bool ev) {
     const int* types = eam_->ntypes > 1 ? types_.data() : nullptr;
     double* part2 = ev ? part + static_cast<long long>(nblk) * kEvStride : nullptr;
     if (mixed_) {
-      GeoQ g{q_.data(), {box_.qscale[0], box_.qscale[1], box_.qscale[2]}};
+      const GeoQ g = make_geoq(q_.data(), box_);
       prof_begin(kProfDensity);
       launch_eam_density<GeoQ, float, float>(g, nl, n_, eam_->d32, types, fp32_.data(), nullptr,
                                              nullptr, ev, part, lpa_, s);
@@ -795,7 +795,7 @@ void Scheduler::initial_forces() {
   build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_,
                       (cutoff_ + cfg_.r_skin) * (cutoff_ + cfg_.r_skin), nbr_.data(), nullptr,
                       cap_, cnt_.data(), ctl_status(), s);
-  launches_ += (cl_.ncells > 8192 ? 8 : 6) + 1;
+  launches_ += cell_list_kernels() + 2;  // cell list + count pass + fill pass
   ++rebuilds_;
   since_rebuild_ = 0;
   enqueue_force(false);

@@ -58,7 +58,7 @@ def test_morse_c0_vs_oracle(cuda, oracle, precision):
     else:
         assert rel_rms(f, fo) < MIXED_FORCE_TOL
         assert abs(e - pe) / abs(pe) < 1e-6
-        assert np.abs(w - wo).max() / np.abs(wo).max() < 1e-6
+        assert np.abs(w - wo).max() / np.abs(wo).max() < MIXED_FORCE_TOL
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
