@@ -314,6 +314,8 @@ def main():
     s32 = make_sched(sysm, eam, "mixed")
     s64.run_until(0)
     s32.run_until(0)
+    lanes32, tune32 = s32.autotune()
+    lanes64, tune64 = s64.autotune()
     f64 = s64.download().forces
     f32 = s32.download().forces.astype(np.float64)
     rel_err = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
@@ -385,6 +387,8 @@ def main():
                 "md_steps_per_bench_step": WINDOW, "parallelism": f"replicas x{world}",
                 "l2": "flushed (256 MiB write) before every bench step, outside its timing",
                 "mean_neighbors_K": K,
+                "lanes_per_atom": {"mixed": lanes32, "fp64": lanes64,
+                                   "autotune_ms_mixed": tune32, "autotune_ms_fp64": tune64},
                 "fp64": {"value": value64, "ms_per_step": ms_fp64 / args.steps},
                 "mixed_over_fp64": value / value64,
                 "force_rel_rms_err_mixed_vs_fp64": rel_err,

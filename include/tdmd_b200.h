@@ -292,6 +292,13 @@ int32_t tdmd_sched_device_state(tdmd_sched* s, void** d_pos4, double** d_vel, vo
 int32_t tdmd_sched_set_profiling(tdmd_sched* s, int32_t on);
 int32_t tdmd_sched_kernel_times(const tdmd_sched* s, double* avg_ms, int64_t* counts,
                                 int32_t ncat);
+/* Autotuner (no reference counterpart): times the scheduler's force passes
+ * on its current state for 1, 2, 4, 8, 16 and 32 lanes per atom, keeps the
+ * fastest and recomputes the forces with it.  ms6 (nullable) receives the
+ * six timings.  Runs by itself on the first run_until when
+ * cfg.lanes_per_atom == 0 and natoms >= 2048.  Results are bit-reproducible
+ * for a fixed lanes-per-atom choice. */
+int32_t tdmd_sched_autotune(tdmd_sched* s, int32_t* chosen_lanes, double* ms6);
 /* Device time (ms) of the last run_until window: CUDA events recorded on the
  * scheduler's stream before its first and after its last enqueued kernel. */
 int32_t tdmd_sched_last_window_ms(const tdmd_sched* s, double* ms);

@@ -137,6 +137,7 @@ SIGNATURES = {
     "tdmd_sched_device_state": [_p, _pp, _pp, _pp],
     "tdmd_sched_stream": [_p, _pp],
     "tdmd_sched_set_profiling": [_p, _i32],
+    "tdmd_sched_autotune": [_p, _pi32, _p],
     "tdmd_sched_last_window_ms": [_p, _pf64],
     "tdmd_sched_kernel_times": [_p, _p, _p, _i32],
 }

@@ -273,6 +273,14 @@ class FastPipelineScheduler:
         call("tdmd_sched_last_window_ms", self._h, C.byref(v))
         return v.value
 
+    def autotune(self):
+        """Pick lanes-per-atom by timing the force passes; returns
+        (chosen, {lanes: ms})."""
+        c = C.c_int32()
+        ms = np.zeros(6, np.float64)
+        call("tdmd_sched_autotune", self._h, C.byref(c), _ptr(ms))
+        return c.value, {1 << k: float(ms[k]) for k in range(6)}
+
     def set_profiling(self, on: bool = True):
         call("tdmd_sched_set_profiling", self._h, 1 if on else 0)
 

@@ -40,8 +40,10 @@ void eam_build_coeffs(tdmd_eam& e);
 // Device copy of one tdmd_eam: FP64 and FP32 r-spline rows plus the FP64
 // embedding table.
 struct EamDevTables {
-  DevArray<double4> rtab64;
+  DevArray<double4> rtab64;  // force rows (b, 2c, 3d, a)
   DevArray<float4> rtab32;
+  DevArray<double4> dtab64;  // density rows (a, b, c, d)
+  DevArray<float4> dtab32;
   DevArray<double4> ftab;
   EamDev<double> d64{};
   EamDev<float> d32{};

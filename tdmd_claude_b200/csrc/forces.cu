@@ -183,15 +183,27 @@ void EamDevTables::upload(const tdmd_eam& e, cudaStream_t stream) {
   const int S = nt + npairs;
   const int nsr = e.nr - 1;
   const int nsf = e.nrho - 1;
+  // Density rows (a, b, c, d) of rho_t, stride nt.
+  std::vector<double4> d64h(static_cast<size_t>(nsr) * nt);
+  std::vector<float4> d32h(static_cast<size_t>(nsr) * nt);
+  // Force rows (b, 2c, 3d, a) of every r-spline, stride S.
   std::vector<double4> r64(static_cast<size_t>(nsr) * S);
   std::vector<float4> r32(static_cast<size_t>(nsr) * S);
+  auto f4 = [](const double4& v) {
+    return make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z),
+                       static_cast<float>(v.w));
+  };
   auto put = [&](int s, const double* coef) {
     for (int k = 0; k < nsr; ++k) {
-      const double4 v = make_double4(coef[k], coef[nsr + k], coef[2 * nsr + k], coef[3 * nsr + k]);
+      const double a = coef[k], b = coef[nsr + k], c = coef[2 * nsr + k], d = coef[3 * nsr + k];
+      const double4 v = make_double4(b, 2.0 * c, 3.0 * d, a);
       r64[static_cast<size_t>(k) * S + s] = v;
-      r32[static_cast<size_t>(k) * S + s] =
-          make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z),
-                      static_cast<float>(v.w));
+      r32[static_cast<size_t>(k) * S + s] = f4(v);
+      if (s < nt) {
+        const double4 u = make_double4(a, b, c, d);
+        d64h[static_cast<size_t>(k) * nt + s] = u;
+        d32h[static_cast<size_t>(k) * nt + s] = f4(u);
+      }
     }
   };
   for (int t = 0; t < nt; ++t) put(t, e.rhoc.data() + static_cast<size_t>(t) * 4 * nsr);
@@ -200,14 +212,21 @@ void EamDevTables::upload(const tdmd_eam& e, cudaStream_t stream) {
   for (int t = 0; t < nt; ++t) {
     const double* c = e.Fc.data() + static_cast<size_t>(t) * 4 * nsf;
     for (int k = 0; k < nsf; ++k)
-      f64[static_cast<size_t>(t) * nsf + k] = make_double4(c[k], c[nsf + k], c[2 * nsf + k], c[3 * nsf + k]);
+      f64[static_cast<size_t>(t) * nsf + k] =
+          make_double4(c[k], c[nsf + k], c[2 * nsf + k], c[3 * nsf + k]);
   }
   rtab64.reserve(r64.size());
   rtab32.reserve(r32.size());
+  dtab64.reserve(d64h.size());
+  dtab32.reserve(d32h.size());
   ftab.reserve(f64.size());
   TDMD_CU(cudaMemcpyAsync(rtab64.data(), r64.data(), r64.size() * sizeof(double4),
                           cudaMemcpyHostToDevice, stream));
   TDMD_CU(cudaMemcpyAsync(rtab32.data(), r32.data(), r32.size() * sizeof(float4),
+                          cudaMemcpyHostToDevice, stream));
+  TDMD_CU(cudaMemcpyAsync(dtab64.data(), d64h.data(), d64h.size() * sizeof(double4),
+                          cudaMemcpyHostToDevice, stream));
+  TDMD_CU(cudaMemcpyAsync(dtab32.data(), d32h.data(), d32h.size() * sizeof(float4),
                           cudaMemcpyHostToDevice, stream));
   TDMD_CU(cudaMemcpyAsync(ftab.data(), f64.data(), f64.size() * sizeof(double4),
                           cudaMemcpyHostToDevice, stream));
@@ -215,9 +234,9 @@ void EamDevTables::upload(const tdmd_eam& e, cudaStream_t stream) {
   TDMD_CU(cudaStreamSynchronize(stream));
   ntypes = nt;
   cutoff = e.cutoff;
-  d64 = EamDev<double>{rtab64.data(), ftab.data(), nt, S, e.nr, e.nrho, e.dr, 1.0 / e.dr,
-                       e.cutoff * e.cutoff, e.drho, e.dr};
-  d32 = EamDev<float>{rtab32.data(), ftab.data(), nt, S, e.nr, e.nrho,
+  d64 = EamDev<double>{dtab64.data(), rtab64.data(), ftab.data(), nt, S, e.nr, e.nrho, e.dr,
+                       1.0 / e.dr, e.cutoff * e.cutoff, e.drho, e.dr};
+  d32 = EamDev<float>{dtab32.data(), rtab32.data(), ftab.data(), nt, S, e.nr, e.nrho,
                       static_cast<float>(e.dr), static_cast<float>(1.0 / e.dr),
                       static_cast<float>(e.cutoff * e.cutoff), e.drho, e.dr};
 }

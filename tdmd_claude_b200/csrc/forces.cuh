@@ -12,18 +12,24 @@
 //    the lanes of a group stride through the atom's neighbor row and merge
 //    their partial sums with xor-shuffles; no atomics anywhere.
 //  * Geometry policies: FP64 positions (double4 records or the reference's
-//    Vec3D AoS, min-image in double), the reference's mixed trick (double
-//    subtract, cast to float), or fixed-point int32 positions whose wrapped
+//    Vec3D AoS, min-image in double), the reference's mixed form (FP64
+//    delta cast to FP32), or fixed-point int32 positions whose wrapped
 //    difference IS the minimum image (scheduler's mixed path, 16-byte
-//    gathers, no FP64 ops per pair).
-//  * Mixed precision: FP32 distances/splines/forces, compensated FP32
-//    (TwoSum) per-atom sums; energies and virial always accumulate in FP64.
+//    gathers).
+//  * Mixed precision: FP32 distances/splines/forces with rsqrt-based 1/r,
+//    an FP64-refined radius for the spline offset and the Morse exponent,
+//    compensated FP32 per-atom sums (Kahan per lane, TwoSum across lanes);
+//    energies and virial always accumulate in FP64.
 //  * Energy/virial (template EV): per-block FP64 partials reduced later in a
 //    fixed order by k_reduce_partials.
-//  * EAM splines: rows of (a,b,c,d) per interval, all r-splines of one
-//    interval contiguous (density of each type, then phi of each pair), so a
-//    pair's lookups share one 32-byte sector for a single-type alloy.  The
-//    embedding F(rho) is always evaluated in FP64 (one lookup per atom).
+//  * EAM splines: the density pass reads rows (a,b,c,d) of rho_t; the force
+//    pass reads derivative-ready rows (b, 2c, 3d, a) of every r-spline of one
+//    interval side by side (density of each type, then phi of each pair), so
+//    a single-type pair's lookups share one 32-byte sector.  The embedding
+//    F(rho) is always evaluated in FP64 (one lookup per atom).
+//  * Scheduler mixed EAM: the density pass emits a gather record
+//    {qx, qy, qz, F'(rho)} per atom; the force pass reads position and F'
+//    of a neighbor in one 16-byte load.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -55,23 +61,39 @@ struct NbrView {
 // --------------------------------------------------------------------------
 // Geometry policies.  own(i) loads atom i once; pair(own, j, p) fills p with
 // r_i - r_j after the minimum image and r^2 in the policy's arithmetic type
-// T; radius(p, r, rd) gives |r_i - r_j| as T (for 1/r and cut tests) and as
-// an FP64 value rd that the spline offset and the Morse exponent use.
-// In FP32, r itself carries an absolute error of ~ulp(r) = 2.4e-7 A at
+// T; radius(p, r, rinv, rd) gives |r_i - r_j| and its inverse as T and as an
+// FP64 value rd that the spline offset and the Morse exponent use.  In
+// FP32, r itself carries an absolute error of ~ulp(r) = 2.4e-7 A at
 // r ~ 2.5 A, which moves the spline argument and, through the large pair
 // forces that cancel in each atom's net force, dominates the mixed-precision
-// force error; rd removes that term.
+// force error; rd removes that term (one Newton step in FP64 from the FP32
+// root, with the residual r^2 - r_f^2 taken from FP64 r^2).
 // --------------------------------------------------------------------------
-template <class T>
 struct PairD {
-  T dx, dy, dz, r2;
-  double r2d;  // precise r^2 (A^2); equals r2 on FP64 geometries
+  double dx, dy, dz, r2;
 };
+
+struct PairF {
+  float dx, dy, dz, r2;
+  double r2d;  // FP64 r^2
+};
+
+struct PairQ {
+  float dx, dy, dz, r2;
+  int ix, iy, iz, w;  // exact fixed-point delta and the neighbor's 4th word
+};
+
+__device__ __forceinline__ void radius_f(float r2, double r2d, float& r, float& rinv, double& rd) {
+  rinv = rsqrtf(r2);
+  r = r2 * rinv;
+  rd = static_cast<double>(r) +
+       static_cast<double>(static_cast<float>(fma(-static_cast<double>(r), r, r2d)) * 0.5f * rinv);
+}
 
 struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
   using T = double;
   using Own = double3;
-  using Pair = PairD<double>;
+  using Pair = PairD;
   const double4* p;
   double L[3], halfL[3];
   int per[3];
@@ -89,8 +111,9 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
     pr.dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
   }
-  __device__ __forceinline__ void radius(const Pair& pr, T& r, double& rd) const {
+  __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
     r = sqrt(pr.r2);
+    rinv = 1.0 / r;
     rd = r;
   }
 };
@@ -98,7 +121,7 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
 struct GeoAoS64 {  // FP64, reference Vec3D AoS
   using T = double;
   using Own = double3;
-  using Pair = PairD<double>;
+  using Pair = PairD;
   const double* p;
   double L[3], halfL[3];
   int per[3];
@@ -114,8 +137,9 @@ struct GeoAoS64 {  // FP64, reference Vec3D AoS
     pr.dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
   }
-  __device__ __forceinline__ void radius(const Pair& pr, T& r, double& rd) const {
+  __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
     r = sqrt(pr.r2);
+    rinv = 1.0 / r;
     rd = r;
   }
 };
@@ -127,7 +151,7 @@ struct GeoAoS64 {  // FP64, reference Vec3D AoS
 struct GeoAoS32 {
   using T = float;
   using Own = double3;
-  using Pair = PairD<float>;
+  using Pair = PairF;
   const double* p;
   double L[3], halfL[3];
   int per[3];
@@ -147,24 +171,16 @@ struct GeoAoS32 {
     pr.r2d = x * x + y * y + z * z;
     pr.r2 = static_cast<float>(pr.r2d);
   }
-  __device__ __forceinline__ void radius(const Pair& pr, T& r, double& rd) const {
-    r = sqrtf(pr.r2);
-    // one Newton step from the FP32 root: rd = r + (r2d - r^2) / (2 r)
-    rd = static_cast<double>(r) +
-         static_cast<double>(static_cast<float>(fma(-static_cast<double>(r), r, pr.r2d)) *
-                             (0.5f / r));
+  __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
+    radius_f(pr.r2, pr.r2d, r, rinv, rd);
   }
 };
 
-// Mixed, scheduler layout: fixed-point int4 {qx,qy,qz,type}.  The wrapped
-// int32 difference is the exact minimum-image delta in units of L/2^32;
-// FP32 components come from one conversion each, the precise r^2 from the
-// exact integers in FP64.
-struct PairQ {
-  float dx, dy, dz, r2;
-  int ix, iy, iz;
-};
-
+// Mixed, scheduler layout: fixed-point int4 records {qx,qy,qz,w}.  The
+// wrapped int32 difference is the exact minimum-image delta in units of
+// Lq/2^32; FP32 components come from one conversion each, the FP64 r^2 from
+// the exact integers (only for pairs inside the cutoff).  w is the type
+// (position records) or F'(rho) bits (the EAM force-pass gather records).
 struct GeoQ {
   using T = float;
   using Own = int4;
@@ -178,19 +194,15 @@ struct GeoQ {
     pr.ix = o.x - b.x;
     pr.iy = o.y - b.y;
     pr.iz = o.z - b.z;
+    pr.w = b.w;
     pr.dx = __fmul_rn(__int2float_rn(pr.ix), s[0]);
     pr.dy = __fmul_rn(__int2float_rn(pr.iy), s[1]);
     pr.dz = __fmul_rn(__int2float_rn(pr.iz), s[2]);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
   }
-  // Only pairs inside the cutoff pay for the FP64 refinement.
-  __device__ __forceinline__ void radius(const Pair& pr, T& r, double& rd) const {
+  __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
     const double x = pr.ix, y = pr.iy, z = pr.iz;
-    const double r2d = x * x * s2[0] + y * y * s2[1] + z * z * s2[2];
-    r = sqrtf(pr.r2);
-    rd = static_cast<double>(r) +
-         static_cast<double>(static_cast<float>(fma(-static_cast<double>(r), r, r2d)) *
-                             (0.5f / r));
+    radius_f(pr.r2, x * x * s2[0] + y * y * s2[1] + z * z * s2[2], r, rinv, rd);
   }
 };
 
@@ -208,7 +220,9 @@ __host__ inline GeoAoS32 make_geo_aos32(const double* p, const DevBox& b) {
 }
 
 // --------------------------------------------------------------------------
-// Accumulators: plain double (FP64) or compensated float (mixed).
+// Accumulators: plain double (FP64) or compensated float (mixed: Kahan per
+// lane -- 4 flops per term, error bounded by 2 eps sum|x| whatever the
+// number of terms -- and error-free TwoSum when lanes merge).
 // --------------------------------------------------------------------------
 template <class T>
 struct Acc;
@@ -221,20 +235,34 @@ struct Acc<double> {
 };
 template <>
 struct Acc<float> {
-  CSum cs;
-  __device__ __forceinline__ void add(float x) { cs.add(x); }
+  float s = 0.f, c = 0.f;  // running sum, compensation (subtracted)
+  __device__ __forceinline__ void add(float x) {
+    const float y = __fsub_rn(x, c);
+    const float t = __fadd_rn(s, y);
+    c = __fsub_rn(__fsub_rn(t, s), y);
+    s = t;
+  }
   __device__ __forceinline__ void shfl_merge(int o) {
-    const float os = __shfl_xor_sync(0xffffffffu, cs.s, o);
-    const float oc = __shfl_xor_sync(0xffffffffu, cs.c, o);
-    cs.merge(os, oc);
+    const float os = __shfl_xor_sync(0xffffffffu, s, o);
+    const float oc = __shfl_xor_sync(0xffffffffu, c, o);
+    // (s - c) + (os - oc) with TwoSum on the leading parts.
+    const float t = __fadd_rn(s, os);
+    const float z = __fsub_rn(t, s);
+    const float e = __fadd_rn(__fsub_rn(s, __fsub_rn(t, z)), __fsub_rn(os, z));
+    s = t;
+    c = __fsub_rn(__fadd_rn(c, oc), e);
   }
   __device__ __forceinline__ double value() const {
-    return static_cast<double>(cs.s) + static_cast<double>(cs.c);
+    return static_cast<double>(s) - static_cast<double>(c);
   }
 };
 
 __device__ __forceinline__ double mul_rn(double a, double b) { return a * b; }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+// FP64 keeps the reference's division by r; FP32 multiplies by rsqrt.
+__device__ __forceinline__ double over_r(double x, double r, double /*rinv*/) { return x / r; }
+__device__ __forceinline__ float over_r(float x, float /*r*/, float rinv) { return x * rinv; }
 
 // Force output: AoS float3 or double3.
 template <class F>
@@ -259,6 +287,18 @@ __device__ __forceinline__ void write_ev_partials(double e, const double (&w)[6]
     for (int k = 0; k < 7; ++k) o[k] = v[k];
     o[7] = 0.0;
   }
+}
+
+template <class T>
+__device__ __forceinline__ void add_virial(double (&w)[6], T fpair, T dx, T dy, T dz) {
+  const double hf = 0.5 * static_cast<double>(fpair);
+  const double ddx = dx, ddy = dy, ddz = dz;
+  w[0] += hf * ddx * ddx;
+  w[1] += hf * ddy * ddy;
+  w[2] += hf * ddz * ddz;
+  w[3] += hf * ddx * ddy;
+  w[4] += hf * ddx * ddz;
+  w[5] += hf * ddy * ddz;
 }
 
 // --------------------------------------------------------------------------
@@ -287,32 +327,24 @@ __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
     const typename Geo::Own o = g.own(i);
     const long long row = nl.row(i);
     const int c = nl.count(i);
+    const T two_d_alpha = T(2) * mp.d * mp.alpha;
     for (int k = sub; k < c; k += LPA) {
       const int j = __ldg(nl.nbr + row + k);
       typename Geo::Pair pr;
       g.pair(o, j, pr);
       if (pr.r2 < mp.rc_sq) {
-        T r;
+        T r, rinv;
         double rd;
-        g.radius(pr, r, rd);
-        const T dx = pr.dx, dy = pr.dy, dz = pr.dz;
+        g.radius(pr, r, rinv, rd);
         const T ex = exp(-mp.alpha * static_cast<T>(rd - mp.r0d));
         const T ome = T(1) - ex;
-        const T dudr = T(2) * mp.d * mp.alpha * ome * ex;
-        const T fpair = -dudr / r;
-        fx.add(mul_rn(fpair, dx));
-        fy.add(mul_rn(fpair, dy));
-        fz.add(mul_rn(fpair, dz));
+        const T fpair = -over_r(two_d_alpha * ome * ex, r, rinv);
+        fx.add(mul_rn(fpair, pr.dx));
+        fy.add(mul_rn(fpair, pr.dy));
+        fz.add(mul_rn(fpair, pr.dz));
         if (EV) {
           pe += 0.5 * static_cast<double>(mp.d * (ome * ome - T(1)));
-          const double hf = 0.5 * static_cast<double>(fpair);
-          const double ddx = dx, ddy = dy, ddz = dz;
-          w[0] += hf * ddx * ddx;
-          w[1] += hf * ddy * ddy;
-          w[2] += hf * ddz * ddz;
-          w[3] += hf * ddx * ddy;
-          w[4] += hf * ddx * ddz;
-          w[5] += hf * ddy * ddz;
+          add_virial(w, fpair, pr.dx, pr.dy, pr.dz);
         }
       }
     }
@@ -343,8 +375,9 @@ struct V4<float> {
 
 template <class T>
 struct EamDev {
-  const typename V4<T>::type* rtab;  // [(nr-1) * S], S = ntypes + npairs
-  const double4* ftab;               // [ntypes * (nrho-1)], FP64 always
+  const typename V4<T>::type* dtab;  // [(nr-1) * nt] (a, b, c, d) of rho_t
+  const typename V4<T>::type* rtab;  // [(nr-1) * S]  (b, 2c, 3d, a), S = nt + npairs
+  const double4* ftab;               // [nt * (nrho-1)] (a, b, c, d) of F_t, FP64
   int ntypes, S, nr, nrho;
   T dr, inv_dr, rc_sq;
   double drho;
@@ -362,26 +395,17 @@ __device__ __forceinline__ int phi_slot(int ti, int tj, int nt) {
 
 // Interval index and offset, SplineTable::eval (eam_alloy.cpp:52-61):
 // idx = int((r - rmin)/dr) clamped to [0, n-2], dx = r - idx*dr (rmin = 0).
-__device__ __forceinline__ int spline_idx(double r, double dr, double /*inv*/, int n,
-                                          double& dx) {
+__device__ __forceinline__ int spline_idx(double r, double dr, int n, double& dx) {
   int idx = static_cast<int>(r / dr);
   idx = idx < 0 ? 0 : (idx > n - 2 ? n - 2 : idx);
   dx = r - static_cast<double>(idx) * dr;
   return idx;
 }
-__device__ __forceinline__ int spline_idx(float r, float dr, float inv_dr, int n, float& dx) {
-  int idx = static_cast<int>(r * inv_dr);
-  idx = idx < 0 ? 0 : (idx > n - 2 ? n - 2 : idx);
-  dx = fmaf(-static_cast<float>(idx), dr, r);
-  return idx;
-}
 
-// Interval of r (index from r in T) and the offset from the FP64 radius.
-__device__ __forceinline__ int spline_at(double r, double rd, double dr, double inv, int n,
-                                         double dr_d, double& sx) {
-  (void)rd;
-  (void)dr_d;
-  return spline_idx(r, dr, inv, n, sx);
+// Interval from r in T, offset from the FP64 radius.
+__device__ __forceinline__ int spline_at(double r, double /*rd*/, double dr, double /*inv*/,
+                                         int n, double /*dr_d*/, double& sx) {
+  return spline_idx(r, dr, n, sx);
 }
 __device__ __forceinline__ int spline_at(float r, double rd, float /*dr*/, float inv_dr, int n,
                                          double dr_d, float& sx) {
@@ -391,6 +415,7 @@ __device__ __forceinline__ int spline_at(float r, double rd, float /*dr*/, float
   return idx;
 }
 
+// (a, b, c, d) rows: value a + x(b + x(c + x d)), derivative b + x(2c + 3d x).
 template <class C, class T>
 __device__ __forceinline__ T spl_val(const C& c, T dx) {
   return c.x + dx * (c.y + dx * (c.z + dx * c.w));
@@ -398,6 +423,15 @@ __device__ __forceinline__ T spl_val(const C& c, T dx) {
 template <class C, class T>
 __device__ __forceinline__ T spl_der(const C& c, T dx) {
   return c.y + dx * (T(2) * c.z + dx * T(3) * c.w);
+}
+// (b, 2c, 3d, a) rows.
+template <class C, class T>
+__device__ __forceinline__ T dspl_der(const C& c, T dx) {
+  return c.x + dx * (c.y + dx * c.z);
+}
+template <class C, class T>
+__device__ __forceinline__ T dspl_val(const C& c, T dx) {
+  return c.w + dx * (c.x + dx * (T(0.5) * c.y + dx * (c.z * T(1.0 / 3.0))));
 }
 
 template <class T>
@@ -417,7 +451,7 @@ __device__ __forceinline__ float4 ldv4<float>(const float4* p) {
 __device__ __forceinline__ void embed_eval(const double4* ftab, int nrho, double drho, int t,
                                            double rho, double& F, double& dF) {
   double dx;
-  const int idx = spline_idx(rho, drho, 0.0, nrho, dx);
+  const int idx = spline_idx(rho, drho, nrho, dx);
   const double4 c = ldv4<double>(ftab + static_cast<long long>(t) * (nrho - 1) + idx);
   F = spl_val(c, dx);
   dF = spl_der(c, dx);
@@ -425,7 +459,8 @@ __device__ __forceinline__ void embed_eval(const double4* ftab, int nrho, double
 
 // Pass 1 (+ fused pass 2): rho_i = sum_j f_tj(r_ij); then fp_i = F'(rho_i)
 // and, with EV, the embedding energy F(rho_i) into the block partials.
-// types == nullptr means a single-type alloy.
+// types == nullptr means a single-type alloy.  gout (GeoQ only, nullable)
+// receives the force pass's gather records {qx, qy, qz, bits(F'(rho))}.
 template <class Geo, int LPA, bool EV, class FP>
 __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
                                                      EamDev<typename Geo::T> e,
@@ -433,6 +468,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
                                                      FP* __restrict__ fp_out,
                                                      double* __restrict__ rho_out,
                                                      double* __restrict__ fpd_out,
+                                                     int4* __restrict__ gout,
                                                      double* __restrict__ partials) {
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -440,8 +476,9 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
   const int sub = tid % LPA;
   const bool active = i < n;
   Acc<T> rho;
+  typename Geo::Own o{};
   if (active) {
-    const typename Geo::Own o = g.own(i);
+    o = g.own(i);
     const long long row = nl.row(i);
     const int c = nl.count(i);
     for (int k = sub; k < c; k += LPA) {
@@ -449,18 +486,18 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
       typename Geo::Pair pr;
       g.pair(o, j, pr);
       if (pr.r2 < e.rc_sq) {
-        T r, sx;
+        T r, rinv, sx;
         double rd;
-        g.radius(pr, r, rd);
+        g.radius(pr, r, rinv, rd);
         const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
         const int tj = types ? __ldg(types + j) - 1 : 0;
-        const auto cf = ldv4<T>(e.rtab + static_cast<long long>(idx) * e.S + tj);
+        const auto cf = ldv4<T>(e.dtab + static_cast<long long>(idx) * e.ntypes + tj);
         rho.add(spl_val(cf, sx));
       }
     }
   }
 #pragma unroll
-  for (int o = LPA / 2; o > 0; o >>= 1) rho.shfl_merge(o);
+  for (int s = LPA / 2; s > 0; s >>= 1) rho.shfl_merge(s);
   double Fi = 0.0;
   if (active && sub == 0) {
     const double rh = rho.value();
@@ -470,6 +507,14 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
     fp_out[i] = static_cast<FP>(dF);
     if (rho_out) rho_out[i] = rh;
     if (fpd_out) fpd_out[i] = dF;
+    if constexpr (sizeof(typename Geo::Own) == sizeof(int4)) {
+      if (gout) {
+        int4 rec;
+        memcpy(&rec, &o, sizeof(rec));
+        rec.w = __float_as_int(static_cast<float>(dF));
+        gout[i] = rec;
+      }
+    }
   }
   if (EV) {
     const double w[6] = {0, 0, 0, 0, 0, 0};
@@ -478,7 +523,9 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
 }
 
 // Pass 3: f_ij = -(phi' + fp_i rho'_tj + fp_j rho'_ti)/r * (r_i - r_j).
-template <class Geo, int LPA, bool EV, class FP, class F>
+// FPG: F'(rho_j) comes with the neighbor's gather record (pair w bits)
+// instead of the fp array.
+template <class Geo, int LPA, bool EV, bool FPG, class FP, class F>
 __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
                                                    EamDev<typename Geo::T> e,
                                                    const int* __restrict__ types,
@@ -503,42 +550,38 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
       typename Geo::Pair pr;
       g.pair(o, j, pr);
       if (pr.r2 < e.rc_sq) {
-        T r, sx;
+        T r, rinv, sx;
         double rd;
-        g.radius(pr, r, rd);
-        const T dx = pr.dx, dy = pr.dy, dz = pr.dz;
+        g.radius(pr, r, rinv, rd);
         const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
         const int tj = types ? __ldg(types + j) - 1 : 0;
         const auto* rowp = e.rtab + static_cast<long long>(idx) * e.S;
         const auto cphi = ldv4<T>(rowp + (types ? phi_slot(ti, tj, e.ntypes) : 1));
-        const auto crj = ldv4<T>(rowp + tj);
-        const T drj = spl_der(crj, sx);
+        const T drj = dspl_der(ldv4<T>(rowp + tj), sx);
         T dri = drj;
-        if (types && tj != ti) dri = spl_der(ldv4<T>(rowp + ti), sx);
-        const T fpj = static_cast<T>(__ldg(fp + j));
-        const T fpair = -(spl_der(cphi, sx) + fpi * drj + fpj * dri) / r;
-        fx.add(mul_rn(fpair, dx));
-        fy.add(mul_rn(fpair, dy));
-        fz.add(mul_rn(fpair, dz));
+        if (types && tj != ti) dri = dspl_der(ldv4<T>(rowp + ti), sx);
+        T fpj;
+        if constexpr (FPG) {
+          fpj = __int_as_float(pr.w);
+        } else {
+          fpj = static_cast<T>(__ldg(fp + j));
+        }
+        const T fpair = -over_r(dspl_der(cphi, sx) + fpi * drj + fpj * dri, r, rinv);
+        fx.add(mul_rn(fpair, pr.dx));
+        fy.add(mul_rn(fpair, pr.dy));
+        fz.add(mul_rn(fpair, pr.dz));
         if (EV) {
-          pe += 0.5 * static_cast<double>(spl_val(cphi, sx));
-          const double hf = 0.5 * static_cast<double>(fpair);
-          const double ddx = dx, ddy = dy, ddz = dz;
-          w[0] += hf * ddx * ddx;
-          w[1] += hf * ddy * ddy;
-          w[2] += hf * ddz * ddz;
-          w[3] += hf * ddx * ddy;
-          w[4] += hf * ddx * ddz;
-          w[5] += hf * ddy * ddz;
+          pe += 0.5 * static_cast<double>(dspl_val(cphi, sx));
+          add_virial(w, fpair, pr.dx, pr.dy, pr.dz);
         }
       }
     }
   }
 #pragma unroll
-  for (int o = LPA / 2; o > 0; o >>= 1) {
-    fx.shfl_merge(o);
-    fy.shfl_merge(o);
-    fz.shfl_merge(o);
+  for (int s = LPA / 2; s > 0; s >>= 1) {
+    fx.shfl_merge(s);
+    fy.shfl_merge(s);
+    fz.shfl_merge(s);
   }
   if (active && sub == 0) out.store(i, fx.value(), fy.value(), fz.value());
   if (EV) write_ev_partials(pe, w, partials);
@@ -549,8 +592,6 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
 __global__ void k_reduce_partials(const double* __restrict__ partials, int nblk,
                                   double* __restrict__ energy, double* __restrict__ virial);
 
-// Launch helpers (forces.cu).  `ev` non-null => energy/virial partials are
-// written there (nblocks * kEvStride doubles) -- see ev_blocks().
 int force_blocks(long long n, int lpa);
 
 }  // namespace tdmd_b200

@@ -40,50 +40,54 @@ void launch_morse(const Geo& g, const NbrView& nl, int n, const MorseP<typename 
   TDMD_LAUNCH_CHECK();
 }
 
-// Density(+embedding) then force.  With ev, the density pass writes records
-// [0, nblk) and the force pass [nblk, 2*nblk) of `partials`.
-template <class Geo, class FP, class F>
+// Density + embedding pass.  gout (fixed-point geometries only) receives
+// the force pass's {q, F'} gather records.
+template <class Geo, class FP>
 void launch_eam_density(const Geo& g, const NbrView& nl, int n,
                         const EamDev<typename Geo::T>& e, const int* types, FP* fp,
-                        double* rho_out, double* fpd_out, bool ev, double* partials, int lpa,
-                        cudaStream_t s) {
+                        double* rho_out, double* fpd_out, int4* gout, bool ev, double* partials,
+                        int lpa, cudaStream_t s) {
   const int nblk = force_blocks(n, lpa);
   TDMD_LPA_DISPATCH(lpa, {
     if (ev)
-      k_eam_density<Geo, L, true, FP><<<nblk, kForceThreads, 0, s>>>(g, nl, n, e, types, fp,
-                                                                     rho_out, fpd_out, partials);
+      k_eam_density<Geo, L, true, FP><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, e, types, fp, rho_out, fpd_out, gout, partials);
     else
-      k_eam_density<Geo, L, false, FP><<<nblk, kForceThreads, 0, s>>>(g, nl, n, e, types, fp,
-                                                                      rho_out, fpd_out, nullptr);
+      k_eam_density<Geo, L, false, FP><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, e, types, fp, rho_out, fpd_out, gout, nullptr);
   });
   TDMD_LAUNCH_CHECK();
 }
 
-template <class Geo, class FP, class F>
+// Force pass.  FPG: the geometry reads gather records that carry F'(rho).
+template <class Geo, bool FPG, class FP, class F>
 void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typename Geo::T>& e,
                       const int* types, const FP* fp, F* forces, bool ev, double* partials,
                       int lpa, cudaStream_t s) {
   const int nblk = force_blocks(n, lpa);
   TDMD_LPA_DISPATCH(lpa, {
     if (ev)
-      k_eam_force<Geo, L, true, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, true, FPG, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, partials);
     else
-      k_eam_force<Geo, L, false, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, false, FPG, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
   });
   TDMD_LAUNCH_CHECK();
 }
 
+// Density then force on the same geometry (free functions).  With ev, the
+// density pass writes records [0, nblk) and the force pass [nblk, 2*nblk).
 template <class Geo, class FP, class F>
 void launch_eam(const Geo& g, const NbrView& nl, int n, const EamDev<typename Geo::T>& e,
                 const int* types, FP* fp, double* rho_out, double* fpd_out, F* forces, bool ev,
                 double* partials, int lpa, cudaStream_t s) {
   const int nblk = force_blocks(n, lpa);
-  launch_eam_density<Geo, FP, F>(g, nl, n, e, types, fp, rho_out, fpd_out, ev, partials, lpa, s);
-  launch_eam_force<Geo, FP, F>(g, nl, n, e, types, fp, forces, ev,
-                               ev ? partials + static_cast<long long>(nblk) * kEvStride : nullptr,
-                               lpa, s);
+  launch_eam_density<Geo, FP>(g, nl, n, e, types, fp, rho_out, fpd_out, nullptr, ev, partials,
+                              lpa, s);
+  launch_eam_force<Geo, false, FP, F>(
+      g, nl, n, e, types, fp, forces, ev,
+      ev ? partials + static_cast<long long>(nblk) * kEvStride : nullptr, lpa, s);
 }
 
 }  // namespace tdmd_b200

@@ -179,6 +179,7 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
   const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];
   const float s0 = b.qscale[0], s1 = b.qscale[1], s2 = b.qscale[2];
   const unsigned lt_mask = (1u << lane) - 1u;
+  int wmax = 0;  // lane 0: this warp's longest row
   for (int a = warp; a < ncen; a += kRowThreads / 32) {
     const int4 ci = staged ? stage[c0 + a] : fetch(c0 + a);
     const int i = ci.w;
@@ -226,10 +227,23 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
     }
     if (lane == 0) {
       counts[i] = cnt;
-      if (status) {
-        if (!row_off && cnt > cap) atomicOr(&status[0], 1);
-        atomicMax(&status[1], cnt);
-      }
+      wmax = cnt > wmax ? cnt : wmax;
+    }
+  }
+  // Status: one atomic per CTA, and only when something needs reporting --
+  // the maximum for a sizing (count-only) pass, the overflow flag when a
+  // padded row is too short.  Per-atom atomics on one address serialise in
+  // L2 and used to dominate this kernel.
+  if (status) {
+    __shared__ int s_max[kRowThreads / 32];
+    if (lane == 0) s_max[warp] = wmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int m = 0;
+      for (int w = 0; w < kRowThreads / 32; ++w) m = s_max[w] > m ? s_max[w] : m;
+      const bool overflow = !row_off && nbr && m > cap;
+      if (overflow) atomicOr(&status[0], 1);
+      if (overflow || !nbr) atomicMax(&status[1], m);
     }
   }
 }

@@ -84,6 +84,11 @@ class Scheduler {
   // Per-kernel timing with CUDA events on the scheduler's stream (disables
   // graph replay while on).  Categories: see ProfCat.
   void set_profiling(bool on);
+  // Times the force passes for lanes-per-atom in {1,2,4,8,16,32} on the
+  // current state, keeps the fastest, recomputes the forces with it.
+  // ms6[k] = ms of candidate 2^k (nullable).
+  void autotune(int* chosen, double* ms6);
+  int lanes_per_atom() const { return lpa_; }
   // Device time of the last run_until window (events on the stream around
   // its enqueued work), ms.
   double last_window_ms() const { return last_window_ms_; }
@@ -154,6 +159,8 @@ class Scheduler {
   DevArray<float> f32_;
   DevArray<int> types_, ids_;
   DevArray<double> masses_;
+  DevArray<double> inv_mm_;  // 1 / (m mvv2e) per type: the kick factor per unit dt
+  DevArray<int4> g_;         // mixed EAM: {qx, qy, qz, bits(F'(rho))} per atom
   mutable DevArray<double> stage_;
   int n_types_ = 0;
 
@@ -189,7 +196,7 @@ class Scheduler {
   double prof_ms_[kProfCount] = {0, 0, 0, 0, 0};
   long long prof_n_[kProfCount] = {0, 0, 0, 0, 0};
 
-  bool uploaded_ = false, initialized_ = false;
+  bool uploaded_ = false, initialized_ = false, tuned_ = false;
   int step_ = 0, since_rebuild_ = 0;
   long long ticks_ = 0, launches_ = 0, rebuilds_ = 0, graph_launches_ = 0, retries_ = 0;
 };

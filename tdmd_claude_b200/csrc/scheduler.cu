@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kThreads) k_kick_drift(double4* __restrict__ p
                                                          double* __restrict__ v,
                                                          const F* __restrict__ f,
                                                          const int* __restrict__ types,
-                                                         const double* __restrict__ masses, int n,
+                                                         const double* __restrict__ inv_mm, int n,
                                                          double dt_arg, SchedCtl* __restrict__ ctl,
                                                          int ctl_dt, DevBox b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) k_kick_drift(double4* __restrict__ p
   const double dt = ctl_dt ? ctl->dt : dt_arg;
   const double kick_dt = FULL ? dt : 0.5 * dt;
   const int t = types[i];
-  const double factor = kick_dt / (masses[t] * kMvv2e);
+  const double factor = kick_dt * inv_mm[t];
   const double s = SCALE ? ctl->scale : 1.0;
   double4 p = pos4[i];
   double vx = v[3ll * i], vy = v[3ll * i + 1], vz = v[3ll * i + 2];
@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(kThreads) k_half_kick_s(double* __restrict__ v
                                                           const F* __restrict__ f,
                                                           const int* __restrict__ types,
                                                           const double* __restrict__ masses,
+                                                          const double* __restrict__ inv_mm,
                                                           int n, double dt_arg,
                                                           const SchedCtl* __restrict__ ctl,
                                                           int ctl_dt,
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(kThreads) k_half_kick_s(double* __restrict__ v
   if (i < n) {
     const double dt = ctl_dt ? ctl->dt : dt_arg;
     const double m = masses[types[i]];
-    const double factor = 0.5 * dt / (m * kMvv2e);
+    const double factor = 0.5 * dt * inv_mm[types[i]];
     const double vx = v[3ll * i] + factor * static_cast<double>(f[3ll * i]);
     const double vy = v[3ll * i + 1] + factor * static_cast<double>(f[3ll * i + 1]);
     const double vz = v[3ll * i + 2] + factor * static_cast<double>(f[3ll * i + 2]);
@@ -173,6 +174,7 @@ __global__ void __launch_bounds__(kThreads) k_ke_integer(const double* __restric
                                                          const F* __restrict__ f,
                                                          const int* __restrict__ types,
                                                          const double* __restrict__ masses,
+                                                         const double* __restrict__ inv_mm,
                                                          int n, double dt,
                                                          double* __restrict__ partials) {
   __shared__ double red[32 * 2];
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(kThreads) k_ke_integer(const double* __restric
   double ke = 0.0, v2 = 0.0;
   if (i < n) {
     const double m = masses[types[i]];
-    const double factor = 0.5 * dt / (m * kMvv2e);
+    const double factor = 0.5 * dt * inv_mm[types[i]];
     const double vx = v[3ll * i] + factor * static_cast<double>(f[3ll * i]);
     const double vy = v[3ll * i + 1] + factor * static_cast<double>(f[3ll * i + 1]);
     const double vz = v[3ll * i + 2] + factor * static_cast<double>(f[3ll * i + 2]);
@@ -419,6 +421,14 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
   }
   TDMD_CU(cudaMemcpyAsync(masses_.data(), masses, sizeof(double) * n_types,
                           cudaMemcpyHostToDevice, s));
+  // Kick factor per unit dt, 1/(m mvv2e) -- the reference divides per atom
+  // (device_velocity_verlet.cu:100-102); one host division per type here.
+  std::vector<double> inv(static_cast<size_t>(n_types), 0.0);
+  for (int t = 0; t < n_types; ++t)
+    inv[static_cast<size_t>(t)] = masses[t] > 0.0 ? 1.0 / (masses[t] * kMvv2e) : 0.0;
+  inv_mm_.reserve(static_cast<size_t>(n_types));
+  TDMD_CU(cudaMemcpyAsync(inv_mm_.data(), inv.data(), sizeof(double) * n_types,
+                          cudaMemcpyHostToDevice, s));
   // Control block: dt, unit scale, fresh chain.
   SchedCtl h{};
   h.dt = cfg_.dt;
@@ -427,13 +437,14 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
     nhc_init(h.eta, h.eta_v, h.eta_m, cfg_.nhc_length, cfg_.t_target, cfg_.t_period, 3 * n_ - 3);
   TDMD_CU(cudaMemcpyAsync(ctl_.data(), &h, sizeof(h), cudaMemcpyHostToDevice, s));
   // Scratch sized for the chosen lanes-per-atom.
-  const int nblk_force = force_blocks(n_ > 0 ? n_ : 1, lpa_);
+  // Energy partials sized for the widest lanes-per-atom the autotuner tries.
+  const int nblk_force = force_blocks(n_ > 0 ? n_ : 1, 32);
   ev_part_.reserve(static_cast<size_t>(2 * nblk_force) * kEvStride);
   // (KE, v2max) per block plus the 2-double result of k_ke_vmax_finish.
   ke_part_.reserve(static_cast<size_t>(2 * ceil_div(n_ > 0 ? n_ : 1, kThreads) + 8));
   if (kind_ == TDMD_POT_EAM) {
     if (mixed_)
-      fp32_.reserve(n);
+      fp32_.reserve(n), g_.reserve(n);
     else
       fp64_.reserve(n);
   }
@@ -534,26 +545,29 @@ void Scheduler::enqueue_force(bool ev) {
     const int* types = eam_->ntypes > 1 ? types_.data() : nullptr;
     double* part2 = ev ? part + static_cast<long long>(nblk) * kEvStride : nullptr;
     if (mixed_) {
+      // Density reads the position records and writes {q, F'} gather
+      // records; the force pass gathers those.
       const GeoQ g = make_geoq(q_.data(), box_);
+      const GeoQ gg = make_geoq(g_.data(), box_);
       prof_begin(kProfDensity);
-      launch_eam_density<GeoQ, float, float>(g, nl, n_, eam_->d32, types, fp32_.data(), nullptr,
-                                             nullptr, ev, part, lpa_, s);
+      launch_eam_density<GeoQ, float>(g, nl, n_, eam_->d32, types, fp32_.data(), nullptr,
+                                      nullptr, g_.data(), ev, part, lpa_, s);
       prof_end(kProfDensity);
       prof_begin(kProfForce);
-      launch_eam_force<GeoQ, float, float>(g, nl, n_, eam_->d32, types, fp32_.data(),
-                                           f32_.data(), ev, part2, lpa_, s);
+      launch_eam_force<GeoQ, true, float, float>(gg, nl, n_, eam_->d32, types, fp32_.data(),
+                                                 f32_.data(), ev, part2, lpa_, s);
       prof_end(kProfForce);
     } else {
       GeoD4 g{pos4_.data(), {box_.L[0], box_.L[1], box_.L[2]},
               {box_.halfL[0], box_.halfL[1], box_.halfL[2]},
               {box_.periodic[0], box_.periodic[1], box_.periodic[2]}};
       prof_begin(kProfDensity);
-      launch_eam_density<GeoD4, double, double>(g, nl, n_, eam_->d64, types, fp64_.data(),
-                                                nullptr, nullptr, ev, part, lpa_, s);
+      launch_eam_density<GeoD4, double>(g, nl, n_, eam_->d64, types, fp64_.data(), nullptr,
+                                        nullptr, nullptr, ev, part, lpa_, s);
       prof_end(kProfDensity);
       prof_begin(kProfForce);
-      launch_eam_force<GeoD4, double, double>(g, nl, n_, eam_->d64, types, fp64_.data(),
-                                              f64_.data(), ev, part2, lpa_, s);
+      launch_eam_force<GeoD4, false, double, double>(g, nl, n_, eam_->d64, types, fp64_.data(),
+                                                     f64_.data(), ev, part2, lpa_, s);
       prof_end(kProfForce);
     }
     launches_ += 2;
@@ -577,15 +591,15 @@ void Scheduler::enqueue_kick_drift_t(F* f, bool full, bool scale) {
   const int ctl_dt = thermo_ ? 1 : 0;
   if (scale)
     k_kick_drift<F, false, true><<<nb, kThreads, 0, s>>>(pos4_.data(), q, vel_.data(), f,
-                                                         types_.data(), masses_.data(), n_,
+                                                         types_.data(), inv_mm_.data(), n_,
                                                          cfg_.dt, ctl_.data(), ctl_dt, box_);
   else if (full)
     k_kick_drift<F, true, false><<<nb, kThreads, 0, s>>>(pos4_.data(), q, vel_.data(), f,
-                                                         types_.data(), masses_.data(), n_,
+                                                         types_.data(), inv_mm_.data(), n_,
                                                          cfg_.dt, ctl_.data(), ctl_dt, box_);
   else
     k_kick_drift<F, false, false><<<nb, kThreads, 0, s>>>(pos4_.data(), q, vel_.data(), f,
-                                                          types_.data(), masses_.data(), n_,
+                                                          types_.data(), inv_mm_.data(), n_,
                                                           cfg_.dt, ctl_.data(), ctl_dt, box_);
   TDMD_LAUNCH_CHECK();
   launches_ += 1;
@@ -606,11 +620,11 @@ void Scheduler::enqueue_half_kick_t(F* f, bool ke) {
   const int nb = ceil_div(n_, kThreads);
   const int ctl_dt = thermo_ ? 1 : 0;
   if (ke)
-    k_half_kick_s<F, true><<<nb, kThreads, 0, s>>>(vel_.data(), f, types_.data(), masses_.data(),
+    k_half_kick_s<F, true><<<nb, kThreads, 0, s>>>(vel_.data(), f, types_.data(), masses_.data(), inv_mm_.data(),
                                                    n_, cfg_.dt, ctl_.data(), ctl_dt,
                                                    ke_part_.data());
   else
-    k_half_kick_s<F, false><<<nb, kThreads, 0, s>>>(vel_.data(), f, types_.data(), masses_.data(),
+    k_half_kick_s<F, false><<<nb, kThreads, 0, s>>>(vel_.data(), f, types_.data(), masses_.data(), inv_mm_.data(),
                                                     n_, cfg_.dt, ctl_.data(), ctl_dt, nullptr);
   TDMD_LAUNCH_CHECK();
   launches_ += 1;
@@ -662,10 +676,10 @@ void Scheduler::enqueue_log_nve() {
   cudaStream_t s = stream_;
   const int nb = ceil_div(n_, kThreads);
   if (mixed_)
-    k_ke_integer<<<nb, kThreads, 0, s>>>(vel_.data(), f32_.data(), types_.data(), masses_.data(),
+    k_ke_integer<<<nb, kThreads, 0, s>>>(vel_.data(), f32_.data(), types_.data(), masses_.data(), inv_mm_.data(),
                                          n_, cfg_.dt, ke_part_.data());
   else
-    k_ke_integer<<<nb, kThreads, 0, s>>>(vel_.data(), f64_.data(), types_.data(), masses_.data(),
+    k_ke_integer<<<nb, kThreads, 0, s>>>(vel_.data(), f64_.data(), types_.data(), masses_.data(), inv_mm_.data(),
                                          n_, cfg_.dt, ke_part_.data());
   TDMD_LAUNCH_CHECK();
   k_log_nve<<<1, 256, 0, s>>>(ctl_.data(), ke_part_.data(), nb, log_.data(), log_cap_);
@@ -853,6 +867,9 @@ void Scheduler::run_until(int target) {
     return;
   }
   if (!initialized_) initial_forces();
+  // lanes_per_atom = 0: measure the candidates once on the first window of
+  // a system large enough for the choice to matter.
+  if (!tuned_ && cfg_.lanes_per_atom == 0 && n_ >= 2048) autotune(nullptr, nullptr);
   if (step_ >= target) {
     TDMD_CU(cudaStreamSynchronize(stream_));
     return;
@@ -963,6 +980,52 @@ void Scheduler::thermostat_state(double* dt, double* eta, double* eta_v) const {
 }
 
 // ----- per-kernel timing -------------------------------------------------------
+// ----- autotuner ---------------------------------------------------------------
+void Scheduler::autotune(int* chosen, double* ms6) {
+  TDMD_REQUIRE(uploaded_, "autotune before upload");
+  if (n_ == 0) return;
+  if (!initialized_) initial_forces();
+  const bool prof = profiling_;
+  profiling_ = false;
+  const long long l0 = launches_;
+  cudaEvent_t e0, e1;
+  TDMD_CU(cudaEventCreate(&e0));
+  TDMD_CU(cudaEventCreate(&e1));
+  const int cand[6] = {1, 2, 4, 8, 16, 32};
+  double best_ms = 1e300;
+  int best = lpa_;
+  for (int k = 0; k < 6; ++k) {
+    lpa_ = cand[k];
+    enqueue_force(false);  // warm
+    double m = 1e300;
+    for (int rep = 0; rep < 3; ++rep) {
+      TDMD_CU(cudaEventRecord(e0, stream_));
+      enqueue_force(false);
+      TDMD_CU(cudaEventRecord(e1, stream_));
+      TDMD_CU(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      TDMD_CU(cudaEventElapsedTime(&ms, e0, e1));
+      m = std::min(m, static_cast<double>(ms));
+    }
+    if (ms6) ms6[k] = m;
+    if (m < best_ms) {
+      best_ms = m;
+      best = cand[k];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // The forces of the current state, summed in the chosen lanes' order.
+  lpa_ = best;
+  enqueue_force(false);
+  TDMD_CU(cudaStreamSynchronize(stream_));
+  launches_ = l0;  // tuning passes are not part of the run's kernel count
+  clear_graphs();
+  tuned_ = true;
+  profiling_ = prof;
+  if (chosen) *chosen = best;
+}
+
 void Scheduler::set_profiling(bool on) {
   profiling_ = on;
   for (int k = 0; k < kProfCount; ++k) {
@@ -1182,3 +1245,12 @@ int32_t tdmd_sched_stream(const tdmd_sched* s, void** stream) {
 }
 
 }  // extern "C"
+
+extern "C" int32_t tdmd_sched_autotune(tdmd_sched* s, int32_t* chosen_lanes, double* ms6) {
+  return guarded([&] {
+    TDMD_REQUIRE(s, "null handle");
+    int c = 0;
+    s->s->autotune(&c, ms6);
+    if (chosen_lanes) *chosen_lanes = c;
+  });
+}

@@ -259,3 +259,18 @@ def test_upload_rejects_bad_types(cuda):
         s.upload(pos, vel, None, bad, None, masses)
     with pytest.raises(TdmdError):
         s.run_until(3)     # nothing uploaded
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_autotune_keeps_forces(cuda, precision):
+    """The autotuner only reorders the per-atom sums: forces stay within
+    rounding, the choice is one of the candidates, later steps still match."""
+    s, sysm, t = _eam_setup(precision, ncell=8)
+    s.run_until(0)
+    f0 = s.download().forces.astype(np.float64)
+    chosen, ms = s.autotune()
+    assert chosen in (1, 2, 4, 8, 16, 32) and all(v > 0 for v in ms.values())
+    f1 = s.download().forces.astype(np.float64)
+    assert rel_rms(f1, f0) < (1e-13 if precision == "fp64" else 1e-6)
+    s.run_until(20)
+    assert s.current_step() == 20
