@@ -58,6 +58,27 @@ struct NbrView {
   }
 };
 
+// Neighbors per lane per sweep: a lane fetches kU indices, then kU
+// positions, then evaluates kU pairs, so its loads overlap.
+constexpr int kU = 4;
+
+// Indices base .. base+kU-1 of a row, -1 past the count.  VEC: 16-byte
+// aligned padded rows (scheduler) -> one int4 load.
+template <bool VEC>
+__device__ __forceinline__ void nbr_batch(const NbrView& nl, long long row, int base, int c,
+                                          int (&j)[kU]) {
+  if constexpr (VEC) {
+    const int4 v = __ldg(reinterpret_cast<const int4*>(nl.nbr + row + base));
+    j[0] = v.x;
+    j[1] = base + 1 < c ? v.y : -1;
+    j[2] = base + 2 < c ? v.z : -1;
+    j[3] = base + 3 < c ? v.w : -1;
+  } else {
+#pragma unroll
+    for (int u = 0; u < kU; ++u) j[u] = base + u < c ? __ldg(nl.nbr + row + base + u) : -1;
+  }
+}
+
 // --------------------------------------------------------------------------
 // Geometry policies.  own(i) loads atom i once; pair(own, j, p) fills p with
 // r_i - r_j after the minimum image and r^2 in the policy's arithmetic type
@@ -116,6 +137,7 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
     rinv = 1.0 / r;
     rd = r;
   }
+  __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
 };
 
 struct GeoAoS64 {  // FP64, reference Vec3D AoS
@@ -142,6 +164,7 @@ struct GeoAoS64 {  // FP64, reference Vec3D AoS
     rinv = 1.0 / r;
     rd = r;
   }
+  __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
 };
 
 // Mixed on the reference layout (free functions): the delta is formed in
@@ -174,6 +197,7 @@ struct GeoAoS32 {
   __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
     radius_f(pr.r2, pr.r2d, r, rinv, rd);
   }
+  __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
 };
 
 // Mixed, scheduler layout: fixed-point int4 records {qx,qy,qz,w}.  The
@@ -204,6 +228,7 @@ struct GeoQ {
     const double x = pr.ix, y = pr.iy, z = pr.iz;
     radius_f(pr.r2, x * x * s2[0] + y * y * s2[1] + z * z * s2[2], r, rinv, rd);
   }
+  __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
 };
 
 __host__ inline GeoQ make_geoq(const int4* q, const DevBox& b) {
@@ -311,7 +336,7 @@ struct MorseP {
   double r0d;
 };
 
-template <class Geo, int LPA, bool EV, class F>
+template <class Geo, int LPA, bool EV, bool VEC, class F>
 __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
                                                MorseP<typename Geo::T> mp, ForceOut<F> out,
                                                double* __restrict__ partials) {
@@ -328,23 +353,33 @@ __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
     const long long row = nl.row(i);
     const int c = nl.count(i);
     const T two_d_alpha = T(2) * mp.d * mp.alpha;
-    for (int k = sub; k < c; k += LPA) {
-      const int j = __ldg(nl.nbr + row + k);
-      typename Geo::Pair pr;
-      g.pair(o, j, pr);
-      if (pr.r2 < mp.rc_sq) {
-        T r, rinv;
-        double rd;
-        g.radius(pr, r, rinv, rd);
-        const T ex = exp(-mp.alpha * static_cast<T>(rd - mp.r0d));
-        const T ome = T(1) - ex;
-        const T fpair = -over_r(two_d_alpha * ome * ex, r, rinv);
-        fx.add(mul_rn(fpair, pr.dx));
-        fy.add(mul_rn(fpair, pr.dy));
-        fz.add(mul_rn(fpair, pr.dz));
-        if (EV) {
-          pe += 0.5 * static_cast<double>(mp.d * (ome * ome - T(1)));
-          add_virial(w, fpair, pr.dx, pr.dy, pr.dz);
+    for (int base = kU * sub; base < c; base += kU * LPA) {
+      int jj[kU];
+      nbr_batch<VEC>(nl, row, base, c, jj);
+      typename Geo::Pair pr[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (jj[u] >= 0)
+          g.pair(o, jj[u], pr[u]);
+        else
+          pr[u].r2 = mp.rc_sq;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (pr[u].r2 < mp.rc_sq) {
+          T r, rinv;
+          double rd;
+          g.radius(pr[u], r, rinv, rd);
+          const T ex = exp(-mp.alpha * static_cast<T>(rd - mp.r0d));
+          const T ome = T(1) - ex;
+          const T fpair = -over_r(two_d_alpha * ome * ex, r, rinv);
+          fx.add(mul_rn(fpair, pr[u].dx));
+          fy.add(mul_rn(fpair, pr[u].dy));
+          fz.add(mul_rn(fpair, pr[u].dz));
+          if (EV) {
+            pe += 0.5 * static_cast<double>(mp.d * (ome * ome - T(1)));
+            add_virial(w, fpair, pr[u].dx, pr[u].dy, pr[u].dz);
+          }
         }
       }
     }
@@ -415,6 +450,19 @@ __device__ __forceinline__ int spline_at(float r, double rd, float /*dr*/, float
   return idx;
 }
 
+// Interval and offset from r alone (density pass).
+template <class T>
+__device__ __forceinline__ int spline_fast(double r, const EamDev<T>& e, double& sx) {
+  return spline_idx(r, e.dr, e.nr, sx);
+}
+template <class T>
+__device__ __forceinline__ int spline_fast(float r, const EamDev<T>& e, float& sx) {
+  int idx = static_cast<int>(r * e.inv_dr);
+  idx = idx < 0 ? 0 : (idx > e.nr - 2 ? e.nr - 2 : idx);
+  sx = fmaf(-static_cast<float>(idx), e.dr, r);
+  return idx;
+}
+
 // (a, b, c, d) rows: value a + x(b + x(c + x d)), derivative b + x(2c + 3d x).
 template <class C, class T>
 __device__ __forceinline__ T spl_val(const C& c, T dx) {
@@ -461,7 +509,7 @@ __device__ __forceinline__ void embed_eval(const double4* ftab, int nrho, double
 // and, with EV, the embedding energy F(rho_i) into the block partials.
 // types == nullptr means a single-type alloy.  gout (GeoQ only, nullable)
 // receives the force pass's gather records {qx, qy, qz, bits(F'(rho))}.
-template <class Geo, int LPA, bool EV, class FP>
+template <class Geo, int LPA, bool EV, bool VEC, class FP>
 __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
                                                      EamDev<typename Geo::T> e,
                                                      const int* __restrict__ types,
@@ -481,18 +529,30 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
     o = g.own(i);
     const long long row = nl.row(i);
     const int c = nl.count(i);
-    for (int k = sub; k < c; k += LPA) {
-      const int j = __ldg(nl.nbr + row + k);
-      typename Geo::Pair pr;
-      g.pair(o, j, pr);
-      if (pr.r2 < e.rc_sq) {
-        T r, rinv, sx;
-        double rd;
-        g.radius(pr, r, rinv, rd);
-        const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
-        const int tj = types ? __ldg(types + j) - 1 : 0;
-        const auto cf = ldv4<T>(e.dtab + static_cast<long long>(idx) * e.ntypes + tj);
-        rho.add(spl_val(cf, sx));
+    for (int base = kU * sub; base < c; base += kU * LPA) {
+      int jj[kU];
+      nbr_batch<VEC>(nl, row, base, c, jj);
+      typename Geo::Pair pr[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (jj[u] >= 0)
+          g.pair(o, jj[u], pr[u]);
+        else
+          pr[u].r2 = e.rc_sq;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (pr[u].r2 < e.rc_sq) {
+          // No FP64-refined radius here: in the mixed path the density's
+          // FP32 radius error is a few percent of the total force error
+          // (the force pass's radius dominates), so it is not worth the
+          // FP64 work.
+          T sx;
+          const int idx = spline_fast(g.radius_fast(pr[u]), e, sx);
+          const int tj = types ? __ldg(types + jj[u]) - 1 : 0;
+          const auto cf = ldv4<T>(e.dtab + static_cast<long long>(idx) * e.ntypes + tj);
+          rho.add(spl_val(cf, sx));
+        }
       }
     }
   }
@@ -525,7 +585,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
 // Pass 3: f_ij = -(phi' + fp_i rho'_tj + fp_j rho'_ti)/r * (r_i - r_j).
 // FPG: F'(rho_j) comes with the neighbor's gather record (pair w bits)
 // instead of the fp array.
-template <class Geo, int LPA, bool EV, bool FPG, class FP, class F>
+template <class Geo, int LPA, bool EV, bool FPG, bool VEC, class FP, class F>
 __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
                                                    EamDev<typename Geo::T> e,
                                                    const int* __restrict__ types,
@@ -545,34 +605,45 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
     const int c = nl.count(i);
     const int ti = types ? __ldg(types + i) - 1 : 0;
     const T fpi = static_cast<T>(__ldg(fp + i));
-    for (int k = sub; k < c; k += LPA) {
-      const int j = __ldg(nl.nbr + row + k);
-      typename Geo::Pair pr;
-      g.pair(o, j, pr);
-      if (pr.r2 < e.rc_sq) {
-        T r, rinv, sx;
-        double rd;
-        g.radius(pr, r, rinv, rd);
-        const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
-        const int tj = types ? __ldg(types + j) - 1 : 0;
-        const auto* rowp = e.rtab + static_cast<long long>(idx) * e.S;
-        const auto cphi = ldv4<T>(rowp + (types ? phi_slot(ti, tj, e.ntypes) : 1));
-        const T drj = dspl_der(ldv4<T>(rowp + tj), sx);
-        T dri = drj;
-        if (types && tj != ti) dri = dspl_der(ldv4<T>(rowp + ti), sx);
-        T fpj;
-        if constexpr (FPG) {
-          fpj = __int_as_float(pr.w);
-        } else {
-          fpj = static_cast<T>(__ldg(fp + j));
-        }
-        const T fpair = -over_r(dspl_der(cphi, sx) + fpi * drj + fpj * dri, r, rinv);
-        fx.add(mul_rn(fpair, pr.dx));
-        fy.add(mul_rn(fpair, pr.dy));
-        fz.add(mul_rn(fpair, pr.dz));
-        if (EV) {
-          pe += 0.5 * static_cast<double>(dspl_val(cphi, sx));
-          add_virial(w, fpair, pr.dx, pr.dy, pr.dz);
+    for (int base = kU * sub; base < c; base += kU * LPA) {
+      int jj[kU];
+      nbr_batch<VEC>(nl, row, base, c, jj);
+      typename Geo::Pair pr[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (jj[u] >= 0)
+          g.pair(o, jj[u], pr[u]);
+        else
+          pr[u].r2 = e.rc_sq;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (pr[u].r2 < e.rc_sq) {
+          T r, rinv, sx;
+          double rd;
+          g.radius(pr[u], r, rinv, rd);
+          const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
+          const int j = jj[u];
+          const int tj = types ? __ldg(types + j) - 1 : 0;
+          const auto* rowp = e.rtab + static_cast<long long>(idx) * e.S;
+          const auto cphi = ldv4<T>(rowp + (types ? phi_slot(ti, tj, e.ntypes) : 1));
+          const T drj = dspl_der(ldv4<T>(rowp + tj), sx);
+          T dri = drj;
+          if (types && tj != ti) dri = dspl_der(ldv4<T>(rowp + ti), sx);
+          T fpj;
+          if constexpr (FPG) {
+            fpj = __int_as_float(pr[u].w);
+          } else {
+            fpj = static_cast<T>(__ldg(fp + j));
+          }
+          const T fpair = -over_r(dspl_der(cphi, sx) + fpi * drj + fpj * dri, r, rinv);
+          fx.add(mul_rn(fpair, pr[u].dx));
+          fy.add(mul_rn(fpair, pr[u].dy));
+          fz.add(mul_rn(fpair, pr[u].dz));
+          if (EV) {
+            pe += 0.5 * static_cast<double>(dspl_val(cphi, sx));
+            add_virial(w, fpair, pr[u].dx, pr[u].dy, pr[u].dz);
+          }
         }
       }
     }

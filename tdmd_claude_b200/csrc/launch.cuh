@@ -13,6 +13,18 @@ constexpr int kForceThreads = 256;
 int force_blocks(long long n, int lpa);
 int default_lpa(long long n);
 
+// VEC (16-byte aligned padded rows) is a runtime property of the view.
+#define TDMD_VEC_DISPATCH(vec, ...)                               \
+  if (vec) {                                                      \
+    constexpr bool V = true;                                      \
+    __VA_ARGS__;                                                  \
+  } else {                                                        \
+    constexpr bool V = false;                                     \
+    __VA_ARGS__;                                                  \
+  }
+
+inline bool vec_rows(const NbrView& nl) { return nl.row_off == nullptr && nl.cap % 4 == 0; }
+
 #define TDMD_LPA_DISPATCH(lpa, ...)                              \
   switch (lpa) {                                                  \
     case 1: { constexpr int L = 1; __VA_ARGS__; } break;          \
@@ -29,14 +41,14 @@ template <class Geo, class F>
 void launch_morse(const Geo& g, const NbrView& nl, int n, const MorseP<typename Geo::T>& mp,
                   F* forces, bool ev, double* partials, int lpa, cudaStream_t s) {
   const int nblk = force_blocks(n, lpa);
-  TDMD_LPA_DISPATCH(lpa, {
+  TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
     if (ev)
-      k_morse<Geo, L, true, F><<<nblk, kForceThreads, 0, s>>>(g, nl, n, mp, ForceOut<F>{forces},
-                                                              partials);
+      k_morse<Geo, L, true, V, F><<<nblk, kForceThreads, 0, s>>>(g, nl, n, mp,
+                                                                 ForceOut<F>{forces}, partials);
     else
-      k_morse<Geo, L, false, F><<<nblk, kForceThreads, 0, s>>>(g, nl, n, mp, ForceOut<F>{forces},
-                                                               nullptr);
-  });
+      k_morse<Geo, L, false, V, F><<<nblk, kForceThreads, 0, s>>>(g, nl, n, mp,
+                                                                  ForceOut<F>{forces}, nullptr);
+  }));
   TDMD_LAUNCH_CHECK();
 }
 
@@ -48,14 +60,14 @@ void launch_eam_density(const Geo& g, const NbrView& nl, int n,
                         double* rho_out, double* fpd_out, int4* gout, bool ev, double* partials,
                         int lpa, cudaStream_t s) {
   const int nblk = force_blocks(n, lpa);
-  TDMD_LPA_DISPATCH(lpa, {
+  TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
     if (ev)
-      k_eam_density<Geo, L, true, FP><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_density<Geo, L, true, V, FP><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, rho_out, fpd_out, gout, partials);
     else
-      k_eam_density<Geo, L, false, FP><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_density<Geo, L, false, V, FP><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, rho_out, fpd_out, gout, nullptr);
-  });
+  }));
   TDMD_LAUNCH_CHECK();
 }
 
@@ -65,14 +77,14 @@ void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typen
                       const int* types, const FP* fp, F* forces, bool ev, double* partials,
                       int lpa, cudaStream_t s) {
   const int nblk = force_blocks(n, lpa);
-  TDMD_LPA_DISPATCH(lpa, {
+  TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
     if (ev)
-      k_eam_force<Geo, L, true, FPG, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, true, FPG, V, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, partials);
     else
-      k_eam_force<Geo, L, false, FPG, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, false, FPG, V, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
-  });
+  }));
   TDMD_LAUNCH_CHECK();
 }
 
