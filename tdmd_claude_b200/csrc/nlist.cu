@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <type_traits>
 
 #include "buffers.cuh"
 #include "common.cuh"
@@ -106,31 +107,34 @@ __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __re
 // --------------------------------------------------------------------------
 // Row build, one CTA per cell.  The 27 stencil cells (dz, dy, dx in -1..1,
 // wrapped) are concatenated in stencil order; their atoms (ID order within
-// each cell) become candidate records {qx, qy, qz, j} with fixed-point
-// coordinates, staged in shared memory when they fit (kStageCap records),
-// read through L1 otherwise.  Each warp takes center-cell atoms in turn and
-// sweeps the candidates 32 at a time:
-//   * FP32 filter: r^2 from the exact int32 differences; a candidate whose
-//     r^2 lies outside the band rl^2 (1 -+ eps) is decided by it.  The FP32
-//     r^2 is within ~5e-7 relative of the FP64 one, plus the fixed-point
-//     quantisation (one unit L/2^32 per component: 2 sqrt(3) rl L/2^32 in
-//     r^2); eps = 1e-5 + 8 (L/2^32)/rl covers both with a wide margin, so
-//     the decision equals the FP64 one;
-//   * otherwise the reference expression decides: delta = r_j - r_i in FP64,
-//     minimum image, (x*x + y*y) + z*z with round-to-nearest ops, < rl^2.
+// each cell) become candidate records {x, y, z, j}: FP32 coordinates
+// relative to the center cell's lower corner, taken from the exact int32
+// fixed-point difference (so the minimum image is already applied when the
+// grid has at least 4 cells per periodic axis; WRAP re-applies it in FP32
+// for 3-cell axes).  Records are staged in shared memory when they fit
+// (kStageCap); otherwise each warp rebuilds them on the fly.  Each warp takes
+// center-cell atoms in turn and sweeps the candidates 32 at a time:
+//   * FP32 filter: a candidate whose r^2 lies outside the band
+//     rl^2 (1 -+ eps) is decided by it.  Each coordinate carries at most
+//     ~2^-23 of its magnitude (< 3 cells) in rounding, plus one fixed-point
+//     unit L/2^32; eps = 3e-5 + 8 (L/2^32)/rl bounds the resulting r^2 error
+//     several times over, so the decision equals the FP64 one;
+//   * inside the band the reference expression decides: delta = r_j - r_i
+//     in FP64, minimum image, (x*x + y*y) + z*z with round-to-nearest ops,
+//     < rl^2.
 // Accepted candidates are compacted with ballot/popc in candidate order, so
 // every row is the reference's per-atom list, bit for bit.
 // --------------------------------------------------------------------------
 constexpr int kRowThreads = 128;
 constexpr int kStageCap = 1536;  // staged candidate records (24 KiB)
 
-template <class Load>
+template <class Load, bool WRAP>
 __global__ void __launch_bounds__(kRowThreads) k_build_cells(
     Load pos, DevBox b, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const int* __restrict__ cell_atoms, double rl2, float lo_f, float hi_f, int* __restrict__ nbr,
     const int* __restrict__ row_off, int cap, int* __restrict__ counts,
     int* __restrict__ status) {
-  __shared__ int4 stage[kStageCap];
+  __shared__ float4 stage[kStageCap];
   __shared__ int s_start[27], s_pre[28];
   const int c = blockIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -159,8 +163,13 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
   __syncthreads();
   const int total = s_pre[27];
   const bool staged = total <= kStageCap;
-  // Candidate record k: cell t with s_pre[t] <= k < s_pre[t+1].
-  auto fetch = [&](int k) -> int4 {
+  // Fixed-point lower corner of the center cell.
+  const int ox = encode_q(b.lo[0] + ix * b.cs[0], b.qlo[0], b.qinv[0]);
+  const int oy = encode_q(b.lo[1] + iy * b.cs[1], b.qlo[1], b.qinv[1]);
+  const int oz = encode_q(b.lo[2] + iz * b.cs[2], b.qlo[2], b.qinv[2]);
+  const float s0 = b.qscale[0], s1 = b.qscale[1], s2 = b.qscale[2];
+  // Candidate record k (cell t with s_pre[t] <= k < s_pre[t+1]).
+  auto record = [&](int k) -> float4 {
     int lo = 0, hi = 27;
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
@@ -168,55 +177,49 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
     }
     const int j = __ldg(cell_atoms + s_start[lo] + (k - s_pre[lo]));
     const double3 p = pos(j);
-    return make_int4(encode_q(p.x, b.qlo[0], b.qinv[0]), encode_q(p.y, b.qlo[1], b.qinv[1]),
-                     encode_q(p.z, b.qlo[2], b.qinv[2]), j);
+    return make_float4(__fmul_rn(__int2float_rn(encode_q(p.x, b.qlo[0], b.qinv[0]) - ox), s0),
+                       __fmul_rn(__int2float_rn(encode_q(p.y, b.qlo[1], b.qinv[1]) - oy), s1),
+                       __fmul_rn(__int2float_rn(encode_q(p.z, b.qlo[2], b.qinv[2]) - oz), s2),
+                       __int_as_float(j));
   };
   if (staged) {
-    for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = fetch(k);
+    for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = record(k);
   }
   __syncthreads();
-  // The center cell is stencil slot 13.
-  const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];
-  const float s0 = b.qscale[0], s1 = b.qscale[1], s2 = b.qscale[2];
+  const float Lx = static_cast<float>(b.L[0]), Ly = static_cast<float>(b.L[1]),
+              Lz = static_cast<float>(b.L[2]);
+  const float hx = 0.5f * Lx, hy = 0.5f * Ly, hz = 0.5f * Lz;
+  const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];  // center = slot 13
   const unsigned lt_mask = (1u << lane) - 1u;
   int wmax = 0;  // lane 0: this warp's longest row
   for (int a = warp; a < ncen; a += kRowThreads / 32) {
-    const int4 ci = staged ? stage[c0 + a] : fetch(c0 + a);
-    const int i = ci.w;
+    const float4 ci = staged ? stage[c0 + a] : record(c0 + a);
+    const int i = __float_as_int(ci.w);
     const long long base = row_off ? static_cast<long long>(row_off[i])
                                    : static_cast<long long>(i) * cap;
     const int limit = row_off ? INT_MAX : cap;
-    double3 pi = make_double3(0, 0, 0);
-    bool have_pi = false;
     int cnt = 0;
     for (int k0 = 0; k0 < total; k0 += 32) {
       const int k = k0 + lane;
-      bool pred = false;
-      int j = -1;
-      if (k < total) {
-        const int4 cj = staged ? stage[k] : fetch(k);
-        j = cj.w;
-        if (j != i) {
-          const float fx = __fmul_rn(__int2float_rn(cj.x - ci.x), s0);
-          const float fy = __fmul_rn(__int2float_rn(cj.y - ci.y), s1);
-          const float fz = __fmul_rn(__int2float_rn(cj.z - ci.z), s2);
-          const float r2f = fx * fx + fy * fy + fz * fz;
-          if (r2f < lo_f) {
-            pred = true;
-          } else if (r2f <= hi_f) {
-            if (!have_pi) {
-              pi = pos(i);
-              have_pi = true;
-            }
-            const double3 pj = pos(j);
-            const double dx = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
-            const double dy = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
-            const double dz = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
-            const double r2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            pred = r2 < rl2;
-          }
-        }
+      float4 cj = make_float4(0.f, 0.f, 0.f, __int_as_float(i));
+      if (k < total) cj = staged ? stage[k] : record(k);
+      const int j = __float_as_int(cj.w);
+      float dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
+      if (WRAP) {
+        dx = min_image1(dx, Lx, hx, b.periodic[0]);
+        dy = min_image1(dy, Ly, hy, b.periodic[1]);
+        dz = min_image1(dz, Lz, hz, b.periodic[2]);
+      }
+      const float r2f = dx * dx + dy * dy + dz * dz;
+      bool pred = j != i && r2f < lo_f;
+      if (j != i && r2f >= lo_f && r2f <= hi_f) {
+        const double3 pi = pos(i), pj = pos(j);
+        const double ex = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
+        const double ey = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
+        const double ez = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
+        const double r2 =
+            __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+        pred = r2 < rl2;
       }
       const unsigned m = __ballot_sync(0xffffffffu, pred);
       if (pred && nbr) {
@@ -232,8 +235,7 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
   }
   // Status: one atomic per CTA, and only when something needs reporting --
   // the maximum for a sizing (count-only) pass, the overflow flag when a
-  // padded row is too short.  Per-atom atomics on one address serialise in
-  // L2 and used to dominate this kernel.
+  // padded row is too short.
   if (status) {
     __shared__ int s_max[kRowThreads / 32];
     if (lane == 0) s_max[warp] = wmax;
@@ -299,19 +301,27 @@ void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout lay
   // Band of the FP32 filter (see k_build_cells).
   const double step = std::max(box.qstep[0], std::max(box.qstep[1], box.qstep[2]));
   const double rl = std::sqrt(r_list_sq);
-  const double eps = 1e-5 + 8.0 * step / (rl > 0.0 ? rl : 1.0);
+  const double eps = 3e-5 + 8.0 * step / (rl > 0.0 ? rl : 1.0);
   const float lo_f = static_cast<float>(r_list_sq * (1.0 - eps));
   const float hi_f = static_cast<float>(r_list_sq * (1.0 + eps));
-  if (layout == PosLayout::AoS3)
-    k_build_cells<<<cl.ncells, kRowThreads, 0, stream>>>(
-        LoadAoS3{static_cast<const double*>(d_pos)}, box, cl.cell_start.data(),
-        cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq, lo_f, hi_f, nbr, row_off, cap,
-        counts, status);
-  else
-    k_build_cells<<<cl.ncells, kRowThreads, 0, stream>>>(
-        LoadD4{static_cast<const double4*>(d_pos)}, box, cl.cell_start.data(),
-        cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq, lo_f, hi_f, nbr, row_off, cap,
-        counts, status);
+  // Relative coordinates are minimum-imaged by the int32 wrap when every
+  // periodic axis has >= 4 cells (candidates then lie within 2 cells of the
+  // corner, under L/2); 3-cell axes re-apply the minimum image in FP32.
+  bool wrap = false;
+  for (int a = 0; a < 3; ++a) wrap = wrap || (box.periodic[a] && box.nc[a] < 4);
+  auto go = [&](auto load, auto wrap_tag) {
+    constexpr bool W = decltype(wrap_tag)::value;
+    k_build_cells<decltype(load), W><<<cl.ncells, kRowThreads, 0, stream>>>(
+        load, box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
+        lo_f, hi_f, nbr, row_off, cap, counts, status);
+  };
+  if (layout == PosLayout::AoS3) {
+    const LoadAoS3 ld{static_cast<const double*>(d_pos)};
+    if (wrap) go(ld, std::true_type{}); else go(ld, std::false_type{});
+  } else {
+    const LoadD4 ld{static_cast<const double4*>(d_pos)};
+    if (wrap) go(ld, std::true_type{}); else go(ld, std::false_type{});
+  }
   TDMD_LAUNCH_CHECK();
 }
 
