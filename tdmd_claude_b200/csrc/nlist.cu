@@ -192,47 +192,54 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
   const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];  // center = slot 13
   const unsigned lt_mask = (1u << lane) - 1u;
   int wmax = 0;  // lane 0: this warp's longest row
-  for (int a = warp; a < ncen; a += kRowThreads / 32) {
-    const float4 ci = staged ? stage[c0 + a] : record(c0 + a);
-    const int i = __float_as_int(ci.w);
-    const long long base = row_off ? static_cast<long long>(row_off[i])
-                                   : static_cast<long long>(i) * cap;
-    const int limit = row_off ? INT_MAX : cap;
-    int cnt = 0;
-    for (int k0 = 0; k0 < total; k0 += 32) {
-      const int k = k0 + lane;
-      float4 cj = make_float4(0.f, 0.f, 0.f, __int_as_float(i));
-      if (k < total) cj = staged ? stage[k] : record(k);
-      const int j = __float_as_int(cj.w);
-      float dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
-      if (WRAP) {
-        dx = min_image1(dx, Lx, hx, b.periodic[0]);
-        dy = min_image1(dy, Ly, hy, b.periodic[1]);
-        dz = min_image1(dz, Lz, hz, b.periodic[2]);
+  // One sweep per candidate source: staged records (the hot path) or
+  // records rebuilt on the fly, so the hot loop carries no second path.
+  auto sweep = [&](auto cand) {
+    for (int a = warp; a < ncen; a += kRowThreads / 32) {
+      const float4 ci = cand(c0 + a);
+      const int i = __float_as_int(ci.w);
+      const long long base = row_off ? static_cast<long long>(row_off[i])
+                                     : static_cast<long long>(i) * cap;
+      const int limit = row_off ? INT_MAX : cap;
+      int cnt = 0;
+      for (int k0 = 0; k0 < total; k0 += 32) {
+        const int k = k0 + lane;
+        const float4 cj = cand(k < total ? k : c0 + a);  // past the end: atom i itself
+        const int j = __float_as_int(cj.w);
+        float dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
+        if (WRAP) {
+          dx = min_image1(dx, Lx, hx, b.periodic[0]);
+          dy = min_image1(dy, Ly, hy, b.periodic[1]);
+          dz = min_image1(dz, Lz, hz, b.periodic[2]);
+        }
+        const float r2f = dx * dx + dy * dy + dz * dz;
+        bool pred = j != i && r2f < lo_f;
+        if (j != i && r2f >= lo_f && r2f <= hi_f) {
+          const double3 pi = pos(i), pj = pos(j);
+          const double ex = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
+          const double ey = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
+          const double ez = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
+          const double r2 =
+              __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+          pred = r2 < rl2;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, pred);
+        if (pred && nbr) {
+          const int p = cnt + __popc(m & lt_mask);
+          if (p < limit) nbr[base + p] = j;
+        }
+        cnt += __popc(m);
       }
-      const float r2f = dx * dx + dy * dy + dz * dz;
-      bool pred = j != i && r2f < lo_f;
-      if (j != i && r2f >= lo_f && r2f <= hi_f) {
-        const double3 pi = pos(i), pj = pos(j);
-        const double ex = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
-        const double ey = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
-        const double ez = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
-        const double r2 =
-            __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-        pred = r2 < rl2;
+      if (lane == 0) {
+        counts[i] = cnt;
+        wmax = cnt > wmax ? cnt : wmax;
       }
-      const unsigned m = __ballot_sync(0xffffffffu, pred);
-      if (pred && nbr) {
-        const int p = cnt + __popc(m & lt_mask);
-        if (p < limit) nbr[base + p] = j;
-      }
-      cnt += __popc(m);
     }
-    if (lane == 0) {
-      counts[i] = cnt;
-      wmax = cnt > wmax ? cnt : wmax;
-    }
-  }
+  };
+  if (staged)
+    sweep([&](int k) { return stage[k]; });
+  else
+    sweep(record);
   // Status: one atomic per CTA, and only when something needs reporting --
   // the maximum for a sizing (count-only) pass, the overflow flag when a
   // padded row is too short.
