@@ -58,6 +58,24 @@ struct NbrView {
   }
 };
 
+// L1 eviction-priority loads: spline rows are re-read by every pair and
+// stay resident (evict_last); neighbor indices are read once and bypass L1
+// (no_allocate), so they do not push rows and position records out.
+__device__ __forceinline__ float4 ld_keep(const float4* p) {
+  float4 v;
+  asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(p));
+  return v;
+}
+__device__ __forceinline__ int4 ld_stream(const int4* p) {
+  int4 v;
+  asm("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p));
+  return v;
+}
+
 // Neighbors per lane per sweep: a lane fetches kU indices, then kU
 // positions, then evaluates kU pairs, so its loads overlap.
 constexpr int kU = 4;
@@ -68,7 +86,7 @@ template <bool VEC>
 __device__ __forceinline__ void nbr_batch(const NbrView& nl, long long row, int base, int c,
                                           int (&j)[kU]) {
   if constexpr (VEC) {
-    const int4 v = __ldg(reinterpret_cast<const int4*>(nl.nbr + row + base));
+    const int4 v = ld_stream(reinterpret_cast<const int4*>(nl.nbr + row + base));
     j[0] = v.x;
     j[1] = base + 1 < c ? v.y : -1;
     j[2] = base + 2 < c ? v.z : -1;
@@ -492,7 +510,7 @@ __device__ __forceinline__ double4 ldv4<double>(const double4* p) {
 }
 template <>
 __device__ __forceinline__ float4 ldv4<float>(const float4* p) {
-  return __ldg(p);
+  return ld_keep(p);
 }
 
 // Embedding F(rho), F'(rho) in FP64 (SplineTable eval/eval_deriv on F).
@@ -509,7 +527,7 @@ __device__ __forceinline__ void embed_eval(const double4* ftab, int nrho, double
 // and, with EV, the embedding energy F(rho_i) into the block partials.
 // types == nullptr means a single-type alloy.  gout (GeoQ only, nullable)
 // receives the force pass's gather records {qx, qy, qz, bits(F'(rho))}.
-template <class Geo, int LPA, bool EV, bool VEC, class FP>
+template <class Geo, int LPA, bool EV, bool VEC, bool MULTI, class FP>
 __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
                                                      EamDev<typename Geo::T> e,
                                                      const int* __restrict__ types,
@@ -549,7 +567,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
           // FP64 work.
           T sx;
           const int idx = spline_fast(g.radius_fast(pr[u]), e, sx);
-          const int tj = types ? __ldg(types + jj[u]) - 1 : 0;
+          const int tj = MULTI ? __ldg(types + jj[u]) - 1 : 0;
           const auto cf = ldv4<T>(e.dtab + static_cast<long long>(idx) * e.ntypes + tj);
           rho.add(spl_val(cf, sx));
         }
@@ -561,7 +579,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
   double Fi = 0.0;
   if (active && sub == 0) {
     const double rh = rho.value();
-    const int ti = types ? __ldg(types + i) - 1 : 0;
+    const int ti = MULTI ? __ldg(types + i) - 1 : 0;
     double dF;
     embed_eval(e.ftab, e.nrho, e.drho, ti, rh, Fi, dF);
     fp_out[i] = static_cast<FP>(dF);
@@ -585,7 +603,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
 // Pass 3: f_ij = -(phi' + fp_i rho'_tj + fp_j rho'_ti)/r * (r_i - r_j).
 // FPG: F'(rho_j) comes with the neighbor's gather record (pair w bits)
 // instead of the fp array.
-template <class Geo, int LPA, bool EV, bool FPG, bool VEC, class FP, class F>
+template <class Geo, int LPA, bool EV, bool FPG, bool VEC, bool MULTI, class FP, class F>
 __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
                                                    EamDev<typename Geo::T> e,
                                                    const int* __restrict__ types,
@@ -603,7 +621,7 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
     const typename Geo::Own o = g.own(i);
     const long long row = nl.row(i);
     const int c = nl.count(i);
-    const int ti = types ? __ldg(types + i) - 1 : 0;
+    const int ti = MULTI ? __ldg(types + i) - 1 : 0;
     const T fpi = static_cast<T>(__ldg(fp + i));
     for (int base = kU * sub; base < c; base += kU * LPA) {
       int jj[kU];
@@ -624,12 +642,12 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
           g.radius(pr[u], r, rinv, rd);
           const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
           const int j = jj[u];
-          const int tj = types ? __ldg(types + j) - 1 : 0;
+          const int tj = MULTI ? __ldg(types + j) - 1 : 0;
           const auto* rowp = e.rtab + static_cast<long long>(idx) * e.S;
-          const auto cphi = ldv4<T>(rowp + (types ? phi_slot(ti, tj, e.ntypes) : 1));
+          const auto cphi = ldv4<T>(rowp + (MULTI ? phi_slot(ti, tj, e.ntypes) : 1));
           const T drj = dspl_der(ldv4<T>(rowp + tj), sx);
           T dri = drj;
-          if (types && tj != ti) dri = dspl_der(ldv4<T>(rowp + ti), sx);
+          if (MULTI && tj != ti) dri = dspl_der(ldv4<T>(rowp + ti), sx);
           T fpj;
           if constexpr (FPG) {
             fpj = __int_as_float(pr[u].w);

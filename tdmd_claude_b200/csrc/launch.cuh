@@ -23,6 +23,17 @@ int default_lpa(long long n);
     __VA_ARGS__;                                                  \
   }
 
+// MULTI: more than one atom type (per-neighbor type loads, pair-slot
+// lookup); single-type alloys compile those out.
+#define TDMD_MULTI_DISPATCH(multi, ...)                           \
+  if (multi) {                                                    \
+    constexpr bool M = true;                                      \
+    __VA_ARGS__;                                                  \
+  } else {                                                        \
+    constexpr bool M = false;                                     \
+    __VA_ARGS__;                                                  \
+  }
+
 inline bool vec_rows(const NbrView& nl) { return nl.row_off == nullptr && nl.cap % 4 == 0; }
 
 #define TDMD_LPA_DISPATCH(lpa, ...)                              \
@@ -60,14 +71,14 @@ void launch_eam_density(const Geo& g, const NbrView& nl, int n,
                         double* rho_out, double* fpd_out, int4* gout, bool ev, double* partials,
                         int lpa, cudaStream_t s) {
   const int nblk = force_blocks(n, lpa);
-  TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
+  TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
     if (ev)
-      k_eam_density<Geo, L, true, V, FP><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_density<Geo, L, true, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, rho_out, fpd_out, gout, partials);
     else
-      k_eam_density<Geo, L, false, V, FP><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_density<Geo, L, false, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, rho_out, fpd_out, gout, nullptr);
-  }));
+  })));
   TDMD_LAUNCH_CHECK();
 }
 
@@ -77,14 +88,14 @@ void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typen
                       const int* types, const FP* fp, F* forces, bool ev, double* partials,
                       int lpa, cudaStream_t s) {
   const int nblk = force_blocks(n, lpa);
-  TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
+  TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
     if (ev)
-      k_eam_force<Geo, L, true, FPG, V, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, true, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, partials);
     else
-      k_eam_force<Geo, L, false, FPG, V, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, false, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
-  }));
+  })));
   TDMD_LAUNCH_CHECK();
 }
 

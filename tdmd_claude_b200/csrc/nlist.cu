@@ -128,6 +128,21 @@ __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __re
 constexpr int kRowThreads = 128;
 constexpr int kStageCap = 1536;  // staged candidate records (24 KiB)
 
+// The reference's decision for one pair (NeighborList::build,
+// neighbor_list.cpp:57-63): delta = r_j - r_i in FP64, minimum image,
+// r^2 = (x*x + y*y) + z*z with round-to-nearest ops, r^2 < rl^2.  Not
+// inlined: it runs for a handful of candidates per rebuild, and as a call
+// it stays out of the filter loop's instruction stream.
+template <class Load>
+__device__ __noinline__ bool exact_within(Load pos, const DevBox& b, int i, int j, double rl2) {
+  const double3 pi = pos(i), pj = pos(j);
+  const double ex = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
+  const double ey = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
+  const double ez = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
+  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+  return r2 < rl2;
+}
+
 template <class Load, bool WRAP>
 __global__ void __launch_bounds__(kRowThreads) k_build_cells(
     Load pos, DevBox b, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
@@ -214,15 +229,7 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
         }
         const float r2f = dx * dx + dy * dy + dz * dz;
         bool pred = j != i && r2f < lo_f;
-        if (j != i && r2f >= lo_f && r2f <= hi_f) {
-          const double3 pi = pos(i), pj = pos(j);
-          const double ex = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
-          const double ey = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
-          const double ez = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
-          const double r2 =
-              __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-          pred = r2 < rl2;
-        }
+        if (j != i && r2f >= lo_f && r2f <= hi_f) pred = exact_within(pos, b, i, j, rl2);
         const unsigned m = __ballot_sync(0xffffffffu, pred);
         if (pred && nbr) {
           const int p = cnt + __popc(m & lt_mask);
