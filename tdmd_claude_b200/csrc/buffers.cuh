@@ -75,6 +75,8 @@ struct CellListDev {
 // the sum.  Multi-block, fixed order.
 void device_exclusive_scan(const int* in, int* out, long long n, int* total, DevArray<int>& tmp,
                            cudaStream_t stream);
+// Kernels one device_exclusive_scan of n items launches (1 or 3).
+int device_scan_launches(long long n);
 
 // Positions are read either as the reference's Vec3D AoS (double[3n]) or as
 // the scheduler's double4 {x, y, z, type} records.

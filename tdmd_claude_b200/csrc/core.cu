@@ -65,6 +65,7 @@ namespace {
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr long long kScanSingleTiles = 16;  // 65536 items
 
 // Block-wide exclusive scan of one int per thread; returns the block total.
 __device__ int block_exclusive_scan(int v, int* smem, int* total) {
@@ -161,6 +162,11 @@ __global__ void k_scan_apply(const int* __restrict__ in, int* __restrict__ out, 
 
 }  // namespace
 
+int device_scan_launches(long long n) {
+  if (n <= 0) return 0;
+  return (n + kScanTile - 1) / kScanTile <= kScanSingleTiles ? 1 : 3;
+}
+
 void device_exclusive_scan(const int* in, int* out, long long n, int* total, DevArray<int>& tmp,
                            cudaStream_t stream) {
   if (n <= 0) {
@@ -168,7 +174,9 @@ void device_exclusive_scan(const int* in, int* out, long long n, int* total, Dev
     return;
   }
   const long long nblocks = (n + kScanTile - 1) / kScanTile;
-  if (nblocks <= 2) {
+  // Up to kScanSingleTiles tiles one block walking the tiles beats three
+  // launches; beyond that, reduce -> scan of block sums -> apply.
+  if (nblocks <= kScanSingleTiles) {
     k_scan_single<<<1, kScanThreads, 0, stream>>>(in, out, n, total);
     TDMD_LAUNCH_CHECK();
     return;

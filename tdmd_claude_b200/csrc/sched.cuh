@@ -128,8 +128,8 @@ class Scheduler {
   void prof_begin(int cat);
   void prof_end(int cat);
   void prof_collect();
-  // bin + scan (1 kernel up to 8192 cells, else 3) + scatter + sort
-  int cell_list_kernels() const { return cl_.ncells > 8192 ? 6 : 4; }
+  // bin + scan + scatter + sort
+  int cell_list_kernels() const { return 3 + device_scan_launches(cl_.ncells); }
   int* ctl_status() const {
     return reinterpret_cast<int*>(reinterpret_cast<char*>(ctl_.data()) +
                                   offsetof(SchedCtl, status));
