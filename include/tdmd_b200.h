@@ -240,6 +240,9 @@ int32_t tdmd_nhc_create(double t_target, double t_period, int32_t chain_length, 
                         int32_t n_dof, tdmd_nhc** out);
 int32_t tdmd_nhc_destroy(tdmd_nhc* nhc);
 int32_t tdmd_nhc_half_step(tdmd_nhc* nhc, double ke_current, double* scale);
+/* NoseHooverChain::set_t_target, device_nose_hoover.cuh:50: changes the
+ * target temperature only (the chain masses are not recomputed). */
+int32_t tdmd_nhc_set_t_target(tdmd_nhc* nhc, double t_target);
 /* state out: eta[M], eta_v[M], eta_m[M]. */
 int32_t tdmd_nhc_state(const tdmd_nhc* nhc, double* eta, double* eta_v, double* eta_m);
 

@@ -1,0 +1,540 @@
+// tdmd_b200.hpp -- header-only C++ layer over the C ABI in tdmd_b200.h that
+// restores the reference's class and function names, namespaces and
+// signatures (tdmd_Claude, src/...), so code written against the reference's
+// GPU path compiles against this library with its includes swapped.
+//
+// Precision follows the reference's build switch (src/core/types.hpp:9-15,
+// 44-61): define TDMD_PRECISION_MIXED for `real = float` and float forces,
+// otherwise (or with TDMD_PRECISION_FP64) everything is double.
+//
+// Errors: every non-zero status becomes a tdmd::Error (std::runtime_error,
+// as src/core/error.hpp:13) carrying the status code; the reference aborts on
+// CUDA failures instead (src/core/device_buffer.cuh:16-24).
+//
+// Needs <cuda_runtime_api.h> for cudaStream_t only.
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include <array>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "tdmd_b200.h"
+
+namespace tdmd {
+
+// --- src/core/types.hpp -----------------------------------------------------
+#if defined(TDMD_PRECISION_MIXED)
+using real = float;
+#else
+using real = double;
+#endif
+using i32 = std::int32_t;
+using i64 = std::int64_t;
+
+template <class T>
+struct Vec3T {
+  T x;
+  T y;
+  T z;
+};
+using Vec3D = Vec3T<double>;
+using Vec3F = Vec3T<float>;
+using Vec3 = Vec3T<real>;
+
+using pos_t = double;
+using vel_t = double;
+using accum_t = double;
+using PositionVec = Vec3D;
+using VelocityVec = Vec3D;
+#if defined(TDMD_PRECISION_MIXED)
+using force_t = float;
+using ForceVec = Vec3F;
+constexpr int32_t kForcePrecision = TDMD_MIXED;
+#else
+using force_t = double;
+using ForceVec = Vec3D;
+constexpr int32_t kForcePrecision = TDMD_FP64;
+#endif
+
+// --- src/core/error.hpp -----------------------------------------------------
+class Error : public std::runtime_error {
+ public:
+  Error(int32_t status, const std::string& what) : std::runtime_error(what), status_(status) {}
+  int32_t status() const noexcept { return status_; }
+
+ private:
+  int32_t status_;
+};
+
+namespace detail {
+inline void check(int32_t rc) {
+  if (rc != TDMD_OK) throw Error(rc, tdmd_last_error());
+}
+inline void* stream_ptr(cudaStream_t s) { return reinterpret_cast<void*>(s); }
+}  // namespace detail
+
+// --- src/core/box.hpp -------------------------------------------------------
+struct Box {
+  Vec3D lo{0, 0, 0};
+  Vec3D hi{0, 0, 0};
+  std::array<bool, 3> periodic{true, true, true};
+
+  Vec3D size() const noexcept { return Vec3D{hi.x - lo.x, hi.y - lo.y, hi.z - lo.z}; }
+
+  tdmd_box to_c() const noexcept {
+    tdmd_box b{};
+    b.lo[0] = lo.x; b.lo[1] = lo.y; b.lo[2] = lo.z;
+    b.hi[0] = hi.x; b.hi[1] = hi.y; b.hi[2] = hi.z;
+    for (int k = 0; k < 3; ++k) b.periodic[k] = periodic[static_cast<size_t>(k)] ? 1 : 0;
+    return b;
+  }
+};
+
+// --- src/potentials -----------------------------------------------------------
+namespace potentials {
+
+// device_morse.cuh:14-20
+struct MorseParams {
+  real d;
+  real alpha;
+  real r0;
+  real rc;
+  real rc_sq;
+
+  tdmd_morse_params to_c() const noexcept {
+    return tdmd_morse_params{d, alpha, r0, rc, rc_sq};
+  }
+};
+
+// device_morse.cuh:37-41: forces stored, *d_energy accumulated.
+inline void compute_morse_gpu(const PositionVec* d_positions, ForceVec* d_forces,
+                              const i32* d_neighbors, const i32* d_offsets, const i32* d_counts,
+                              i32 natoms, const Box& box, const MorseParams& params,
+                              accum_t* d_energy, cudaStream_t stream = 0) {
+  const tdmd_box b = box.to_c();
+  const tdmd_morse_params p = params.to_c();
+  detail::check(tdmd_morse_compute(reinterpret_cast<const double*>(d_positions), d_forces,
+                                   kForcePrecision, d_neighbors, d_offsets, d_counts, natoms, &b,
+                                   &p, d_energy, nullptr, detail::stream_ptr(stream)));
+}
+
+// eam_alloy.hpp:47-93 (tables; the CPU compute_forces stays in the reference).
+class EamAlloy {
+ public:
+  EamAlloy() = default;
+  EamAlloy(const EamAlloy&) = delete;
+  EamAlloy& operator=(const EamAlloy&) = delete;
+  EamAlloy(EamAlloy&& o) noexcept : h_(o.h_) { o.h_ = nullptr; }
+  ~EamAlloy() {
+    if (h_) tdmd_eam_destroy(h_);
+  }
+
+  // eam_alloy.cpp:90-192
+  void read_setfl(const std::string& filename) {
+    tdmd_eam* h = nullptr;
+    detail::check(tdmd_eam_read_setfl(filename.c_str(), &h));
+    if (h_) tdmd_eam_destroy(h_);
+    h_ = h;
+  }
+  real cutoff() const {
+    double c = 0;
+    detail::check(tdmd_eam_info(h_, nullptr, nullptr, nullptr, nullptr, nullptr, &c));
+    return static_cast<real>(c);
+  }
+  i32 ntypes() const {
+    int32_t n = 0;
+    detail::check(tdmd_eam_info(h_, &n, nullptr, nullptr, nullptr, nullptr, nullptr));
+    return n;
+  }
+  const tdmd_eam* handle() const noexcept { return h_; }
+
+ private:
+  tdmd_eam* h_ = nullptr;
+};
+
+// device_eam.cuh:26-50
+class DeviceEam {
+ public:
+  DeviceEam() = default;
+  DeviceEam(const DeviceEam&) = delete;
+  DeviceEam& operator=(const DeviceEam&) = delete;
+  ~DeviceEam() {
+    if (h_) tdmd_device_eam_destroy(h_);
+  }
+
+  void upload_tables(const EamAlloy& eam) {
+    tdmd_device_eam* h = nullptr;
+    detail::check(tdmd_device_eam_create(eam.handle(), &h));
+    if (h_) tdmd_device_eam_destroy(h_);
+    h_ = h;
+    cutoff_ = eam.cutoff();
+  }
+  void compute(const PositionVec* d_positions, ForceVec* d_forces, const i32* d_types,
+               const i32* d_neighbors, const i32* d_offsets, const i32* d_counts, i32 natoms,
+               const Box& box, accum_t* d_energy, cudaStream_t stream = 0) {
+    const tdmd_box b = box.to_c();
+    detail::check(tdmd_device_eam_compute(h_, reinterpret_cast<const double*>(d_positions),
+                                          d_forces, kForcePrecision, d_types, d_neighbors,
+                                          d_offsets, d_counts, natoms, &b, d_energy, nullptr,
+                                          nullptr, nullptr, detail::stream_ptr(stream)));
+  }
+  real cutoff() const noexcept { return cutoff_; }
+
+ private:
+  tdmd_device_eam* h_ = nullptr;
+  real cutoff_ = 0;
+};
+
+}  // namespace potentials
+
+// --- src/domain/device_cell_list.cuh:16-60 -------------------------------------
+namespace domain {
+
+class DeviceCellList {
+ public:
+  DeviceCellList() { detail::check(tdmd_cell_list_create(&h_)); }
+  DeviceCellList(const DeviceCellList&) = delete;
+  DeviceCellList& operator=(const DeviceCellList&) = delete;
+  ~DeviceCellList() { tdmd_cell_list_destroy(h_); }
+
+  void build(const PositionVec* d_positions, i64 natoms, const Box& box, real r_list) {
+    const tdmd_box b = box.to_c();
+    detail::check(tdmd_cell_list_build(h_, reinterpret_cast<const double*>(d_positions), natoms,
+                                       &b, r_list, nullptr));
+    detail::check(tdmd_cell_list_get(h_, &atoms_, &offsets_, &counts_, &atom_cells_, nc_));
+  }
+  i32 ncells_x() const noexcept { return nc_[0]; }
+  i32 ncells_y() const noexcept { return nc_[1]; }
+  i32 ncells_z() const noexcept { return nc_[2]; }
+  i32 ncells_total() const noexcept { return nc_[0] * nc_[1] * nc_[2]; }
+  const i32* d_cell_offsets() const noexcept { return offsets_; }
+  const i32* d_cell_counts() const noexcept { return counts_; }
+  const i32* d_cell_atoms() const noexcept { return atoms_; }
+  const i32* d_atom_cells() const noexcept { return atom_cells_; }
+
+ private:
+  tdmd_cell_list* h_ = nullptr;
+  const int32_t* atoms_ = nullptr;
+  const int32_t* offsets_ = nullptr;
+  const int32_t* counts_ = nullptr;
+  const int32_t* atom_cells_ = nullptr;
+  int32_t nc_[3] = {0, 0, 0};
+};
+
+}  // namespace domain
+
+// --- src/neighbors/device_neighbor_list.cuh:20-65 ------------------------------
+namespace neighbors {
+
+class DeviceNeighborList {
+ public:
+  DeviceNeighborList() { detail::check(tdmd_nlist_create(&h_)); }
+  DeviceNeighborList(const DeviceNeighborList&) = delete;
+  DeviceNeighborList& operator=(const DeviceNeighborList&) = delete;
+  ~DeviceNeighborList() { tdmd_nlist_destroy(h_); }
+
+  void build(const PositionVec* d_positions, i64 natoms, const Box& box, real r_cut, real r_skin,
+             cudaStream_t stream = 0) {
+    const tdmd_box b = box.to_c();
+    detail::check(tdmd_nlist_build(h_, reinterpret_cast<const double*>(d_positions), natoms, &b,
+                                   r_cut, r_skin, detail::stream_ptr(stream)));
+    int64_t total = 0;
+    detail::check(tdmd_nlist_get(h_, &nbrs_, &offsets_, &counts_, &max_neighbors_, &total));
+    r_cut_ = r_cut;
+    r_skin_ = r_skin;
+  }
+  const i32* d_neighbors() const noexcept { return nbrs_; }
+  const i32* d_counts() const noexcept { return counts_; }
+  const i32* d_offsets() const noexcept { return offsets_; }
+  real cutoff() const noexcept { return r_cut_; }
+  real skin() const noexcept { return r_skin_; }
+  i32 max_neighbors() const noexcept { return max_neighbors_; }
+
+ private:
+  tdmd_nlist* h_ = nullptr;
+  const int32_t* nbrs_ = nullptr;
+  const int32_t* offsets_ = nullptr;
+  const int32_t* counts_ = nullptr;
+  int32_t max_neighbors_ = 0;
+  real r_cut_ = 0;
+  real r_skin_ = 0;
+};
+
+}  // namespace neighbors
+
+// --- src/integrator -----------------------------------------------------------
+namespace integrator {
+
+namespace detail_masses {
+// The C ABI takes FP64 device masses.  In the FP64 build `real` is double
+// and the pointer passes through.  In the mixed build (float masses, as the
+// reference's `real`) the entries up to the largest type in d_types are
+// widened into a small per-thread device array first; that costs a read of
+// the types and two small copies per call, which the scheduler path never
+// pays (it keeps its own FP64 masses).
+#if defined(TDMD_PRECISION_MIXED)
+struct Widened {
+  double* d = nullptr;
+  size_t cap = 0;
+  ~Widened() {
+    if (d) cudaFree(d);
+  }
+};
+inline const double* masses(const real* d_masses, const i32* d_types, i32 natoms,
+                            cudaStream_t stream) {
+  thread_local Widened w;
+  void* s = ::tdmd::detail::stream_ptr(stream);
+  std::vector<int32_t> types(static_cast<size_t>(natoms > 0 ? natoms : 0));
+  if (!types.empty())
+    ::tdmd::detail::check(tdmd_copy(types.data(), d_types, sizeof(int32_t) * types.size(), s));
+  int32_t tmax = 0;
+  for (int32_t t : types) tmax = t > tmax ? t : tmax;
+  std::vector<float> hf(static_cast<size_t>(tmax) + 1);
+  ::tdmd::detail::check(tdmd_copy(hf.data(), d_masses, sizeof(float) * hf.size(), s));
+  std::vector<double> hd(hf.begin(), hf.end());
+  if (w.cap < hd.size()) {
+    if (w.d) cudaFree(w.d);
+    w.d = nullptr;
+    w.cap = 0;
+    if (cudaMalloc(reinterpret_cast<void**>(&w.d), sizeof(double) * hd.size()) != cudaSuccess)
+      throw Error(TDMD_ERR_OUT_OF_MEMORY, "mass buffer allocation failed");
+    w.cap = hd.size();
+  }
+  ::tdmd::detail::check(tdmd_copy(w.d, hd.data(), sizeof(double) * hd.size(), s));
+  return w.d;
+}
+#else
+inline const double* masses(const real* d_masses, const i32*, i32, cudaStream_t) {
+  return d_masses;
+}
+#endif
+}  // namespace detail_masses
+
+// device_velocity_verlet.cuh:13-59
+inline void device_half_kick(VelocityVec* d_velocities, const ForceVec* d_forces,
+                             const i32* d_types, const real* d_masses, i32 natoms, real dt,
+                             cudaStream_t stream = 0) {
+  ::tdmd::detail::check(tdmd_vv_half_kick(
+      reinterpret_cast<double*>(d_velocities), d_forces, kForcePrecision, d_types,
+      detail_masses::masses(d_masses, d_types, natoms, stream), natoms, dt, ::tdmd::detail::stream_ptr(stream)));
+}
+inline void device_drift(PositionVec* d_positions, const VelocityVec* d_velocities, i32 natoms,
+                         real dt, const Box& box, cudaStream_t stream = 0) {
+  const tdmd_box b = box.to_c();
+  ::tdmd::detail::check(tdmd_vv_drift(reinterpret_cast<double*>(d_positions),
+                                      reinterpret_cast<const double*>(d_velocities), natoms, dt,
+                                      &b, ::tdmd::detail::stream_ptr(stream)));
+}
+inline void device_fused_half_kick_drift(VelocityVec* d_velocities, PositionVec* d_positions,
+                                         const ForceVec* d_forces, const i32* d_types,
+                                         const real* d_masses, i32 natoms, real dt,
+                                         const Box& box, cudaStream_t stream = 0) {
+  const tdmd_box b = box.to_c();
+  ::tdmd::detail::check(tdmd_vv_fused_kick_drift(
+      reinterpret_cast<double*>(d_velocities), reinterpret_cast<double*>(d_positions), d_forces,
+      kForcePrecision, d_types, detail_masses::masses(d_masses, d_types, natoms, stream), natoms, dt, &b, 0,
+      ::tdmd::detail::stream_ptr(stream)));
+}
+inline void device_fused_full_kick_drift(VelocityVec* d_velocities, PositionVec* d_positions,
+                                         const ForceVec* d_forces, const i32* d_types,
+                                         const real* d_masses, i32 natoms, real dt,
+                                         const Box& box, cudaStream_t stream = 0) {
+  const tdmd_box b = box.to_c();
+  ::tdmd::detail::check(tdmd_vv_fused_kick_drift(
+      reinterpret_cast<double*>(d_velocities), reinterpret_cast<double*>(d_positions), d_forces,
+      kForcePrecision, d_types, detail_masses::masses(d_masses, d_types, natoms, stream), natoms, dt, &b, 1,
+      ::tdmd::detail::stream_ptr(stream)));
+}
+inline void device_zero_forces(ForceVec* d_forces, i32 natoms, cudaStream_t stream = 0) {
+  ::tdmd::detail::check(
+      tdmd_vv_zero_forces(d_forces, kForcePrecision, natoms, ::tdmd::detail::stream_ptr(stream)));
+}
+
+// device_nose_hoover.cuh:26-88
+struct NHCConfig {
+  real t_target{300.0};
+  real t_period{0.1};
+  i32 chain_length{3};
+};
+
+class NoseHooverChain {
+ public:
+  NoseHooverChain(const NHCConfig& cfg, real dt, i32 n_dof) : cfg_(cfg) {
+    ::tdmd::detail::check(
+        tdmd_nhc_create(cfg.t_target, cfg.t_period, cfg.chain_length, dt, n_dof, &h_));
+  }
+  NoseHooverChain(const NoseHooverChain&) = delete;
+  NoseHooverChain& operator=(const NoseHooverChain&) = delete;
+  ~NoseHooverChain() { tdmd_nhc_destroy(h_); }
+
+  real half_step(accum_t ke_current) {
+    double scale = 1.0;
+    ::tdmd::detail::check(tdmd_nhc_half_step(h_, ke_current, &scale));
+    return static_cast<real>(scale);
+  }
+  real t_target() const noexcept { return cfg_.t_target; }
+  void set_t_target(real t) {
+    ::tdmd::detail::check(tdmd_nhc_set_t_target(h_, t));
+    cfg_.t_target = t;
+  }
+
+ private:
+  NHCConfig cfg_;
+  tdmd_nhc* h_ = nullptr;
+};
+
+inline accum_t device_compute_ke(const VelocityVec* d_velocities, const i32* d_types,
+                                 const real* d_masses, i32 natoms) {
+  double ke = 0;
+  ::tdmd::detail::check(tdmd_reduce_ke(reinterpret_cast<const double*>(d_velocities), d_types,
+                                       detail_masses::masses(d_masses, d_types, natoms, 0), natoms, &ke,
+                                       nullptr));
+  return ke;
+}
+inline void device_scale_velocities(VelocityVec* d_velocities, i32 natoms, real factor) {
+  ::tdmd::detail::check(
+      tdmd_scale_velocities(reinterpret_cast<double*>(d_velocities), natoms, factor, nullptr));
+}
+// The zone variant scales atoms [first_atom, first_atom + atom_count).
+inline void device_scale_velocities_zone(VelocityVec* d_velocities, i32 first_atom,
+                                         i32 atom_count, real factor,
+                                         cudaStream_t stream = nullptr) {
+  ::tdmd::detail::check(tdmd_scale_velocities(reinterpret_cast<double*>(d_velocities + first_atom),
+                                              atom_count, factor,
+                                              ::tdmd::detail::stream_ptr(stream)));
+}
+inline accum_t device_compute_vmax(const VelocityVec* d_velocities, i32 natoms) {
+  double v = 0;
+  ::tdmd::detail::check(
+      tdmd_reduce_vmax(reinterpret_cast<const double*>(d_velocities), natoms, &v, nullptr));
+  return v;
+}
+
+}  // namespace integrator
+
+// --- src/scheduler/fast_pipeline_scheduler.cuh:36-192 --------------------------
+namespace scheduler {
+
+enum class PotentialKind {
+  Morse,
+  Eam,
+};
+
+// The reference's three fields first (so FastPipelineConfig{dt, skin, R}
+// still works), then this library's additions with their defaults.
+struct FastPipelineConfig {
+  real dt{real{0.001}};
+  real r_skin{real{1.0}};
+  i32 rebuild_every{10};
+  bool use_graphs{true};
+  i32 lanes_per_atom{0};
+  real t_target{0};
+  real t_period{real{0.1}};
+  i32 nhc_length{3};
+  bool adaptive_dt{false};
+  real dt_min{real{0.0001}};
+  real dt_max{real{0.002}};
+  real c2{real{0.05}};
+  i32 energy_every{0};
+  i32 energy_log_capacity{0};
+
+  tdmd_fast_pipeline_config to_c() const {
+    tdmd_fast_pipeline_config c;
+    tdmd_fast_pipeline_config_default(&c);
+    c.dt = dt;
+    c.r_skin = r_skin;
+    c.rebuild_every = rebuild_every;
+    c.precision = kForcePrecision;
+    c.use_graphs = use_graphs ? 1 : 0;
+    c.lanes_per_atom = lanes_per_atom;
+    c.t_target = t_target;
+    c.t_period = t_period;
+    c.nhc_length = nhc_length;
+    c.adaptive_dt = adaptive_dt ? 1 : 0;
+    c.dt_min = dt_min;
+    c.dt_max = dt_max;
+    c.c2 = c2;
+    c.energy_every = energy_every;
+    c.energy_log_capacity = energy_log_capacity;
+    return c;
+  }
+};
+
+struct FastPipelineStats {
+  i64 ticks{0};
+  i64 kernel_launches{0};
+  i64 rebuilds{0};
+};
+
+class FastPipelineScheduler {
+ public:
+  FastPipelineScheduler(const Box& box, i32 natoms, const potentials::MorseParams& params,
+                        const FastPipelineConfig& cfg) {
+    const tdmd_box b = box.to_c();
+    const tdmd_morse_params p = params.to_c();
+    const tdmd_fast_pipeline_config c = cfg.to_c();
+    ::tdmd::detail::check(tdmd_sched_create_morse(&b, natoms, &p, &c, &h_));
+    refresh();
+  }
+  FastPipelineScheduler(const Box& box, i32 natoms, const potentials::EamAlloy& eam,
+                        const FastPipelineConfig& cfg) {
+    const tdmd_box b = box.to_c();
+    const tdmd_fast_pipeline_config c = cfg.to_c();
+    ::tdmd::detail::check(tdmd_sched_create_eam(&b, natoms, eam.handle(), &c, &h_));
+    refresh();
+  }
+  ~FastPipelineScheduler() { tdmd_sched_destroy(h_); }
+  FastPipelineScheduler(const FastPipelineScheduler&) = delete;
+  FastPipelineScheduler& operator=(const FastPipelineScheduler&) = delete;
+
+  void upload(const PositionVec* positions, const VelocityVec* velocities, const ForceVec* forces,
+              const i32* types, const i32* ids, const real* masses, i32 n_types) {
+    std::vector<double> m(masses, masses + n_types);
+    ::tdmd::detail::check(tdmd_sched_upload(h_, reinterpret_cast<const double*>(positions),
+                                            reinterpret_cast<const double*>(velocities), forces,
+                                            types, ids, m.data(), n_types));
+    refresh();
+  }
+  void run_until(i32 target_step) {
+    ::tdmd::detail::check(tdmd_sched_run_until(h_, target_step));
+    refresh();
+  }
+  void download(PositionVec* positions, VelocityVec* velocities, ForceVec* forces, i32* types,
+                i32* ids, i32 natoms) const {
+    ::tdmd::detail::check(tdmd_sched_download(h_, reinterpret_cast<double*>(positions),
+                                              reinterpret_cast<double*>(velocities), forces,
+                                              types, ids, natoms));
+  }
+  const FastPipelineStats& stats() const noexcept { return stats_; }
+  i32 current_step() const noexcept { return step_; }
+  PotentialKind potential_kind() const noexcept { return kind_; }
+  real interaction_cutoff() const noexcept { return cutoff_; }
+  tdmd_sched* handle() const noexcept { return h_; }
+
+ private:
+  void refresh() {
+    tdmd_fast_pipeline_stats s{};
+    ::tdmd::detail::check(tdmd_sched_stats(h_, &s));
+    stats_ = FastPipelineStats{s.ticks, s.kernel_launches, s.rebuilds};
+    ::tdmd::detail::check(tdmd_sched_current_step(h_, &step_));
+    int32_t k = 0;
+    ::tdmd::detail::check(tdmd_sched_potential_kind(h_, &k));
+    kind_ = k == TDMD_POT_EAM ? PotentialKind::Eam : PotentialKind::Morse;
+    double c = 0;
+    ::tdmd::detail::check(tdmd_sched_interaction_cutoff(h_, &c));
+    cutoff_ = static_cast<real>(c);
+  }
+
+  tdmd_sched* h_ = nullptr;
+  FastPipelineStats stats_{};
+  i32 step_ = 0;
+  PotentialKind kind_ = PotentialKind::Morse;
+  real cutoff_ = 0;
+};
+
+}  // namespace scheduler
+}  // namespace tdmd

@@ -9,7 +9,7 @@
  * tdmd_Claude source tree).  Build: see oracle/Makefile
  * (gcc -O2 -ffp-contract=off, so no FMA contraction changes rounding).
  *
- * Parity pins (checked by tests/test_oracle_*.py):
+ * Parity pins (checked by tests/test_oracle.py):
  *   - two-atom analytic Morse and the run-0 LAMMPS force dumps of the
  *     reference's VerifyLab cases (golden fixtures under tests/golden/);
  *   - the reference CPU path itself, compiled from its sources into

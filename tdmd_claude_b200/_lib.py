@@ -118,6 +118,7 @@ SIGNATURES = {
     "tdmd_scale_velocities": [_p, _i32, _f64, _p],
     "tdmd_nhc_create": [_f64, _f64, _i32, _f64, _i32, _pp],
     "tdmd_nhc_destroy": [_p],
+    "tdmd_nhc_set_t_target": [_p, _f64],
     "tdmd_nhc_half_step": [_p, _f64, _pf64],
     "tdmd_nhc_state": [_p, _p, _p, _p],
     "tdmd_sched_create_morse": [C.POINTER(Box), _i32, C.POINTER(MorseParams),

@@ -346,6 +346,13 @@ int32_t tdmd_nhc_half_step(tdmd_nhc* h, double ke_current, double* scale) {
   });
 }
 
+int32_t tdmd_nhc_set_t_target(tdmd_nhc* h, double t_target) {
+  return guarded([&] {
+    TDMD_REQUIRE(h, "null handle");
+    h->t_target = t_target;  // chain masses keep their construction-time value
+  });
+}
+
 int32_t tdmd_nhc_state(const tdmd_nhc* h, double* eta, double* eta_v, double* eta_m) {
   return guarded([&] {
     TDMD_REQUIRE(h, "null handle");
