@@ -188,6 +188,26 @@ int32_t tdmd_morse_compute(const double* d_positions, void* d_forces, int32_t pr
                            const tdmd_morse_params* params, double* d_energy, double* d_virial,
                            void* stream);
 
+/* No counterpart in the reference.  Same arguments and results as
+ * tdmd_morse_compute, but it allocates no device memory: the per-block
+ * energy/virial partials live in a fixed 1 MiB scratch array compiled into
+ * the library, one per device.  For callers that size all device memory up
+ * front and must not let a force call draw on the CUDA memory pool.
+ *  - natoms above TDMD_MORSE_NOALLOC_MAX_ATOMS is rejected
+ *    (TDMD_ERR_INVALID_ARGUMENT) before any launch;
+ *  - d_energy / d_virial are added to (zero them for this call's totals);
+ *    the scratch itself needs no zeroing;
+ *  - two calls in flight on one device at the same time share the scratch
+ *    and race: order them on one stream;
+ *  - the first call on each device (made with that device current) looks
+ *    up the scratch address; make it before any stream capture begins. */
+#define TDMD_MORSE_NOALLOC_MAX_ATOMS 524288
+int32_t tdmd_morse_compute_noalloc(const double* d_positions, void* d_forces, int32_t precision,
+                                   const int32_t* d_neighbors, const int32_t* d_offsets,
+                                   const int32_t* d_counts, int32_t natoms, const tdmd_box* box,
+                                   const tdmd_morse_params* params, double* d_energy,
+                                   double* d_virial, void* stream);
+
 /* DeviceEam, src/potentials/device_eam.cuh:26-75: device copy of the
  * tables plus rho/fp scratch. */
 typedef struct tdmd_device_eam tdmd_device_eam;
