@@ -64,18 +64,54 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """SM clock and throttle reasons sampled during the timed region: every
+    10 ms through NVML, or every 200 ms through nvidia-smi where NVML is
+    unavailable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []      # (sm_mhz, max_mhz, reasons bitmask)
+        self.stop_flag = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll_nvml(self):
+        nv, h = self.nvml
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                                     int(get_reasons(h))))
+            except Exception:
+                pass
+            self.stop_flag.wait(0.01)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self.t = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -91,6 +127,20 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_flag.set()
+            self.t.join(timeout=2)
+            # NVML reason bits: sw power cap 0x4, hw slowdown 0x8,
+            # sw thermal 0x20, hw thermal 0x40.
+            bits = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                    "hw_thermal_slowdown": 0x40}
+            if not self.samples:
+                return None
+            reasons = sorted({nm for nm, b in bits.items()
+                              for _, _, r in self.samples if r & b})
+            return {"sm_mhz": float(np.median([x[0] for x in self.samples])),
+                    "sm_max_mhz": float(max(x[1] for x in self.samples)), "reasons": reasons,
+                    "samples": len(self.samples), "source": "nvml, 10 ms"}
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -100,7 +150,6 @@ class ClockSampler:
             self.proc.kill()
         self.t.join(timeout=2)
         sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
@@ -110,13 +159,13 @@ class ClockSampler:
                 smax = max(smax, float(p[2]))
             except ValueError:
                 continue
-            for nm, v in zip(names, p[5:9]):
+            for nm, v in zip(self.NAMES, p[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ---------------------------------------------------------------------------
@@ -251,6 +300,22 @@ def cpu_baseline_sample(sysm, t, nsteps):
     return sec, kind
 
 
+def nve_drift(sysm, eam, precision, lanes, nsteps, every=100):
+    """Total-energy drift of an NVE run from the device energy log:
+    least-squares slope of E_total/N against time (eV/atom/ns) and the
+    largest |E_total - E_0|/N."""
+    s = make_sched(sysm, eam, precision, lanes_per_atom=lanes, energy_every=every,
+                   energy_log_capacity=nsteps // every + 1)
+    s.run_until(nsteps)
+    log = s.energy_log()
+    s.close()
+    t_ns = log[:, 0] * DT * 1e-3
+    e = (log[:, 1] + log[:, 2]) / sysm.n
+    slope = float(np.polyfit(t_ns, e, 1)[0]) if len(e) > 1 else None
+    return {"steps": nsteps, "ns": nsteps * DT * 1e-3, "slope_ev_per_atom_per_ns": slope,
+            "max_abs_dev_ev_per_atom": float(np.abs(e - e[0]).max()) if len(e) else None}
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
     if rank != 0:
@@ -287,6 +352,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the mixed timed windows (for profiler captures); no JSON line")
+    ap.add_argument("--lanes", type=int, default=2,
+                    help="lanes per atom for --kernels-only (no autotune there)")
+    ap.add_argument("--drift-steps", type=int, default=50000,
+                    help="NVE steps for the energy-drift figure (0 = skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
@@ -306,8 +375,16 @@ def main():
 
     sysm, t = workload(seed=4321 + rank)
     eam = make_eam(t)
-    K = mean_neighbors(sysm, t.cutoff)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    if args.kernels_only:
+        s32 = make_sched(sysm, eam, "mixed", lanes_per_atom=args.lanes)
+        s32.run_until(0)
+        timed_windows(s32, args.steps, args.warmup, flush, torch, dist)
+        s32.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    K = mean_neighbors(sysm, t.cutoff)
 
     # Force accuracy of the mixed path vs FP64 on the same state.
     s64 = make_sched(sysm, eam, "fp64")
@@ -319,12 +396,6 @@ def main():
     f64 = s64.download().forces
     f32 = s32.download().forces.astype(np.float64)
     rel_err = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
-
-    if args.kernels_only:
-        timed_windows(s32, args.steps, args.warmup, flush, torch, dist)
-        for s in (s32, s64):
-            s.close()
-        return
 
     # Headline: mixed.
     clocks = ClockSampler(local)
@@ -348,6 +419,19 @@ def main():
     timed_windows(s64, max(5, args.steps // 3), 1, flush, torch, None)
     kt64 = s64.kernel_times()
     s64.set_profiling(False)
+
+    # NVT (Nose-Hoover chain 3, tau 0.1 ps, 300 K), same protocol.
+    snvt = make_sched(sysm, eam, "mixed", lanes_per_atom=lanes32, t_target=300.0,
+                      t_period=0.1, nhc_length=3)
+    snvt.run_until(0)
+    ms_nvt, _, _, _ = timed_windows(snvt, args.steps, args.warmup, flush, torch, dist)
+    snvt.close()
+    value_nvt = units / (ms_nvt * 1e-3)
+
+    drift = None
+    if args.drift_steps > 0:
+        drift = {"mixed": nve_drift(sysm, eam, "mixed", lanes32, args.drift_steps),
+                 "fp64": nve_drift(sysm, eam, "fp64", lanes64, args.drift_steps)}
 
     hbm, peak_kind = measured_peaks()
     force_bytes = sysm.n * (48 + 24 * K)          # gather model, mixed force pass
@@ -392,6 +476,9 @@ def main():
                 "fp64": {"value": value64, "ms_per_step": ms_fp64 / args.steps},
                 "mixed_over_fp64": value / value64,
                 "force_rel_rms_err_mixed_vs_fp64": rel_err,
+                "nvt_mixed": {"value": value_nvt, "ms_per_step": ms_nvt / args.steps,
+                              "thermostat": "Nose-Hoover chain 3, tau 0.1 ps, 300 K"},
+                "nve_drift": drift,
                 "wall_s_timed_region": wall_mixed,
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
