@@ -316,6 +316,42 @@ def nve_drift(sysm, eam, precision, lanes, nsteps, every=100):
             "max_abs_dev_ev_per_atom": float(np.abs(e - e[0]).max()) if len(e) else None}
 
 
+def batch_bench(steps, warmup, flush, torch, precision="mixed"):
+    """Batched replicas: 512 independent Cu FCC Morse systems (n^3 cells,
+    n uniform 4..16, 100-1500 K), NVE, K = 10 steps per graph-replayed
+    window; aggregate atom-steps/s and per-replica energy drift."""
+    from tdmd_claude_b200 import Box, MorseParams, ReplicaBatch, make_config
+    from tdmd_claude_b200 import workloads as W
+    systems = W.replica_set(512)
+    b = ReplicaBatch([Box.make(s.lo, s.hi) for s in systems], [s.n for s in systems],
+                     MorseParams.make(*W.MORSE_CU),
+                     make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW, precision=precision,
+                                 energy_every=WINDOW,
+                                 energy_log_capacity=steps + warmup + 8))
+    b.upload(np.concatenate([s.positions for s in systems]),
+             np.concatenate([s.velocities for s in systems]),
+             np.concatenate([s.types for s in systems]), systems[0].masses)
+    b.run_until(0)
+    ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, None)
+    steps_log, pk = b.energy_log()
+    info = b.info()
+    natoms = np.array([s.n for s in systems], np.float64)
+    etot = (pk[:, :, 0] + pk[:, :, 1]) / natoms          # eV/atom per window
+    t_ns = steps_log * DT * 1e-3
+    slopes = np.polyfit(t_ns, etot, 1)[0] if len(t_ns) > 1 else np.zeros(len(systems))
+    b.close()
+    value = info["natoms"] * WINDOW * steps / (ms * 1e-3)
+    return {"value": value, "unit": "atom-steps/s", "ms_per_window": ms / steps,
+            "replicas": len(systems), "atoms": info["natoms"], "precision": precision,
+            "lanes_per_atom": info["lanes_per_atom"], "kernel_launches_timed": launches,
+            "drift_ev_per_atom_per_ns": {"median_abs": float(np.median(np.abs(slopes))),
+                                         "max_abs": float(np.max(np.abs(slopes))),
+                                         "over_ps": float(t_ns[-1] - t_ns[0]) * 1e3
+                                         if len(t_ns) > 1 else 0.0},
+            "workload": "512 Cu FCC Morse replicas, n^3 cells n~U{4..16}, T~U(100,1500) K, "
+                        "rc 6.0 skin 0.3, K=10 steps per graph"}
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
     if rank != 0:
@@ -354,6 +390,8 @@ def main():
                     help="only the mixed timed windows (for profiler captures); no JSON line")
     ap.add_argument("--lanes", type=int, default=2,
                     help="lanes per atom for --kernels-only (no autotune there)")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-replica (512 Morse systems) figure")
     ap.add_argument("--drift-steps", type=int, default=50000,
                     help="NVE steps for the energy-drift figure (0 = skip)")
     args = ap.parse_args()
@@ -433,6 +471,11 @@ def main():
         drift = {"mixed": nve_drift(sysm, eam, "mixed", lanes32, args.drift_steps),
                  "fp64": nve_drift(sysm, eam, "fp64", lanes64, args.drift_steps)}
 
+    batch = None
+    if not args.no_batch:
+        batch = {"mixed": batch_bench(args.steps, args.warmup, flush, torch, "mixed"),
+                 "fp64": batch_bench(args.steps, args.warmup, flush, torch, "fp64")}
+
     hbm, peak_kind = measured_peaks()
     force_bytes = sysm.n * (48 + 24 * K)          # gather model, mixed force pass
     dens_bytes = sysm.n * (40 + 20 * K)
@@ -479,6 +522,7 @@ def main():
                 "nvt_mixed": {"value": value_nvt, "ms_per_step": ms_nvt / args.steps,
                               "thermostat": "Nose-Hoover chain 3, tau 0.1 ps, 300 K"},
                 "nve_drift": drift,
+                "batched_replicas": batch,
                 "wall_s_timed_region": wall_mixed,
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

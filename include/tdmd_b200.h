@@ -328,6 +328,54 @@ int32_t tdmd_sched_last_window_ms(const tdmd_sched* s, double* ms);
 /* The stream the scheduler enqueues on (a cudaStream_t). */
 int32_t tdmd_sched_stream(const tdmd_sched* s, void** stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batched replicas (no reference counterpart: the reference runs one       */
+/* system per FastPipelineScheduler and only plans multi-step fusion,        */
+/* docs gpu-strategy.md:67-82).  Many independent Morse systems of uneven   */
+/* sizes advance together: every phase is one launch over all replicas and  */
+/* each run_until window is replayed as one CUDA graph.  Each replica       */
+/* follows FastPipelineScheduler's NVE semantics (same step order, rebuild  */
+/* every cfg.rebuild_every steps, velocities at integer time after          */
+/* run_until); with equal lanes_per_atom its trajectory is bit-identical to */
+/* a single scheduler's.  NVT and adaptive dt are rejected                  */
+/* (TDMD_ERR_UNSUPPORTED).                                                  */
+/* ------------------------------------------------------------------------ */
+typedef struct tdmd_batch tdmd_batch;
+/* boxes[nreplicas], natoms[nreplicas]; every periodic edge must exceed
+ * 2 (rc + r_skin). */
+int32_t tdmd_batch_create_morse(int32_t nreplicas, const tdmd_box* boxes, const int32_t* natoms,
+                                const tdmd_morse_params* params,
+                                const tdmd_fast_pipeline_config* cfg, tdmd_batch** out);
+int32_t tdmd_batch_destroy(tdmd_batch* b);
+/* Arrays hold all replicas back to back in replica order (positions and
+ * velocities double[3*total], types int32[total]); masses[n_types] are
+ * shared by all replicas.  Resets the step counter and the energy log. */
+int32_t tdmd_batch_upload(tdmd_batch* b, const double* positions, const double* velocities,
+                          const int32_t* types, const double* masses, int32_t n_types);
+int32_t tdmd_batch_run_until(tdmd_batch* b, int32_t target_step);
+/* Any pointer may be NULL; forces are float (mixed) or double (FP64). */
+int32_t tdmd_batch_download(const tdmd_batch* b, double* positions, double* velocities,
+                            void* forces);
+/* Potential and kinetic energy per replica (double[nreplicas] each). */
+int32_t tdmd_batch_energies(tdmd_batch* b, double* pe, double* ke);
+/* Energy log: with cfg.energy_every > 0, every run_until window that ends
+ * on a multiple of energy_every appends {step} and {pe, ke} per replica
+ * (up to cfg.energy_log_capacity windows, default 1024).  Copies up to
+ * `cap` windows: steps[cap], pe_ke[cap][nreplicas][2]; *count = windows
+ * logged. */
+int32_t tdmd_batch_energy_log(const tdmd_batch* b, double* steps, double* pe_ke, int32_t cap,
+                              int32_t* count);
+int32_t tdmd_batch_stats(const tdmd_batch* b, tdmd_fast_pipeline_stats* out);
+int32_t tdmd_batch_info(const tdmd_batch* b, int32_t* nreplicas, int64_t* natoms_total,
+                        int32_t* lanes_per_atom, int32_t* current_step);
+/* Times the batched force pass for 1..32 lanes per atom and keeps the
+ * fastest (runs by itself on the first run_until when cfg.lanes_per_atom
+ * is 0 and the batch has >= 2048 atoms). */
+int32_t tdmd_batch_autotune(tdmd_batch* b, int32_t* chosen_lanes, double* ms6);
+/* Device time of the last run_until window (events on the batch's stream). */
+int32_t tdmd_batch_last_window_ms(const tdmd_batch* b, double* ms);
+int32_t tdmd_batch_stream(const tdmd_batch* b, void** stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -7,7 +7,8 @@ in include/tdmd_b200.h.  This package is the Python face of that ABI (see
 api.py); the C++ face is include/tdmd_b200.hpp.
 """
 from .api import (DeviceCellList, DeviceEam, DeviceNeighborList, EamAlloy,  # noqa: F401
-                  FastPipelineScheduler, NoseHooverChain, compute_morse_gpu, device_compute_ke,
+                  FastPipelineScheduler, NoseHooverChain, ReplicaBatch, compute_morse_gpu,
+                  device_compute_ke,
                   device_compute_vmax, device_drift, device_fused_full_kick_drift,
                   device_fused_half_kick_drift, device_half_kick, device_scale_velocities,
                   device_zero_forces, make_config)
@@ -16,7 +17,7 @@ from ._lib import (TDMD_FP64, TDMD_MIXED, TDMD_POT_EAM, TDMD_POT_MORSE, Box,  # 
 
 __all__ = [
     "Box", "MorseParams", "FastPipelineConfig", "FastPipelineStats", "TdmdError", "EamAlloy",
-    "FastPipelineScheduler", "DeviceNeighborList", "DeviceCellList", "DeviceEam",
+    "FastPipelineScheduler", "ReplicaBatch", "DeviceNeighborList", "DeviceCellList", "DeviceEam",
     "compute_morse_gpu", "device_half_kick", "device_drift", "device_fused_half_kick_drift",
     "device_fused_full_kick_drift", "device_zero_forces", "device_compute_ke",
     "device_compute_vmax", "device_scale_velocities", "NoseHooverChain", "make_config",

@@ -139,6 +139,19 @@ SIGNATURES = {
     "tdmd_sched_thermostat_state": [_p, _pf64, _p, _p],
     "tdmd_sched_device_state": [_p, _pp, _pp, _pp],
     "tdmd_sched_stream": [_p, _pp],
+    "tdmd_batch_create_morse": [_i32, C.POINTER(Box), _p, C.POINTER(MorseParams),
+                                C.POINTER(FastPipelineConfig), _pp],
+    "tdmd_batch_destroy": [_p],
+    "tdmd_batch_upload": [_p, _p, _p, _p, _p, _i32],
+    "tdmd_batch_run_until": [_p, _i32],
+    "tdmd_batch_download": [_p, _p, _p, _p],
+    "tdmd_batch_energies": [_p, _p, _p],
+    "tdmd_batch_energy_log": [_p, _p, _p, _i32, _pi32],
+    "tdmd_batch_stats": [_p, C.POINTER(FastPipelineStats)],
+    "tdmd_batch_info": [_p, _pi32, C.POINTER(C.c_int64), _pi32, _pi32],
+    "tdmd_batch_autotune": [_p, _pi32, _p],
+    "tdmd_batch_last_window_ms": [_p, _pf64],
+    "tdmd_batch_stream": [_p, _pp],
     "tdmd_sched_set_profiling": [_p, _i32],
     "tdmd_sched_autotune": [_p, _pi32, _p],
     "tdmd_sched_last_window_ms": [_p, _pf64],

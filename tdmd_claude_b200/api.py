@@ -300,6 +300,111 @@ class FastPipelineScheduler:
 
 
 # ---------------------------------------------------------------------------
+# Batched replicas (no reference counterpart; see tdmd_batch_* in the header)
+# ---------------------------------------------------------------------------
+class ReplicaBatch:
+    """Many independent Morse systems advanced together (NVE).
+
+    boxes: list of Box, natoms: list of int.  Arrays passed to upload hold
+    all replicas back to back in replica order."""
+
+    def __init__(self, boxes, natoms, params: MorseParams, cfg: FastPipelineConfig | None = None):
+        self.nrep = len(boxes)
+        self.natoms = np.ascontiguousarray(natoms, dtype=np.int32)
+        assert self.natoms.size == self.nrep
+        self.total = int(self.natoms.sum())
+        self.offsets = np.concatenate([[0], np.cumsum(self.natoms)]).astype(np.int64)
+        self.cfg = cfg if cfg is not None else make_config()
+        self.mixed = self.cfg.precision == TDMD_MIXED
+        barr = (Box * self.nrep)(*boxes)
+        h = C.c_void_p()
+        call("tdmd_batch_create_morse", self.nrep, barr, _ptr(self.natoms), C.byref(params),
+             C.byref(self.cfg), C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            try:
+                lib().tdmd_batch_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+    def upload(self, positions, velocities, types, masses):
+        n = self.total
+        pos = _f64(positions).reshape(n, 3)
+        vel = _f64(velocities).reshape(n, 3)
+        typ = _i32(types)
+        m = _f64(masses)
+        call("tdmd_batch_upload", self._h, _ptr(pos), _ptr(vel), _ptr(typ), _ptr(m), m.size)
+
+    def run_until(self, target_step: int):
+        call("tdmd_batch_run_until", self._h, int(target_step))
+
+    def download(self):
+        n = self.total
+        pos = np.zeros((n, 3), np.float64)
+        vel = np.zeros((n, 3), np.float64)
+        frc = np.zeros((n, 3), np.float32 if self.mixed else np.float64)
+        call("tdmd_batch_download", self._h, _ptr(pos), _ptr(vel), _ptr(frc))
+        return pos, vel, frc
+
+    def replica(self, arr, r):
+        return arr[self.offsets[r]:self.offsets[r + 1]]
+
+    def energies(self):
+        pe = np.zeros(self.nrep, np.float64)
+        ke = np.zeros(self.nrep, np.float64)
+        call("tdmd_batch_energies", self._h, _ptr(pe), _ptr(ke))
+        return pe, ke
+
+    def energy_log(self):
+        """(steps[w], pe_ke[w, nrep, 2]) of the logged windows."""
+        cnt = C.c_int32()
+        call("tdmd_batch_energy_log", self._h, None, None, 0, C.byref(cnt))
+        w = cnt.value
+        steps = np.zeros(max(w, 1), np.float64)
+        pk = np.zeros((max(w, 1), self.nrep, 2), np.float64)
+        call("tdmd_batch_energy_log", self._h, _ptr(steps), _ptr(pk), w, C.byref(cnt))
+        return steps[:w], pk[:w]
+
+    def stats(self) -> FastPipelineStats:
+        s = FastPipelineStats()
+        call("tdmd_batch_stats", self._h, C.byref(s))
+        return s
+
+    def current_step(self) -> int:
+        return self.info()["step"]
+
+    def info(self):
+        nr, lanes, step = C.c_int32(), C.c_int32(), C.c_int32()
+        tot = C.c_int64()
+        call("tdmd_batch_info", self._h, C.byref(nr), C.byref(tot), C.byref(lanes),
+             C.byref(step))
+        return {"nreplicas": nr.value, "natoms": tot.value, "lanes_per_atom": lanes.value,
+                "step": step.value}
+
+    def autotune(self):
+        c = C.c_int32()
+        ms = np.zeros(6, np.float64)
+        call("tdmd_batch_autotune", self._h, C.byref(c), _ptr(ms))
+        return c.value, {1 << k: float(ms[k]) for k in range(6)}
+
+    def last_window_ms(self) -> float:
+        v = C.c_double()
+        call("tdmd_batch_last_window_ms", self._h, C.byref(v))
+        return v.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        call("tdmd_batch_stream", self._h, C.byref(s))
+        return s.value or 0
+
+
+# ---------------------------------------------------------------------------
 # Free functions on device arrays (torch CUDA tensors).
 # ---------------------------------------------------------------------------
 def _dev_to_numpy(ptr: int, count: int, dtype) -> np.ndarray:

@@ -100,7 +100,7 @@ __device__ __forceinline__ void nbr_batch(const NbrView& nl, long long row, int 
 // --------------------------------------------------------------------------
 // Geometry policies.  own(i) loads atom i once; pair(own, j, p) fills p with
 // r_i - r_j after the minimum image and r^2 in the policy's arithmetic type
-// T; radius(p, r, rinv, rd) gives |r_i - r_j| and its inverse as T and as an
+// T; radius(own, p, r, rinv, rd) gives |r_i - r_j| and its inverse as T and as an
 // FP64 value rd that the spline offset and the Morse exponent use.  In
 // FP32, r itself carries an absolute error of ~ulp(r) = 2.4e-7 A at
 // r ~ 2.5 A, which moves the spline argument and, through the large pair
@@ -150,7 +150,8 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
     pr.dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
   }
-  __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
+  __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
+                                         double& rd) const {
     r = sqrt(pr.r2);
     rinv = 1.0 / r;
     rd = r;
@@ -177,7 +178,8 @@ struct GeoAoS64 {  // FP64, reference Vec3D AoS
     pr.dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
   }
-  __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
+  __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
+                                         double& rd) const {
     r = sqrt(pr.r2);
     rinv = 1.0 / r;
     rd = r;
@@ -212,7 +214,8 @@ struct GeoAoS32 {
     pr.r2d = x * x + y * y + z * z;
     pr.r2 = static_cast<float>(pr.r2d);
   }
-  __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
+  __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
+                                         double& rd) const {
     radius_f(pr.r2, pr.r2d, r, rinv, rd);
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
@@ -242,7 +245,8 @@ struct GeoQ {
     pr.dz = __fmul_rn(__int2float_rn(pr.iz), s[2]);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
   }
-  __device__ __forceinline__ void radius(const Pair& pr, T& r, T& rinv, double& rd) const {
+  __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
+                                         double& rd) const {
     const double x = pr.ix, y = pr.iy, z = pr.iz;
     radius_f(pr.r2, x * x * s2[0] + y * y * s2[1] + z * z * s2[2], r, rinv, rd);
   }
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
         if (pr[u].r2 < mp.rc_sq) {
           T r, rinv;
           double rd;
-          g.radius(pr[u], r, rinv, rd);
+          g.radius(o, pr[u], r, rinv, rd);
           const T ex = exp(-mp.alpha * static_cast<T>(rd - mp.r0d));
           const T ome = T(1) - ex;
           const T fpair = -over_r(two_d_alpha * ome * ex, r, rinv);
@@ -639,7 +643,7 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
         if (pr[u].r2 < e.rc_sq) {
           T r, rinv, sx;
           double rd;
-          g.radius(pr[u], r, rinv, rd);
+          g.radius(o, pr[u], r, rinv, rd);
           const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
           const int j = jj[u];
           const int tj = MULTI ? __ldg(types + j) - 1 : 0;

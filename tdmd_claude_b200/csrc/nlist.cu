@@ -27,6 +27,7 @@
 
 #include "buffers.cuh"
 #include "common.cuh"
+#include "replicas.cuh"
 
 namespace tdmd_b200 {
 
@@ -133,25 +134,38 @@ constexpr int kStageCap = 1536;  // staged candidate records (24 KiB)
 // r^2 = (x*x + y*y) + z*z with round-to-nearest ops, r^2 < rl^2.  Not
 // inlined: it runs for a handful of candidates per rebuild, and as a call
 // it stays out of the filter loop's instruction stream.
+// The box travels as scalars: a reference to it would make every thread
+// copy the whole box into local memory at kernel start.
 template <class Load>
-__device__ __noinline__ bool exact_within(Load pos, const DevBox& b, int i, int j, double rl2) {
+__device__ __noinline__ bool exact_within(Load pos, int i, int j, double rl2, double Lx, double Ly,
+                                          double Lz, double hx, double hy, double hz, int px,
+                                          int py, int pz) {
   const double3 pi = pos(i), pj = pos(j);
-  const double ex = min_image1(__dsub_rn(pj.x, pi.x), b.L[0], b.halfL[0], b.periodic[0]);
-  const double ey = min_image1(__dsub_rn(pj.y, pi.y), b.L[1], b.halfL[1], b.periodic[1]);
-  const double ez = min_image1(__dsub_rn(pj.z, pi.z), b.L[2], b.halfL[2], b.periodic[2]);
+  const double ex = min_image1(__dsub_rn(pj.x, pi.x), Lx, hx, px);
+  const double ey = min_image1(__dsub_rn(pj.y, pi.y), Ly, hy, py);
+  const double ez = min_image1(__dsub_rn(pj.z, pi.z), Lz, hz, pz);
   const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
   return r2 < rl2;
 }
 
+// Shared memory of one row-building CTA.
+struct RowSmem {
+  float4 stage[kStageCap];
+  int s_start[27], s_pre[28];
+  int s_max[kRowThreads / 32];
+};
+
+// Rows of the atoms of cell c of box b's grid; cell_start / cell_count index
+// that grid's cells, cell_atoms and the atom indices are global.
 template <class Load, bool WRAP>
-__global__ void __launch_bounds__(kRowThreads) k_build_cells(
-    Load pos, DevBox b, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
-    const int* __restrict__ cell_atoms, double rl2, float lo_f, float hi_f, int* __restrict__ nbr,
-    const int* __restrict__ row_off, int cap, int* __restrict__ counts,
-    int* __restrict__ status) {
-  __shared__ float4 stage[kStageCap];
-  __shared__ int s_start[27], s_pre[28];
-  const int c = blockIdx.x;
+__device__ __forceinline__ void build_cell_rows(
+    RowSmem& sm, Load pos, const DevBox& b, int c, const int* __restrict__ cell_start,
+    const int* __restrict__ cell_count, const int* __restrict__ cell_atoms, double rl2,
+    float lo_f, float hi_f, int* __restrict__ nbr, const int* __restrict__ row_off, int cap,
+    int* __restrict__ counts, int* __restrict__ status) {
+  float4* const stage = sm.stage;
+  int* const s_start = sm.s_start;
+  int* const s_pre = sm.s_pre;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int ncx = b.nc[0], ncy = b.nc[1], ncz = b.nc[2];
   const int ncxy = ncx * ncy;
@@ -229,7 +243,9 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
         }
         const float r2f = dx * dx + dy * dy + dz * dz;
         bool pred = j != i && r2f < lo_f;
-        if (j != i && r2f >= lo_f && r2f <= hi_f) pred = exact_within(pos, b, i, j, rl2);
+        if (j != i && r2f >= lo_f && r2f <= hi_f) pred = exact_within(pos, i, j, rl2, b.L[0], b.L[1], b.L[2], b.halfL[0],
+                                         b.halfL[1], b.halfL[2], b.periodic[0], b.periodic[1],
+                                         b.periodic[2]);
         const unsigned m = __ballot_sync(0xffffffffu, pred);
         if (pred && nbr) {
           const int p = cnt + __popc(m & lt_mask);
@@ -251,7 +267,7 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
   // the maximum for a sizing (count-only) pass, the overflow flag when a
   // padded row is too short.
   if (status) {
-    __shared__ int s_max[kRowThreads / 32];
+    int* const s_max = sm.s_max;
     if (lane == 0) s_max[warp] = wmax;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -262,6 +278,58 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
       if (overflow || !nbr) atomicMax(&status[1], m);
     }
   }
+}
+
+template <class Load, bool WRAP>
+__global__ void __launch_bounds__(kRowThreads) k_build_cells(
+    Load pos, DevBox b, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
+    const int* __restrict__ cell_atoms, double rl2, float lo_f, float hi_f, int* __restrict__ nbr,
+    const int* __restrict__ row_off, int cap, int* __restrict__ counts,
+    int* __restrict__ status) {
+  __shared__ RowSmem sm;
+  build_cell_rows<Load, WRAP>(sm, pos, b, blockIdx.x, cell_start, cell_count, cell_atoms, rl2,
+                              lo_f, hi_f, nbr, row_off, cap, counts, status);
+}
+
+// Batched replicas: one CTA per cell of any replica (cells of replica r are
+// global cells [cell0, cell0 + ncells)); the replica's box, filter band and
+// 3-cell-axis flag come from its descriptor.
+__global__ void __launch_bounds__(kRowThreads) k_build_cells_batch(
+    LoadD4 pos, const RepDesc* __restrict__ reps, const int* __restrict__ cell_rep,
+    const int* __restrict__ cell_start, const int* __restrict__ cell_count,
+    const int* __restrict__ cell_atoms, double rl2, int* __restrict__ nbr, int cap,
+    int* __restrict__ counts, int* __restrict__ status) {
+  __shared__ RowSmem sm;
+  __shared__ RepDesc d;
+  const int gc = blockIdx.x;
+  if (threadIdx.x == 0) d = reps[__ldg(cell_rep + gc)];
+  __syncthreads();
+  if (d.wrap)
+    build_cell_rows<LoadD4, true>(sm, pos, d.box, gc - d.cell0, cell_start + d.cell0,
+                                  cell_count + d.cell0, cell_atoms, rl2, d.lo_f, d.hi_f, nbr,
+                                  nullptr, cap, counts, status);
+  else
+    build_cell_rows<LoadD4, false>(sm, pos, d.box, gc - d.cell0, cell_start + d.cell0,
+                                   cell_count + d.cell0, cell_atoms, rl2, d.lo_f, d.hi_f, nbr,
+                                   nullptr, cap, counts, status);
+}
+
+// Batched binning: the replica of atom i is rep[i]; its cell is the
+// replica's first global cell plus the local index in the replica's grid.
+__global__ void k_bin_atoms_batch(LoadD4 pos, const int* __restrict__ rep,
+                                  const RepDesc* __restrict__ reps, int n,
+                                  int* __restrict__ atom_cell, int* __restrict__ cell_count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDesc* d = reps + __ldg(rep + i);
+  const DevBox& b = d->box;
+  const double3 p = pos(i);
+  const int ix = cell_coord(p.x, b.lo[0], b.cs[0], b.nc[0]);
+  const int iy = cell_coord(p.y, b.lo[1], b.cs[1], b.nc[1]);
+  const int iz = cell_coord(p.z, b.lo[2], b.cs[2], b.nc[2]);
+  const int c = d->cell0 + iz * b.nc[0] * b.nc[1] + iy * b.nc[0] + ix;
+  atom_cell[i] = c;
+  atomicAdd(&cell_count[c], 1);
 }
 
 }  // namespace
@@ -307,22 +375,69 @@ void build_cell_list(CellListDev& cl, const void* d_pos, PosLayout layout, long 
   TDMD_LAUNCH_CHECK();
 }
 
+void row_filter_band(const DevBox& box, double r_list_sq, float* lo_f, float* hi_f, int* wrap) {
+  // Band of the FP32 filter (see build_cell_rows).
+  const double step = std::max(box.qstep[0], std::max(box.qstep[1], box.qstep[2]));
+  const double rl = std::sqrt(r_list_sq);
+  const double eps = 3e-5 + 8.0 * step / (rl > 0.0 ? rl : 1.0);
+  *lo_f = static_cast<float>(r_list_sq * (1.0 - eps));
+  *hi_f = static_cast<float>(r_list_sq * (1.0 + eps));
+  // Relative coordinates are minimum-imaged by the int32 wrap when every
+  // periodic axis has >= 4 cells (candidates then lie within 2 cells of the
+  // corner, under L/2); 3-cell axes re-apply the minimum image in FP32.
+  int w = 0;
+  for (int a = 0; a < 3; ++a) w = w || (box.periodic[a] && box.nc[a] < 4);
+  *wrap = w;
+}
+
+void build_cell_list_batch(CellListDev& cl, const double4* pos, const int* rep,
+                           const RepDesc* reps, long long n, int ncells_total,
+                           cudaStream_t stream) {
+  TDMD_REQUIRE(n >= 0 && n < INT_MAX, "atom count out of range");
+  cl.nc[0] = cl.nc[1] = cl.nc[2] = 0;
+  cl.ncells = ncells_total;
+  cl.natoms = n;
+  cl.atom_cell.reserve(static_cast<size_t>(n));
+  cl.cell_atoms.reserve(static_cast<size_t>(n));
+  cl.cell_count.reserve(static_cast<size_t>(ncells_total));
+  cl.cell_start.reserve(static_cast<size_t>(ncells_total));
+  cl.cursor.reserve(static_cast<size_t>(ncells_total));
+  if (n == 0) return;
+  TDMD_CU(cudaMemsetAsync(cl.cell_count.data(), 0, sizeof(int) * ncells_total, stream));
+  const int nb = ceil_div(n, 256);
+  k_bin_atoms_batch<<<nb, 256, 0, stream>>>(LoadD4{pos}, rep, reps, static_cast<int>(n),
+                                            cl.atom_cell.data(), cl.cell_count.data());
+  TDMD_LAUNCH_CHECK();
+  device_exclusive_scan(cl.cell_count.data(), cl.cell_start.data(), ncells_total, nullptr,
+                        cl.scan_tmp, stream);
+  TDMD_CU(cudaMemcpyAsync(cl.cursor.data(), cl.cell_start.data(), sizeof(int) * ncells_total,
+                          cudaMemcpyDeviceToDevice, stream));
+  k_scatter_atoms<<<nb, 256, 0, stream>>>(cl.atom_cell.data(), static_cast<int>(n),
+                                          cl.cursor.data(), cl.cell_atoms.data());
+  TDMD_LAUNCH_CHECK();
+  k_sort_cells<<<ceil_div(1ll * ncells_total * 32, 256), 256, 0, stream>>>(
+      cl.cell_start.data(), cl.cell_count.data(), ncells_total, cl.cell_atoms.data());
+  TDMD_LAUNCH_CHECK();
+}
+
+void build_neighbor_rows_batch(const CellListDev& cl, const double4* pos, const RepDesc* reps,
+                               const int* cell_rep, double r_list_sq, int* nbr, int cap,
+                               int* counts, int* status, cudaStream_t stream) {
+  if (cl.natoms == 0 || cl.ncells == 0) return;
+  k_build_cells_batch<<<cl.ncells, kRowThreads, 0, stream>>>(
+      LoadD4{pos}, reps, cell_rep, cl.cell_start.data(), cl.cell_count.data(),
+      cl.cell_atoms.data(), r_list_sq, nbr, cap, counts, status);
+  TDMD_LAUNCH_CHECK();
+}
+
 void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout layout,
                          long long n, const DevBox& box, double r_list_sq, int* nbr,
                          const int* row_off, int cap, int* counts, int* status,
                          cudaStream_t stream) {
   if (n == 0) return;
-  // Band of the FP32 filter (see k_build_cells).
-  const double step = std::max(box.qstep[0], std::max(box.qstep[1], box.qstep[2]));
-  const double rl = std::sqrt(r_list_sq);
-  const double eps = 3e-5 + 8.0 * step / (rl > 0.0 ? rl : 1.0);
-  const float lo_f = static_cast<float>(r_list_sq * (1.0 - eps));
-  const float hi_f = static_cast<float>(r_list_sq * (1.0 + eps));
-  // Relative coordinates are minimum-imaged by the int32 wrap when every
-  // periodic axis has >= 4 cells (candidates then lie within 2 cells of the
-  // corner, under L/2); 3-cell axes re-apply the minimum image in FP32.
-  bool wrap = false;
-  for (int a = 0; a < 3; ++a) wrap = wrap || (box.periodic[a] && box.nc[a] < 4);
+  float lo_f = 0.f, hi_f = 0.f;
+  int wrap = 0;
+  row_filter_band(box, r_list_sq, &lo_f, &hi_f, &wrap);
   auto go = [&](auto load, auto wrap_tag) {
     constexpr bool W = decltype(wrap_tag)::value;
     k_build_cells<decltype(load), W><<<cl.ncells, kRowThreads, 0, stream>>>(

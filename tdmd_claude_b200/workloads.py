@@ -160,3 +160,19 @@ def ternary(ncell: int, seed: int = 99, t_target: float = 1000.0) -> System:
     n = 4 * ncell ** 3
     types = rng.integers(1, 4, size=n).astype(np.int32)
     return fcc_system(ncell, 3.56, t_target, seed, types=types, masses=(58.69, 58.93, 52.00))
+
+
+# Morse parameters of the 256-atom Cu case (D eV, alpha 1/A, r0 A, rc A).
+MORSE_CU = (0.3429, 1.3588, 2.866, 6.0)
+
+
+def replica_set(nrep: int = 512, seed: int = 2024, nmin: int = 4, nmax: int = 16,
+                tmin: float = 100.0, tmax: float = 1500.0) -> list:
+    """Independent Cu FCC Morse systems: replica r has n_r^3 cells with n_r
+    uniform in [nmin, nmax] (256 to 16,384 atoms for 4..16), temperature
+    uniform in [tmin, tmax] K, its own seeded jitter and velocities."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(nmin, nmax + 1, size=nrep)
+    ts = rng.uniform(tmin, tmax, size=nrep)
+    return [fcc_system(int(n), 3.615, float(t), seed + 1 + r) for r, (n, t) in
+            enumerate(zip(ns, ts))]

@@ -1,0 +1,134 @@
+"""Batched replicas (tdmd_batch_*) through the C ABI.
+
+Each replica follows FastPipelineScheduler's NVE semantics with the same
+per-atom arithmetic, so with equal lanes per atom a replica's trajectory is
+bit-identical to a single scheduler's on that replica (both precisions);
+per-replica energies agree with the scheduler's to 1e-12 relative (only the
+summation order differs)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+# (FCC cells per edge, temperature K): 3-cell and wider grids, uneven sizes.
+SPECS = [(4, 300.0), (6, 900.0), (5, 1500.0), (7, 100.0), (4, 600.0)]
+
+
+def _systems(specs, seed=20):
+    from tdmd_claude_b200 import workloads as W
+    return [W.fcc_system(n, 3.615, t, seed + k) for k, (n, t) in enumerate(specs)]
+
+
+def _morse():
+    from tdmd_claude_b200 import MorseParams
+    return MorseParams.make(*golden("ref_morse_256.json")["morse"])
+
+
+def _batch(systems, precision, lanes=4, use_graphs=True, **kw):
+    from tdmd_claude_b200 import Box, ReplicaBatch, make_config
+    cfg = make_config(dt=0.001, r_skin=0.3, rebuild_every=10, precision=precision,
+                      lanes_per_atom=lanes, use_graphs=use_graphs, **kw)
+    b = ReplicaBatch([Box.make(s.lo, s.hi) for s in systems], [s.n for s in systems], _morse(),
+                     cfg)
+    b.upload(np.concatenate([s.positions for s in systems]),
+             np.concatenate([s.velocities for s in systems]),
+             np.concatenate([s.types for s in systems]), systems[0].masses)
+    return b
+
+
+def _single(s, precision, lanes=4):
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, make_config
+    cfg = make_config(dt=0.001, r_skin=0.3, rebuild_every=10, precision=precision,
+                      lanes_per_atom=lanes)
+    sc = FastPipelineScheduler(Box.make(s.lo, s.hi), s.n, _morse(), cfg)
+    sc.upload(s.positions, s.velocities, None, s.types, s.ids, s.masses)
+    return sc
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_replicas_equal_single_schedulers(cuda, precision):
+    systems = _systems(SPECS)
+    b = _batch(systems, precision)
+    for target in (10, 25):
+        b.run_until(target)
+    pos, vel, frc = b.download()
+    pe_b, ke_b = b.energies()
+    for r, s in enumerate(systems):
+        sc = _single(s, precision)
+        sc.run_until(10)
+        sc.run_until(25)
+        st = sc.download()
+        assert np.array_equal(b.replica(pos, r), st.positions), r
+        assert np.array_equal(b.replica(vel, r), st.velocities), r
+        assert np.array_equal(b.replica(frc, r), st.forces), r
+        pe, ke, _ = sc.energies()
+        assert abs(pe_b[r] - pe) <= 1e-12 * abs(pe), r
+        assert abs(ke_b[r] - ke) <= 1e-12 * abs(ke), r
+        sc.close()
+    info = b.info()
+    assert info["step"] == 25 and info["nreplicas"] == len(SPECS)
+    st = b.stats()
+    assert st.ticks == 25 and st.rebuilds == 3 and st.graph_launches > 0
+
+
+def test_batch_graphs_equal_direct_launches(cuda):
+    systems = _systems(SPECS[:3], seed=40)
+    a = _batch(systems, "mixed", use_graphs=True)
+    d = _batch(systems, "mixed", use_graphs=False)
+    for t in (10, 20, 37):
+        a.run_until(t)
+        d.run_until(t)
+    pa, va, _ = a.download()
+    pd, vd, _ = d.download()
+    assert np.array_equal(pa, pd) and np.array_equal(va, vd)
+    assert d.stats().graph_launches == 0
+
+
+def test_batch_empty_replica_and_energy_log(cuda):
+    from tdmd_claude_b200 import Box, ReplicaBatch, make_config
+    from tdmd_claude_b200 import workloads as W
+    s0 = W.fcc_system(4, 3.615, 300.0, 3)
+    s1 = W.fcc_system(5, 3.615, 800.0, 4)
+    cfg = make_config(dt=0.001, r_skin=0.3, rebuild_every=10, precision="mixed",
+                      lanes_per_atom=4, energy_every=10, energy_log_capacity=8)
+    boxes = [Box.make(s0.lo, s0.hi), Box.make((0, 0, 0), (20, 20, 20)), Box.make(s1.lo, s1.hi)]
+    b = ReplicaBatch(boxes, [s0.n, 0, s1.n], _morse(), cfg)
+    b.upload(np.concatenate([s0.positions, s1.positions]),
+             np.concatenate([s0.velocities, s1.velocities]),
+             np.concatenate([s0.types, s1.types]), s0.masses)
+    for t in (10, 20, 30):
+        b.run_until(t)
+    steps, pk = b.energy_log()
+    assert np.array_equal(steps, [10, 20, 30])
+    assert pk.shape == (3, 3, 2)
+    assert np.all(pk[:, 1, :] == 0.0)          # the empty replica
+    pe, ke = b.energies()
+    assert np.allclose(pk[-1, :, 0], pe, rtol=0, atol=0)
+    assert np.allclose(pk[-1, :, 1], ke, rtol=0, atol=0)
+    # the first replica alone gives the same trajectory
+    pos, _, _ = b.download()
+    sc = _single(s0, "mixed")
+    sc.run_until(10)
+    sc.run_until(20)
+    sc.run_until(30)
+    assert np.array_equal(b.replica(pos, 0), sc.download().positions)
+    # total energy of each replica stays close (Morse has no shift at rc,
+    # so pairs crossing rc move it slightly)
+    etot = pk[:, [0, 2], 0] + pk[:, [0, 2], 1]
+    assert np.all(np.abs(etot - etot[0]) / np.array([s0.n, s1.n]) < 1e-3)
+
+
+def test_batch_autotune_keeps_forces(cuda):
+    systems = _systems(SPECS[:4], seed=60)
+    b = _batch(systems, "mixed", lanes=0)
+    b.run_until(0)
+    _, _, f0 = b.download()
+    lanes, ms = b.autotune()
+    assert lanes in ms and all(v > 0 for v in ms.values())
+    _, _, f1 = b.download()
+    rel = np.sqrt(((f1 - f0) ** 2).sum() / (f0.astype(np.float64) ** 2).sum())
+    assert rel < 1e-5

@@ -171,3 +171,20 @@ def test_reference_reads_our_data_file(ref_lib):
                                      vel.ctypes.data, ty.ctypes.data, ids.ctypes.data,
                                      m.ctypes.data) == 0
     assert np.array_equal(pos, s.positions) and np.array_equal(vel, s.velocities)
+
+
+def test_batch_rejects_thermostat_and_bad_boxes(L):
+    import ctypes as C
+    from tdmd_claude_b200 import Box, MorseParams, make_config
+    boxes = (Box * 1)(Box.make((0, 0, 0), (20, 20, 20)))
+    natoms = (C.c_int32 * 1)(10)
+    p = MorseParams.make(0.3429, 1.3588, 2.866, 6.0)
+    h = C.c_void_p()
+    cfg = make_config(t_target=300.0)
+    assert L.tdmd_batch_create_morse(1, boxes, natoms, C.byref(p), C.byref(cfg),
+                                     C.byref(h)) == 8      # TDMD_ERR_UNSUPPORTED
+    small = (Box * 1)(Box.make((0, 0, 0), (10, 10, 10)))    # edge < 2 (rc + skin)
+    assert L.tdmd_batch_create_morse(1, small, natoms, C.byref(p), C.byref(make_config()),
+                                     C.byref(h)) == 1      # TDMD_ERR_INVALID_ARGUMENT
+    assert L.tdmd_batch_create_morse(0, boxes, natoms, C.byref(p), C.byref(make_config()),
+                                     C.byref(h)) == 1
