@@ -352,6 +352,31 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed"):
                         "rc 6.0 skin 0.3, K=10 steps per graph"}
 
 
+def ternary_bench(steps, warmup, flush, torch):
+    """Equiatomic random ternary FCC alloy, 100^3 cells = 4,000,000 atoms
+    (a = 3.56 A), per-species analytic EAM, mixed precision, NVT
+    (Nose-Hoover chain 3, 1000 K, tau 0.1 ps), adaptive dt =
+    clamp(0.05 rc / v_max, 0.1 fs, 2 fs)."""
+    from tdmd_claude_b200 import workloads as W
+    sysm = W.ternary(100, t_target=1000.0)
+    t = W.ternary_eam_tables()
+    eam = make_eam(t)
+    s = make_sched(sysm, eam, "mixed", t_target=1000.0, t_period=0.1, nhc_length=3,
+                   adaptive_dt=True, dt_min=0.0001, dt_max=0.002, c2=0.05)
+    s.run_until(0)
+    ms, _, launches, _ = timed_windows(s, steps, warmup, flush, torch, None)
+    dt, _, _ = s.thermostat_state()
+    pe, ke, _ = s.energies()
+    s.close()
+    n_dof = 3 * sysm.n - 3
+    temp = 2.0 * ke / (n_dof * 8.617333262e-5)
+    return {"value": sysm.n * WINDOW * steps / (ms * 1e-3), "unit": "atom-steps/s",
+            "ms_per_window": ms / steps, "atoms": sysm.n, "precision": "mixed",
+            "kernel_launches_timed": launches, "dt_ps_at_end": dt, "temperature_K_at_end": temp,
+            "workload": "ternary FCC alloy 100^3 cells (4,000,000 atoms), EAM 3 species, "
+                        "NVT NHC-3 1000 K, adaptive dt"}
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
     if rank != 0:
@@ -390,6 +415,8 @@ def main():
                     help="only the mixed timed windows (for profiler captures); no JSON line")
     ap.add_argument("--lanes", type=int, default=2,
                     help="lanes per atom for --kernels-only (no autotune there)")
+    ap.add_argument("--no-ternary", action="store_true",
+                    help="skip the 4M-atom ternary NVT + adaptive-dt figure")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-replica (512 Morse systems) figure")
     ap.add_argument("--drift-steps", type=int, default=50000,
@@ -476,6 +503,9 @@ def main():
         batch = {"mixed": batch_bench(args.steps, args.warmup, flush, torch, "mixed"),
                  "fp64": batch_bench(args.steps, args.warmup, flush, torch, "fp64")}
 
+    ternary = None if args.no_ternary else ternary_bench(max(3, args.steps // 3), 3, flush,
+                                                           torch)
+
     hbm, peak_kind = measured_peaks()
     force_bytes = sysm.n * (48 + 24 * K)          # gather model, mixed force pass
     dens_bytes = sysm.n * (40 + 20 * K)
@@ -523,6 +553,7 @@ def main():
                               "thermostat": "Nose-Hoover chain 3, tau 0.1 ps, 300 K"},
                 "nve_drift": drift,
                 "batched_replicas": batch,
+                "ternary_4m_nvt_adaptive": ternary,
                 "wall_s_timed_region": wall_mixed,
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -376,6 +376,40 @@ int32_t tdmd_batch_autotune(tdmd_batch* b, int32_t* chosen_lanes, double* ms6);
 int32_t tdmd_batch_last_window_ms(const tdmd_batch* b, double* ms);
 int32_t tdmd_batch_stream(const tdmd_batch* b, void** stream);
 
+/* ------------------------------------------------------------------------ */
+/* Force matching (no reference counterpart: the reference computes no      */
+/* gradients).  Loss over nsnap snapshots of natoms atoms in one box,       */
+/*   L = 1/(3 nsnap natoms) * sum |F_i(theta) - T_i|^2,                     */
+/* with the Morse or EAM forces of this library, and its gradient by the   */
+/* adjoint of the force expressions (FP64 accumulation).  Parameters,      */
+/* coefficients, loss and gradients are DEVICE pointers, so a fitting loop  */
+/* runs without host round trips; calls on one tdmd_fit share its scratch  */
+/* and must be ordered on one stream.                                       */
+/* ------------------------------------------------------------------------ */
+typedef struct tdmd_fit tdmd_fit;
+/* Host positions double[nsnap*natoms*3], types int32[nsnap*natoms]
+ * (1-based); neighbor lists with r_list = cutoff are built here once. */
+int32_t tdmd_fit_create(int32_t nsnap, int32_t natoms, const tdmd_box* box,
+                        const double* positions, const int32_t* types, double cutoff,
+                        int32_t precision, tdmd_fit** out);
+int32_t tdmd_fit_destroy(tdmd_fit* f);
+/* Target forces, host double[nsnap*natoms*3]. */
+int32_t tdmd_fit_set_targets(tdmd_fit* f, const double* targets);
+/* Morse (cutoff = the fit's cutoff): d_params = {D, alpha, r0}; writes
+ * *d_loss and d_grad[3] = dL/d{D, alpha, r0} (nullable: loss only) and the
+ * predicted forces d_forces[3*M] (nullable). */
+int32_t tdmd_fit_morse(tdmd_fit* f, const double* d_params, double* d_loss, double* d_grad,
+                       double* d_forces, void* stream);
+/* EAM with spline coefficients packed a|b|c|d per spline as
+ * tdmd_eam_coeffs gives them: d_F[ntypes][4(nrho-1)], d_rho[ntypes][4(nr-1)],
+ * d_phi[npairs][4(nr-1)] (cutoff = the fit's cutoff).  Gradients have the
+ * same layout and are overwritten; pass all three or none. */
+int32_t tdmd_fit_eam(tdmd_fit* f, int32_t ntypes, int32_t nrho, double drho, int32_t nr,
+                     double dr, const double* d_F, const double* d_rho, const double* d_phi,
+                     double* d_loss, double* d_gF, double* d_grho, double* d_gphi,
+                     double* d_forces, void* stream);
+int32_t tdmd_fit_info(const tdmd_fit* f, int64_t* natoms_total, int32_t* lanes_per_atom);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -107,6 +107,14 @@ def lib():
                                  _f64, _f64, _i32, _f64, _f64, _f64, C.c_void_p, C.c_void_p,
                                  C.c_void_p]
         L.orc_md_run.restype = _i32
+        L.orc_morse_fm_loss_grad.argtypes = [_i32, _i64, _f64p, C.POINTER(OrcBox), _f64, _f64,
+                                             _f64, _f64, _f64p, _f64p]
+        L.orc_morse_fm_loss_grad.restype = _f64
+        L.orc_eam_fm_loss_grad.argtypes = [C.c_void_p, _i32, _i64, _f64p, _i32p,
+                                           C.POINTER(OrcBox), _f64p, _f64p, _f64p, _f64p]
+        L.orc_eam_fm_loss_grad.restype = _f64
+        L.orc_eam_set_coeffs.argtypes = [C.c_void_p, _i32, _i32, _f64p]
+        L.orc_eam_set_coeffs.restype = _i32
         _lib = L
     return _lib
 
@@ -323,6 +331,41 @@ class OracleEam:
                                   C.addressof(ep))
         return dict(pe=pe, forces=f, rho=rho, fp=fp, virial=w, e_embed=ee.value,
                     e_pair=ep.value)
+
+
+    def set_coeffs(self, kind, idx, coef):
+        """Overwrites one spline's packed a|b|c|d coefficients."""
+        rc = lib().orc_eam_set_coeffs(self.h, kind, idx, _c64(coef))
+        assert rc == 0
+
+    def fm_loss_grad(self, pos, types, lo, hi, target, periodic=(1, 1, 1)):
+        """Force-matching loss over snapshots pos[s, n, 3] (same box) against
+        target[s, n, 3] and its gradient w.r.t. every spline coefficient:
+        (loss, gF[nt, 4(nrho-1)], grho[nt, 4(nr-1)], gphi[npairs, 4(nr-1)])."""
+        pos = _c64(pos)
+        ns, n = pos.shape[0], pos.shape[1]
+        types = _c32(np.broadcast_to(np.asarray(types, np.int32).reshape(-1, n), (ns, n)))
+        nt = self.ntypes
+        gF = np.zeros((nt, 4 * (self.nrho - 1)), np.float64)
+        grho = np.zeros((nt, 4 * (self.nr - 1)), np.float64)
+        gphi = np.zeros((nt * (nt + 1) // 2, 4 * (self.nr - 1)), np.float64)
+        b = make_box(lo, hi, periodic)
+        loss = lib().orc_eam_fm_loss_grad(self.h, ns, n, pos.reshape(-1), types.reshape(-1),
+                                          C.byref(b), _c64(target).reshape(-1), gF.reshape(-1),
+                                          grho.reshape(-1), gphi.reshape(-1))
+        return loss, gF, grho, gphi
+
+
+def morse_fm_loss_grad(pos, lo, hi, D, alpha, r0, rc, target, periodic=(1, 1, 1)):
+    """Force-matching loss of Morse (D, alpha, r0) over snapshots pos[s, n, 3]
+    against target[s, n, 3] and its gradient (dL/dD, dL/dalpha, dL/dr0)."""
+    pos = _c64(pos)
+    ns, n = pos.shape[0], pos.shape[1]
+    g = np.zeros(3, np.float64)
+    b = make_box(lo, hi, periodic)
+    loss = lib().orc_morse_fm_loss_grad(ns, n, pos.reshape(-1), C.byref(b), D, alpha, r0, rc,
+                                        _c64(target).reshape(-1), g)
+    return loss, g
 
 
 def kinetic_energy(vel, types, masses):

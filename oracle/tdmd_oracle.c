@@ -692,3 +692,234 @@ int32_t orc_md_run(const orc_potential* pot, double* pos, double* vel, double* f
   free(nhc);
   return step;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Force matching (no reference counterpart: the reference computes no      */
+/* gradients).  Loss over nsnap snapshots of n atoms each (same box):        */
+/*   L = 1/(3 nsnap n) * sum_s sum_i |F_i(theta) - T_i|^2                    */
+/* with F from the half-list Morse / EAM forces above (r_list = rc).         */
+/* Gradient by the adjoint of the force expressions, in FP64:                */
+/*   G_i = dL/dF_i = 2 (F_i - T_i) / (3 nsnap n),                            */
+/*   q_ij = G_i . (r_i - r_j) / r_ij  (ordered pair).                        */
+/* ------------------------------------------------------------------------ */
+static void fm_list(const double* pos, int64_t n, const orc_box* b, double rc, int32_t* counts,
+                    int32_t* offsets, int32_t** nbrs, int64_t* cap) {
+  for (;;) {
+    const int64_t tot = orc_neighbor_list(pos, n, b, rc, 0.0, 1, counts, offsets, *nbrs, *cap);
+    if (tot <= *cap) return;
+    free(*nbrs);
+    *cap = tot + tot / 4 + 16;
+    *nbrs = (int32_t*)malloc(sizeof(int32_t) * (size_t)*cap);
+  }
+}
+
+/* Morse: fpair(r) = -2 D a (1 - e) e / r, e = exp(-a (r - r0)), F_i = sum
+ * fpair d_ij, so dL/dtheta = sum over ordered pairs of q_ij r_ij dfpair/dtheta
+ * with
+ *   dfpair/dD  = fpair / D,
+ *   dfpair/da  = -2 D [ (1 - e) e - a (1 - 2e)(r - r0) e ] / r,
+ *   dfpair/dr0 = -2 D a^2 (1 - 2e) e / r.
+ * grad3 = {dL/dD, dL/dalpha, dL/dr0}. */
+double orc_morse_fm_loss_grad(int32_t nsnap, int64_t n, const double* pos, const orc_box* b,
+                              double D, double alpha, double r0, double rc,
+                              const double* target, double* grad3) {
+  int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+  int32_t* offsets = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+  int64_t cap = 64 * (n > 0 ? n : 1);
+  int32_t* nbrs = (int32_t*)malloc(sizeof(int32_t) * (size_t)cap);
+  double* f = (double*)malloc(sizeof(double) * 3 * (size_t)(n > 0 ? n : 1));
+  double* G = (double*)malloc(sizeof(double) * 3 * (size_t)(n > 0 ? n : 1));
+  const double c = 1.0 / (3.0 * (double)nsnap * (double)n);
+  const double rc_sq = rc * rc;
+  double loss = 0.0;
+  double g[3] = {0.0, 0.0, 0.0};
+  for (int32_t s = 0; s < nsnap; ++s) {
+    const double* p = pos + (size_t)s * 3 * (size_t)n;
+    const double* t = target + (size_t)s * 3 * (size_t)n;
+    fm_list(p, n, b, rc, counts, offsets, &nbrs, &cap);
+    orc_morse_forces(p, n, b, D, alpha, r0, rc, counts, offsets, nbrs, f, NULL);
+    for (int64_t k = 0; k < 3 * n; ++k) {
+      const double e = f[k] - t[k];
+      loss += c * e * e;
+      G[k] = 2.0 * c * e;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      for (int32_t k = 0; k < counts[i]; ++k) {
+        const int32_t j = nbrs[offsets[i] + k];
+        double d[3] = {p[3 * i] - p[3 * j], p[3 * i + 1] - p[3 * j + 1], p[3 * i + 2] - p[3 * j + 2]};
+        min_image(d, b);
+        const double r2 = len_sq(d);
+        if (r2 >= rc_sq) continue;
+        const double r = sqrt(r2);
+        const double ex = exp(-alpha * (r - r0));
+        const double ome = 1.0 - ex;
+        /* sum of both ordered pairs: (G_i - G_j) . d  (d = r_i - r_j) */
+        const double gd = (G[3 * i] - G[3 * j]) * d[0] + (G[3 * i + 1] - G[3 * j + 1]) * d[1] +
+                          (G[3 * i + 2] - G[3 * j + 2]) * d[2];
+        const double fpair = -2.0 * D * alpha * ome * ex / r;
+        g[0] += gd * fpair / D;
+        g[1] += gd * (-2.0 * D * (ome * ex - alpha * (1.0 - 2.0 * ex) * (r - r0) * ex) / r);
+        g[2] += gd * (-2.0 * D * alpha * alpha * (1.0 - 2.0 * ex) * ex / r);
+      }
+    }
+  }
+  if (grad3) memcpy(grad3, g, sizeof(g));
+  free(counts);
+  free(offsets);
+  free(nbrs);
+  free(f);
+  free(G);
+  return loss;
+}
+
+/* Interval index and offset of a spline argument (SplineTable::eval,
+ * eam_alloy.cpp:53-62). */
+static int32_t spl_idx(int32_t n, double dx_step, double x, double* dx) {
+  int32_t idx = (int32_t)(x / dx_step);
+  if (idx < 0) idx = 0;
+  if (idx >= n - 1) idx = n - 2;
+  *dx = x - (double)idx * dx_step;
+  return idx;
+}
+
+/* Adds w * d(value)/d(a,b,c,d) or w * d(derivative)/d(a,b,c,d) of interval
+ * idx into a packed a|b|c|d gradient of one spline (ns intervals). */
+static void spl_add_value(double* g, int32_t ns, int32_t idx, double dx, double w) {
+  g[idx] += w;
+  g[ns + idx] += w * dx;
+  g[2 * ns + idx] += w * dx * dx;
+  g[3 * ns + idx] += w * dx * dx * dx;
+}
+static void spl_add_deriv(double* g, int32_t ns, int32_t idx, double dx, double w) {
+  g[ns + idx] += w;
+  g[2 * ns + idx] += w * 2.0 * dx;
+  g[3 * ns + idx] += w * 3.0 * dx * dx;
+}
+
+/* EAM: fpair_ij = -(phi'_p(r) + F'_i rho'_tj(r) + F'_j rho'_ti(r)) / r.
+ * With the adjoint density weight
+ *   w_a = -sum_j rho'_tj(r_aj) (G_a - G_j) . d_aj / r_aj
+ * the gradient w.r.t. every coefficient (layout of orc_eam: F, rho, phi,
+ * each spline a|b|c|d) is
+ *   phi_p : -(q_ij + q_ji) * dphi'/dc at r_ij          (each pair)
+ *   rho_tj: -(q_ij + q_ji) F'_i * drho'/dc at r_ij     (and i<->j)
+ *           + w_i F''_i * drho/dc at r_ij              (and i<->j)
+ *   F_ta  : w_a * dF'/dc at rho_a.
+ * gF, grho, gphi are overwritten. */
+double orc_eam_fm_loss_grad(const orc_eam* e, int32_t nsnap, int64_t n, const double* pos,
+                            const int32_t* types, const orc_box* b, const double* target,
+                            double* gF, double* grho, double* gphi) {
+  const int32_t nt = e->ntypes;
+  const int32_t npairs = nt * (nt + 1) / 2;
+  const int32_t nsr = e->nr - 1, nsf = e->nrho - 1;
+  memset(gF, 0, sizeof(double) * (size_t)nt * 4 * (size_t)nsf);
+  memset(grho, 0, sizeof(double) * (size_t)nt * 4 * (size_t)nsr);
+  memset(gphi, 0, sizeof(double) * (size_t)npairs * 4 * (size_t)nsr);
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * nn);
+  int32_t* offsets = (int32_t*)malloc(sizeof(int32_t) * nn);
+  int64_t cap = 64 * (int64_t)nn;
+  int32_t* nbrs = (int32_t*)malloc(sizeof(int32_t) * (size_t)cap);
+  double* f = (double*)malloc(sizeof(double) * 3 * nn);
+  double* G = (double*)malloc(sizeof(double) * 3 * nn);
+  double* rho = (double*)malloc(sizeof(double) * nn);
+  double* fp = (double*)malloc(sizeof(double) * nn);
+  double* w = (double*)malloc(sizeof(double) * nn);
+  const double c = 1.0 / (3.0 * (double)nsnap * (double)n);
+  const double rc_sq = e->cutoff * e->cutoff;
+  double loss = 0.0;
+  for (int32_t s = 0; s < nsnap; ++s) {
+    const double* p = pos + (size_t)s * 3 * nn;
+    const int32_t* ty = types + (size_t)s * nn;
+    const double* t = target + (size_t)s * 3 * nn;
+    fm_list(p, n, b, e->cutoff, counts, offsets, &nbrs, &cap);
+    orc_eam_forces(e, p, ty, n, b, counts, offsets, nbrs, f, rho, fp, NULL, NULL, NULL);
+    for (int64_t k = 0; k < 3 * n; ++k) {
+      const double d = f[k] - t[k];
+      loss += c * d * d;
+      G[k] = 2.0 * c * d;
+    }
+    memset(w, 0, sizeof(double) * nn);
+    /* pass A: phi and direct rho gradients, adjoint density weights */
+    for (int64_t i = 0; i < n; ++i) {
+      const int32_t ti = ty[i] - 1;
+      for (int32_t k = 0; k < counts[i]; ++k) {
+        const int32_t j = nbrs[offsets[i] + k];
+        const int32_t tj = ty[j] - 1;
+        double d[3] = {p[3 * i] - p[3 * j], p[3 * i + 1] - p[3 * j + 1], p[3 * i + 2] - p[3 * j + 2]};
+        min_image(d, b);
+        const double r2 = len_sq(d);
+        if (r2 >= rc_sq) continue;
+        const double r = sqrt(r2);
+        const double qq = ((G[3 * i] - G[3 * j]) * d[0] + (G[3 * i + 1] - G[3 * j + 1]) * d[1] +
+                           (G[3 * i + 2] - G[3 * j + 2]) * d[2]) / r;
+        double dx;
+        const int32_t idx = spl_idx(e->nr, e->dr, r, &dx);
+        const int32_t pp = phi_index(ti, tj, nt);
+        spl_add_deriv(gphi + (size_t)pp * 4 * nsr, nsr, idx, dx, -qq);
+        spl_add_deriv(grho + (size_t)tj * 4 * nsr, nsr, idx, dx, -qq * fp[i]);
+        spl_add_deriv(grho + (size_t)ti * 4 * nsr, nsr, idx, dx, -qq * fp[j]);
+        const double drj = orc_spline_deriv(e->rho_coef + (size_t)tj * 4 * nsr, e->nr, e->dr, 0.0, r);
+        const double dri = orc_spline_deriv(e->rho_coef + (size_t)ti * 4 * nsr, e->nr, e->dr, 0.0, r);
+        w[i] -= drj * qq;
+        w[j] -= dri * qq; /* (G_j - G_i) . d_ji = qq * r */
+      }
+    }
+    /* F gradients at rho_a; F''(rho_a) for pass B */
+    for (int64_t a = 0; a < n; ++a) {
+      const int32_t ta = ty[a] - 1;
+      const double* fc = e->F_coef + (size_t)ta * 4 * nsf;
+      double dx;
+      const int32_t idx = spl_idx(e->nrho, e->drho, rho[a], &dx);
+      spl_add_deriv(gF + (size_t)ta * 4 * nsf, nsf, idx, dx, w[a]);
+      const double fpp = 2.0 * fc[2 * nsf + idx] + 6.0 * fc[3 * nsf + idx] * dx;
+      w[a] *= fpp; /* now w_a F''_a */
+    }
+    /* pass B: rho value gradients through rho_a */
+    for (int64_t i = 0; i < n; ++i) {
+      const int32_t ti = ty[i] - 1;
+      for (int32_t k = 0; k < counts[i]; ++k) {
+        const int32_t j = nbrs[offsets[i] + k];
+        const int32_t tj = ty[j] - 1;
+        double d[3] = {p[3 * i] - p[3 * j], p[3 * i + 1] - p[3 * j + 1], p[3 * i + 2] - p[3 * j + 2]};
+        min_image(d, b);
+        const double r2 = len_sq(d);
+        if (r2 >= rc_sq) continue;
+        const double r = sqrt(r2);
+        double dx;
+        const int32_t idx = spl_idx(e->nr, e->dr, r, &dx);
+        spl_add_value(grho + (size_t)tj * 4 * nsr, nsr, idx, dx, w[i]);
+        spl_add_value(grho + (size_t)ti * 4 * nsr, nsr, idx, dx, w[j]);
+      }
+    }
+  }
+  free(counts);
+  free(offsets);
+  free(nbrs);
+  free(f);
+  free(G);
+  free(rho);
+  free(fp);
+  free(w);
+  return loss;
+}
+
+/* Overwrites one spline's packed coefficients (kind 0 = F, 1 = rho,
+ * 2 = phi), so a caller can evaluate the loss at perturbed coefficients. */
+int32_t orc_eam_set_coeffs(orc_eam* e, int32_t kind, int32_t idx, const double* in) {
+  const int32_t nt = e->ntypes;
+  const int32_t npairs = nt * (nt + 1) / 2;
+  if (kind == 0 && idx >= 0 && idx < nt) {
+    memcpy(e->F_coef + (size_t)idx * 4 * (e->nrho - 1), in, sizeof(double) * 4 * (size_t)(e->nrho - 1));
+    return 0;
+  }
+  if (kind == 1 && idx >= 0 && idx < nt) {
+    memcpy(e->rho_coef + (size_t)idx * 4 * (e->nr - 1), in, sizeof(double) * 4 * (size_t)(e->nr - 1));
+    return 0;
+  }
+  if (kind == 2 && idx >= 0 && idx < npairs) {
+    memcpy(e->phi_coef + (size_t)idx * 4 * (e->nr - 1), in, sizeof(double) * 4 * (size_t)(e->nr - 1));
+    return 0;
+  }
+  return 1;
+}

@@ -152,6 +152,12 @@ SIGNATURES = {
     "tdmd_batch_autotune": [_p, _pi32, _p],
     "tdmd_batch_last_window_ms": [_p, _pf64],
     "tdmd_batch_stream": [_p, _pp],
+    "tdmd_fit_create": [_i32, _i32, C.POINTER(Box), _p, _p, _f64, _i32, _pp],
+    "tdmd_fit_destroy": [_p],
+    "tdmd_fit_set_targets": [_p, _p],
+    "tdmd_fit_morse": [_p, _p, _p, _p, _p, _p],
+    "tdmd_fit_eam": [_p, _i32, _i32, _f64, _i32, _f64, _p, _p, _p, _p, _p, _p, _p, _p, _p],
+    "tdmd_fit_info": [_p, C.POINTER(C.c_int64), _pi32],
     "tdmd_sched_set_profiling": [_p, _i32],
     "tdmd_sched_autotune": [_p, _pi32, _p],
     "tdmd_sched_last_window_ms": [_p, _pf64],

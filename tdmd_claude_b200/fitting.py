@@ -1,0 +1,202 @@
+"""Force-matching fits of Morse parameters and EAM spline coefficients.
+
+The loss and its gradient come from the C ABI (tdmd_fit_*: the adjoint of
+the force expressions on the GPU, FP64 accumulation).  torch supplies device
+tensors, the optimizer and the autograd plumbing only: MorseLoss and EamLoss
+are torch.autograd.Functions whose forward runs the loss + gradient kernels
+once and whose backward scales that gradient.
+
+No reference counterpart (the reference computes no gradients); the force
+definitions are those of src/potentials/morse.hpp:37-55 and
+src/potentials/eam_alloy.cpp:196-295.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from ._lib import TDMD_FP64, TDMD_MIXED, Box, call, lib
+
+
+def _dptr(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _cur_stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class ForceMatch:
+    """Snapshots positions[s, n, 3] (one box, 1-based types[s, n] or [n]),
+    neighbor lists with r_list = cutoff built once on the device."""
+
+    def __init__(self, positions, types, box: Box, cutoff: float, precision: str = "fp64"):
+        pos = np.ascontiguousarray(positions, dtype=np.float64)
+        self.nsnap, self.natoms = pos.shape[0], pos.shape[1]
+        typ = np.ascontiguousarray(np.broadcast_to(
+            np.asarray(types, np.int32).reshape(-1, self.natoms), (self.nsnap, self.natoms)),
+            dtype=np.int32)
+        self.cutoff = float(cutoff)
+        self.precision = precision
+        h = C.c_void_p()
+        call("tdmd_fit_create", self.nsnap, self.natoms, C.byref(box),
+             pos.ctypes.data_as(C.c_void_p), typ.ctypes.data_as(C.c_void_p), self.cutoff,
+             TDMD_FP64 if precision == "fp64" else TDMD_MIXED, C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            try:
+                lib().tdmd_fit_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+    def set_targets(self, targets):
+        t = np.ascontiguousarray(targets, dtype=np.float64)
+        assert t.size == 3 * self.nsnap * self.natoms
+        call("tdmd_fit_set_targets", self._h, t.ctypes.data_as(C.c_void_p))
+
+    # raw calls on device tensors (float64, cuda) ---------------------------
+    def morse(self, params, loss, grad=None, forces=None):
+        call("tdmd_fit_morse", self._h, _dptr(params), _dptr(loss), _dptr(grad), _dptr(forces),
+             _cur_stream())
+
+    def eam(self, tables: dict, F, rho, phi, loss, gF=None, grho=None, gphi=None, forces=None):
+        call("tdmd_fit_eam", self._h, int(tables["ntypes"]), int(tables["nrho"]),
+             float(tables["drho"]), int(tables["nr"]), float(tables["dr"]), _dptr(F),
+             _dptr(rho), _dptr(phi), _dptr(loss), _dptr(gF), _dptr(grho), _dptr(gphi),
+             _dptr(forces), _cur_stream())
+
+    def morse_forces(self, params):
+        import torch
+        p = torch.as_tensor(np.asarray(params, np.float64), device="cuda")
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        f = torch.zeros(self.nsnap * self.natoms * 3, dtype=torch.float64, device="cuda")
+        if not getattr(self, "_has_targets", False):
+            self.set_targets(np.zeros(3 * self.nsnap * self.natoms))
+            self._has_targets = True
+        self.morse(p, loss, None, f)
+        return f.cpu().numpy().reshape(self.nsnap, self.natoms, 3)
+
+    def eam_forces(self, tables: dict, F, rho, phi):
+        import torch
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        f = torch.zeros(self.nsnap * self.natoms * 3, dtype=torch.float64, device="cuda")
+        if not getattr(self, "_has_targets", False):
+            self.set_targets(np.zeros(3 * self.nsnap * self.natoms))
+            self._has_targets = True
+        self.eam(tables, F, rho, phi, loss, forces=f)
+        return f.cpu().numpy().reshape(self.nsnap, self.natoms, 3)
+
+
+def _autograd():
+    import torch
+
+    class MorseLoss(torch.autograd.Function):
+        """loss(params[3] = D, alpha, r0) with the adjoint gradient."""
+
+        @staticmethod
+        def forward(ctx, params, fm):
+            loss = torch.empty(1, dtype=torch.float64, device=params.device)
+            grad = torch.empty(3, dtype=torch.float64, device=params.device)
+            fm.morse(params.detach().contiguous(), loss, grad)
+            ctx.save_for_backward(grad)
+            return loss.reshape(())
+
+        @staticmethod
+        def backward(ctx, gout):
+            (grad,) = ctx.saved_tensors
+            return gout * grad, None
+
+    class EamLoss(torch.autograd.Function):
+        """loss(F, rho, phi spline coefficients) with the adjoint gradient."""
+
+        @staticmethod
+        def forward(ctx, F, rho, phi, fm, tables):
+            loss = torch.empty(1, dtype=torch.float64, device=F.device)
+            gF, gr, gp = torch.empty_like(F), torch.empty_like(rho), torch.empty_like(phi)
+            fm.eam(tables, F.detach().contiguous(), rho.detach().contiguous(),
+                   phi.detach().contiguous(), loss, gF, gr, gp)
+            ctx.save_for_backward(gF, gr, gp)
+            return loss.reshape(())
+
+        @staticmethod
+        def backward(ctx, gout):
+            gF, gr, gp = ctx.saved_tensors
+            return gout * gF, gout * gr, gout * gp, None, None
+
+    return MorseLoss, EamLoss
+
+
+def morse_loss(params, fm: ForceMatch):
+    return _autograd()[0].apply(params, fm)
+
+
+def eam_loss(F, rho, phi, fm: ForceMatch, tables: dict):
+    return _autograd()[1].apply(F, rho, phi, fm, tables)
+
+
+def adam_fit(loss_fn, params: list, steps: int = 200, lr: float = 1e-3):
+    """Runs `steps` Adam steps on loss_fn(*params); returns (losses, seconds)
+    with the time measured by CUDA events around the loop."""
+    import torch
+    opt = torch.optim.Adam(params, lr=lr)
+    losses = torch.zeros(steps, dtype=torch.float64, device=params[0].device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for k in range(steps):
+        opt.zero_grad(set_to_none=True)
+        loss = loss_fn(*params)
+        loss.backward()
+        opt.step()
+        losses[k] = loss.detach()
+    end.record()
+    torch.cuda.synchronize()
+    return losses.cpu().numpy(), start.elapsed_time(end) * 1e-3
+
+
+def eam_table_meta(eam) -> dict:
+    """ntypes / nrho / drho / nr / dr of an EamAlloy (api.EamAlloy)."""
+    inf = eam.info()
+    return {k: inf[k] for k in ("ntypes", "nrho", "drho", "nr", "dr")}
+
+
+def eam_coeff_tensors(eam, device="cuda"):
+    """(F, rho, phi) packed coefficient tensors of an EamAlloy."""
+    import torch
+    inf = eam.info()
+    nt = inf["ntypes"]
+    F = np.stack([eam.coeffs(0, t) for t in range(nt)])
+    rho = np.stack([eam.coeffs(1, t) for t in range(nt)])
+    phi = np.stack([eam.coeffs(2, p) for p in range(nt * (nt + 1) // 2)])
+    return tuple(torch.as_tensor(a, dtype=torch.float64, device=device).contiguous()
+                 for a in (F, rho, phi))
+
+
+def eam_snapshots(eam, ncell=10, a=3.615, t=1200.0, nsnap=64, every=100, seed=77, dt=0.001):
+    """Snapshots of an FP64 NVE run (FastPipelineScheduler, this library):
+    ncell^3 FCC cells at temperature t, one snapshot every `every` steps.
+    Returns (positions[nsnap, n, 3], types[n], lo, hi)."""
+    from .api import FastPipelineScheduler, make_config
+    from .workloads import fcc_system
+    s = fcc_system(ncell, a, t, seed)
+    box = Box.make(s.lo, s.hi)
+    sc = FastPipelineScheduler(box, s.n, eam, make_config(dt=dt, r_skin=0.3, rebuild_every=10,
+                                                         precision="fp64"))
+    sc.upload(s.positions, s.velocities, None, s.types, s.ids, s.masses)
+    out = np.zeros((nsnap, s.n, 3), np.float64)
+    t0 = time.perf_counter()
+    for k in range(nsnap):
+        sc.run_until((k + 1) * every)
+        out[k] = sc.download().positions
+    sc.close()
+    _ = t0
+    return out, s.types.copy(), s.lo, s.hi
