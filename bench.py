@@ -377,6 +377,81 @@ def ternary_bench(steps, warmup, flush, torch):
                         "NVT NHC-3 1000 K, adaptive dt"}
 
 
+def fit_bench(torch, adam_steps=200, nsnap=64):
+    """Force matching: nsnap snapshots of a 10^3-cell Cu FCC (4,000 atoms)
+    FP64 NVE run at 1200 K (one every 100 steps, config-1 EAM); targets from
+    the FP64 forces of parameters perturbed by seeded 5 % Gaussian noise;
+    loss = mean squared force error.  Adjoint gradients (mixed precision,
+    FP64 accumulation) for Morse (D, alpha, r0) and all EAM spline
+    coefficients; Adam steps timed with CUDA events; the Morse adjoint is
+    checked against central differences (h = 1e-6 relative) of the FP64
+    loss."""
+    from tdmd_claude_b200 import Box
+    from tdmd_claude_b200 import fitting as FT
+    from tdmd_claude_b200 import workloads as W
+    rng = np.random.default_rng(4242)
+    t = W.cu_eam_tables()
+    eam = make_eam(t)
+    pos, types, lo, hi = FT.eam_snapshots(eam, ncell=10, t=1200.0, nsnap=nsnap, every=100)
+    box = Box.make(lo, hi)
+    out = {"snapshots": nsnap, "atoms_per_snapshot": int(pos.shape[1]), "adam_steps": adam_steps}
+    # Morse
+    m0 = np.array(W.MORSE_CU[:3])
+    true = m0 * (1.0 + 0.05 * rng.standard_normal(3))
+    ref64 = FT.ForceMatch(pos, types, box, W.MORSE_CU[3], "fp64")
+    tgt = ref64.morse_forces(true)
+    ref64.set_targets(tgt)
+    fm = FT.ForceMatch(pos, types, box, W.MORSE_CU[3], "mixed")
+    fm.set_targets(tgt)
+
+    def loss64(p):
+        prm = torch.tensor(p, dtype=torch.float64, device="cuda")
+        lo_ = torch.zeros(1, dtype=torch.float64, device="cuda")
+        g = torch.zeros(3, dtype=torch.float64, device="cuda")
+        ref64.morse(prm, lo_, g)
+        return float(lo_.item()), g.cpu().numpy()
+
+    _, g64 = loss64(m0)
+    fd = []
+    for k in range(3):
+        h = 1e-6 * m0[k]
+        up, dn = m0.copy(), m0.copy()
+        up[k] += h
+        dn[k] -= h
+        fd.append((loss64(up)[0] - loss64(dn)[0]) / (2 * h))
+    p = torch.tensor(m0, dtype=torch.float64, device="cuda", requires_grad=True)
+    losses, sec = FT.adam_fit(lambda q: FT.morse_loss(q, fm), [p], steps=adam_steps, lr=5e-3)
+    out["morse"] = {
+        "ms_per_adam_step": 1e3 * sec / adam_steps, "loss_first": float(losses[0]),
+        "loss_last": float(losses[-1]), "params_true": true.tolist(),
+        "params_fit": p.detach().cpu().numpy().tolist(), "params_start": m0.tolist(),
+        "adjoint_vs_central_fd_rel": [abs(fd[k] - g64[k]) / abs(g64[k]) for k in range(3)]}
+    # EAM: perturbed analytic parameters -> targets; fit all coefficients.
+    f = 1.0 + 0.05 * rng.standard_normal(4)
+    tp = W.analytic_eam(beta_f=(5.0 * f[0],), A_phi=(0.6 * f[1],), E_F=(1.2 * f[2],),
+                        beta_phi=8.0 * f[3])
+    eam_p = make_eam(tp)
+    meta = FT.eam_table_meta(eam_p)
+    Fp, rp, pp = FT.eam_coeff_tensors(eam_p)
+    fm.close()
+    ref64.close()
+    # the EAM tables end at their cutoff: lists and pairs use it
+    ref64 = FT.ForceMatch(pos, types, box, t.cutoff, "fp64")
+    fm = FT.ForceMatch(pos, types, box, t.cutoff, "mixed")
+    tgt = ref64.eam_forces(meta, Fp, rp, pp)
+    fm.set_targets(tgt)
+    F, rho, phi = (x.clone().requires_grad_(True) for x in FT.eam_coeff_tensors(eam))
+    losses, sec = FT.adam_fit(lambda a, b, c: FT.eam_loss(a, b, c, fm, meta), [F, rho, phi],
+                              steps=adam_steps, lr=1e-4)
+    out["eam"] = {"ms_per_adam_step": 1e3 * sec / adam_steps, "loss_first": float(losses[0]),
+                  "loss_last": float(losses[-1]),
+                  "coefficients": int(F.numel() + rho.numel() + phi.numel()),
+                  "perturbation_factors": f.tolist()}
+    fm.close()
+    ref64.close()
+    return out
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
     if rank != 0:
@@ -415,6 +490,8 @@ def main():
                     help="only the mixed timed windows (for profiler captures); no JSON line")
     ap.add_argument("--lanes", type=int, default=2,
                     help="lanes per atom for --kernels-only (no autotune there)")
+    ap.add_argument("--no-fit", action="store_true",
+                    help="skip the force-matching (adjoint + Adam) figure")
     ap.add_argument("--no-ternary", action="store_true",
                     help="skip the 4M-atom ternary NVT + adaptive-dt figure")
     ap.add_argument("--no-batch", action="store_true",
@@ -503,6 +580,7 @@ def main():
         batch = {"mixed": batch_bench(args.steps, args.warmup, flush, torch, "mixed"),
                  "fp64": batch_bench(args.steps, args.warmup, flush, torch, "fp64")}
 
+    fitfig = None if args.no_fit else fit_bench(torch)
     ternary = None if args.no_ternary else ternary_bench(max(3, args.steps // 3), 3, flush,
                                                            torch)
 
@@ -554,6 +632,7 @@ def main():
                 "nve_drift": drift,
                 "batched_replicas": batch,
                 "ternary_4m_nvt_adaptive": ternary,
+                "force_matching": fitfig,
                 "wall_s_timed_region": wall_mixed,
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -402,8 +402,9 @@ int32_t tdmd_fit_morse(tdmd_fit* f, const double* d_params, double* d_loss, doub
                        double* d_forces, void* stream);
 /* EAM with spline coefficients packed a|b|c|d per spline as
  * tdmd_eam_coeffs gives them: d_F[ntypes][4(nrho-1)], d_rho[ntypes][4(nr-1)],
- * d_phi[npairs][4(nr-1)] (cutoff = the fit's cutoff).  Gradients have the
- * same layout and are overwritten; pass all three or none. */
+ * d_phi[npairs][4(nr-1)]; the fit's cutoff must not exceed the r tables'
+ * range (nr-1)*dr.  Gradients have the same layout and are overwritten;
+ * pass all three or none. */
 int32_t tdmd_fit_eam(tdmd_fit* f, int32_t ntypes, int32_t nrho, double drho, int32_t nr,
                      double dr, const double* d_F, const double* d_rho, const double* d_phi,
                      double* d_loss, double* d_gF, double* d_grho, double* d_gphi,

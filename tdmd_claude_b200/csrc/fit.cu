@@ -630,6 +630,10 @@ void Fit::eam(int ntypes, int nrho, double drho, int nr, double dr, const double
   TDMD_REQUIRE(has_targets_, "targets not set");
   TDMD_REQUIRE(ntypes >= 1 && ntypes <= 64, "ntypes out of range");
   TDMD_REQUIRE(max_type_ <= ntypes, "an atom type exceeds the table's element count");
+  // Pairs up to the fit's cutoff evaluate the r tables: past their last knot
+  // the cubic of the last interval would be extrapolated.
+  TDMD_REQUIRE(rc_ <= static_cast<double>(nr - 1) * dr * (1.0 + 1e-12),
+               "the fit's cutoff exceeds the range of the EAM r tables");
   TDMD_REQUIRE(nrho >= 2 && nr >= 2 && drho > 0.0 && dr > 0.0, "bad spline grid");
   TDMD_REQUIRE(F && rho && phi && d_loss, "null coefficient or loss pointer");
   const bool grad = gF || grho || gphi;

@@ -163,3 +163,41 @@ def test_autograd_wrappers_and_adam(cuda):
     losses, _ = adam_fit(lambda a, b, c: eam_loss(a, b, c, fm, meta), [F, rho, phi], steps=20,
                          lr=1e-4)
     assert losses[-1] < losses[0]
+
+
+def test_eam_gradient_vs_oracle_many_atoms(cuda, oracle):
+    """40,000 atoms (10 snapshots of 10^3 cells): the kernels run with 8
+    lanes per atom here (the small cases above use 32)."""
+    torch = cuda
+    from tdmd_claude_b200.fitting import eam_coeff_tensors, eam_table_meta
+    pos, types, lo, hi, tgt = _snapshots(1, 50, nsnap=10, ncell=10)
+    t, eam = _tables(1)
+    from tdmd_claude_b200 import Box
+    from tdmd_claude_b200.fitting import ForceMatch
+    fm = ForceMatch(pos, types, Box.make(lo, hi), t.cutoff, "fp64")
+    fm.set_targets(tgt)
+    F, rho, phi = eam_coeff_tensors(eam)
+    loss, gF, gr, gp = _eam_gpu(fm, torch, eam_table_meta(eam), F, rho, phi)
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    lo_, oF, orho, ophi = oe.fm_loss_grad(pos, types, lo, hi, tgt)
+    assert abs(loss - lo_) <= 1e-10 * lo_
+    for got, ref in ((gF, oF), (gr, orho), (gp, ophi)):
+        assert np.abs(got[0] - ref[0]).max() <= 1e-9 * np.abs(ref[0]).max()
+
+
+def test_eam_fit_rejects_cutoff_past_tables(cuda):
+    torch = cuda
+    from tdmd_claude_b200 import TdmdError
+    from tdmd_claude_b200.fitting import eam_coeff_tensors, eam_table_meta
+    pos, types, lo, hi, tgt = _snapshots(1, 60)
+    _, eam = _tables(1)
+    fm = _fm(pos, types, lo, hi, "fp64")      # cutoff 5.0 = the tables' end: accepted
+    fm.set_targets(tgt)
+    F, rho, phi = eam_coeff_tensors(eam)
+    _eam_gpu(fm, torch, eam_table_meta(eam), F, rho, phi)
+    from tdmd_claude_b200 import Box
+    from tdmd_claude_b200.fitting import ForceMatch
+    far = ForceMatch(pos, types, Box.make(lo, hi), 5.2, "fp64")
+    far.set_targets(tgt)
+    with pytest.raises(TdmdError):
+        _eam_gpu(far, torch, eam_table_meta(eam), F, rho, phi)

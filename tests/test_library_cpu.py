@@ -188,3 +188,19 @@ def test_batch_rejects_thermostat_and_bad_boxes(L):
                                      C.byref(h)) == 1      # TDMD_ERR_INVALID_ARGUMENT
     assert L.tdmd_batch_create_morse(0, boxes, natoms, C.byref(p), C.byref(make_config()),
                                      C.byref(h)) == 1
+
+
+def test_fit_rejects_bad_arguments(L):
+    import ctypes as C
+    from tdmd_claude_b200 import Box
+    box = Box.make((0, 0, 0), (20, 20, 20))
+    pos = np.zeros((1, 2, 3))
+    pos[0, 1, 0] = 2.5
+    typ = np.ones(2, np.int32)
+    h = C.c_void_p()
+    p, t = pos.ctypes.data_as(C.c_void_p), typ.ctypes.data_as(C.c_void_p)
+    assert L.tdmd_fit_create(0, 2, C.byref(box), p, t, 5.0, 0, C.byref(h)) == 1
+    assert L.tdmd_fit_create(1, 2, C.byref(box), p, t, -1.0, 0, C.byref(h)) == 1
+    assert L.tdmd_fit_create(1, 2, C.byref(box), p, t, 5.0, 7, C.byref(h)) == 1
+    small = Box.make((0, 0, 0), (8, 8, 8))               # edge < 2 cutoff
+    assert L.tdmd_fit_create(1, 2, C.byref(small), p, t, 5.0, 0, C.byref(h)) == 1
