@@ -36,6 +36,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "integrate.cuh"
 
 namespace tdmd_b200 {
 
@@ -604,15 +605,54 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
   }
 }
 
+// The next step's fused kick + drift, applied by a force pass to each atom
+// right after its force: v += dt F/(m mvv2e), x += dt v with the
+// single-image wrap, fixed-point record refreshed (fused_kick_drift_kernel,
+// device_velocity_verlet.cu:88-130, full kick).  Only for a force pass that
+// reads gather records, never the positions it updates.
+struct KickDrift {
+  double4* pos4;
+  int4* q;
+  double* v;
+  const int* types;
+  const double* inv_mm;  // 1 / (m mvv2e) per type
+  double dt;
+  long long* step;       // device step counter, +1 per kick-drift
+  DevBox b;
+};
+
+__device__ __forceinline__ void kick_drift_atom(const KickDrift& k, int i, float fx, float fy,
+                                                float fz) {
+  const int t = __ldg(k.types + i);
+  const double factor = k.dt * __ldg(k.inv_mm + t);
+  double vx = k.v[3ll * i], vy = k.v[3ll * i + 1], vz = k.v[3ll * i + 2];
+  vx += factor * static_cast<double>(fx);
+  vy += factor * static_cast<double>(fy);
+  vz += factor * static_cast<double>(fz);
+  double4 p = k.pos4[i];
+  p.x = wrap_single(p.x + k.dt * vx, k.b.lo[0], k.b.L[0], k.b.periodic[0]);
+  p.y = wrap_single(p.y + k.dt * vy, k.b.lo[1], k.b.L[1], k.b.periodic[1]);
+  p.z = wrap_single(p.z + k.dt * vz, k.b.lo[2], k.b.L[2], k.b.periodic[2]);
+  k.v[3ll * i] = vx;
+  k.v[3ll * i + 1] = vy;
+  k.v[3ll * i + 2] = vz;
+  k.pos4[i] = p;
+  k.q[i] = make_int4(encode_q(p.x, k.b.qlo[0], k.b.qinv[0]), encode_q(p.y, k.b.qlo[1], k.b.qinv[1]),
+                     encode_q(p.z, k.b.qlo[2], k.b.qinv[2]), t);
+}
+
 // Pass 3: f_ij = -(phi' + fp_i rho'_tj + fp_j rho'_ti)/r * (r_i - r_j).
 // FPG: F'(rho_j) comes with the neighbor's gather record (pair w bits)
-// instead of the fp array.
-template <class Geo, int LPA, bool EV, bool FPG, bool VEC, bool MULTI, class FP, class F>
+// instead of the fp array.  KD (FPG, float forces): then the next step's
+// kick + drift of the same atom.
+template <class Geo, int LPA, bool EV, bool FPG, bool VEC, bool MULTI, class FP, class F,
+          bool KD = false>
 __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
                                                    EamDev<typename Geo::T> e,
                                                    const int* __restrict__ types,
                                                    const FP* __restrict__ fp, ForceOut<F> out,
-                                                   double* __restrict__ partials) {
+                                                   double* __restrict__ partials,
+                                                   KickDrift kd = {}) {
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;
@@ -676,7 +716,15 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
     fy.shfl_merge(s);
     fz.shfl_merge(s);
   }
-  if (active && sub == 0) out.store(i, fx.value(), fy.value(), fz.value());
+  if (active && sub == 0) {
+    out.store(i, fx.value(), fy.value(), fz.value());
+    if constexpr (KD) {
+      static_assert(FPG && sizeof(F) == sizeof(float), "fused kick-drift: mixed gather pass");
+      kick_drift_atom(kd, i, static_cast<float>(fx.value()), static_cast<float>(fy.value()),
+                      static_cast<float>(fz.value()));
+    }
+  }
+  if (KD && blockIdx.x == 0 && threadIdx.x == 0) *kd.step += 1;
   if (EV) write_ev_partials(pe, w, partials);
 }
 

@@ -83,18 +83,29 @@ void launch_eam_density(const Geo& g, const NbrView& nl, int n,
 }
 
 // Force pass.  FPG: the geometry reads gather records that carry F'(rho).
+// kd (nullable; FPG with float forces only): also apply the next step's
+// kick + drift to each atom after its force.
 template <class Geo, bool FPG, class FP, class F>
 void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typename Geo::T>& e,
                       const int* types, const FP* fp, F* forces, bool ev, double* partials,
-                      int lpa, cudaStream_t s) {
+                      int lpa, cudaStream_t s, const KickDrift* kd = nullptr) {
   const int nblk = force_blocks(n, lpa);
   TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
     if (ev)
       k_eam_force<Geo, L, true, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, partials);
-    else
+    else if constexpr (FPG && sizeof(F) == sizeof(float)) {
+      if (kd)
+        k_eam_force<Geo, L, false, FPG, V, M, FP, F, true><<<nblk, kForceThreads, 0, s>>>(
+            g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr, *kd);
+      else
+        k_eam_force<Geo, L, false, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+            g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
+    } else {
+      TDMD_REQUIRE(kd == nullptr, "fused kick-drift needs the mixed gather-record pass");
       k_eam_force<Geo, L, false, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
+    }
   })));
   TDMD_LAUNCH_CHECK();
 }

@@ -40,10 +40,12 @@ struct CtlParams {
 };
 
 struct StepPlan {
-  bool first;    // first step of the run_until window
-  bool last;     // last step of the window
-  bool rebuild;  // neighbor rebuild after this step's drift
-  bool ev;       // energy-log step
+  bool first;      // first step of the run_until window
+  bool last;       // last step of the window
+  bool rebuild;    // neighbor rebuild after this step's drift
+  bool ev;         // energy-log step
+  bool kd_fused;   // this step's kick + drift ran inside the previous force pass
+  bool fuse_next;  // this step's force pass also kicks and drifts for the next step
 };
 
 enum ProfCat : int {
@@ -106,7 +108,10 @@ class Scheduler {
   void grow_capacity(int max_count);
   void initial_forces();
   void enqueue_rebuild();
-  void enqueue_force(bool ev);
+  // kd: the force pass also applies the next step's full kick + drift
+  // (mixed EAM, NVE; the force pass reads gather records, not positions).
+  void enqueue_force(bool ev, bool kd = false);
+  bool can_fuse_kick() const { return mixed_ && kind_ == TDMD_POT_EAM && !thermo_; }
   template <class F>
   void enqueue_kick_drift_t(F* f, bool full, bool scale);
   void enqueue_kick_drift(bool full, bool scale);

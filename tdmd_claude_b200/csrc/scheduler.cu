@@ -523,7 +523,8 @@ void Scheduler::enqueue_rebuild() {
 }
 
 // ----- forces ---------------------------------------------------------------
-void Scheduler::enqueue_force(bool ev) {
+void Scheduler::enqueue_force(bool ev, bool kd) {
+  TDMD_REQUIRE(!kd || can_fuse_kick(), "fused kick-drift needs the mixed EAM NVE path");
   cudaStream_t s = stream_;
   const NbrView nl{nbr_.data(), nullptr, cnt_.data(), cap_};
   const int nblk = force_blocks(n_, lpa_);
@@ -554,8 +555,14 @@ void Scheduler::enqueue_force(bool ev) {
                                       nullptr, g_.data(), ev, part, lpa_, s);
       prof_end(kProfDensity);
       prof_begin(kProfForce);
+      const KickDrift kdr{pos4_.data(), q_.data(), vel_.data(), types_.data(), inv_mm_.data(),
+                          cfg_.dt,
+                          reinterpret_cast<long long*>(reinterpret_cast<char*>(ctl_.data()) +
+                                                       offsetof(SchedCtl, step)),
+                          box_};
       launch_eam_force<GeoQ, true, float, float>(gg, nl, n_, eam_->d32, types, fp32_.data(),
-                                                 f32_.data(), ev, part2, lpa_, s);
+                                                 f32_.data(), ev, part2, lpa_, s,
+                                                 kd ? &kdr : nullptr);
       prof_end(kProfForce);
     } else {
       GeoD4 g{pos4_.data(), {box_.L[0], box_.L[1], box_.L[2]},
@@ -697,9 +704,9 @@ void Scheduler::enqueue_apply_scale() {
 // One step as planned (see plan_steps): the kernels of the step.
 void Scheduler::enqueue_step(const StepPlan& st) {
   if (!thermo_) {
-    enqueue_kick_drift(/*full=*/!st.first, /*scale=*/false);
+    if (!st.kd_fused) enqueue_kick_drift(/*full=*/!st.first, /*scale=*/false);
     if (st.rebuild) enqueue_rebuild();
-    enqueue_force(st.ev);
+    enqueue_force(st.ev, st.fuse_next);
     if (st.ev) enqueue_log_nve();
   } else {
     if (st.first) {
@@ -734,7 +741,8 @@ void Scheduler::run_segment(const std::vector<StepPlan>& seg, bool finalize) {
   std::vector<int> key;
   key.reserve(seg.size() + 1);
   for (const auto& st : seg)
-    key.push_back((st.first ? 1 : 0) | (st.rebuild ? 2 : 0) | (st.ev ? 4 : 0) | (st.last ? 8 : 0));
+    key.push_back((st.first ? 1 : 0) | (st.rebuild ? 2 : 0) | (st.ev ? 4 : 0) | (st.last ? 8 : 0) |
+                  (st.kd_fused ? 16 : 0) | (st.fuse_next ? 32 : 0));
   key.push_back(finalize ? 1 : 0);
   const long long l0 = launches_;
   if (!cfg_.use_graphs || profiling_) {
@@ -794,6 +802,10 @@ std::vector<StepPlan> Scheduler::plan_steps(int target, int* since_out) const {
     if (st.rebuild) since = 0;
     ++since;
     st.ev = cfg_.energy_every > 0 && ((s + 1) % cfg_.energy_every == 0);
+    // Mixed EAM NVE: a force pass that logs no energy and is followed by
+    // another step of the window also kicks and drifts for that step.
+    st.fuse_next = can_fuse_kick() && !st.ev && !st.last;
+    st.kd_fused = !plan.empty() && plan.back().fuse_next;
     plan.push_back(st);
   }
   *since_out = since;

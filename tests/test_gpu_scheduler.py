@@ -274,3 +274,26 @@ def test_autotune_keeps_forces(cuda, precision):
     assert rel_rms(f1, f0) < (1e-13 if precision == "fp64" else 1e-6)
     s.run_until(20)
     assert s.current_step() == 20
+
+
+@pytest.mark.parametrize("use_graphs", [True, False])
+def test_mixed_eam_fused_kick_equals_unfused(cuda, use_graphs):
+    """Mixed EAM NVE fuses the next step's kick + drift into the force pass
+    except on energy-log steps.  Logging every step (nothing fused) and
+    logging never (all but window-end steps fused) give bit-identical
+    trajectories; a log every 5 steps carries the right step numbers."""
+    runs = []
+    for every in (0, 1, 5):
+        s, sysm, _ = _eam_setup("mixed", ncell=5, lanes_per_atom=4, use_graphs=use_graphs,
+                                energy_every=every, energy_log_capacity=64)
+        for t in (7, 20, 33):
+            s.run_until(t)
+        st = s.download()
+        runs.append((st.positions, st.velocities, st.forces))
+        if every == 5:
+            log = s.energy_log()
+            assert np.array_equal(log[:, 0], np.arange(5, 31, 5))
+        s.close()
+    for k in range(3):
+        assert np.array_equal(runs[0][k], runs[1][k])
+        assert np.array_equal(runs[0][k], runs[2][k])
