@@ -157,7 +157,7 @@ struct RowSmem {
 
 // Rows of the atoms of cell c of box b's grid; cell_start / cell_count index
 // that grid's cells, cell_atoms and the atom indices are global.
-template <class Load, bool WRAP>
+template <class Load, bool WRAP, bool WRITE>
 __device__ __forceinline__ void build_cell_rows(
     RowSmem& sm, Load pos, const DevBox& b, int c, const int* __restrict__ cell_start,
     const int* __restrict__ cell_count, const int* __restrict__ cell_atoms, double rl2,
@@ -191,7 +191,11 @@ __device__ __forceinline__ void build_cell_rows(
   }
   __syncthreads();
   const int total = s_pre[27];
-  const bool staged = total <= kStageCap;
+  // Staged records are padded to whole 32-candidate sweeps with sentinels
+  // far outside any box (their r^2 overflows to +inf and fails both the
+  // filter and the band), so the staged sweep needs no bounds select.
+  const int padded = (total + 31) & ~31;
+  const bool staged = padded <= kStageCap;
   // Fixed-point lower corner of the center cell.
   const int ox = encode_q(b.lo[0] + ix * b.cs[0], b.qlo[0], b.qinv[0]);
   const int oy = encode_q(b.lo[1] + iy * b.cs[1], b.qlo[1], b.qinv[1]);
@@ -213,6 +217,8 @@ __device__ __forceinline__ void build_cell_rows(
   };
   if (staged) {
     for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = record(k);
+    for (int k = total + threadIdx.x; k < padded; k += kRowThreads)
+      stage[k] = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
   }
   __syncthreads();
   const float Lx = static_cast<float>(b.L[0]), Ly = static_cast<float>(b.L[1]),
@@ -223,7 +229,8 @@ __device__ __forceinline__ void build_cell_rows(
   int wmax = 0;  // lane 0: this warp's longest row
   // One sweep per candidate source: staged records (the hot path) or
   // records rebuilt on the fly, so the hot loop carries no second path.
-  auto sweep = [&](auto cand) {
+  auto sweep = [&](auto cand, auto padded_tag) {
+    constexpr bool kPadded = decltype(padded_tag)::value;
     for (int a = warp; a < ncen; a += kRowThreads / 32) {
       const float4 ci = cand(c0 + a);
       const int i = __float_as_int(ci.w);
@@ -233,7 +240,8 @@ __device__ __forceinline__ void build_cell_rows(
       int cnt = 0;
       for (int k0 = 0; k0 < total; k0 += 32) {
         const int k = k0 + lane;
-        const float4 cj = cand(k < total ? k : c0 + a);  // past the end: atom i itself
+        // past the end: a sentinel (staged) or atom i itself (rebuilt records)
+        const float4 cj = cand(kPadded ? k : (k < total ? k : c0 + a));
         const int j = __float_as_int(cj.w);
         float dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
         if (WRAP) {
@@ -247,7 +255,7 @@ __device__ __forceinline__ void build_cell_rows(
                                          b.halfL[1], b.halfL[2], b.periodic[0], b.periodic[1],
                                          b.periodic[2]);
         const unsigned m = __ballot_sync(0xffffffffu, pred);
-        if (pred && nbr) {
+        if (WRITE && pred) {
           const int p = cnt + __popc(m & lt_mask);
           if (p < limit) nbr[base + p] = j;
         }
@@ -260,9 +268,9 @@ __device__ __forceinline__ void build_cell_rows(
     }
   };
   if (staged)
-    sweep([&](int k) { return stage[k]; });
+    sweep([&](int k) { return stage[k]; }, std::true_type{});
   else
-    sweep(record);
+    sweep(record, std::false_type{});
   // Status: one atomic per CTA, and only when something needs reporting --
   // the maximum for a sizing (count-only) pass, the overflow flag when a
   // padded row is too short.
@@ -273,27 +281,28 @@ __device__ __forceinline__ void build_cell_rows(
     if (threadIdx.x == 0) {
       int m = 0;
       for (int w = 0; w < kRowThreads / 32; ++w) m = s_max[w] > m ? s_max[w] : m;
-      const bool overflow = !row_off && nbr && m > cap;
+      const bool overflow = WRITE && !row_off && m > cap;
       if (overflow) atomicOr(&status[0], 1);
-      if (overflow || !nbr) atomicMax(&status[1], m);
+      if (overflow || !WRITE) atomicMax(&status[1], m);
     }
   }
 }
 
-template <class Load, bool WRAP>
+template <class Load, bool WRAP, bool WRITE>
 __global__ void __launch_bounds__(kRowThreads) k_build_cells(
     Load pos, DevBox b, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const int* __restrict__ cell_atoms, double rl2, float lo_f, float hi_f, int* __restrict__ nbr,
     const int* __restrict__ row_off, int cap, int* __restrict__ counts,
     int* __restrict__ status) {
   __shared__ RowSmem sm;
-  build_cell_rows<Load, WRAP>(sm, pos, b, blockIdx.x, cell_start, cell_count, cell_atoms, rl2,
-                              lo_f, hi_f, nbr, row_off, cap, counts, status);
+  build_cell_rows<Load, WRAP, WRITE>(sm, pos, b, blockIdx.x, cell_start, cell_count, cell_atoms,
+                                     rl2, lo_f, hi_f, nbr, row_off, cap, counts, status);
 }
 
 // Batched replicas: one CTA per cell of any replica (cells of replica r are
 // global cells [cell0, cell0 + ncells)); the replica's box, filter band and
 // 3-cell-axis flag come from its descriptor.
+template <bool WRITE>
 __global__ void __launch_bounds__(kRowThreads) k_build_cells_batch(
     LoadD4 pos, const RepDesc* __restrict__ reps, const int* __restrict__ cell_rep,
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
@@ -305,11 +314,11 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells_batch(
   if (threadIdx.x == 0) d = reps[__ldg(cell_rep + gc)];
   __syncthreads();
   if (d.wrap)
-    build_cell_rows<LoadD4, true>(sm, pos, d.box, gc - d.cell0, cell_start + d.cell0,
+    build_cell_rows<LoadD4, true, WRITE>(sm, pos, d.box, gc - d.cell0, cell_start + d.cell0,
                                   cell_count + d.cell0, cell_atoms, rl2, d.lo_f, d.hi_f, nbr,
                                   nullptr, cap, counts, status);
   else
-    build_cell_rows<LoadD4, false>(sm, pos, d.box, gc - d.cell0, cell_start + d.cell0,
+    build_cell_rows<LoadD4, false, WRITE>(sm, pos, d.box, gc - d.cell0, cell_start + d.cell0,
                                    cell_count + d.cell0, cell_atoms, rl2, d.lo_f, d.hi_f, nbr,
                                    nullptr, cap, counts, status);
 }
@@ -424,9 +433,14 @@ void build_neighbor_rows_batch(const CellListDev& cl, const double4* pos, const 
                                const int* cell_rep, double r_list_sq, int* nbr, int cap,
                                int* counts, int* status, cudaStream_t stream) {
   if (cl.natoms == 0 || cl.ncells == 0) return;
-  k_build_cells_batch<<<cl.ncells, kRowThreads, 0, stream>>>(
-      LoadD4{pos}, reps, cell_rep, cl.cell_start.data(), cl.cell_count.data(),
-      cl.cell_atoms.data(), r_list_sq, nbr, cap, counts, status);
+  if (nbr)
+    k_build_cells_batch<true><<<cl.ncells, kRowThreads, 0, stream>>>(
+        LoadD4{pos}, reps, cell_rep, cl.cell_start.data(), cl.cell_count.data(),
+        cl.cell_atoms.data(), r_list_sq, nbr, cap, counts, status);
+  else
+    k_build_cells_batch<false><<<cl.ncells, kRowThreads, 0, stream>>>(
+        LoadD4{pos}, reps, cell_rep, cl.cell_start.data(), cl.cell_count.data(),
+        cl.cell_atoms.data(), r_list_sq, nullptr, cap, counts, status);
   TDMD_LAUNCH_CHECK();
 }
 
@@ -440,9 +454,14 @@ void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout lay
   row_filter_band(box, r_list_sq, &lo_f, &hi_f, &wrap);
   auto go = [&](auto load, auto wrap_tag) {
     constexpr bool W = decltype(wrap_tag)::value;
-    k_build_cells<decltype(load), W><<<cl.ncells, kRowThreads, 0, stream>>>(
-        load, box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
-        lo_f, hi_f, nbr, row_off, cap, counts, status);
+    if (nbr)
+      k_build_cells<decltype(load), W, true><<<cl.ncells, kRowThreads, 0, stream>>>(
+          load, box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
+          lo_f, hi_f, nbr, row_off, cap, counts, status);
+    else
+      k_build_cells<decltype(load), W, false><<<cl.ncells, kRowThreads, 0, stream>>>(
+          load, box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
+          lo_f, hi_f, nullptr, row_off, cap, counts, status);
   };
   if (layout == PosLayout::AoS3) {
     const LoadAoS3 ld{static_cast<const double*>(d_pos)};
