@@ -815,13 +815,36 @@ std::vector<StepPlan> Scheduler::plan_steps(int target, int* since_out) const {
 void Scheduler::initial_forces() {
   const bool prof = profiling_;
   profiling_ = false;  // timing covers the steps of run_until windows only
-  size_neighbor_list();
   cudaStream_t s = stream_;
+  const double rl2 = (cutoff_ + cfg_.r_skin) * (cutoff_ + cfg_.r_skin);
+  // The first upload sizes the rows with a count pass; later uploads reuse
+  // the capacity and fill directly, counting a second fill only when a row
+  // did not fit.
+  int passes = 1;
+  const bool reuse = cap_ > 0;
+  if (reuse) {
+    build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, s);
+    cnt_.reserve(static_cast<size_t>(n_));
+  } else {
+    size_neighbor_list();
+    ++passes;
+  }
   TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
-  build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_,
-                      (cutoff_ + cfg_.r_skin) * (cutoff_ + cfg_.r_skin), nbr_.data(), nullptr,
+  build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl2, nbr_.data(), nullptr,
                       cap_, cnt_.data(), ctl_status(), s);
-  launches_ += cell_list_kernels() + 2;  // cell list + count pass + fill pass
+  if (reuse) {
+    int st[4];
+    TDMD_CU(cudaMemcpyAsync(st, ctl_status(), sizeof(st), cudaMemcpyDeviceToHost, s));
+    TDMD_CU(cudaStreamSynchronize(s));
+    if (st[0]) {
+      grow_capacity(st[1]);
+      TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
+      build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl2, nbr_.data(), nullptr,
+                          cap_, cnt_.data(), ctl_status(), s);
+      ++passes;
+    }
+  }
+  launches_ += cell_list_kernels() + passes;  // cell list + (count pass) + fill pass(es)
   ++rebuilds_;
   since_rebuild_ = 0;
   enqueue_force(false);

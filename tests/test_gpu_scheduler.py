@@ -297,3 +297,26 @@ def test_mixed_eam_fused_kick_equals_unfused(cuda, use_graphs):
     for k in range(3):
         assert np.array_equal(runs[0][k], runs[1][k])
         assert np.array_equal(runs[0][k], runs[2][k])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_reupload_reuses_or_grows_rows(cuda, precision):
+    """A second upload fills the rows into the capacity sized by the first;
+    when a row no longer fits (a denser state) it grows and refills.  Forces
+    equal those of a fresh scheduler on the same state."""
+    s, sysm, _ = _eam_setup(precision, ncell=6, lanes_per_atom=4)
+    s.run_until(0)
+    cap0 = s.stats().nlist_capacity
+    # squeeze the atoms into 75 % of the box: 134 neighbors within r_list
+    # on the ideal lattice, past the capacity the first state sized
+    lo = np.array(sysm.lo)
+    dense = lo + 0.75 * (sysm.positions - lo)
+    for pos in (sysm.positions, dense):
+        s.upload(pos, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+        s.run_until(0)
+        fresh, _, _ = _eam_setup(precision, ncell=6, lanes_per_atom=4)
+        fresh.upload(pos, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+        fresh.run_until(0)
+        assert np.array_equal(s.download().forces, fresh.download().forces)
+        fresh.close()
+    assert s.stats().nlist_capacity > cap0
