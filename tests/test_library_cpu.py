@@ -204,3 +204,21 @@ def test_fit_rejects_bad_arguments(L):
     assert L.tdmd_fit_create(1, 2, C.byref(box), p, t, 5.0, 7, C.byref(h)) == 1
     small = Box.make((0, 0, 0), (8, 8, 8))               # edge < 2 cutoff
     assert L.tdmd_fit_create(1, 2, C.byref(small), p, t, 5.0, 0, C.byref(h)) == 1
+
+
+def test_standalone_banner_usage_and_argument_errors():
+    """The tdmd_standalone command line (no GPU needed for these paths)."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "tdmd_claude_b200", "bin", "tdmd_standalone")
+    run = lambda *a: subprocess.run([sys.executable, exe, *a], capture_output=True,  # noqa: E731
+                                    text=True, timeout=120)
+    out = run("--help")
+    assert out.returncode == 0 and "--data <file>" in out.stdout
+    out = run()
+    assert out.returncode == 0 and "Use --data <file>" in out.stdout
+    out = run("--morse", "1,2")
+    assert out.returncode == 1 and "D,alpha,r0,rc" in out.stderr
+    out = run("--precision", "fp16")
+    assert out.returncode == 1
