@@ -118,10 +118,24 @@ struct PairF {
   double r2d;  // FP64 r^2
 };
 
+// res: the FP64 r^2 of the exact fixed-point delta minus r2, rounded to
+// float -- all that the radius refinement needs of the delta, so a pair in
+// flight holds six words instead of eight.
 struct PairQ {
   float dx, dy, dz, r2;
-  int ix, iy, iz, w;  // exact fixed-point delta and the neighbor's 4th word
+  float res;
+  int w;  // the neighbor's 4th word
 };
+
+// |r| and 1/|r| in FP32 and the FP64-refined radius from a PairQ: with
+// r = sqrt(r2) in FP32, r2d - r*r = res + (r2 - r*r), the second term exact
+// by FMA; one Newton step rd = r + (r2d - r*r) / (2r).
+__device__ __forceinline__ void radius_q(float r2, float res, float& r, float& rinv, double& rd) {
+  rinv = rsqrtf(r2);
+  r = r2 * rinv;
+  const float corr = (res + fmaf(-r, r, r2)) * 0.5f * rinv;
+  rd = static_cast<double>(r) + static_cast<double>(corr);
+}
 
 __device__ __forceinline__ void radius_f(float r2, double r2d, float& r, float& rinv, double& rd) {
   rinv = rsqrtf(r2);
@@ -237,19 +251,19 @@ struct GeoQ {
   __device__ __forceinline__ Own own(int i) const { return __ldg(q + i); }
   __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
     const int4 b = __ldg(q + j);
-    pr.ix = o.x - b.x;
-    pr.iy = o.y - b.y;
-    pr.iz = o.z - b.z;
+    const int ix = o.x - b.x, iy = o.y - b.y, iz = o.z - b.z;
     pr.w = b.w;
-    pr.dx = __fmul_rn(__int2float_rn(pr.ix), s[0]);
-    pr.dy = __fmul_rn(__int2float_rn(pr.iy), s[1]);
-    pr.dz = __fmul_rn(__int2float_rn(pr.iz), s[2]);
+    pr.dx = __fmul_rn(__int2float_rn(ix), s[0]);
+    pr.dy = __fmul_rn(__int2float_rn(iy), s[1]);
+    pr.dz = __fmul_rn(__int2float_rn(iz), s[2]);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
+    const double x = ix, y = iy, z = iz;
+    pr.res = static_cast<float>(x * x * s2[0] + y * y * s2[1] + z * z * s2[2] -
+                                static_cast<double>(pr.r2));
   }
   __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
                                          double& rd) const {
-    const double x = pr.ix, y = pr.iy, z = pr.iz;
-    radius_f(pr.r2, x * x * s2[0] + y * y * s2[1] + z * z * s2[2], r, rinv, rd);
+    radius_q(pr.r2, pr.res, r, rinv, rd);
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
 };

@@ -43,19 +43,19 @@ struct GeoQB {
   }
   __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
     const int4 b = __ldg(q + j);
-    pr.ix = o.q.x - b.x;
-    pr.iy = o.q.y - b.y;
-    pr.iz = o.q.z - b.z;
+    const int ix = o.q.x - b.x, iy = o.q.y - b.y, iz = o.q.z - b.z;
     pr.w = b.w;
-    pr.dx = __fmul_rn(__int2float_rn(pr.ix), o.s0);
-    pr.dy = __fmul_rn(__int2float_rn(pr.iy), o.s1);
-    pr.dz = __fmul_rn(__int2float_rn(pr.iz), o.s2);
+    pr.dx = __fmul_rn(__int2float_rn(ix), o.s0);
+    pr.dy = __fmul_rn(__int2float_rn(iy), o.s1);
+    pr.dz = __fmul_rn(__int2float_rn(iz), o.s2);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
+    const double x = ix, y = iy, z = iz;
+    pr.res = static_cast<float>(x * x * o.t0 + y * y * o.t1 + z * z * o.t2 -
+                                static_cast<double>(pr.r2));
   }
-  __device__ __forceinline__ void radius(const Own& o, const Pair& pr, T& r, T& rinv,
+  __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
                                          double& rd) const {
-    const double x = pr.ix, y = pr.iy, z = pr.iz;
-    radius_f(pr.r2, x * x * o.t0 + y * y * o.t1 + z * z * o.t2, r, rinv, rd);
+    radius_q(pr.r2, pr.res, r, rinv, rd);
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
 };
