@@ -305,8 +305,16 @@ int32_t tdmd_sched_thermostat_state(const tdmd_sched* s, double* dt, double* eta
                                     double* eta_v);
 /* Device pointers of the scheduler's state (for zero-copy callers):
  * positions as double4[n] {x,y,z,type}, velocities double[3n], forces
- * (double or float)[3n]; valid until the next upload/destroy. */
+ * (double or float)[3n]; valid until the next upload/destroy.  The arrays
+ * are in the scheduler's internal atom order (see tdmd_sched_atom_order). */
 int32_t tdmd_sched_device_state(tdmd_sched* s, void** d_pos4, double** d_vel, void** d_forces);
+/* No reference counterpart.  The scheduler holds the atoms in the cell
+ * order of the uploaded positions, so that an atom's neighbors sit at
+ * nearby indices whatever order the caller used; *d_order (device
+ * int32[n]) gives, for each internal index, the caller's index.  Neighbor
+ * rows and results are those of the caller's order (cells list their atoms
+ * by the caller's index); upload and download convert. */
+int32_t tdmd_sched_atom_order(const tdmd_sched* s, const int32_t** d_order);
 /* Per-kernel timing (no reference counterpart; the reference profiles only
  * from outside with nsys/ncu).  While on, windows run without graph replay
  * and CUDA events on the scheduler's stream bracket each phase; averages in

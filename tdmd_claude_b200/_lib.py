@@ -138,6 +138,7 @@ SIGNATURES = {
     "tdmd_sched_energy_log": [_p, _p, _i32, _pi32],
     "tdmd_sched_thermostat_state": [_p, _pf64, _p, _p],
     "tdmd_sched_device_state": [_p, _pp, _pp, _pp],
+    "tdmd_sched_atom_order": [_p, _pp],
     "tdmd_sched_stream": [_p, _pp],
     "tdmd_batch_create_morse": [_i32, C.POINTER(Box), _p, C.POINTER(MorseParams),
                                 C.POINTER(FastPipelineConfig), _pp],

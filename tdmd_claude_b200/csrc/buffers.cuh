@@ -83,9 +83,11 @@ int device_scan_launches(long long n);
 enum class PosLayout { AoS3, D4 };
 
 // Builds the cell list of n atoms (positions on the device, laid out per
-// `layout`) on `stream`.  Grid and cell size come from `box`.
+// `layout`) on `stream`.  Grid and cell size come from `box`.  Atoms within
+// a cell are ordered by index, or by key[index] when key is given (arrays
+// held in an internal order; key[i] = the caller's index of atom i).
 void build_cell_list(CellListDev& cl, const void* d_pos, PosLayout layout, long long n,
-                     const DevBox& box, cudaStream_t stream);
+                     const DevBox& box, cudaStream_t stream, const int* key = nullptr);
 
 // Neighbor list build over a built cell list.
 //   row_off == nullptr: padded rows, entry k of atom i at nbr[i*cap + k];

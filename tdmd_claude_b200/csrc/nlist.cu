@@ -75,9 +75,12 @@ __global__ void k_scatter_atoms(const int* __restrict__ atom_cell, int n,
 
 // Restores ID-ascending order inside each cell: one warp per cell, rank
 // sort through shuffles for cells of up to 32 atoms (a lane's rank is the
-// number of smaller ids), lane-0 insertion sort beyond that.
+// number of smaller ids), lane-0 insertion sort beyond that.  key (nullable)
+// gives each array index its ID when the arrays are held in another order
+// than the caller's (the scheduler's cell-ordered layout); keys are unique.
 __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __restrict__ cell_count,
-                             int ncells, int* __restrict__ cell_atoms) {
+                             int ncells, int* __restrict__ cell_atoms,
+                             const int* __restrict__ key) {
   const long long gw = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (gw >= ncells) return;  // uniform per warp
@@ -86,17 +89,19 @@ __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __re
   const int m = cell_count[c];
   if (m <= 32) {
     const int v = lane < m ? a[lane] : INT_MAX;
+    const int kv = lane < m ? (key ? __ldg(key + v) : v) : INT_MAX;
     int rank = 0;
 #pragma unroll
-    for (int k = 0; k < 32; ++k) rank += __shfl_sync(0xffffffffu, v, k) < v ? 1 : 0;
+    for (int k = 0; k < 32; ++k) rank += __shfl_sync(0xffffffffu, kv, k) < kv ? 1 : 0;
     if (lane < m) a[rank] = v;
     return;
   }
   if (lane == 0) {
     for (int k = 1; k < m; ++k) {
       const int v = a[k];
+      const int kv = key ? __ldg(key + v) : v;
       int j = k - 1;
-      while (j >= 0 && a[j] > v) {
+      while (j >= 0 && (key ? __ldg(key + a[j]) : a[j]) > kv) {
         a[j + 1] = a[j];
         --j;
       }
@@ -344,7 +349,7 @@ __global__ void k_bin_atoms_batch(LoadD4 pos, const int* __restrict__ rep,
 }  // namespace
 
 void build_cell_list(CellListDev& cl, const void* d_pos, PosLayout layout, long long n,
-                     const DevBox& box, cudaStream_t stream) {
+                     const DevBox& box, cudaStream_t stream, const int* key) {
   TDMD_REQUIRE(n >= 0 && n < INT_MAX, "atom count out of range");
   const long long ncells = 1ll * box.nc[0] * box.nc[1] * box.nc[2];
   TDMD_REQUIRE(ncells < INT_MAX / 2, "cell grid too large");
@@ -380,7 +385,7 @@ void build_cell_list(CellListDev& cl, const void* d_pos, PosLayout layout, long 
   k_sort_cells<<<ceil_div(ncells * 32, 256), 256, 0, stream>>>(cl.cell_start.data(),
                                                                 cl.cell_count.data(),
                                                                 static_cast<int>(ncells),
-                                                                cl.cell_atoms.data());
+                                                                cl.cell_atoms.data(), key);
   TDMD_LAUNCH_CHECK();
 }
 
@@ -425,7 +430,7 @@ void build_cell_list_batch(CellListDev& cl, const double4* pos, const int* rep,
                                           cl.cursor.data(), cl.cell_atoms.data());
   TDMD_LAUNCH_CHECK();
   k_sort_cells<<<ceil_div(1ll * ncells_total * 32, 256), 256, 0, stream>>>(
-      cl.cell_start.data(), cl.cell_count.data(), ncells_total, cl.cell_atoms.data());
+      cl.cell_start.data(), cl.cell_count.data(), ncells_total, cl.cell_atoms.data(), nullptr);
   TDMD_LAUNCH_CHECK();
 }
 

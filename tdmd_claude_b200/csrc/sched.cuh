@@ -95,6 +95,7 @@ class Scheduler {
   // its enqueued work), ms.
   double last_window_ms() const { return last_window_ms_; }
   void kernel_times(double* avg_ms, long long* counts, int ncat) const;
+  const int* atom_order() const { return order_.data(); }
   void device_state(void** pos4, double** vel, void** forces) {
     if (pos4) *pos4 = pos4_.data();
     if (vel) *vel = vel_.data();
@@ -135,6 +136,10 @@ class Scheduler {
   void prof_collect();
   // bin + scan + scatter + sort
   int cell_list_kernels() const { return 3 + device_scan_launches(cl_.ncells); }
+  void reorder_by_cell();
+  void build_cells() {
+    build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, stream_, order_.data());
+  }
   int* ctl_status() const {
     return reinterpret_cast<int*>(reinterpret_cast<char*>(ctl_.data()) +
                                   offsetof(SchedCtl, status));
@@ -167,6 +172,13 @@ class Scheduler {
   DevArray<double> inv_mm_;  // 1 / (m mvv2e) per type: the kick factor per unit dt
   DevArray<int4> g_;         // mixed EAM: {qx, qy, qz, bits(F'(rho))} per atom
   mutable DevArray<double> stage_;
+  // Atoms are held in the cell order of the uploaded positions (neighbors of
+  // an atom then sit at nearby indices, whatever order the caller used);
+  // order_[k] is the caller's index of internal atom k.  Cell lists sort
+  // their members by that index, so every neighbor row lists the same atoms
+  // in the same order as without the reordering.
+  DevArray<int> order_;
+  DevArray<double4> perm_tmp_;
   int n_types_ = 0;
 
   // Neighbor list: padded rows of cap_ entries.

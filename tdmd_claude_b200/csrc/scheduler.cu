@@ -23,6 +23,7 @@
 // overflow the window is re-run from a device snapshot with a larger
 // capacity), and all energy/virial sums are fixed-order FP64 reductions.
 #include <algorithm>
+#include <type_traits>
 #include <climits>
 #include <cmath>
 #include <list>
@@ -62,13 +63,39 @@ __global__ void k_pack_positions(const double* __restrict__ x, const int* __rest
                      encode_q(pz, b.qlo[2], b.qinv[2]), t);
 }
 
-__global__ void k_unpack_positions(const double4* __restrict__ pos4, int n, double* __restrict__ x) {
+
+struct D3 {
+  double x, y, z;
+};
+struct F3 {
+  float x, y, z;
+};
+
+// dst[i] = src[idx[i]]
+template <class T>
+__global__ void k_gather(const T* __restrict__ src, const int* __restrict__ idx, int n,
+                         T* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[idx[i]];
+}
+
+// dst[idx[i]] = src[i]
+template <class T>
+__global__ void k_scatter(const T* __restrict__ src, const int* __restrict__ idx, int n,
+                          T* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[idx[i]] = src[i];
+}
+
+__global__ void k_scatter_positions(const double4* __restrict__ pos4, const int* __restrict__ idx,
+                                    int n, double* __restrict__ x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 p = pos4[i];
-  x[3ll * i] = p.x;
-  x[3ll * i + 1] = p.y;
-  x[3ll * i + 2] = p.z;
+  const long long k = idx[i];
+  x[3 * k] = p.x;
+  x[3 * k + 1] = p.y;
+  x[3 * k + 2] = p.z;
 }
 
 // Kick (half or full dt, optionally after the pending NHC scale) + drift +
@@ -418,6 +445,7 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
     k_pack_positions<<<ceil_div(n_, kThreads), kThreads, 0, s>>>(
         stage_.data(), types_.data(), n_, box_, pos4_.data(), mixed_ ? q_.data() : nullptr);
     TDMD_LAUNCH_CHECK();
+    reorder_by_cell();
   }
   TDMD_CU(cudaMemcpyAsync(masses_.data(), masses, sizeof(double) * n_types,
                           cudaMemcpyHostToDevice, s));
@@ -459,34 +487,74 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
   since_rebuild_ = 0;
 }
 
+// Permutes the uploaded state into the cell order of its positions:
+// order_ = the cell list's atoms (index order within each cell).
+void Scheduler::reorder_by_cell() {
+  cudaStream_t s = stream_;
+  const size_t n = static_cast<size_t>(n_);
+  build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, s);
+  order_.reserve(n);
+  perm_tmp_.reserve(n);
+  TDMD_CU(cudaMemcpyAsync(order_.data(), cl_.cell_atoms.data(), n * sizeof(int),
+                          cudaMemcpyDeviceToDevice, s));
+  const int nb = ceil_div(n_, kThreads);
+  auto permute = [&](auto* arr) {
+    using T = std::remove_pointer_t<decltype(arr)>;
+    T* tmp = reinterpret_cast<T*>(perm_tmp_.data());
+    k_gather<T><<<nb, kThreads, 0, s>>>(arr, order_.data(), n_, tmp);
+    TDMD_LAUNCH_CHECK();
+    TDMD_CU(cudaMemcpyAsync(arr, tmp, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  };
+  permute(pos4_.data());
+  permute(reinterpret_cast<D3*>(vel_.data()));
+  permute(types_.data());
+  permute(ids_.data());
+  if (mixed_) {
+    permute(q_.data());
+    permute(reinterpret_cast<F3*>(f32_.data()));
+  } else {
+    permute(reinterpret_cast<D3*>(f64_.data()));
+  }
+}
+
 void Scheduler::download(double* x, double* v, void* f, int* types, int* ids, int natoms) const {
   TDMD_REQUIRE(uploaded_, "download before upload");
   TDMD_REQUIRE(natoms >= 0 && natoms <= n_, "natoms out of range");
   const size_t n = static_cast<size_t>(natoms);
   if (n == 0) return;
   cudaStream_t s = stream_;
+  // Every array goes back to the caller's order through the staging
+  // buffer (stream order serializes its reuse), then the first natoms.
+  const int nb = ceil_div(n_, kThreads);
+  const int* ord = order_.data();
   if (x) {
-    k_unpack_positions<<<ceil_div(natoms, kThreads), kThreads, 0, s>>>(pos4_.data(), natoms,
-                                                                        stage_.data());
+    k_scatter_positions<<<nb, kThreads, 0, s>>>(pos4_.data(), ord, n_, stage_.data());
     TDMD_LAUNCH_CHECK();
     TDMD_CU(cudaMemcpyAsync(x, stage_.data(), 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
-  if (v) TDMD_CU(cudaMemcpyAsync(v, vel_.data(), 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  auto unpermute = [&](const auto* arr, void* out) {
+    using T = std::remove_const_t<std::remove_pointer_t<decltype(arr)>>;
+    T* tmp = reinterpret_cast<T*>(stage_.data());
+    k_scatter<T><<<nb, kThreads, 0, s>>>(arr, ord, n_, tmp);
+    TDMD_LAUNCH_CHECK();
+    TDMD_CU(cudaMemcpyAsync(out, tmp, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  };
+  if (v) unpermute(reinterpret_cast<const D3*>(vel_.data()), v);
   if (f) {
     if (mixed_)
-      TDMD_CU(cudaMemcpyAsync(f, f32_.data(), 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+      unpermute(reinterpret_cast<const F3*>(f32_.data()), f);
     else
-      TDMD_CU(cudaMemcpyAsync(f, f64_.data(), 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+      unpermute(reinterpret_cast<const D3*>(f64_.data()), f);
   }
-  if (types) TDMD_CU(cudaMemcpyAsync(types, types_.data(), n * sizeof(int), cudaMemcpyDeviceToHost, s));
-  if (ids) TDMD_CU(cudaMemcpyAsync(ids, ids_.data(), n * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (types) unpermute(static_cast<const int*>(types_.data()), types);
+  if (ids) unpermute(static_cast<const int*>(ids_.data()), ids);
   TDMD_CU(cudaStreamSynchronize(s));
 }
 
 // ----- neighbor list ------------------------------------------------------
 void Scheduler::size_neighbor_list() {
   cudaStream_t s = stream_;
-  build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, s);
+  build_cells();
   cnt_.reserve(static_cast<size_t>(n_));
   const double rl = cutoff_ + cfg_.r_skin;
   TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
@@ -513,7 +581,7 @@ void Scheduler::grow_capacity(int max_count) {
 void Scheduler::enqueue_rebuild() {
   cudaStream_t s = stream_;
   prof_begin(kProfRebuild);
-  build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, s);
+  build_cells();
   const double rl = cutoff_ + cfg_.r_skin;
   build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl * rl, nbr_.data(), nullptr,
                       cap_, cnt_.data(), ctl_status(), s);
@@ -823,7 +891,7 @@ void Scheduler::initial_forces() {
   int passes = 1;
   const bool reuse = cap_ > 0;
   if (reuse) {
-    build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, s);
+    build_cells();
     cnt_.reserve(static_cast<size_t>(n_));
   } else {
     size_neighbor_list();
@@ -951,7 +1019,7 @@ void Scheduler::run_until(int target) {
     step_ = step0;
     since_rebuild_ = since0;
     // The restored positions need a list built into the new capacity.
-    build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, stream_);
+    build_cells();
     build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_,
                         (cutoff_ + cfg_.r_skin) * (cutoff_ + cfg_.r_skin), nbr_.data(), nullptr,
                         cap_, cnt_.data(), nullptr, stream_);
@@ -1237,6 +1305,13 @@ int32_t tdmd_sched_thermostat_state(const tdmd_sched* s, double* dt, double* eta
   return guarded([&] {
     TDMD_REQUIRE(s, "null handle");
     s->s->thermostat_state(dt, eta, eta_v);
+  });
+}
+
+int32_t tdmd_sched_atom_order(const tdmd_sched* s, const int32_t** d_order) {
+  return guarded([&] {
+    TDMD_REQUIRE(s && d_order, "null argument");
+    *d_order = s->s->atom_order();
   });
 }
 

@@ -320,3 +320,32 @@ def test_reupload_reuses_or_grows_rows(cuda, precision):
         assert np.array_equal(s.download().forces, fresh.download().forces)
         fresh.close()
     assert s.stats().nlist_capacity > cap0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_arbitrary_atom_order(cuda, oracle, precision):
+    """A shuffled upload (held internally in cell order) gives the oracle's
+    trajectory for that order atom for atom and downloads in the caller's
+    order (cells list their atoms by the caller's index, so every neighbor
+    row is the one the caller's order defines)."""
+    from tdmd_claude_b200 import Box, EamAlloy, FastPipelineScheduler, make_config
+    from tdmd_claude_b200 import workloads as W
+    t = W.cu_eam_tables()
+    sysm = W.fcc_system(6, 3.615, 300.0, seed=21)
+    eam = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    perm = np.random.default_rng(3).permutation(sysm.n)
+    pos, vel = sysm.positions[perm], sysm.velocities[perm]
+    s = FastPipelineScheduler(Box.make(sysm.lo, sysm.hi), sysm.n, eam,
+                              make_config(r_skin=0.3, precision=precision, lanes_per_atom=4))
+    s.upload(pos, vel, None, sysm.types[perm], sysm.ids[perm], sysm.masses)
+    s.run_until(0)
+    st0 = s.download()
+    assert np.array_equal(st0.positions, pos) and np.array_equal(st0.ids, sysm.ids[perm])
+    s.run_until(30)
+    st = s.download()
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    r = oracle.md_run(pos, vel, sysm.types[perm], sysm.masses, sysm.lo, sysm.hi, 0.001, 0.3, 10,
+                      [30], eam=oe)
+    L = np.array(sysm.hi) - np.array(sysm.lo)
+    tol = 1e-10 if precision == "fp64" else 5e-4
+    assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < tol
