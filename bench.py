@@ -227,11 +227,8 @@ def timed_windows(sched, steps, warmup, flush, torch, dist=None):
         dist.barrier()
     wall = time.perf_counter() - t0
     launches = sched.stats().kernel_launches - l0
-    total = float(np.sum(ms))
-    if dist is not None:
-        t = torch.tensor([total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    from tdmd_claude_b200.replicas import max_over_ranks
+    total = max_over_ranks(float(np.sum(ms)), dist, "cuda")
     return total, wall, launches, ms
 
 
@@ -316,13 +313,17 @@ def nve_drift(sysm, eam, precision, lanes, nsteps, every=100):
             "max_abs_dev_ev_per_atom": float(np.abs(e - e[0]).max()) if len(e) else None}
 
 
-def batch_bench(steps, warmup, flush, torch, precision="mixed"):
+def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=0, world=1):
     """Batched replicas: 512 independent Cu FCC Morse systems (n^3 cells,
     n uniform 4..16, 100-1500 K), NVE, K = 10 steps per graph-replayed
     window; aggregate atom-steps/s and per-replica energy drift."""
     from tdmd_claude_b200 import Box, MorseParams, ReplicaBatch, make_config
     from tdmd_claude_b200 import workloads as W
+    from tdmd_claude_b200.replicas import lpt_partition, sum_over_ranks
     systems = W.replica_set(512)
+    if world > 1:  # whole replicas per rank, balanced by atom count
+        mine = lpt_partition([s.n for s in systems], world)[rank]
+        systems = [systems[i] for i in mine]
     b = ReplicaBatch([Box.make(s.lo, s.hi) for s in systems], [s.n for s in systems],
                      MorseParams.make(*W.MORSE_CU),
                      make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW, precision=precision,
@@ -332,7 +333,7 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed"):
              np.concatenate([s.velocities for s in systems]),
              np.concatenate([s.types for s in systems]), systems[0].masses)
     b.run_until(0)
-    ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, None)
+    ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, dist)
     steps_log, pk = b.energy_log()
     info = b.info()
     natoms = np.array([s.n for s in systems], np.float64)
@@ -340,9 +341,10 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed"):
     t_ns = steps_log * DT * 1e-3
     slopes = np.polyfit(t_ns, etot, 1)[0] if len(t_ns) > 1 else np.zeros(len(systems))
     b.close()
-    value = info["natoms"] * WINDOW * steps / (ms * 1e-3)
+    atoms = sum_over_ranks(info["natoms"], dist, "cuda")
+    value = atoms * WINDOW * steps / (ms * 1e-3)
     return {"value": value, "unit": "atom-steps/s", "ms_per_window": ms / steps,
-            "replicas": len(systems), "atoms": info["natoms"], "precision": precision,
+            "replicas": 512, "atoms": int(atoms), "ranks": world, "precision": precision,
             "lanes_per_atom": info["lanes_per_atom"], "kernel_launches_timed": launches,
             "drift_ev_per_atom_per_ns": {"median_abs": float(np.median(np.abs(slopes))),
                                          "max_abs": float(np.max(np.abs(slopes))),
@@ -501,6 +503,12 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
+    if world > 1:
+        # N replicas: the headline, e2e and the sharded batch figure; the
+        # single-GPU extras (drift, force matching, 4 M-atom ternary) are not
+        # repeated per rank.
+        args.no_fit = args.no_ternary = True
+        args.drift_steps = 0
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -577,8 +585,8 @@ def main():
 
     batch = None
     if not args.no_batch:
-        batch = {"mixed": batch_bench(args.steps, args.warmup, flush, torch, "mixed"),
-                 "fp64": batch_bench(args.steps, args.warmup, flush, torch, "fp64")}
+        batch = {p: batch_bench(args.steps, args.warmup, flush, torch, p, dist, rank, world)
+                 for p in ("mixed", "fp64")}
 
     fitfig = None if args.no_fit else fit_bench(torch)
     ternary = None if args.no_ternary else ternary_bench(max(3, args.steps // 3), 3, flush,
