@@ -593,7 +593,9 @@ def main():
                                                            torch)
 
     hbm, peak_kind = measured_peaks()
-    force_bytes = sysm.n * (48 + 24 * K)          # gather model, mixed force pass
+    # gather model of the mixed force pass, plus the next step's kick + drift
+    # it carries on (WINDOW-1) of WINDOW launches (144 B per atom)
+    force_bytes = sysm.n * (48 + 24 * K) + sysm.n * 144 * (WINDOW - 1) / WINDOW
     dens_bytes = sysm.n * (40 + 20 * K)
     force_ms = kt["force"][0]
     achieved = force_bytes / (force_ms * 1e-3) / 1e9 if force_ms > 0 else None
@@ -647,7 +649,8 @@ def main():
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "kernel": "k_eam_force<GeoQ> (mixed)", "peak_source": peak_kind,
                          "bytes_per_launch": force_bytes, "ms_per_launch": force_ms,
-                         "model": "gather model n*(48+24K) B, K = mean full-list length"},
+                         "model": "gather model n*(48+24K) B, K = mean full-list length, "
+                                  "+ 144 B/atom kick-drift on 9 of 10 launches"},
             "kernel_ms": {"mixed": kt, "fp64": kt64,
                           "density_bytes_per_launch": dens_bytes},
             "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
