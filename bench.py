@@ -454,6 +454,27 @@ def fit_bench(torch, adam_steps=200, nsnap=64):
     return out
 
 
+def batch_eam_bench(steps, warmup, flush, torch, eam, precision, nrep=8):
+    """nrep replicas of the headline system (32^3 Cu FCC cells, 131,072
+    atoms each, own seeds) as one EAM batch: every pass is one launch over
+    all nrep * 131,072 atoms; NVE, windows of 10 steps."""
+    from tdmd_claude_b200 import Box, ReplicaBatch, make_config
+    from tdmd_claude_b200 import workloads as W
+    systems = [W.fcc_system(NCELL, 3.615, 300.0, 5000 + r) for r in range(nrep)]
+    b = ReplicaBatch([Box.make(s.lo, s.hi) for s in systems], [s.n for s in systems], eam,
+                     make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW, precision=precision))
+    b.upload(np.concatenate([s.positions for s in systems]),
+             np.concatenate([s.velocities for s in systems]),
+             np.concatenate([s.types for s in systems]), systems[0].masses)
+    b.run_until(0)
+    ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, None)
+    info = b.info()
+    b.close()
+    return {"value": info["natoms"] * WINDOW * steps / (ms * 1e-3), "unit": "atom-steps/s",
+            "ms_per_window": ms / steps, "replicas": nrep, "atoms": info["natoms"],
+            "lanes_per_atom": info["lanes_per_atom"], "kernel_launches_timed": launches}
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
     if rank != 0:
@@ -588,6 +609,12 @@ def main():
         batch = {p: batch_bench(args.steps, args.warmup, flush, torch, p, dist, rank, world)
                  for p in ("mixed", "fp64")}
 
+    beam = None
+    if not args.no_batch:
+        beam = {p: batch_eam_bench(args.steps, args.warmup, flush, torch, eam, p)
+                for p in ("mixed", "fp64")}
+        beam["mixed_batched_over_plain_fp64"] = beam["mixed"]["value"] / value64
+        beam["mixed_over_fp64_batched"] = beam["mixed"]["value"] / beam["fp64"]["value"]
     fitfig = None if args.no_fit else fit_bench(torch)
     ternary = None if args.no_ternary else ternary_bench(max(3, args.steps // 3), 3, flush,
                                                            torch)
@@ -641,6 +668,7 @@ def main():
                               "thermostat": "Nose-Hoover chain 3, tau 0.1 ps, 300 K"},
                 "nve_drift": drift,
                 "batched_replicas": batch,
+                "batched_eam_131k_x8": beam,
                 "ternary_4m_nvt_adaptive": ternary,
                 "force_matching": fitfig,
                 "wall_s_timed_region": wall_mixed,

@@ -339,7 +339,7 @@ int32_t tdmd_sched_stream(const tdmd_sched* s, void** stream);
 /* ------------------------------------------------------------------------ */
 /* Batched replicas (no reference counterpart: the reference runs one       */
 /* system per FastPipelineScheduler and only plans multi-step fusion,        */
-/* docs gpu-strategy.md:67-82).  Many independent Morse systems of uneven   */
+/* docs gpu-strategy.md:67-82).  Many independent Morse or EAM systems of   */
 /* sizes advance together: every phase is one launch over all replicas and  */
 /* each run_until window is replayed as one CUDA graph.  Each replica       */
 /* follows FastPipelineScheduler's NVE semantics (same step order, rebuild  */
@@ -354,6 +354,11 @@ typedef struct tdmd_batch tdmd_batch;
 int32_t tdmd_batch_create_morse(int32_t nreplicas, const tdmd_box* boxes, const int32_t* natoms,
                                 const tdmd_morse_params* params,
                                 const tdmd_fast_pipeline_config* cfg, tdmd_batch** out);
+/* EAM replicas sharing one set of tables (each replica's trajectory equals
+ * a single EAM FastPipelineScheduler's with the same lanes_per_atom). */
+int32_t tdmd_batch_create_eam(int32_t nreplicas, const tdmd_box* boxes, const int32_t* natoms,
+                              const tdmd_eam* eam, const tdmd_fast_pipeline_config* cfg,
+                              tdmd_batch** out);
 int32_t tdmd_batch_destroy(tdmd_batch* b);
 /* Arrays hold all replicas back to back in replica order (positions and
  * velocities double[3*total], types int32[total]); masses[n_types] are

@@ -142,6 +142,7 @@ SIGNATURES = {
     "tdmd_sched_stream": [_p, _pp],
     "tdmd_batch_create_morse": [_i32, C.POINTER(Box), _p, C.POINTER(MorseParams),
                                 C.POINTER(FastPipelineConfig), _pp],
+    "tdmd_batch_create_eam": [_i32, C.POINTER(Box), _p, _p, C.POINTER(FastPipelineConfig), _pp],
     "tdmd_batch_destroy": [_p],
     "tdmd_batch_upload": [_p, _p, _p, _p, _p, _i32],
     "tdmd_batch_run_until": [_p, _i32],

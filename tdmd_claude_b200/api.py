@@ -303,12 +303,13 @@ class FastPipelineScheduler:
 # Batched replicas (no reference counterpart; see tdmd_batch_* in the header)
 # ---------------------------------------------------------------------------
 class ReplicaBatch:
-    """Many independent Morse systems advanced together (NVE).
+    """Many independent Morse or EAM systems advanced together (NVE).
 
-    boxes: list of Box, natoms: list of int.  Arrays passed to upload hold
-    all replicas back to back in replica order."""
+    boxes: list of Box, natoms: list of int, potential: MorseParams or
+    EamAlloy (shared by all replicas).  Arrays passed to upload hold all
+    replicas back to back in replica order."""
 
-    def __init__(self, boxes, natoms, params: MorseParams, cfg: FastPipelineConfig | None = None):
+    def __init__(self, boxes, natoms, params, cfg: FastPipelineConfig | None = None):
         self.nrep = len(boxes)
         self.natoms = np.ascontiguousarray(natoms, dtype=np.int32)
         assert self.natoms.size == self.nrep
@@ -318,8 +319,14 @@ class ReplicaBatch:
         self.mixed = self.cfg.precision == TDMD_MIXED
         barr = (Box * self.nrep)(*boxes)
         h = C.c_void_p()
-        call("tdmd_batch_create_morse", self.nrep, barr, _ptr(self.natoms), C.byref(params),
-             C.byref(self.cfg), C.byref(h))
+        self._eam = None
+        if isinstance(params, EamAlloy):
+            self._eam = params
+            call("tdmd_batch_create_eam", self.nrep, barr, _ptr(self.natoms), params.handle,
+                 C.byref(self.cfg), C.byref(h))
+        else:
+            call("tdmd_batch_create_morse", self.nrep, barr, _ptr(self.natoms), C.byref(params),
+                 C.byref(self.cfg), C.byref(h))
         self._h = h
 
     def __del__(self):

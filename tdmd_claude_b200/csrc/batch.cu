@@ -22,10 +22,12 @@
 #include <cmath>
 #include <list>
 #include <map>
+#include <memory>
 #include <vector>
 
 #include "buffers.cuh"
 #include "common.cuh"
+#include "eam_tables.cuh"
 #include "forces.cuh"
 #include "integrate.cuh"
 #include "launch.cuh"
@@ -74,6 +76,55 @@ __global__ void __launch_bounds__(kThreads) k_morse_atom_pe(Geo g, NbrView nl, i
 #pragma unroll
   for (int s = LPA / 2; s > 0; s >>= 1) pe += __shfl_xor_sync(0xffffffffu, pe, s);
   if (i < n && sub == 0) pe_atom[i] = pe;
+}
+
+// Per-atom EAM energy F_ti(rho_i) + 1/2 sum_j phi(r_ij), with the force
+// pass's spline rows and offsets; only on energy-log windows.
+template <class Geo, int LPA, bool VEC, bool MULTI>
+__global__ void __launch_bounds__(kThreads) k_eam_atom_pe(Geo g, NbrView nl, int n,
+                                                          EamDev<typename Geo::T> e,
+                                                          const int* __restrict__ types,
+                                                          const double* __restrict__ rho,
+                                                          double* __restrict__ pe_atom) {
+  using T = typename Geo::T;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = tid / LPA;
+  const int sub = tid % LPA;
+  double pe = 0.0;
+  if (i < n) {
+    const typename Geo::Own o = g.own(i);
+    const int ti = MULTI ? __ldg(types + i) - 1 : 0;
+    const long long row = nl.row(i);
+    const int c = nl.count(i);
+    for (int base = kU * sub; base < c; base += kU * LPA) {
+      int jj[kU];
+      nbr_batch<VEC>(nl, row, base, c, jj);
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (jj[u] < 0) continue;
+        typename Geo::Pair pr;
+        g.pair(o, jj[u], pr);
+        if (pr.r2 < e.rc_sq) {
+          T r, rinv, sx;
+          double rd;
+          g.radius(o, pr, r, rinv, rd);
+          const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
+          const int tj = MULTI ? __ldg(types + jj[u]) - 1 : 0;
+          const auto cphi = ldv4<T>(e.rtab + static_cast<long long>(idx) * e.S +
+                                    (MULTI ? phi_slot(ti, tj, e.ntypes) : 1));
+          pe += 0.5 * static_cast<double>(dspl_val(cphi, sx));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int s = LPA / 2; s > 0; s >>= 1) pe += __shfl_xor_sync(0xffffffffu, pe, s);
+  if (i < n && sub == 0) {
+    const int ti = MULTI ? __ldg(types + i) - 1 : 0;
+    double Fi, dF;
+    embed_eval(e.ftab, e.nrho, e.drho, ti, rho[i], Fi, dF);
+    pe_atom[i] = pe + Fi;
+  }
 }
 
 // Per-replica (PE, KE) in a fixed order: one CTA per replica.
@@ -177,8 +228,9 @@ struct BatchStep {
 
 class Batch {
  public:
-  Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_morse_params& p,
-        const tdmd_fast_pipeline_config& cfg);
+  // Exactly one of morse / eam is given.
+  Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_morse_params* morse,
+        const tdmd_eam* eam, const tdmd_fast_pipeline_config& cfg);
   ~Batch();
   Batch(const Batch&) = delete;
   Batch& operator=(const Batch&) = delete;
@@ -226,6 +278,10 @@ class Batch {
   double rc_, rl2_;
   MorseP<double> m64_;
   MorseP<float> m32_;
+  std::unique_ptr<EamDevTables> eam_;  // EAM replicas (same tables for all)
+  DevArray<float> fp32_;
+  DevArray<double> fp64_, rho_;
+  DevArray<int4> g_;                   // mixed EAM gather records {q, bits(F')}
   std::vector<RepDesc> hreps_;
   int ncells_ = 0;
   int lpa_ = 0;
@@ -265,9 +321,10 @@ class Batch {
   std::vector<double> log_;
 };
 
-Batch::Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_morse_params& p,
-             const tdmd_fast_pipeline_config& cfg)
+Batch::Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_morse_params* morse,
+             const tdmd_eam* eam, const tdmd_fast_pipeline_config& cfg)
     : nrep_(nrep), cfg_(cfg), mixed_(cfg.precision == TDMD_MIXED) {
+  TDMD_REQUIRE((morse != nullptr) != (eam != nullptr), "give a Morse or an EAM potential");
   TDMD_REQUIRE(nrep >= 1, "need at least one replica");
   TDMD_REQUIRE(boxes && natoms, "null boxes or natoms");
   TDMD_REQUIRE(cfg.dt > 0.0, "dt must be positive");
@@ -276,14 +333,20 @@ Batch::Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_mors
   TDMD_REQUIRE(cfg.precision == TDMD_FP64 || cfg.precision == TDMD_MIXED, "unknown precision");
   if (cfg.t_target > 0.0 || cfg.adaptive_dt)
     throw Error{TDMD_ERR_UNSUPPORTED, "batched replicas run NVE with a fixed dt"};
-  TDMD_REQUIRE(p.rc > 0.0, "cutoff must be positive");
-  rc_ = p.rc;
-  const double rl = p.rc + cfg.r_skin;
+  if (morse) {
+    const tdmd_morse_params& p = *morse;
+    TDMD_REQUIRE(p.rc > 0.0, "cutoff must be positive");
+    rc_ = p.rc;
+    const double rc_sq = p.rc_sq > 0.0 ? p.rc_sq : p.rc * p.rc;
+    m64_ = MorseP<double>{p.d, p.alpha, p.r0, rc_sq, p.r0};
+    m32_ = MorseP<float>{static_cast<float>(p.d), static_cast<float>(p.alpha),
+                         static_cast<float>(p.r0), static_cast<float>(rc_sq), p.r0};
+  } else {
+    TDMD_REQUIRE(eam->cutoff > 0.0, "cutoff must be positive");
+    rc_ = eam->cutoff;
+  }
+  const double rl = rc_ + cfg.r_skin;
   rl2_ = rl * rl;
-  const double rc_sq = p.rc_sq > 0.0 ? p.rc_sq : p.rc * p.rc;
-  m64_ = MorseP<double>{p.d, p.alpha, p.r0, rc_sq, p.r0};
-  m32_ = MorseP<float>{static_cast<float>(p.d), static_cast<float>(p.alpha),
-                       static_cast<float>(p.r0), static_cast<float>(rc_sq), p.r0};
   hreps_.resize(static_cast<size_t>(nrep));
   std::vector<RepScale> sc(static_cast<size_t>(nrep));
   std::vector<RepImg> img(static_cast<size_t>(nrep));
@@ -325,6 +388,10 @@ Batch::Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_mors
   TDMD_CU(cudaEventCreate(&win_ev_[0]));
   TDMD_CU(cudaEventCreate(&win_ev_[1]));
   cudaStream_t s = stream_;
+  if (eam) {
+    eam_ = std::make_unique<EamDevTables>();
+    eam_->upload(*eam, s);
+  }
   reps_.reserve(hreps_.size());
   scales_.reserve(sc.size());
   imgs_.reserve(img.size());
@@ -374,9 +441,19 @@ void Batch::upload(const double* x, const double* v, const int* types, const dou
   const size_t n = static_cast<size_t>(n_);
   for (size_t i = 0; i < n; ++i)
     TDMD_REQUIRE(types[i] >= 1 && types[i] < n_types, "atom type out of range of masses");
+  if (eam_)
+    for (size_t i = 0; i < n; ++i)
+      TDMD_REQUIRE(types[i] <= eam_->ntypes, "atom type beyond the EAM element count");
   clear_graphs();
   cudaStream_t s = stream_;
   const size_t nn = std::max<size_t>(n, 1);
+  if (eam_) {
+    rho_.reserve(nn);
+    if (mixed_)
+      fp32_.reserve(nn), g_.reserve(nn);
+    else
+      fp64_.reserve(nn);
+  }
   pos4_.reserve(nn);
   vel_.reserve(3 * nn);
   types_.reserve(nn);
@@ -466,6 +543,27 @@ void Batch::force() {
   cudaStream_t s = stream_;
   const NbrView nl = view();
   const int n = static_cast<int>(n_);
+  if (eam_) {
+    // Density + embedding, then forces, over all replicas at once (the
+    // single scheduler's passes on the batched geometries).
+    const int* types = eam_->ntypes > 1 ? types_.data() : nullptr;
+    if (mixed_) {
+      const GeoQB g{q_.data(), rep_.data(), scales_.data()};
+      const GeoQB gg{g_.data(), rep_.data(), scales_.data()};
+      launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), nullptr, nullptr,
+                                       g_.data(), false, nullptr, lpa_, s);
+      launch_eam_force<GeoQB, true, float, float>(gg, nl, n, eam_->d32, types, fp32_.data(),
+                                                  f32_.data(), false, nullptr, lpa_, s);
+    } else {
+      const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
+      launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), nullptr,
+                                         nullptr, nullptr, false, nullptr, lpa_, s);
+      launch_eam_force<GeoD4B, false, double, double>(g, nl, n, eam_->d64, types, fp64_.data(),
+                                                      f64_.data(), false, nullptr, lpa_, s);
+    }
+    launches_ += 2;
+    return;
+  }
   if (mixed_) {
     const GeoQB g{q_.data(), rep_.data(), scales_.data()};
     launch_morse(g, nl, n, m32_, f32_.data(), false, nullptr, lpa_, s);
@@ -727,15 +825,41 @@ void Batch::reduce_energies(double* out) {
   const NbrView nl = view();
   const int n = static_cast<int>(n_);
   const int nblk = force_blocks(n_, lpa_);
-  TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa_, {
-    if (mixed_)
-      k_morse_atom_pe<GeoQB, L, V><<<nblk, kThreads, 0, s>>>(
-          GeoQB{q_.data(), rep_.data(), scales_.data()}, nl, n, m32_, pe_atom_.data());
-    else
-      k_morse_atom_pe<GeoD4B, L, V><<<nblk, kThreads, 0, s>>>(
-          GeoD4B{pos4_.data(), rep_.data(), imgs_.data()}, nl, n, m64_, pe_atom_.data());
-  }));
-  TDMD_LAUNCH_CHECK();
+  if (eam_) {
+    // rho_i of the current positions, then F(rho_i) + 1/2 sum_j phi(r_ij)
+    const int* types = eam_->ntypes > 1 ? types_.data() : nullptr;
+    if (mixed_) {
+      const GeoQB g{q_.data(), rep_.data(), scales_.data()};
+      launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), rho_.data(),
+                                       nullptr, g_.data(), false, nullptr, lpa_, s);
+      TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(
+          lpa_, {
+            k_eam_atom_pe<GeoQB, L, V, M><<<nblk, kThreads, 0, s>>>(
+                g, nl, n, eam_->d32, types, rho_.data(), pe_atom_.data());
+          })));
+    } else {
+      const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
+      launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), rho_.data(),
+                                         nullptr, nullptr, false, nullptr, lpa_, s);
+      TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(
+          lpa_, {
+            k_eam_atom_pe<GeoD4B, L, V, M><<<nblk, kThreads, 0, s>>>(
+                g, nl, n, eam_->d64, types, rho_.data(), pe_atom_.data());
+          })));
+    }
+    TDMD_LAUNCH_CHECK();
+    launches_ += 1;
+  } else {
+    TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa_, {
+      if (mixed_)
+        k_morse_atom_pe<GeoQB, L, V><<<nblk, kThreads, 0, s>>>(
+            GeoQB{q_.data(), rep_.data(), scales_.data()}, nl, n, m32_, pe_atom_.data());
+      else
+        k_morse_atom_pe<GeoD4B, L, V><<<nblk, kThreads, 0, s>>>(
+            GeoD4B{pos4_.data(), rep_.data(), imgs_.data()}, nl, n, m64_, pe_atom_.data());
+    }));
+    TDMD_LAUNCH_CHECK();
+  }
   k_rep_energy<<<nrep_, kThreads, 0, s>>>(pe_atom_.data(), vel_.data(), types_.data(),
                                           masses_.data(), reps_.data(), eout_.data());
   TDMD_LAUNCH_CHECK();
@@ -780,9 +904,9 @@ using namespace tdmd_b200;
 
 struct tdmd_batch {
   Batch b;
-  tdmd_batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_morse_params& p,
-             const tdmd_fast_pipeline_config& cfg)
-      : b(nrep, boxes, natoms, p, cfg) {}
+  tdmd_batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_morse_params* p,
+             const tdmd_eam* e, const tdmd_fast_pipeline_config& cfg)
+      : b(nrep, boxes, natoms, p, e, cfg) {}
 };
 
 extern "C" {
@@ -792,7 +916,16 @@ int32_t tdmd_batch_create_morse(int32_t nreplicas, const tdmd_box* boxes, const 
                                 const tdmd_fast_pipeline_config* cfg, tdmd_batch** out) {
   return guarded([&] {
     TDMD_REQUIRE(out && params && cfg, "null argument");
-    *out = new tdmd_batch(nreplicas, boxes, natoms, *params, *cfg);
+    *out = new tdmd_batch(nreplicas, boxes, natoms, params, nullptr, *cfg);
+  });
+}
+
+int32_t tdmd_batch_create_eam(int32_t nreplicas, const tdmd_box* boxes, const int32_t* natoms,
+                              const tdmd_eam* eam, const tdmd_fast_pipeline_config* cfg,
+                              tdmd_batch** out) {
+  return guarded([&] {
+    TDMD_REQUIRE(out && eam && cfg, "null argument");
+    *out = new tdmd_batch(nreplicas, boxes, natoms, nullptr, eam, *cfg);
   });
 }
 

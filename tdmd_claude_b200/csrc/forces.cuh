@@ -146,6 +146,7 @@ __device__ __forceinline__ void radius_f(float r2, double r2d, float& r, float& 
 
 struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
   using T = double;
+  static constexpr bool kRecords = false;  // no fixed-point gather records
   using Own = double3;
   using Pair = PairD;
   const double4* p;
@@ -176,6 +177,7 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
 
 struct GeoAoS64 {  // FP64, reference Vec3D AoS
   using T = double;
+  static constexpr bool kRecords = false;
   using Own = double3;
   using Pair = PairD;
   const double* p;
@@ -208,6 +210,7 @@ struct GeoAoS64 {  // FP64, reference Vec3D AoS
 // min-image step).
 struct GeoAoS32 {
   using T = float;
+  static constexpr bool kRecords = false;
   using Own = double3;
   using Pair = PairF;
   const double* p;
@@ -245,10 +248,12 @@ struct GeoQ {
   using T = float;
   using Own = int4;
   using Pair = PairQ;
+  static constexpr bool kRecords = true;  // own() is the atom's fixed-point record
   const int4* q;
   float s[3];
   double s2[3];  // (Lq/2^32)^2 per axis
   __device__ __forceinline__ Own own(int i) const { return __ldg(q + i); }
+  __device__ __forceinline__ int4 record(const Own& o) const { return o; }
   __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
     const int4 b = __ldg(q + j);
     const int ix = o.x - b.x, iy = o.y - b.y, iz = o.z - b.z;
@@ -604,10 +609,9 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
     fp_out[i] = static_cast<FP>(dF);
     if (rho_out) rho_out[i] = rh;
     if (fpd_out) fpd_out[i] = dF;
-    if constexpr (sizeof(typename Geo::Own) == sizeof(int4)) {
+    if constexpr (Geo::kRecords) {
       if (gout) {
-        int4 rec;
-        memcpy(&rec, &o, sizeof(rec));
+        int4 rec = g.record(o);
         rec.w = __float_as_int(static_cast<float>(dF));
         gout[i] = rec;
       }

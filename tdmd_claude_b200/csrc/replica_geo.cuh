@@ -26,9 +26,11 @@ struct GeoQB {
     double t0, t1, t2;
   };
   using Pair = PairQ;
+  static constexpr bool kRecords = true;
   const int4* q;
   const int* rep;
   const RepScale* sc;
+  __device__ __forceinline__ int4 record(const Own& o) const { return o.q; }
   __device__ __forceinline__ Own own(int i) const {
     Own o;
     o.q = __ldg(q + i);
@@ -69,6 +71,7 @@ struct GeoD4B {
     int p0, p1, p2;
   };
   using Pair = PairD;
+  static constexpr bool kRecords = false;
   const double4* p;
   const int* rep;
   const RepImg* img;

@@ -132,3 +132,44 @@ def test_batch_autotune_keeps_forces(cuda):
     _, _, f1 = b.download()
     rel = np.sqrt(((f1 - f0) ** 2).sum() / (f0.astype(np.float64) ** 2).sum())
     assert rel < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("ternary", [False, True])
+def test_eam_batch_replicas_equal_single_schedulers(cuda, precision, ternary):
+    """EAM replicas (shared tables) advance exactly like single EAM
+    schedulers (which fuse the next kick into the force pass in mixed NVE,
+    bit-identically); per-replica energies match theirs to 1e-12."""
+    from tdmd_claude_b200 import Box, EamAlloy, FastPipelineScheduler, ReplicaBatch, make_config
+    from tdmd_claude_b200 import workloads as W
+    t = W.ternary_eam_tables() if ternary else W.cu_eam_tables()
+    eam = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    rng = np.random.default_rng(8)
+    systems = []
+    for k, (n, temp) in enumerate([(5, 300.0), (4, 900.0), (6, 600.0)]):
+        types = rng.integers(1, t.ntypes + 1, size=4 * n ** 3).astype(np.int32)
+        systems.append(W.fcc_system(n, 3.615, temp, 70 + k, types=types,
+                                    masses=(63.546,) * t.ntypes))
+    cfg = dict(dt=0.001, r_skin=0.3, rebuild_every=10, precision=precision, lanes_per_atom=4)
+    b = ReplicaBatch([Box.make(s.lo, s.hi) for s in systems], [s.n for s in systems], eam,
+                     make_config(**cfg))
+    b.upload(np.concatenate([s.positions for s in systems]),
+             np.concatenate([s.velocities for s in systems]),
+             np.concatenate([s.types for s in systems]), systems[0].masses)
+    for target in (10, 23):
+        b.run_until(target)
+    pos, vel, frc = b.download()
+    pe_b, ke_b = b.energies()
+    for r, s in enumerate(systems):
+        sc = FastPipelineScheduler(Box.make(s.lo, s.hi), s.n, eam, make_config(**cfg))
+        sc.upload(s.positions, s.velocities, None, s.types, s.ids, s.masses)
+        sc.run_until(10)
+        sc.run_until(23)
+        st = sc.download()
+        assert np.array_equal(b.replica(pos, r), st.positions), r
+        assert np.array_equal(b.replica(vel, r), st.velocities), r
+        assert np.array_equal(b.replica(frc, r), st.forces), r
+        pe, ke, _ = sc.energies()
+        assert abs(pe_b[r] - pe) <= 1e-12 * abs(pe), r
+        assert abs(ke_b[r] - ke) <= 1e-12 * abs(ke), r
+        sc.close()
