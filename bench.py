@@ -475,6 +475,50 @@ def batch_eam_bench(steps, warmup, flush, torch, eam, precision, nrep=8):
             "lanes_per_atom": info["lanes_per_atom"], "kernel_launches_timed": launches}
 
 
+def reference_gpu_sample(sysm, t, windows=10, warm=5):
+    """The reference's own GPU FastPipelineScheduler (oracle/_ref, compiled
+    from its sources, FP64 and mixed builds) on the same system: host wall
+    clock around whole run_until windows (it synchronizes the host inside a
+    rebuild).  None where those libraries or a GPU are absent."""
+    import ctypes as C
+    out = {}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except Exception:
+        return None
+    from tdmd_claude_b200 import io as TIO
+    for prec in ("fp64", "mixed"):
+        path = os.path.join(ROOT, "oracle", "_ref", f"libtdmd_ref_gpu_{prec}.so")
+        if not os.path.exists(path):
+            continue
+        L = C.CDLL(path)
+        L.refgpu_run_eam.restype = C.c_double
+        L.refgpu_last_error.restype = C.c_char_p
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
+        L.refgpu_run_eam.argtypes = [C.c_char_p, f64p, f64p, i32p, f64p, C.c_int32, C.c_int32,
+                                     f64p, f64p, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                     C.c_int32, C.c_int32]
+        with tempfile.TemporaryDirectory() as d:
+            setfl = os.path.join(d, "cu.eam.alloy")
+            TIO.write_setfl(setfl, t)
+            sec = L.refgpu_run_eam(setfl.encode(), np.ascontiguousarray(sysm.positions),
+                                   np.ascontiguousarray(sysm.velocities),
+                                   np.ascontiguousarray(sysm.types, dtype=np.int32),
+                                   np.ascontiguousarray(sysm.masses), sysm.masses.size, sysm.n,
+                                   np.array(sysm.lo, np.float64), np.array(sysm.hi, np.float64),
+                                   DT, SKIN, WINDOW, WINDOW, warm, windows)
+        if sec <= 0:
+            out[prec] = {"error": L.refgpu_last_error().decode()}
+            continue
+        out[prec] = {"value": sysm.n * WINDOW * windows / sec, "unit": "atom-steps/s",
+                     "ms_per_window": 1e3 * sec / windows,
+                     "timing": "host wall clock around run_until windows"}
+    return out or None
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
     if rank != 0:
@@ -498,6 +542,10 @@ def run_reference(args, rank, world):
         "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_gpu:
+        # context only (the arm's value is the CPU reference): the reference's
+        # own GPU FastPipelineScheduler on the same system and GPU
+        line["reference_gpu_same_box"] = reference_gpu_sample(sysm, t)
     print(json.dumps(line), flush=True)
 
 
@@ -513,6 +561,8 @@ def main():
                     help="only the mixed timed windows (for profiler captures); no JSON line")
     ap.add_argument("--lanes", type=int, default=2,
                     help="lanes per atom for --kernels-only (no autotune there)")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own GPU scheduler")
     ap.add_argument("--no-fit", action="store_true",
                     help="skip the force-matching (adjoint + Adam) figure")
     ap.add_argument("--no-ternary", action="store_true",

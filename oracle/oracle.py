@@ -46,13 +46,15 @@ class OrcPotential(C.Structure):
 
 
 def build(ref: bool | None = None) -> None:
-    """Compile liboracle.so (and _ref/ when the reference tree exists)."""
+    """Compile liboracle.so (and, when the reference tree exists, _ref/: its
+    CPU path for the oracle's pins and the CPU baseline, and its GPU
+    scheduler in both precision builds for the same-box comparison)."""
     targets = ["all"]
     ref_tree = os.environ.get("TDMD_REFERENCE_TREE", "/root/reference")
     if ref is None:
         ref = os.path.isdir(os.path.join(ref_tree, "src"))
     if ref:
-        targets.append("ref")
+        targets += ["ref", "refgpu"]
     subprocess.run(["make", "-s", "-C", _HERE, f"REF={ref_tree}", *targets], check=True)
 
 

@@ -222,6 +222,8 @@ __global__ void __launch_bounds__(kThreads) k_half_kick_batch(double* __restrict
 
 struct BatchStep {
   bool first, rebuild;
+  bool kd_fused;   // kick + drift done by the previous step's force pass
+  bool fuse_next;  // this force pass also kicks and drifts for the next step
 };
 
 }  // namespace
@@ -260,7 +262,7 @@ class Batch {
 
  private:
   void rebuild(int* status);
-  void force();
+  void force(bool kd = false);
   void kick_drift(bool full);
   void half_kick();
   void enqueue_step(const BatchStep& st);
@@ -539,10 +541,11 @@ void Batch::rebuild(int* status) {
   ++rebuilds_;
 }
 
-void Batch::force() {
+void Batch::force(bool kd) {
   cudaStream_t s = stream_;
   const NbrView nl = view();
   const int n = static_cast<int>(n_);
+  TDMD_REQUIRE(!kd || (eam_ && mixed_), "fused kick-drift needs the mixed EAM batch");
   if (eam_) {
     // Density + embedding, then forces, over all replicas at once (the
     // single scheduler's passes on the batched geometries).
@@ -552,8 +555,13 @@ void Batch::force() {
       const GeoQB gg{g_.data(), rep_.data(), scales_.data()};
       launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), nullptr, nullptr,
                                        g_.data(), false, nullptr, lpa_, s);
+      // kd: the next step's kick + drift in the same pass (the force pass
+      // reads gather records only), each atom in its replica's box
+      const KickDrift kdr{pos4_.data(), q_.data(), vel_.data(), types_.data(), inv_mm_.data(),
+                          cfg_.dt, nullptr, DevBox{}, rep_.data(), reps_.data()};
       launch_eam_force<GeoQB, true, float, float>(gg, nl, n, eam_->d32, types, fp32_.data(),
-                                                  f32_.data(), false, nullptr, lpa_, s);
+                                                  f32_.data(), false, nullptr, lpa_, s,
+                                                  kd ? &kdr : nullptr);
     } else {
       const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
       launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), nullptr,
@@ -619,15 +627,17 @@ void Batch::half_kick() {
 // kick-drift (half kick on the first step of a window), rebuild when due,
 // forces; the window closes with a half kick.
 void Batch::enqueue_step(const BatchStep& st) {
-  kick_drift(!st.first);
+  if (!st.kd_fused) kick_drift(!st.first);
   if (st.rebuild) rebuild(status_.data());
-  force();
+  force(st.fuse_next);
 }
 
 void Batch::run_segment(const std::vector<BatchStep>& seg, bool finalize) {
   std::vector<int> key;
   key.reserve(seg.size() + 1);
-  for (const auto& st : seg) key.push_back((st.first ? 1 : 0) | (st.rebuild ? 2 : 0));
+  for (const auto& st : seg)
+    key.push_back((st.first ? 1 : 0) | (st.rebuild ? 2 : 0) | (st.kd_fused ? 4 : 0) |
+                  (st.fuse_next ? 8 : 0));
   key.push_back(finalize ? 1 : 0);
   const long long l0 = launches_;
   if (!cfg_.use_graphs) {
@@ -765,6 +775,10 @@ void Batch::run_until(int target) {
       b.rebuild = since >= cfg_.rebuild_every;
       if (b.rebuild) since = 0;
       ++since;
+      // mixed EAM: every force pass but the window's last also kicks and
+      // drifts for the next step (energies are logged after the window)
+      b.fuse_next = eam_ && mixed_ && st + 1 < target;
+      b.kd_fused = !plan.empty() && plan.back().fuse_next;
       plan.push_back(b);
     }
     size_t a = 0;

@@ -37,6 +37,7 @@
 
 #include "common.cuh"
 #include "integrate.cuh"
+#include "replicas.cuh"
 
 namespace tdmd_b200 {
 
@@ -635,12 +636,16 @@ struct KickDrift {
   const int* types;
   const double* inv_mm;  // 1 / (m mvv2e) per type
   double dt;
-  long long* step;       // device step counter, +1 per kick-drift
+  long long* step;       // device step counter, +1 per kick-drift (nullable)
   DevBox b;
+  // Batched replicas: atom i's box is reps[rep[i]].box instead of b.
+  const int* rep;
+  const RepDesc* reps;
 };
 
 __device__ __forceinline__ void kick_drift_atom(const KickDrift& k, int i, float fx, float fy,
                                                 float fz) {
+  const DevBox& b = k.reps ? k.reps[__ldg(k.rep + i)].box : k.b;
   const int t = __ldg(k.types + i);
   const double factor = k.dt * __ldg(k.inv_mm + t);
   double vx = k.v[3ll * i], vy = k.v[3ll * i + 1], vz = k.v[3ll * i + 2];
@@ -648,15 +653,15 @@ __device__ __forceinline__ void kick_drift_atom(const KickDrift& k, int i, float
   vy += factor * static_cast<double>(fy);
   vz += factor * static_cast<double>(fz);
   double4 p = k.pos4[i];
-  p.x = wrap_single(p.x + k.dt * vx, k.b.lo[0], k.b.L[0], k.b.periodic[0]);
-  p.y = wrap_single(p.y + k.dt * vy, k.b.lo[1], k.b.L[1], k.b.periodic[1]);
-  p.z = wrap_single(p.z + k.dt * vz, k.b.lo[2], k.b.L[2], k.b.periodic[2]);
+  p.x = wrap_single(p.x + k.dt * vx, b.lo[0], b.L[0], b.periodic[0]);
+  p.y = wrap_single(p.y + k.dt * vy, b.lo[1], b.L[1], b.periodic[1]);
+  p.z = wrap_single(p.z + k.dt * vz, b.lo[2], b.L[2], b.periodic[2]);
   k.v[3ll * i] = vx;
   k.v[3ll * i + 1] = vy;
   k.v[3ll * i + 2] = vz;
   k.pos4[i] = p;
-  k.q[i] = make_int4(encode_q(p.x, k.b.qlo[0], k.b.qinv[0]), encode_q(p.y, k.b.qlo[1], k.b.qinv[1]),
-                     encode_q(p.z, k.b.qlo[2], k.b.qinv[2]), t);
+  k.q[i] = make_int4(encode_q(p.x, b.qlo[0], b.qinv[0]), encode_q(p.y, b.qlo[1], b.qinv[1]),
+                     encode_q(p.z, b.qlo[2], b.qinv[2]), t);
 }
 
 // Pass 3: f_ij = -(phi' + fp_i rho'_tj + fp_j rho'_ti)/r * (r_i - r_j).
@@ -742,7 +747,7 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
                       static_cast<float>(fz.value()));
     }
   }
-  if (KD && blockIdx.x == 0 && threadIdx.x == 0) *kd.step += 1;
+  if (KD && kd.step && blockIdx.x == 0 && threadIdx.x == 0) *kd.step += 1;
   if (EV) write_ev_partials(pe, w, partials);
 }
 

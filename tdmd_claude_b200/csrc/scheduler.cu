@@ -627,7 +627,7 @@ void Scheduler::enqueue_force(bool ev, bool kd) {
                           cfg_.dt,
                           reinterpret_cast<long long*>(reinterpret_cast<char*>(ctl_.data()) +
                                                        offsetof(SchedCtl, step)),
-                          box_};
+                          box_, nullptr, nullptr};
       launch_eam_force<GeoQ, true, float, float>(gg, nl, n_, eam_->d32, types, fp32_.data(),
                                                  f32_.data(), ev, part2, lpa_, s,
                                                  kd ? &kdr : nullptr);
