@@ -538,6 +538,15 @@ __device__ __forceinline__ float4 ldv4<float>(const float4* p) {
   return ld_keep(p);
 }
 
+// Both force rows of a single-type FP32 bin, (rho'_t) then (phi'), 32 bytes
+// on a 32-byte boundary (one sector), in one 256-bit load: one L1 request per
+// pair instead of two.
+__device__ __forceinline__ void ld_rows2(const float4* p, float4& a, float4& b) {
+  asm("ld.global.nc.L1::evict_last.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+
 // Embedding F(rho), F'(rho) in FP64 (SplineTable eval/eval_deriv on F).
 __device__ __forceinline__ void embed_eval(const double4* ftab, int nrho, double drho, int t,
                                            double rho, double& F, double& dF) {
@@ -711,8 +720,14 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
           const int j = jj[u];
           const int tj = MULTI ? __ldg(types + j) - 1 : 0;
           const auto* rowp = e.rtab + static_cast<long long>(idx) * e.S;
-          const auto cphi = ldv4<T>(rowp + (MULTI ? phi_slot(ti, tj, e.ntypes) : 1));
-          const T drj = dspl_der(ldv4<T>(rowp + tj), sx);
+          typename V4<T>::type cphi, crho;
+          if constexpr (!MULTI && sizeof(T) == sizeof(float)) {
+            ld_rows2(rowp, crho, cphi);  // single type: S = 2, slots rho', phi'
+          } else {
+            cphi = ldv4<T>(rowp + (MULTI ? phi_slot(ti, tj, e.ntypes) : 1));
+            crho = ldv4<T>(rowp + tj);
+          }
+          const T drj = dspl_der(crho, sx);
           T dri = drj;
           if (MULTI && tj != ti) dri = dspl_der(ldv4<T>(rowp + ti), sx);
           T fpj;
