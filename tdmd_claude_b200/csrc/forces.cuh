@@ -70,6 +70,14 @@ __device__ __forceinline__ float4 ld_keep(const float4* p) {
       : "l"(p));
   return v;
 }
+// One 32-byte record (32-byte aligned) in one 256-bit load.
+__device__ __forceinline__ double4 ld_d4(const double4* p) {
+  double4 v;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+      : "l"(p));
+  return v;
+}
 __device__ __forceinline__ int4 ld_stream(const int4* p) {
   int4 v;
   asm("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
@@ -154,10 +162,8 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
   double L[3], halfL[3];
   int per[3];
   __device__ __forceinline__ double3 load(int i) const {
-    const double2* q = reinterpret_cast<const double2*>(p + i);
-    const double2 a = __ldg(q);
-    const double b = __ldg(reinterpret_cast<const double*>(q + 1));
-    return make_double3(a.x, a.y, b);
+    const double4 a = ld_d4(p + i);
+    return make_double3(a.x, a.y, a.z);
   }
   __device__ __forceinline__ Own own(int i) const { return load(i); }
   __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
@@ -529,9 +535,7 @@ template <class T>
 __device__ __forceinline__ typename V4<T>::type ldv4(const typename V4<T>::type* p);
 template <>
 __device__ __forceinline__ double4 ldv4<double>(const double4* p) {
-  const double2* q = reinterpret_cast<const double2*>(p);
-  const double2 a = __ldg(q), b = __ldg(q + 1);
-  return make_double4(a.x, a.y, b.x, b.y);
+  return ld_d4(p);
 }
 template <>
 __device__ __forceinline__ float4 ldv4<float>(const float4* p) {

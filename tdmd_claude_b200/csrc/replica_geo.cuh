@@ -76,10 +76,8 @@ struct GeoD4B {
   const int* rep;
   const RepImg* img;
   __device__ __forceinline__ double3 load(int i) const {
-    const double2* q = reinterpret_cast<const double2*>(p + i);
-    const double2 a = __ldg(q);
-    const double b = __ldg(reinterpret_cast<const double*>(q + 1));
-    return make_double3(a.x, a.y, b);
+    const double4 a = ld_d4(p + i);
+    return make_double3(a.x, a.y, a.z);
   }
   __device__ __forceinline__ Own own(int i) const {
     const double3 a = load(i);
