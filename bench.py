@@ -201,6 +201,45 @@ def mean_neighbors(sysm, cutoff):
     return float(c.mean())
 
 
+def fcc_neighbors(a, r_list):
+    """Sites of a perfect FCC lattice (constant a) within r_list of a site:
+    the listed full-list length K the gather model counts."""
+    m = int(np.ceil(2.0 * r_list / a)) + 1
+    g = np.arange(-m, m + 1)
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    fcc = ((x + y + z) % 2) == 0          # FCC sites in units of a/2
+    r2 = (x * x + y * y + z * z) * (0.5 * a) ** 2
+    return int(np.count_nonzero(fcc & (r2 > 0) & (r2 < r_list * r_list)))
+
+
+def cell_occupancy(n, L, r_list):
+    """Atoms per cell of the reference grid, nc = max(3, floor(L / r_list))."""
+    nc = max(3, int(np.floor(L / r_list)))
+    return n / nc ** 3
+
+
+def path_roofline(value, pot, precision, K, n_cell, hbm_gbs, R=None):
+    """Whole-step gather model (bytes per atom-step) and the fraction of the
+    measured HBM bandwidth it implies at `value` atom-steps/s.  Per atom-step:
+    EAM FP64 224 + 64K, mixed 228 + 44K; Morse FP64 168 + 28K, mixed
+    152 + 20K; plus the list build amortised over R steps,
+    (27 n_cell (s_pos + 4) + 4K + 24) / R with s_pos = 24 (FP64) / 16 (mixed).
+    Every neighbor access counts once (no cache reuse); spline tables are
+    cache-resident."""
+    R = R or WINDOW
+    mixed = precision == "mixed"
+    if pot == "eam":
+        base = 228 + 44 * K if mixed else 224 + 64 * K
+    else:
+        base = 152 + 20 * K if mixed else 168 + 28 * K
+    s_pos = 16 if mixed else 24
+    b = base + (27 * n_cell * (s_pos + 4) + 4 * K + 24) / R
+    ach = value * b / 1e9
+    return {"bytes_per_atom_step": round(float(b), 1), "K": K, "atoms_per_cell": round(n_cell, 2),
+            "achieved_gbs": ach, "frac": ach / hbm_gbs if hbm_gbs else None,
+            "model": "gather model, whole step + list build / R"}
+
+
 def timed_windows(sched, steps, warmup, flush, torch, dist=None):
     """Device ms per window (L2 flushed before each), max over ranks."""
     stream = torch.cuda.ExternalStream(sched.stream())
@@ -342,8 +381,15 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
     slopes = np.polyfit(t_ns, etot, 1)[0] if len(t_ns) > 1 else np.zeros(len(systems))
     b.close()
     atoms = sum_over_ranks(info["natoms"], dist, "cuda")
+    slopes = np.atleast_1d(slopes)
     value = atoms * WINDOW * steps / (ms * 1e-3)
+    hbm, _ = measured_peaks()
+    K = fcc_neighbors(3.615, W.MORSE_CU[3] + SKIN)
+    occ = float(np.sum([s.n * cell_occupancy(s.n, s.hi[0] - s.lo[0], W.MORSE_CU[3] + SKIN)
+                        for s in systems]) / np.sum([s.n for s in systems]))
     return {"value": value, "unit": "atom-steps/s", "ms_per_window": ms / steps,
+            "timesteps_per_s_each_replica": WINDOW * steps / (ms * 1e-3),
+            "path_roofline": path_roofline(value, "morse", precision, K, occ, hbm),
             "replicas": 512, "atoms": int(atoms), "ranks": world, "precision": precision,
             "lanes_per_atom": info["lanes_per_atom"], "kernel_launches_timed": launches,
             "drift_ev_per_atom_per_ns": {"median_abs": float(np.median(np.abs(slopes))),
@@ -351,7 +397,8 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
                                          "over_ps": float(t_ns[-1] - t_ns[0]) * 1e3
                                          if len(t_ns) > 1 else 0.0},
             "workload": "512 Cu FCC Morse replicas, n^3 cells n~U{4..16}, T~U(100,1500) K, "
-                        "rc 6.0 skin 0.3, K=10 steps per graph"}
+                        "rc 6.0 skin 0.3, K=10 steps per graph",
+            "_slopes": slopes}
 
 
 def ternary_bench(steps, warmup, flush, torch):
@@ -372,7 +419,14 @@ def ternary_bench(steps, warmup, flush, torch):
     s.close()
     n_dof = 3 * sysm.n - 3
     temp = 2.0 * ke / (n_dof * 8.617333262e-5)
-    return {"value": sysm.n * WINDOW * steps / (ms * 1e-3), "unit": "atom-steps/s",
+    value = sysm.n * WINDOW * steps / (ms * 1e-3)
+    hbm, _ = measured_peaks()
+    rl = t.cutoff + SKIN
+    return {"value": value, "unit": "atom-steps/s",
+            "timesteps_per_s": WINDOW * steps / (ms * 1e-3),
+            "path_roofline": path_roofline(value, "eam", "mixed", fcc_neighbors(3.56, rl),
+                                           cell_occupancy(sysm.n, sysm.hi[0] - sysm.lo[0], rl),
+                                           hbm),
             "ms_per_window": ms / steps, "atoms": sysm.n, "precision": "mixed",
             "kernel_launches_timed": launches, "dt_ps_at_end": dt, "temperature_K_at_end": temp,
             "workload": "ternary FCC alloy 100^3 cells (4,000,000 atoms), EAM 3 species, "
@@ -470,7 +524,14 @@ def batch_eam_bench(steps, warmup, flush, torch, eam, precision, nrep=8):
     ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, None)
     info = b.info()
     b.close()
-    return {"value": info["natoms"] * WINDOW * steps / (ms * 1e-3), "unit": "atom-steps/s",
+    value = info["natoms"] * WINDOW * steps / (ms * 1e-3)
+    hbm, _ = measured_peaks()
+    rl = eam.cutoff() + SKIN
+    s0 = systems[0]
+    return {"value": value, "unit": "atom-steps/s",
+            "timesteps_per_s_each_replica": WINDOW * steps / (ms * 1e-3),
+            "path_roofline": path_roofline(value, "eam", precision, fcc_neighbors(3.615, rl),
+                                           cell_occupancy(s0.n, s0.hi[0] - s0.lo[0], rl), hbm),
             "ms_per_window": ms / steps, "replicas": nrep, "atoms": info["natoms"],
             "lanes_per_atom": info["lanes_per_atom"], "kernel_launches_timed": launches}
 
@@ -658,6 +719,16 @@ def main():
     if not args.no_batch:
         batch = {p: batch_bench(args.steps, args.warmup, flush, torch, p, dist, rank, world)
                  for p in ("mixed", "fp64")}
+        # The Morse pair term is truncated at rc without a shift (as the
+        # reference's), so E_total jumps by U(rc) each time a pair crosses
+        # rc: the per-replica drift above is that physics, alike in FP64.
+        # The precision effect is the per-replica mixed - FP64 difference.
+        dd = np.abs(batch["mixed"].pop("_slopes") - batch["fp64"].pop("_slopes"))
+        batch["drift_mixed_minus_fp64_ev_per_atom_per_ns"] = {
+            "median_abs": float(np.median(dd)), "max_abs": float(np.max(dd)),
+            "note": "Morse truncated at rc without shift (reference form): E_total "
+                    "jumps by U(rc) = -9.6 meV per pair crossing, so single-run drift "
+                    "is physical; same seeds and windows in both precisions"}
 
     beam = None
     if not args.no_batch:
@@ -670,6 +741,7 @@ def main():
                                                            torch)
 
     hbm, peak_kind = measured_peaks()
+    occ = cell_occupancy(sysm.n, sysm.hi[0] - sysm.lo[0], eam.cutoff() + SKIN)
     # gather model of the mixed force pass, plus the next step's kick + drift
     # it carries on (WINDOW-1) of WINDOW launches (144 B per atom)
     force_bytes = sysm.n * (48 + 24 * K) + sysm.n * 144 * (WINDOW - 1) / WINDOW
@@ -711,7 +783,11 @@ def main():
                 "mean_neighbors_K": K,
                 "lanes_per_atom": {"mixed": lanes32, "fp64": lanes64,
                                    "autotune_ms_mixed": tune32, "autotune_ms_fp64": tune64},
-                "fp64": {"value": value64, "ms_per_step": ms_fp64 / args.steps},
+                "timesteps_per_s": value / sysm.n,
+                "path_roofline": path_roofline(value, "eam", "mixed", K, occ, hbm),
+                "fp64": {"value": value64, "ms_per_step": ms_fp64 / args.steps,
+                         "timesteps_per_s": value64 / sysm.n,
+                         "path_roofline": path_roofline(value64, "eam", "fp64", K, occ, hbm)},
                 "mixed_over_fp64": value / value64,
                 "force_rel_rms_err_mixed_vs_fp64": rel_err,
                 "nvt_mixed": {"value": value_nvt, "ms_per_step": ms_nvt / args.steps,
