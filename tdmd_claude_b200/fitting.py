@@ -143,9 +143,13 @@ def eam_loss(F, rho, phi, fm: ForceMatch, tables: dict):
     return _autograd()[1].apply(F, rho, phi, fm, tables)
 
 
-def adam_fit(loss_fn, params: list, steps: int = 200, lr: float = 1e-3):
+def adam_fit(loss_fn, params: list, steps: int = 200, lr: float = 1e-3,
+             lr_final: float | None = None):
     """Runs `steps` Adam steps on loss_fn(*params); returns (losses, seconds)
-    with the time measured by CUDA events around the loop."""
+    with the time measured by CUDA events around the loop.  lr_final: the
+    step size decays from lr to lr_final on a cosine (constant without)."""
+    import math
+
     import torch
     opt = torch.optim.Adam(params, lr=lr)
     losses = torch.zeros(steps, dtype=torch.float64, device=params[0].device)
@@ -153,6 +157,10 @@ def adam_fit(loss_fn, params: list, steps: int = 200, lr: float = 1e-3):
     torch.cuda.synchronize()
     start.record()
     for k in range(steps):
+        if lr_final is not None:
+            c = 0.5 * (1.0 + math.cos(math.pi * k / max(1, steps - 1)))
+            for grp in opt.param_groups:
+                grp["lr"] = lr_final + (lr - lr_final) * c
         opt.zero_grad(set_to_none=True)
         loss = loss_fn(*params)
         loss.backward()
