@@ -177,6 +177,15 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* smem) {
   }
 }
 
+// One read-only 32-byte record (32-byte aligned) in one 256-bit load.
+__device__ __forceinline__ double4 ld_d4(const double4* p) {
+  double4 v;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+      : "l"(p));
+  return v;
+}
+
 inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
 
 // Number of SMs of the current device (148 on B200), cached per process.

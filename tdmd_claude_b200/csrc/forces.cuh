@@ -70,14 +70,6 @@ __device__ __forceinline__ float4 ld_keep(const float4* p) {
       : "l"(p));
   return v;
 }
-// One 32-byte record (32-byte aligned) in one 256-bit load.
-__device__ __forceinline__ double4 ld_d4(const double4* p) {
-  double4 v;
-  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
-      : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
-      : "l"(p));
-  return v;
-}
 __device__ __forceinline__ int4 ld_stream(const int4* p) {
   int4 v;
   asm("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"

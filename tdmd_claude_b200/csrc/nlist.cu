@@ -44,10 +44,8 @@ struct LoadAoS3 {
 struct LoadD4 {
   const double4* p;
   __device__ __forceinline__ double3 operator()(int i) const {
-    const double2* q = reinterpret_cast<const double2*>(p + i);
-    const double2 a = __ldg(q);
-    const double b = __ldg(reinterpret_cast<const double*>(q + 1));
-    return make_double3(a.x, a.y, b);
+    const double4 a = ld_d4(p + i);
+    return make_double3(a.x, a.y, a.z);
   }
 };
 
