@@ -352,7 +352,8 @@ def nve_drift(sysm, eam, precision, lanes, nsteps, every=100):
             "max_abs_dev_ev_per_atom": float(np.abs(e - e[0]).max()) if len(e) else None}
 
 
-def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=0, world=1):
+def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=0, world=1,
+                lanes=None):
     """Batched replicas: 512 independent Cu FCC Morse systems (n^3 cells,
     n uniform 4..16, 100-1500 K), NVE, K = 10 steps per graph-replayed
     window; aggregate atom-steps/s and per-replica energy drift."""
@@ -366,8 +367,8 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
     b = ReplicaBatch([Box.make(s.lo, s.hi) for s in systems], [s.n for s in systems],
                      MorseParams.make(*W.MORSE_CU),
                      make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW, precision=precision,
-                                 energy_every=WINDOW,
-                                 energy_log_capacity=steps + warmup + 8))
+                                 energy_every=WINDOW, energy_log_capacity=steps + warmup + 8,
+                                 **({"lanes_per_atom": lanes} if lanes else {})))
     b.upload(np.concatenate([s.positions for s in systems]),
              np.concatenate([s.velocities for s in systems]),
              np.concatenate([s.types for s in systems]), systems[0].masses)
@@ -643,8 +644,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the mixed timed windows (for profiler captures); no JSON line")
-    ap.add_argument("--lanes", type=int, default=2,
-                    help="lanes per atom for --kernels-only (no autotune there)")
+    ap.add_argument("--case", default="eam-mixed",
+                    choices=["eam-mixed", "eam-fp64", "eam-nvt-ev", "morse-batch",
+                             "morse-batch-fp64"],
+                    help="workload of --kernels-only: the 131,072-atom EAM system (mixed, "
+                         "FP64, or mixed NVT with energy/virial every step), or the 512 "
+                         "Morse replicas")
+    ap.add_argument("--lanes", type=int, default=None,
+                    help="lanes per atom for --kernels-only (EAM: default 2, no autotune; "
+                         "Morse replicas: autotuned unless given)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip timing the reference's own GPU scheduler")
     ap.add_argument("--no-fit", action="store_true",
@@ -682,10 +690,20 @@ def main():
     eam = make_eam(t)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     if args.kernels_only:
-        s32 = make_sched(sysm, eam, "mixed", lanes_per_atom=args.lanes)
-        s32.run_until(0)
-        timed_windows(s32, args.steps, args.warmup, flush, torch, dist)
-        s32.close()
+        if args.case.startswith("morse-batch"):
+            prec = "fp64" if args.case.endswith("fp64") else "mixed"
+            batch_bench(args.steps, args.warmup, flush, torch, prec, dist, rank, world,
+                        args.lanes)
+        else:
+            prec = "fp64" if args.case == "eam-fp64" else "mixed"
+            kw = {}
+            if args.case == "eam-nvt-ev":
+                kw = dict(t_target=300.0, t_period=0.1, nhc_length=3, energy_every=1,
+                          energy_log_capacity=16)
+            s32 = make_sched(sysm, eam, prec, lanes_per_atom=args.lanes or 2, **kw)
+            s32.run_until(0)
+            timed_windows(s32, args.steps, args.warmup, flush, torch, dist)
+            s32.close()
         if dist is not None:
             dist.destroy_process_group()
         return

@@ -224,6 +224,8 @@ struct BatchStep {
   bool first, rebuild;
   bool kd_fused;   // kick + drift done by the previous step's force pass
   bool fuse_next;  // this force pass also kicks and drifts for the next step
+  bool log_e;      // window end of a logged window: the force pass also writes
+                   // per-atom energies, reduced per replica after the half kick
 };
 
 }  // namespace
@@ -262,7 +264,8 @@ class Batch {
 
  private:
   void rebuild(int* status);
-  void force(bool kd = false);
+  void force(bool kd = false, bool pe_atom = false);
+  void rep_energy();
   void kick_drift(bool full);
   void half_kick();
   void enqueue_step(const BatchStep& st);
@@ -541,7 +544,7 @@ void Batch::rebuild(int* status) {
   ++rebuilds_;
 }
 
-void Batch::force(bool kd) {
+void Batch::force(bool kd, bool pea) {
   cudaStream_t s = stream_;
   const NbrView nl = view();
   const int n = static_cast<int>(n_);
@@ -554,30 +557,36 @@ void Batch::force(bool kd) {
       const GeoQB g{q_.data(), rep_.data(), scales_.data()};
       const GeoQB gg{g_.data(), rep_.data(), scales_.data()};
       launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), nullptr, nullptr,
-                                       g_.data(), false, nullptr, lpa_, s);
+                                       g_.data(), false, nullptr, lpa_, s,
+                                       pea ? pe_atom_.data() : nullptr);
       // kd: the next step's kick + drift in the same pass (the force pass
       // reads gather records only), each atom in its replica's box
       const KickDrift kdr{pos4_.data(), q_.data(), vel_.data(), types_.data(), inv_mm_.data(),
                           cfg_.dt, nullptr, DevBox{}, rep_.data(), reps_.data()};
       launch_eam_force<GeoQB, true, float, float>(gg, nl, n, eam_->d32, types, fp32_.data(),
-                                                  f32_.data(), false, nullptr, lpa_, s,
-                                                  kd ? &kdr : nullptr);
+                                                  f32_.data(), pea, nullptr, lpa_, s,
+                                                  kd ? &kdr : nullptr,
+                                                  pea ? pe_atom_.data() : nullptr);
     } else {
       const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
       launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), nullptr,
-                                         nullptr, nullptr, false, nullptr, lpa_, s);
+                                         nullptr, nullptr, false, nullptr, lpa_, s,
+                                         pea ? pe_atom_.data() : nullptr);
       launch_eam_force<GeoD4B, false, double, double>(g, nl, n, eam_->d64, types, fp64_.data(),
-                                                      f64_.data(), false, nullptr, lpa_, s);
+                                                      f64_.data(), pea, nullptr, lpa_, s,
+                                                      nullptr, pea ? pe_atom_.data() : nullptr);
     }
     launches_ += 2;
     return;
   }
   if (mixed_) {
     const GeoQB g{q_.data(), rep_.data(), scales_.data()};
-    launch_morse(g, nl, n, m32_, f32_.data(), false, nullptr, lpa_, s);
+    launch_morse(g, nl, n, m32_, f32_.data(), pea, nullptr, lpa_, s,
+                 pea ? pe_atom_.data() : nullptr);
   } else {
     const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
-    launch_morse(g, nl, n, m64_, f64_.data(), false, nullptr, lpa_, s);
+    launch_morse(g, nl, n, m64_, f64_.data(), pea, nullptr, lpa_, s,
+                 pea ? pe_atom_.data() : nullptr);
   }
   ++launches_;
 }
@@ -629,7 +638,7 @@ void Batch::half_kick() {
 void Batch::enqueue_step(const BatchStep& st) {
   if (!st.kd_fused) kick_drift(!st.first);
   if (st.rebuild) rebuild(status_.data());
-  force(st.fuse_next);
+  force(st.fuse_next, st.log_e);
 }
 
 void Batch::run_segment(const std::vector<BatchStep>& seg, bool finalize) {
@@ -637,12 +646,19 @@ void Batch::run_segment(const std::vector<BatchStep>& seg, bool finalize) {
   key.reserve(seg.size() + 1);
   for (const auto& st : seg)
     key.push_back((st.first ? 1 : 0) | (st.rebuild ? 2 : 0) | (st.kd_fused ? 4 : 0) |
-                  (st.fuse_next ? 8 : 0));
+                  (st.fuse_next ? 8 : 0) | (st.log_e ? 16 : 0));
   key.push_back(finalize ? 1 : 0);
   const long long l0 = launches_;
+  // the window's closing half kick, then (logged windows) the per-replica
+  // energies of the integer-time state
+  auto close = [&] {
+    if (!finalize) return;
+    half_kick();
+    if (!seg.empty() && seg.back().log_e) rep_energy();
+  };
   if (!cfg_.use_graphs) {
     for (const auto& st : seg) enqueue_step(st);
-    if (finalize) half_kick();
+    close();
     return;
   }
   auto it = graphs_.find(key);
@@ -659,7 +675,7 @@ void Batch::run_segment(const std::vector<BatchStep>& seg, bool finalize) {
     TDMD_CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     try {
       for (const auto& st : seg) enqueue_step(st);
-      if (finalize) half_kick();
+      close();
     } catch (...) {
       cudaStreamEndCapture(stream_, &g);
       if (g) cudaGraphDestroy(g);
@@ -769,6 +785,11 @@ void Batch::run_until(int target) {
     TDMD_CU(cudaMemsetAsync(status_.data(), 0, sizeof(int) * 4, s));
     std::vector<BatchStep> plan;
     int since = since_rebuild_;
+    // energy log of windows whose last step is a multiple of energy_every
+    // (velocities at integer time), computed inside the window
+    const int log_cap = cfg_.energy_log_capacity > 0 ? cfg_.energy_log_capacity : 1024;
+    const bool log_now = cfg_.energy_every > 0 && target % cfg_.energy_every == 0 &&
+                         static_cast<int>(log_steps_.size()) < log_cap;
     for (int st = step_; st < target; ++st) {
       BatchStep b{};
       b.first = st == step_;
@@ -779,6 +800,7 @@ void Batch::run_until(int target) {
       // drifts for the next step (energies are logged after the window)
       b.fuse_next = eam_ && mixed_ && st + 1 < target;
       b.kd_fused = !plan.empty() && plan.back().fuse_next;
+      b.log_e = log_now && st + 1 == target;
       plan.push_back(b);
     }
     size_t a = 0;
@@ -801,6 +823,14 @@ void Batch::run_until(int target) {
     if (!st[0]) {
       step_ = target;
       since_rebuild_ = since;
+      if (log_now) {
+        std::vector<double> e(2 * static_cast<size_t>(nrep_));
+        TDMD_CU(cudaMemcpyAsync(e.data(), eout_.data(), sizeof(double) * e.size(),
+                                cudaMemcpyDeviceToHost, s));
+        TDMD_CU(cudaStreamSynchronize(s));
+        log_steps_.push_back(static_cast<double>(step_));
+        log_.insert(log_.end(), e.begin(), e.end());
+      }
       break;
     }
     if (attempt >= 3)
@@ -820,17 +850,6 @@ void Batch::run_until(int target) {
     // restored state (the window start).
     rebuild(nullptr);
     force();
-  }
-  // Energy log at the end of windows whose last step is a multiple of
-  // energy_every (velocities are at integer time here).
-  if (cfg_.energy_every > 0 && step_ % cfg_.energy_every == 0) {
-    const int cap = cfg_.energy_log_capacity > 0 ? cfg_.energy_log_capacity : 1024;
-    if (static_cast<int>(log_steps_.size()) < cap) {
-      std::vector<double> e(2 * static_cast<size_t>(nrep_));
-      reduce_energies(e.data());
-      log_steps_.push_back(static_cast<double>(step_));
-      log_.insert(log_.end(), e.begin(), e.end());
-    }
   }
 }
 
@@ -874,13 +893,19 @@ void Batch::reduce_energies(double* out) {
     }));
     TDMD_LAUNCH_CHECK();
   }
-  k_rep_energy<<<nrep_, kThreads, 0, s>>>(pe_atom_.data(), vel_.data(), types_.data(),
-                                          masses_.data(), reps_.data(), eout_.data());
-  TDMD_LAUNCH_CHECK();
-  launches_ += 2;
+  launches_ += 1;
+  rep_energy();
   TDMD_CU(cudaMemcpyAsync(out, eout_.data(), sizeof(double) * 2 * nrep_, cudaMemcpyDeviceToHost,
                           s));
   TDMD_CU(cudaStreamSynchronize(s));
+}
+
+// Per-replica (PE, KE) from pe_atom_ and the velocities, into eout_.
+void Batch::rep_energy() {
+  k_rep_energy<<<nrep_, kThreads, 0, stream_>>>(pe_atom_.data(), vel_.data(), types_.data(),
+                                                masses_.data(), reps_.data(), eout_.data());
+  TDMD_LAUNCH_CHECK();
+  ++launches_;
 }
 
 void Batch::energies(double* pe, double* ke) {

@@ -377,10 +377,13 @@ struct MorseP {
   double r0d;
 };
 
-template <class Geo, int LPA, bool EV, bool VEC, class F>
+// EV: 0 forces only; 1 also energy + virial into per-block partials and,
+// where pe_atom is given, per-atom energies; 2 forces + per-atom energies.
+template <class Geo, int LPA, int EV, bool VEC, class F>
 __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
                                                MorseP<typename Geo::T> mp, ForceOut<F> out,
-                                               double* __restrict__ partials) {
+                                               double* __restrict__ partials,
+                                               double* __restrict__ pe_atom) {
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;
@@ -419,7 +422,7 @@ __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
           fz.add(mul_rn(fpair, pr[u].dz));
           if (EV) {
             pe += 0.5 * static_cast<double>(mp.d * (ome * ome - T(1)));
-            add_virial(w, fpair, pr[u].dx, pr[u].dy, pr[u].dz);
+            if (EV == 1) add_virial(w, fpair, pr[u].dx, pr[u].dy, pr[u].dz);
           }
         }
       }
@@ -432,7 +435,16 @@ __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
     fz.shfl_merge(o);
   }
   if (active && sub == 0) out.store(i, fx.value(), fy.value(), fz.value());
-  if (EV) write_ev_partials(pe, w, partials);
+  if (EV) {
+    // per-atom energy (nullable): the lanes' sums merged pairwise
+    if (pe_atom) {
+      double pa = pe;
+#pragma unroll
+      for (int o = LPA / 2; o > 0; o >>= 1) pa += __shfl_xor_sync(0xffffffffu, pa, o);
+      if (active && sub == 0) pe_atom[i] = pa;
+    }
+    if (EV == 1 && partials) write_ev_partials(pe, w, partials);
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -565,7 +577,8 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
                                                      double* __restrict__ rho_out,
                                                      double* __restrict__ fpd_out,
                                                      int4* __restrict__ gout,
-                                                     double* __restrict__ partials) {
+                                                     double* __restrict__ partials,
+                                                     double* __restrict__ e_out) {
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;
@@ -615,6 +628,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
     fp_out[i] = static_cast<FP>(dF);
     if (rho_out) rho_out[i] = rh;
     if (fpd_out) fpd_out[i] = dF;
+    if (e_out) e_out[i] = Fi;
     if constexpr (Geo::kRecords) {
       if (gout) {
         int4 rec = g.record(o);
@@ -623,7 +637,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
       }
     }
   }
-  if (EV) {
+  if (EV && partials) {
     const double w[6] = {0, 0, 0, 0, 0, 0};
     write_ev_partials(Fi, w, partials);
   }
@@ -673,14 +687,15 @@ __device__ __forceinline__ void kick_drift_atom(const KickDrift& k, int i, float
 // FPG: F'(rho_j) comes with the neighbor's gather record (pair w bits)
 // instead of the fp array.  KD (FPG, float forces): then the next step's
 // kick + drift of the same atom.
-template <class Geo, int LPA, bool EV, bool FPG, bool VEC, bool MULTI, class FP, class F,
+template <class Geo, int LPA, int EV, bool FPG, bool VEC, bool MULTI, class FP, class F,
           bool KD = false>
 __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
                                                    EamDev<typename Geo::T> e,
                                                    const int* __restrict__ types,
                                                    const FP* __restrict__ fp, ForceOut<F> out,
                                                    double* __restrict__ partials,
-                                                   KickDrift kd = {}) {
+                                                   KickDrift kd = {},
+                                                   double* __restrict__ pe_atom = nullptr) {
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;
@@ -738,7 +753,7 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
           fz.add(mul_rn(fpair, pr[u].dz));
           if (EV) {
             pe += 0.5 * static_cast<double>(dspl_val(cphi, sx));
-            add_virial(w, fpair, pr[u].dx, pr[u].dy, pr[u].dz);
+            if (EV == 1) add_virial(w, fpair, pr[u].dx, pr[u].dy, pr[u].dz);
           }
         }
       }
@@ -759,7 +774,17 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
     }
   }
   if (KD && kd.step && blockIdx.x == 0 && threadIdx.x == 0) *kd.step += 1;
-  if (EV) write_ev_partials(pe, w, partials);
+  if (EV) {
+    // per-atom energy (nullable): the lanes' pair sums merged pairwise, plus
+    // the embedding energy F(rho_i) the density pass stored there
+    if (pe_atom) {
+      double pa = pe;
+#pragma unroll
+      for (int o = LPA / 2; o > 0; o >>= 1) pa += __shfl_xor_sync(0xffffffffu, pa, o);
+      if (active && sub == 0) pe_atom[i] = pa + pe_atom[i];
+    }
+    if (EV == 1 && partials) write_ev_partials(pe, w, partials);
+  }
 }
 
 // Sums nblk partial records (kEvStride doubles each) in block order and

@@ -47,63 +47,75 @@ inline bool vec_rows(const NbrView& nl) { return nl.row_off == nullptr && nl.cap
     default: throw Error{TDMD_ERR_INVALID_ARGUMENT, "lanes per atom must be 1,2,4,8,16,32"}; \
   }
 
-// Morse forces; with ev, per-block partials (force_blocks records).
+// Morse forces; with ev, per-block partials (force_blocks records; nullable)
+// and per-atom energies (pe_atom, nullable).
 template <class Geo, class F>
 void launch_morse(const Geo& g, const NbrView& nl, int n, const MorseP<typename Geo::T>& mp,
-                  F* forces, bool ev, double* partials, int lpa, cudaStream_t s) {
+                  F* forces, bool ev, double* partials, int lpa, cudaStream_t s,
+                  double* pe_atom = nullptr) {
   const int nblk = force_blocks(n, lpa);
   TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
-    if (ev)
-      k_morse<Geo, L, true, V, F><<<nblk, kForceThreads, 0, s>>>(g, nl, n, mp,
-                                                                 ForceOut<F>{forces}, partials);
+    if (ev && !partials && pe_atom)  // per-atom energies only
+      k_morse<Geo, L, 2, V, F><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, mp, ForceOut<F>{forces}, nullptr, pe_atom);
+    else if (ev)
+      k_morse<Geo, L, 1, V, F><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, mp, ForceOut<F>{forces}, partials, pe_atom);
     else
-      k_morse<Geo, L, false, V, F><<<nblk, kForceThreads, 0, s>>>(g, nl, n, mp,
-                                                                  ForceOut<F>{forces}, nullptr);
+      k_morse<Geo, L, 0, V, F><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, mp, ForceOut<F>{forces}, nullptr, nullptr);
   }));
   TDMD_LAUNCH_CHECK();
 }
 
 // Density + embedding pass.  gout (fixed-point geometries only) receives
-// the force pass's {q, F'} gather records.
+// the force pass's {q, F'} gather records; e_out (nullable) each atom's
+// embedding energy F(rho_i).
 template <class Geo, class FP>
 void launch_eam_density(const Geo& g, const NbrView& nl, int n,
                         const EamDev<typename Geo::T>& e, const int* types, FP* fp,
                         double* rho_out, double* fpd_out, int4* gout, bool ev, double* partials,
-                        int lpa, cudaStream_t s) {
+                        int lpa, cudaStream_t s, double* e_out = nullptr) {
   const int nblk = force_blocks(n, lpa);
   TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
     if (ev)
       k_eam_density<Geo, L, true, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, e, types, fp, rho_out, fpd_out, gout, partials);
+          g, nl, n, e, types, fp, rho_out, fpd_out, gout, partials, e_out);
     else
       k_eam_density<Geo, L, false, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, e, types, fp, rho_out, fpd_out, gout, nullptr);
+          g, nl, n, e, types, fp, rho_out, fpd_out, gout, nullptr, e_out);
   })));
   TDMD_LAUNCH_CHECK();
 }
 
 // Force pass.  FPG: the geometry reads gather records that carry F'(rho).
 // kd (nullable; FPG with float forces only): also apply the next step's
-// kick + drift to each atom after its force.
+// kick + drift to each atom after its force.  With ev: per-block partials
+// (nullable) and per-atom energies added to pe_atom (nullable; holds
+// F(rho_i) from the density pass).
 template <class Geo, bool FPG, class FP, class F>
 void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typename Geo::T>& e,
                       const int* types, const FP* fp, F* forces, bool ev, double* partials,
-                      int lpa, cudaStream_t s, const KickDrift* kd = nullptr) {
+                      int lpa, cudaStream_t s, const KickDrift* kd = nullptr,
+                      double* pe_atom = nullptr) {
   const int nblk = force_blocks(n, lpa);
   TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
-    if (ev)
-      k_eam_force<Geo, L, true, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, e, types, fp, ForceOut<F>{forces}, partials);
+    if (ev && !partials && pe_atom)  // per-atom energies only
+      k_eam_force<Geo, L, 2, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr, KickDrift{}, pe_atom);
+    else if (ev)
+      k_eam_force<Geo, L, 1, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+          g, nl, n, e, types, fp, ForceOut<F>{forces}, partials, KickDrift{}, pe_atom);
     else if constexpr (FPG && sizeof(F) == sizeof(float)) {
       if (kd)
-        k_eam_force<Geo, L, false, FPG, V, M, FP, F, true><<<nblk, kForceThreads, 0, s>>>(
+        k_eam_force<Geo, L, 0, FPG, V, M, FP, F, true><<<nblk, kForceThreads, 0, s>>>(
             g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr, *kd);
       else
-        k_eam_force<Geo, L, false, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+        k_eam_force<Geo, L, 0, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
             g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
     } else {
       TDMD_REQUIRE(kd == nullptr, "fused kick-drift needs the mixed gather-record pass");
-      k_eam_force<Geo, L, false, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, 0, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
     }
   })));

@@ -151,8 +151,10 @@ def test_eam_batch_replicas_equal_single_schedulers(cuda, precision, ternary):
         systems.append(W.fcc_system(n, 3.615, temp, 70 + k, types=types,
                                     masses=(63.546,) * t.ntypes))
     cfg = dict(dt=0.001, r_skin=0.3, rebuild_every=10, precision=precision, lanes_per_atom=4)
+    # energy log at every window end: the window's last force pass writes the
+    # per-atom energies, which must equal the separate energy passes
     b = ReplicaBatch([Box.make(s.lo, s.hi) for s in systems], [s.n for s in systems], eam,
-                     make_config(**cfg))
+                     make_config(**cfg, energy_every=1, energy_log_capacity=4))
     b.upload(np.concatenate([s.positions for s in systems]),
              np.concatenate([s.velocities for s in systems]),
              np.concatenate([s.types for s in systems]), systems[0].masses)
@@ -160,6 +162,9 @@ def test_eam_batch_replicas_equal_single_schedulers(cuda, precision, ternary):
         b.run_until(target)
     pos, vel, frc = b.download()
     pe_b, ke_b = b.energies()
+    log_steps, pk = b.energy_log()
+    assert np.array_equal(log_steps, [10, 23])
+    assert np.array_equal(pk[-1, :, 0], pe_b) and np.array_equal(pk[-1, :, 1], ke_b)
     for r, s in enumerate(systems):
         sc = FastPipelineScheduler(Box.make(s.lo, s.hi), s.n, eam, make_config(**cfg))
         sc.upload(s.positions, s.velocities, None, s.types, s.ids, s.masses)
