@@ -336,12 +336,12 @@ def cpu_baseline_sample(sysm, t, nsteps):
     return sec, kind
 
 
-def nve_drift(sysm, eam, precision, lanes, nsteps, every=100):
+def nve_drift(sysm, eam, precision, lanes, nsteps, every=100, nbr_batch=0):
     """Total-energy drift of an NVE run from the device energy log:
     least-squares slope of E_total/N against time (eV/atom/ns) and the
     largest |E_total - E_0|/N."""
-    s = make_sched(sysm, eam, precision, lanes_per_atom=lanes, energy_every=every,
-                   energy_log_capacity=nsteps // every + 1)
+    s = make_sched(sysm, eam, precision, lanes_per_atom=lanes, nbr_batch=nbr_batch,
+                   energy_every=every, energy_log_capacity=nsteps // every + 1)
     s.run_until(nsteps)
     log = s.energy_log()
     s.close()
@@ -376,6 +376,7 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
     ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, dist)
     steps_log, pk = b.energy_log()
     info = b.info()
+    info["nbr_batch"] = b.stats().nbr_batch
     natoms = np.array([s.n for s in systems], np.float64)
     etot = (pk[:, :, 0] + pk[:, :, 1]) / natoms          # eV/atom per window
     t_ns = steps_log * DT * 1e-3
@@ -392,7 +393,8 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
             "timesteps_per_s_each_replica": WINDOW * steps / (ms * 1e-3),
             "path_roofline": path_roofline(value, "morse", precision, K, occ, hbm),
             "replicas": 512, "atoms": int(atoms), "ranks": world, "precision": precision,
-            "lanes_per_atom": info["lanes_per_atom"], "kernel_launches_timed": launches,
+            "lanes_per_atom": info["lanes_per_atom"], "nbr_batch": info["nbr_batch"],
+            "kernel_launches_timed": launches,
             "drift_ev_per_atom_per_ns": {"median_abs": float(np.median(np.abs(slopes))),
                                          "max_abs": float(np.max(np.abs(slopes))),
                                          "over_ps": float(t_ns[-1] - t_ns[0]) * 1e3
@@ -547,6 +549,7 @@ def batch_eam_bench(steps, warmup, flush, torch, eam, precision, nrep=8):
     b.run_until(0)
     ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, None)
     info = b.info()
+    info["nbr_batch"] = b.stats().nbr_batch
     b.close()
     value = info["natoms"] * WINDOW * steps / (ms * 1e-3)
     hbm, _ = measured_peaks()
@@ -557,7 +560,8 @@ def batch_eam_bench(steps, warmup, flush, torch, eam, precision, nrep=8):
             "path_roofline": path_roofline(value, "eam", precision, fcc_neighbors(3.615, rl),
                                            cell_occupancy(s0.n, s0.hi[0] - s0.lo[0], rl), hbm),
             "ms_per_window": ms / steps, "replicas": nrep, "atoms": info["natoms"],
-            "lanes_per_atom": info["lanes_per_atom"], "kernel_launches_timed": launches}
+            "lanes_per_atom": info["lanes_per_atom"], "nbr_batch": info["nbr_batch"],
+            "kernel_launches_timed": launches}
 
 
 def reference_gpu_sample(sysm, t, windows=10, warm=5):
@@ -714,8 +718,8 @@ def main():
     s32 = make_sched(sysm, eam, "mixed")
     s64.run_until(0)
     s32.run_until(0)
-    lanes32, tune32 = s32.autotune()
-    lanes64, tune64 = s64.autotune()
+    lanes32, nb32, tune32 = s32.autotune()
+    lanes64, nb64, tune64 = s64.autotune()
     f64 = s64.download().forces
     f32 = s32.download().forces.astype(np.float64)
     rel_err = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
@@ -744,7 +748,8 @@ def main():
     s64.set_profiling(False)
 
     # NVT (Nose-Hoover chain 3, tau 0.1 ps, 300 K), same protocol.
-    snvt = make_sched(sysm, eam, "mixed", lanes_per_atom=lanes32, t_target=300.0,
+    snvt = make_sched(sysm, eam, "mixed", lanes_per_atom=lanes32, nbr_batch=nb32,
+                      t_target=300.0,
                       t_period=0.1, nhc_length=3)
     snvt.run_until(0)
     ms_nvt, _, _, _ = timed_windows(snvt, args.steps, args.warmup, flush, torch, dist)
@@ -753,8 +758,10 @@ def main():
 
     drift = None
     if args.drift_steps > 0:
-        drift = {"mixed": nve_drift(sysm, eam, "mixed", lanes32, args.drift_steps),
-                 "fp64": nve_drift(sysm, eam, "fp64", lanes64, args.drift_steps)}
+        drift = {"mixed": nve_drift(sysm, eam, "mixed", lanes32, args.drift_steps,
+                                    nbr_batch=nb32),
+                 "fp64": nve_drift(sysm, eam, "fp64", lanes64, args.drift_steps,
+                                   nbr_batch=nb64)}
 
     batch = None
     if not args.no_batch:
@@ -823,7 +830,9 @@ def main():
                 "l2": "flushed (256 MiB write) before every bench step, outside its timing",
                 "mean_neighbors_K": K,
                 "lanes_per_atom": {"mixed": lanes32, "fp64": lanes64,
-                                   "autotune_ms_mixed": tune32, "autotune_ms_fp64": tune64},
+                                   "nbr_batch": {"mixed": nb32, "fp64": nb64},
+                                   "autotune_ms_mixed": tune32, "autotune_ms_fp64": tune64,
+                                   "autotune_keys": "<lanes per atom>x<neighbors per lane sweep>"},
                 "timesteps_per_s": value / sysm.n,
                 "path_roofline": path_roofline(value, "eam", "mixed", K, occ, hbm),
                 "fp64": {"value": value64, "ms_per_step": ms_fp64 / args.steps,

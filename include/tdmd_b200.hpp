@@ -441,6 +441,7 @@ struct FastPipelineConfig {
   real c2{real{0.05}};
   i32 energy_every{0};
   i32 energy_log_capacity{0};
+  i32 nbr_batch{0};  // neighbors per lane sweep: 0 = autotuned, else 2 or 4
 
   tdmd_fast_pipeline_config to_c() const {
     tdmd_fast_pipeline_config c;
@@ -460,6 +461,7 @@ struct FastPipelineConfig {
     c.c2 = c2;
     c.energy_every = energy_every;
     c.energy_log_capacity = energy_log_capacity;
+    c.nbr_batch = nbr_batch;
     return c;
   }
 };

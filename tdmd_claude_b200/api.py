@@ -61,10 +61,18 @@ def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
+def _autotune(fn, handle):
+    c, u = C.c_int32(), C.c_int32()
+    ms = np.zeros(12, np.float64)
+    call(fn, handle, C.byref(c), C.byref(u), _ptr(ms))
+    return c.value, u.value, {f"{1 << k}x{b}": float(ms[6 * i + k])
+                              for i, b in enumerate((2, 4)) for k in range(6) if ms[6 * i + k] >= 0}
+
+
 def make_config(dt=0.001, r_skin=1.0, rebuild_every=10, precision="fp64", use_graphs=True,
                 lanes_per_atom=0, t_target=0.0, t_period=0.1, nhc_length=3, adaptive_dt=False,
                 dt_min=0.0001, dt_max=0.002, c2=0.05, energy_every=0,
-                energy_log_capacity=0) -> FastPipelineConfig:
+                energy_log_capacity=0, nbr_batch=0) -> FastPipelineConfig:
     """FastPipelineConfig{dt, r_skin, rebuild_every} plus this library's knobs."""
     cfg = FastPipelineConfig()
     lib().tdmd_fast_pipeline_config_default(C.byref(cfg))
@@ -76,6 +84,7 @@ def make_config(dt=0.001, r_skin=1.0, rebuild_every=10, precision="fp64", use_gr
     cfg.adaptive_dt = 1 if adaptive_dt else 0
     cfg.dt_min, cfg.dt_max, cfg.c2 = float(dt_min), float(dt_max), float(c2)
     cfg.energy_every, cfg.energy_log_capacity = int(energy_every), int(energy_log_capacity)
+    cfg.nbr_batch = int(nbr_batch)
     return cfg
 
 
@@ -274,12 +283,9 @@ class FastPipelineScheduler:
         return v.value
 
     def autotune(self):
-        """Pick lanes-per-atom by timing the force passes; returns
-        (chosen, {lanes: ms})."""
-        c = C.c_int32()
-        ms = np.zeros(6, np.float64)
-        call("tdmd_sched_autotune", self._h, C.byref(c), _ptr(ms))
-        return c.value, {1 << k: float(ms[k]) for k in range(6)}
+        """Pick lanes per atom and neighbors per lane sweep by timing the
+        force passes; returns (lanes, batch, {"<lanes>x<batch>": ms})."""
+        return _autotune("tdmd_sched_autotune", self._h)
 
     def set_profiling(self, on: bool = True):
         call("tdmd_sched_set_profiling", self._h, 1 if on else 0)
@@ -395,10 +401,8 @@ class ReplicaBatch:
                 "step": step.value}
 
     def autotune(self):
-        c = C.c_int32()
-        ms = np.zeros(6, np.float64)
-        call("tdmd_batch_autotune", self._h, C.byref(c), _ptr(ms))
-        return c.value, {1 << k: float(ms[k]) for k in range(6)}
+        """As FastPipelineScheduler.autotune, for the whole batch."""
+        return _autotune("tdmd_batch_autotune", self._h)
 
     def last_window_ms(self) -> float:
         v = C.c_double()

@@ -41,7 +41,7 @@ constexpr int kThreads = 256;
 
 // Per-atom Morse energy (1/2 U per listed pair), the same expression as the
 // force kernel's energy term; only on energy-log windows.
-template <class Geo, int LPA, bool VEC>
+template <class Geo, int LPA, int U, bool VEC>
 __global__ void __launch_bounds__(kThreads) k_morse_atom_pe(Geo g, NbrView nl, int n,
                                                             MorseP<typename Geo::T> mp,
                                                             double* __restrict__ pe_atom) {
@@ -54,11 +54,11 @@ __global__ void __launch_bounds__(kThreads) k_morse_atom_pe(Geo g, NbrView nl, i
     const typename Geo::Own o = g.own(i);
     const long long row = nl.row(i);
     const int c = nl.count(i);
-    for (int base = kU * sub; base < c; base += kU * LPA) {
-      int jj[kU];
+    for (int base = U * sub; base < c; base += U * LPA) {
+      int jj[U];
       nbr_batch<VEC>(nl, row, base, c, jj);
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+      for (int u = 0; u < U; ++u) {
         if (jj[u] < 0) continue;
         typename Geo::Pair pr;
         g.pair(o, jj[u], pr);
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kThreads) k_morse_atom_pe(Geo g, NbrView nl, i
 
 // Per-atom EAM energy F_ti(rho_i) + 1/2 sum_j phi(r_ij), with the force
 // pass's spline rows and offsets; only on energy-log windows.
-template <class Geo, int LPA, bool VEC, bool MULTI>
+template <class Geo, int LPA, int U, bool VEC, bool MULTI>
 __global__ void __launch_bounds__(kThreads) k_eam_atom_pe(Geo g, NbrView nl, int n,
                                                           EamDev<typename Geo::T> e,
                                                           const int* __restrict__ types,
@@ -96,11 +96,11 @@ __global__ void __launch_bounds__(kThreads) k_eam_atom_pe(Geo g, NbrView nl, int
     const int ti = MULTI ? __ldg(types + i) - 1 : 0;
     const long long row = nl.row(i);
     const int c = nl.count(i);
-    for (int base = kU * sub; base < c; base += kU * LPA) {
-      int jj[kU];
+    for (int base = U * sub; base < c; base += U * LPA) {
+      int jj[U];
       nbr_batch<VEC>(nl, row, base, c, jj);
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+      for (int u = 0; u < U; ++u) {
         if (jj[u] < 0) continue;
         typename Geo::Pair pr;
         g.pair(o, jj[u], pr);
@@ -245,7 +245,7 @@ class Batch {
   void run_until(int target);
   void energies(double* pe, double* ke);
   void energy_log(double* steps, double* pe_ke, int cap, int* count) const;
-  void autotune(int* chosen, double* ms6);
+  void autotune(int* chosen, int* chosen_batch, double* ms12);
   void stats(tdmd_fast_pipeline_stats* o) const {
     *o = tdmd_fast_pipeline_stats{};
     o->ticks = ticks_;
@@ -254,10 +254,13 @@ class Batch {
     o->graph_launches = graph_launches_;
     o->nlist_retries = retries_;
     o->nlist_capacity = cap_;
+    o->lanes_per_atom = lpa_;
+    o->nbr_batch = nu_;
   }
   int nreplicas() const { return nrep_; }
   long long natoms() const { return n_; }
   int lanes() const { return lpa_; }
+  int nbr_batch() const { return nu_; }
   int step() const { return step_; }
   double last_window_ms() const { return last_window_ms_; }
   cudaStream_t stream() const { return stream_; }
@@ -290,6 +293,7 @@ class Batch {
   std::vector<RepDesc> hreps_;
   int ncells_ = 0;
   int lpa_ = 0;
+  int nu_ = kU;  // neighbors per lane per sweep (2 or 4)
   int cap_ = 0;
   int n_types_ = 0;
   bool uploaded_ = false, initialized_ = false, tuned_ = false;
@@ -389,6 +393,9 @@ Batch::Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_mors
   lpa_ = cfg.lanes_per_atom > 0 ? cfg.lanes_per_atom : default_lpa(n_ > 0 ? n_ : 1);
   TDMD_REQUIRE(lpa_ == 1 || lpa_ == 2 || lpa_ == 4 || lpa_ == 8 || lpa_ == 16 || lpa_ == 32,
                "lanes_per_atom must be 1,2,4,8,16 or 32");
+  TDMD_REQUIRE(cfg.nbr_batch == 0 || cfg.nbr_batch == 2 || cfg.nbr_batch == 4,
+               "nbr_batch must be 0 (tuned), 2 or 4");
+  nu_ = cfg.nbr_batch > 0 ? cfg.nbr_batch : kU;
   TDMD_CU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   TDMD_CU(cudaEventCreate(&win_ev_[0]));
   TDMD_CU(cudaEventCreate(&win_ev_[1]));
@@ -557,23 +564,23 @@ void Batch::force(bool kd, bool pea) {
       const GeoQB g{q_.data(), rep_.data(), scales_.data()};
       const GeoQB gg{g_.data(), rep_.data(), scales_.data()};
       launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), nullptr, nullptr,
-                                       g_.data(), false, nullptr, lpa_, s,
+                                       g_.data(), false, nullptr, Tune{lpa_, nu_}, s,
                                        pea ? pe_atom_.data() : nullptr);
       // kd: the next step's kick + drift in the same pass (the force pass
       // reads gather records only), each atom in its replica's box
       const KickDrift kdr{pos4_.data(), q_.data(), vel_.data(), types_.data(), inv_mm_.data(),
                           cfg_.dt, nullptr, DevBox{}, rep_.data(), reps_.data()};
       launch_eam_force<GeoQB, true, float, float>(gg, nl, n, eam_->d32, types, fp32_.data(),
-                                                  f32_.data(), pea, nullptr, lpa_, s,
+                                                  f32_.data(), pea, nullptr, Tune{lpa_, nu_}, s,
                                                   kd ? &kdr : nullptr,
                                                   pea ? pe_atom_.data() : nullptr);
     } else {
       const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
       launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), nullptr,
-                                         nullptr, nullptr, false, nullptr, lpa_, s,
+                                         nullptr, nullptr, false, nullptr, Tune{lpa_, nu_}, s,
                                          pea ? pe_atom_.data() : nullptr);
       launch_eam_force<GeoD4B, false, double, double>(g, nl, n, eam_->d64, types, fp64_.data(),
-                                                      f64_.data(), pea, nullptr, lpa_, s,
+                                                      f64_.data(), pea, nullptr, Tune{lpa_, nu_}, s,
                                                       nullptr, pea ? pe_atom_.data() : nullptr);
     }
     launches_ += 2;
@@ -581,11 +588,11 @@ void Batch::force(bool kd, bool pea) {
   }
   if (mixed_) {
     const GeoQB g{q_.data(), rep_.data(), scales_.data()};
-    launch_morse(g, nl, n, m32_, f32_.data(), pea, nullptr, lpa_, s,
+    launch_morse(g, nl, n, m32_, f32_.data(), pea, nullptr, Tune{lpa_, nu_}, s,
                  pea ? pe_atom_.data() : nullptr);
   } else {
     const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
-    launch_morse(g, nl, n, m64_, f64_.data(), pea, nullptr, lpa_, s,
+    launch_morse(g, nl, n, m64_, f64_.data(), pea, nullptr, Tune{lpa_, nu_}, s,
                  pea ? pe_atom_.data() : nullptr);
   }
   ++launches_;
@@ -720,36 +727,48 @@ void Batch::initial_forces() {
   initialized_ = true;
 }
 
-void Batch::autotune(int* chosen, double* ms6) {
+// Sweeps lanes per atom {1, ..., 32} x neighbors per lane sweep {2, 4}
+// (only cfg.nbr_batch when that is fixed); ms12[6 * (batch == 4) + k] gets
+// the time of lanes 2^k, -1 where not measured.
+void Batch::autotune(int* chosen, int* chosen_batch, double* ms12) {
   TDMD_REQUIRE(uploaded_, "autotune before upload");
   if (n_ == 0) return;
   if (!initialized_) initial_forces();
   cudaStream_t s = stream_;
   const int cands[6] = {1, 2, 4, 8, 16, 32};
+  const int batches[2] = {2, 4};
   double best = 1e30;
-  int best_l = lpa_;
-  for (int k = 0; k < 6; ++k) {
-    lpa_ = cands[k];
-    force();  // warm
-    TDMD_CU(cudaEventRecord(win_ev_[0], s));
-    for (int rep = 0; rep < 5; ++rep) force();
-    TDMD_CU(cudaEventRecord(win_ev_[1], s));
-    TDMD_CU(cudaEventSynchronize(win_ev_[1]));
-    float ms = 0.f;
-    TDMD_CU(cudaEventElapsedTime(&ms, win_ev_[0], win_ev_[1]));
-    const double per = ms / 5.0;
-    if (ms6) ms6[k] = per;
-    if (per < best) {
-      best = per;
-      best_l = cands[k];
+  int best_l = lpa_, best_u = nu_;
+  for (int b = 0; b < 2; ++b) {
+    for (int k = 0; k < 6; ++k) {
+      if (ms12) ms12[6 * b + k] = -1.0;
+      if (cfg_.nbr_batch > 0 && batches[b] != cfg_.nbr_batch) continue;
+      lpa_ = cands[k];
+      nu_ = batches[b];
+      force();  // warm
+      TDMD_CU(cudaEventRecord(win_ev_[0], s));
+      for (int rep = 0; rep < 5; ++rep) force();
+      TDMD_CU(cudaEventRecord(win_ev_[1], s));
+      TDMD_CU(cudaEventSynchronize(win_ev_[1]));
+      float ms = 0.f;
+      TDMD_CU(cudaEventElapsedTime(&ms, win_ev_[0], win_ev_[1]));
+      const double per = ms / 5.0;
+      if (ms12) ms12[6 * b + k] = per;
+      if (per < best) {
+        best = per;
+        best_l = cands[k];
+        best_u = batches[b];
+      }
     }
   }
   lpa_ = best_l;
+  nu_ = best_u;
   clear_graphs();
-  force();  // forces of the current state with the chosen lanes
+  force();  // forces of the current state with the chosen shape
   TDMD_CU(cudaStreamSynchronize(s));
   tuned_ = true;
   if (chosen) *chosen = lpa_;
+  if (chosen_batch) *chosen_batch = nu_;
 }
 
 void Batch::run_until(int target) {
@@ -759,7 +778,7 @@ void Batch::run_until(int target) {
     return;
   }
   if (!initialized_) initial_forces();
-  if (!tuned_ && cfg_.lanes_per_atom == 0 && n_ >= 2048) autotune(nullptr, nullptr);
+  if (!tuned_ && cfg_.lanes_per_atom == 0 && n_ >= 2048) autotune(nullptr, nullptr, nullptr);
   if (step_ >= target) {
     TDMD_CU(cudaStreamSynchronize(stream_));
     return;
@@ -858,37 +877,38 @@ void Batch::reduce_energies(double* out) {
   const NbrView nl = view();
   const int n = static_cast<int>(n_);
   const int nblk = force_blocks(n_, lpa_);
+  const Tune tn{lpa_, nu_};
   if (eam_) {
     // rho_i of the current positions, then F(rho_i) + 1/2 sum_j phi(r_ij)
     const int* types = eam_->ntypes > 1 ? types_.data() : nullptr;
     if (mixed_) {
       const GeoQB g{q_.data(), rep_.data(), scales_.data()};
       launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), rho_.data(),
-                                       nullptr, g_.data(), false, nullptr, lpa_, s);
-      TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(
-          lpa_, {
-            k_eam_atom_pe<GeoQB, L, V, M><<<nblk, kThreads, 0, s>>>(
+                                       nullptr, g_.data(), false, nullptr, Tune{lpa_, nu_}, s);
+      TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(
+          tn, {
+            k_eam_atom_pe<GeoQB, L, U, V, M><<<nblk, kThreads, 0, s>>>(
                 g, nl, n, eam_->d32, types, rho_.data(), pe_atom_.data());
           })));
     } else {
       const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
       launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), rho_.data(),
-                                         nullptr, nullptr, false, nullptr, lpa_, s);
-      TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(
-          lpa_, {
-            k_eam_atom_pe<GeoD4B, L, V, M><<<nblk, kThreads, 0, s>>>(
+                                         nullptr, nullptr, false, nullptr, Tune{lpa_, nu_}, s);
+      TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(
+          tn, {
+            k_eam_atom_pe<GeoD4B, L, U, V, M><<<nblk, kThreads, 0, s>>>(
                 g, nl, n, eam_->d64, types, rho_.data(), pe_atom_.data());
           })));
     }
     TDMD_LAUNCH_CHECK();
     launches_ += 1;
   } else {
-    TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa_, {
+    TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
       if (mixed_)
-        k_morse_atom_pe<GeoQB, L, V><<<nblk, kThreads, 0, s>>>(
+        k_morse_atom_pe<GeoQB, L, U, V><<<nblk, kThreads, 0, s>>>(
             GeoQB{q_.data(), rep_.data(), scales_.data()}, nl, n, m32_, pe_atom_.data());
       else
-        k_morse_atom_pe<GeoD4B, L, V><<<nblk, kThreads, 0, s>>>(
+        k_morse_atom_pe<GeoD4B, L, U, V><<<nblk, kThreads, 0, s>>>(
             GeoD4B{pos4_.data(), rep_.data(), imgs_.data()}, nl, n, m64_, pe_atom_.data());
     }));
     TDMD_LAUNCH_CHECK();
@@ -1029,10 +1049,11 @@ int32_t tdmd_batch_info(const tdmd_batch* b, int32_t* nreplicas, int64_t* natoms
   });
 }
 
-int32_t tdmd_batch_autotune(tdmd_batch* b, int32_t* chosen_lanes, double* ms6) {
+int32_t tdmd_batch_autotune(tdmd_batch* b, int32_t* chosen_lanes, int32_t* chosen_batch,
+                            double* ms12) {
   return guarded([&] {
     TDMD_REQUIRE(b, "null handle");
-    b->b.autotune(chosen_lanes, ms6);
+    b->b.autotune(chosen_lanes, chosen_batch, ms12);
   });
 }
 

@@ -78,16 +78,30 @@ __device__ __forceinline__ int4 ld_stream(const int4* p) {
   return v;
 }
 
-// Neighbors per lane per sweep: a lane fetches kU indices, then kU
-// positions, then evaluates kU pairs, so its loads overlap.
+// Neighbors per lane per sweep (U): a lane fetches U indices, then U
+// positions, then evaluates U pairs, so its loads overlap.  U is 2 or 4,
+// chosen by the autotuner; kU is the choice without tuning.
 constexpr int kU = 4;
 
-// Indices base .. base+kU-1 of a row, -1 past the count.  VEC: 16-byte
-// aligned padded rows (scheduler) -> one int4 load.
-template <bool VEC>
+__device__ __forceinline__ int2 ld_stream2(const int2* p) {
+  int2 v;
+  asm("ld.global.nc.L1::no_allocate.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+  return v;
+}
+
+// Indices base .. base+U-1 of a row (base < c, base a multiple of U), -1
+// past the count.  VEC: padded rows whose start is 16-byte aligned and whose
+// capacity is a multiple of 4 (vec_rows), so the vector read stays inside
+// the row: one int2 load for U = 2, one int4 load for U = 4.
+template <bool VEC, int U>
 __device__ __forceinline__ void nbr_batch(const NbrView& nl, long long row, int base, int c,
-                                          int (&j)[kU]) {
-  if constexpr (VEC) {
+                                          int (&j)[U]) {
+  static_assert(U == 2 || U == 4, "neighbor batch: 2 or 4");
+  if constexpr (VEC && U == 2) {
+    const int2 v = ld_stream2(reinterpret_cast<const int2*>(nl.nbr + row + base));
+    j[0] = v.x;
+    j[1] = base + 1 < c ? v.y : -1;
+  } else if constexpr (VEC) {
     const int4 v = ld_stream(reinterpret_cast<const int4*>(nl.nbr + row + base));
     j[0] = v.x;
     j[1] = base + 1 < c ? v.y : -1;
@@ -95,7 +109,7 @@ __device__ __forceinline__ void nbr_batch(const NbrView& nl, long long row, int 
     j[3] = base + 3 < c ? v.w : -1;
   } else {
 #pragma unroll
-    for (int u = 0; u < kU; ++u) j[u] = base + u < c ? __ldg(nl.nbr + row + base + u) : -1;
+    for (int u = 0; u < U; ++u) j[u] = base + u < c ? __ldg(nl.nbr + row + base + u) : -1;
   }
 }
 
@@ -379,7 +393,7 @@ struct MorseP {
 
 // EV: 0 forces only; 1 also energy + virial into per-block partials and,
 // where pe_atom is given, per-atom energies; 2 forces + per-atom energies.
-template <class Geo, int LPA, int EV, bool VEC, class F>
+template <class Geo, int LPA, int U, int EV, bool VEC, class F>
 __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
                                                MorseP<typename Geo::T> mp, ForceOut<F> out,
                                                double* __restrict__ partials,
@@ -397,19 +411,19 @@ __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
     const long long row = nl.row(i);
     const int c = nl.count(i);
     const T two_d_alpha = T(2) * mp.d * mp.alpha;
-    for (int base = kU * sub; base < c; base += kU * LPA) {
-      int jj[kU];
+    for (int base = U * sub; base < c; base += U * LPA) {
+      int jj[U];
       nbr_batch<VEC>(nl, row, base, c, jj);
-      typename Geo::Pair pr[kU];
+      typename Geo::Pair pr[U];
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+      for (int u = 0; u < U; ++u) {
         if (jj[u] >= 0)
           g.pair(o, jj[u], pr[u]);
         else
           pr[u].r2 = mp.rc_sq;
       }
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+      for (int u = 0; u < U; ++u) {
         if (pr[u].r2 < mp.rc_sq) {
           T r, rinv;
           double rd;
@@ -569,7 +583,7 @@ __device__ __forceinline__ void embed_eval(const double4* ftab, int nrho, double
 // and, with EV, the embedding energy F(rho_i) into the block partials.
 // types == nullptr means a single-type alloy.  gout (GeoQ only, nullable)
 // receives the force pass's gather records {qx, qy, qz, bits(F'(rho))}.
-template <class Geo, int LPA, bool EV, bool VEC, bool MULTI, class FP>
+template <class Geo, int LPA, int U, bool EV, bool VEC, bool MULTI, class FP>
 __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
                                                      EamDev<typename Geo::T> e,
                                                      const int* __restrict__ types,
@@ -590,19 +604,19 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
     o = g.own(i);
     const long long row = nl.row(i);
     const int c = nl.count(i);
-    for (int base = kU * sub; base < c; base += kU * LPA) {
-      int jj[kU];
+    for (int base = U * sub; base < c; base += U * LPA) {
+      int jj[U];
       nbr_batch<VEC>(nl, row, base, c, jj);
-      typename Geo::Pair pr[kU];
+      typename Geo::Pair pr[U];
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+      for (int u = 0; u < U; ++u) {
         if (jj[u] >= 0)
           g.pair(o, jj[u], pr[u]);
         else
           pr[u].r2 = e.rc_sq;
       }
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+      for (int u = 0; u < U; ++u) {
         if (pr[u].r2 < e.rc_sq) {
           // No FP64-refined radius here: in the mixed path the density's
           // FP32 radius error is a few percent of the total force error
@@ -687,7 +701,7 @@ __device__ __forceinline__ void kick_drift_atom(const KickDrift& k, int i, float
 // FPG: F'(rho_j) comes with the neighbor's gather record (pair w bits)
 // instead of the fp array.  KD (FPG, float forces): then the next step's
 // kick + drift of the same atom.
-template <class Geo, int LPA, int EV, bool FPG, bool VEC, bool MULTI, class FP, class F,
+template <class Geo, int LPA, int U, int EV, bool FPG, bool VEC, bool MULTI, class FP, class F,
           bool KD = false>
 __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
                                                    EamDev<typename Geo::T> e,
@@ -710,19 +724,19 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
     const int c = nl.count(i);
     const int ti = MULTI ? __ldg(types + i) - 1 : 0;
     const T fpi = static_cast<T>(__ldg(fp + i));
-    for (int base = kU * sub; base < c; base += kU * LPA) {
-      int jj[kU];
+    for (int base = U * sub; base < c; base += U * LPA) {
+      int jj[U];
       nbr_batch<VEC>(nl, row, base, c, jj);
-      typename Geo::Pair pr[kU];
+      typename Geo::Pair pr[U];
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+      for (int u = 0; u < U; ++u) {
         if (jj[u] >= 0)
           g.pair(o, jj[u], pr[u]);
         else
           pr[u].r2 = e.rc_sq;
       }
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+      for (int u = 0; u < U; ++u) {
         if (pr[u].r2 < e.rc_sq) {
           T r, rinv, sx;
           double rd;

@@ -47,22 +47,41 @@ inline bool vec_rows(const NbrView& nl) { return nl.row_off == nullptr && nl.cap
     default: throw Error{TDMD_ERR_INVALID_ARGUMENT, "lanes per atom must be 1,2,4,8,16,32"}; \
   }
 
+// Launch shape of the gather passes: lanes per atom and neighbors per lane
+// per sweep.  A bare lanes count means the untuned sweep of kU.
+struct Tune {
+  int lpa;
+  int nu;
+  Tune(int lanes = 1, int batch = kU) : lpa(lanes), nu(batch) {}
+};
+
+#define TDMD_NU_DISPATCH(nu, ...)                                \
+  switch (nu) {                                                   \
+    case 2: { constexpr int U = 2; __VA_ARGS__; } break;          \
+    case 4: { constexpr int U = 4; __VA_ARGS__; } break;          \
+    default: throw Error{TDMD_ERR_INVALID_ARGUMENT, "neighbor batch must be 2 or 4"}; \
+  }
+
+// Defines L (lanes per atom) and U (neighbor batch) for the body.
+#define TDMD_TUNE_DISPATCH(tn, ...) \
+  TDMD_NU_DISPATCH((tn).nu, TDMD_LPA_DISPATCH((tn).lpa, __VA_ARGS__))
+
 // Morse forces; with ev, per-block partials (force_blocks records; nullable)
 // and per-atom energies (pe_atom, nullable).
 template <class Geo, class F>
 void launch_morse(const Geo& g, const NbrView& nl, int n, const MorseP<typename Geo::T>& mp,
-                  F* forces, bool ev, double* partials, int lpa, cudaStream_t s,
+                  F* forces, bool ev, double* partials, Tune tn, cudaStream_t s,
                   double* pe_atom = nullptr) {
-  const int nblk = force_blocks(n, lpa);
-  TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
+  const int nblk = force_blocks(n, tn.lpa);
+  TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
     if (ev && !partials && pe_atom)  // per-atom energies only
-      k_morse<Geo, L, 2, V, F><<<nblk, kForceThreads, 0, s>>>(
+      k_morse<Geo, L, U, 2, V, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, mp, ForceOut<F>{forces}, nullptr, pe_atom);
     else if (ev)
-      k_morse<Geo, L, 1, V, F><<<nblk, kForceThreads, 0, s>>>(
+      k_morse<Geo, L, U, 1, V, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, mp, ForceOut<F>{forces}, partials, pe_atom);
     else
-      k_morse<Geo, L, 0, V, F><<<nblk, kForceThreads, 0, s>>>(
+      k_morse<Geo, L, U, 0, V, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, mp, ForceOut<F>{forces}, nullptr, nullptr);
   }));
   TDMD_LAUNCH_CHECK();
@@ -75,14 +94,14 @@ template <class Geo, class FP>
 void launch_eam_density(const Geo& g, const NbrView& nl, int n,
                         const EamDev<typename Geo::T>& e, const int* types, FP* fp,
                         double* rho_out, double* fpd_out, int4* gout, bool ev, double* partials,
-                        int lpa, cudaStream_t s, double* e_out = nullptr) {
-  const int nblk = force_blocks(n, lpa);
-  TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
+                        Tune tn, cudaStream_t s, double* e_out = nullptr) {
+  const int nblk = force_blocks(n, tn.lpa);
+  TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
     if (ev)
-      k_eam_density<Geo, L, true, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_density<Geo, L, U, true, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, rho_out, fpd_out, gout, partials, e_out);
     else
-      k_eam_density<Geo, L, false, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_density<Geo, L, U, false, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, rho_out, fpd_out, gout, nullptr, e_out);
   })));
   TDMD_LAUNCH_CHECK();
@@ -96,26 +115,26 @@ void launch_eam_density(const Geo& g, const NbrView& nl, int n,
 template <class Geo, bool FPG, class FP, class F>
 void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typename Geo::T>& e,
                       const int* types, const FP* fp, F* forces, bool ev, double* partials,
-                      int lpa, cudaStream_t s, const KickDrift* kd = nullptr,
+                      Tune tn, cudaStream_t s, const KickDrift* kd = nullptr,
                       double* pe_atom = nullptr) {
-  const int nblk = force_blocks(n, lpa);
-  TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_LPA_DISPATCH(lpa, {
+  const int nblk = force_blocks(n, tn.lpa);
+  TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
     if (ev && !partials && pe_atom)  // per-atom energies only
-      k_eam_force<Geo, L, 2, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, U, 2, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr, KickDrift{}, pe_atom);
     else if (ev)
-      k_eam_force<Geo, L, 1, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, U, 1, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, partials, KickDrift{}, pe_atom);
     else if constexpr (FPG && sizeof(F) == sizeof(float)) {
       if (kd)
-        k_eam_force<Geo, L, 0, FPG, V, M, FP, F, true><<<nblk, kForceThreads, 0, s>>>(
+        k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F, true><<<nblk, kForceThreads, 0, s>>>(
             g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr, *kd);
       else
-        k_eam_force<Geo, L, 0, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+        k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
             g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
     } else {
       TDMD_REQUIRE(kd == nullptr, "fused kick-drift needs the mixed gather-record pass");
-      k_eam_force<Geo, L, 0, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
+      k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
           g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
     }
   })));
@@ -127,13 +146,13 @@ void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typen
 template <class Geo, class FP, class F>
 void launch_eam(const Geo& g, const NbrView& nl, int n, const EamDev<typename Geo::T>& e,
                 const int* types, FP* fp, double* rho_out, double* fpd_out, F* forces, bool ev,
-                double* partials, int lpa, cudaStream_t s) {
-  const int nblk = force_blocks(n, lpa);
+                double* partials, Tune tn, cudaStream_t s) {
+  const int nblk = force_blocks(n, tn.lpa);
   launch_eam_density<Geo, FP>(g, nl, n, e, types, fp, rho_out, fpd_out, nullptr, ev, partials,
-                              lpa, s);
+                              tn, s);
   launch_eam_force<Geo, false, FP, F>(
       g, nl, n, e, types, fp, forces, ev,
-      ev ? partials + static_cast<long long>(nblk) * kEvStride : nullptr, lpa, s);
+      ev ? partials + static_cast<long long>(nblk) * kEvStride : nullptr, tn, s);
 }
 
 }  // namespace tdmd_b200

@@ -89,7 +89,7 @@ class Scheduler {
   // Times the force passes for lanes-per-atom in {1,2,4,8,16,32} on the
   // current state, keeps the fastest, recomputes the forces with it.
   // ms6[k] = ms of candidate 2^k (nullable).
-  void autotune(int* chosen, double* ms6);
+  void autotune(int* chosen, int* chosen_batch, double* ms12);
   int lanes_per_atom() const { return lpa_; }
   // Device time of the last run_until window (events on the stream around
   // its enqueued work), ms.
@@ -157,6 +157,7 @@ class Scheduler {
   double cutoff_ = 0.0;
   bool mixed_ = false, nvt_ = false, thermo_ = false;
   int lpa_ = 8;
+  int nu_ = kU;  // neighbors per lane per sweep (2 or 4)
   MorseP<double> m64_{};
   MorseP<float> m32_{};
   std::unique_ptr<EamDevTables> eam_;

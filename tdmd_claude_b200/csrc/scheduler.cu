@@ -399,6 +399,9 @@ void Scheduler::finish_setup() {
   lpa_ = cfg_.lanes_per_atom > 0 ? cfg_.lanes_per_atom : default_lpa(n_ > 0 ? n_ : 1);
   TDMD_REQUIRE(lpa_ == 1 || lpa_ == 2 || lpa_ == 4 || lpa_ == 8 || lpa_ == 16 || lpa_ == 32,
                "lanes_per_atom must be 1,2,4,8,16 or 32");
+  TDMD_REQUIRE(cfg_.nbr_batch == 0 || cfg_.nbr_batch == 2 || cfg_.nbr_batch == 4,
+               "nbr_batch must be 0 (tuned), 2 or 4");
+  nu_ = cfg_.nbr_batch > 0 ? cfg_.nbr_batch : kU;
 }
 
 void Scheduler::upload(const double* x, const double* v, const void* f, const int* types,
@@ -601,12 +604,12 @@ void Scheduler::enqueue_force(bool ev, bool kd) {
     prof_begin(kProfForce);
     if (mixed_) {
       const GeoQ g = make_geoq(q_.data(), box_);
-      launch_morse(g, nl, n_, m32_, f32_.data(), ev, part, lpa_, s);
+      launch_morse(g, nl, n_, m32_, f32_.data(), ev, part, Tune{lpa_, nu_}, s);
     } else {
       GeoD4 g{pos4_.data(), {box_.L[0], box_.L[1], box_.L[2]},
               {box_.halfL[0], box_.halfL[1], box_.halfL[2]},
               {box_.periodic[0], box_.periodic[1], box_.periodic[2]}};
-      launch_morse(g, nl, n_, m64_, f64_.data(), ev, part, lpa_, s);
+      launch_morse(g, nl, n_, m64_, f64_.data(), ev, part, Tune{lpa_, nu_}, s);
     }
     prof_end(kProfForce);
     launches_ += 1;
@@ -620,7 +623,7 @@ void Scheduler::enqueue_force(bool ev, bool kd) {
       const GeoQ gg = make_geoq(g_.data(), box_);
       prof_begin(kProfDensity);
       launch_eam_density<GeoQ, float>(g, nl, n_, eam_->d32, types, fp32_.data(), nullptr,
-                                      nullptr, g_.data(), ev, part, lpa_, s);
+                                      nullptr, g_.data(), ev, part, Tune{lpa_, nu_}, s);
       prof_end(kProfDensity);
       prof_begin(kProfForce);
       const KickDrift kdr{pos4_.data(), q_.data(), vel_.data(), types_.data(), inv_mm_.data(),
@@ -629,7 +632,7 @@ void Scheduler::enqueue_force(bool ev, bool kd) {
                                                        offsetof(SchedCtl, step)),
                           box_, nullptr, nullptr};
       launch_eam_force<GeoQ, true, float, float>(gg, nl, n_, eam_->d32, types, fp32_.data(),
-                                                 f32_.data(), ev, part2, lpa_, s,
+                                                 f32_.data(), ev, part2, Tune{lpa_, nu_}, s,
                                                  kd ? &kdr : nullptr);
       prof_end(kProfForce);
     } else {
@@ -638,11 +641,11 @@ void Scheduler::enqueue_force(bool ev, bool kd) {
               {box_.periodic[0], box_.periodic[1], box_.periodic[2]}};
       prof_begin(kProfDensity);
       launch_eam_density<GeoD4, double>(g, nl, n_, eam_->d64, types, fp64_.data(), nullptr,
-                                        nullptr, nullptr, ev, part, lpa_, s);
+                                        nullptr, nullptr, ev, part, Tune{lpa_, nu_}, s);
       prof_end(kProfDensity);
       prof_begin(kProfForce);
       launch_eam_force<GeoD4, false, double, double>(g, nl, n_, eam_->d64, types, fp64_.data(),
-                                                     f64_.data(), ev, part2, lpa_, s);
+                                                     f64_.data(), ev, part2, Tune{lpa_, nu_}, s);
       prof_end(kProfForce);
     }
     launches_ += 2;
@@ -972,7 +975,7 @@ void Scheduler::run_until(int target) {
   if (!initialized_) initial_forces();
   // lanes_per_atom = 0: measure the candidates once on the first window of
   // a system large enough for the choice to matter.
-  if (!tuned_ && cfg_.lanes_per_atom == 0 && n_ >= 2048) autotune(nullptr, nullptr);
+  if (!tuned_ && cfg_.lanes_per_atom == 0 && n_ >= 2048) autotune(nullptr, nullptr, nullptr);
   if (step_ >= target) {
     TDMD_CU(cudaStreamSynchronize(stream_));
     return;
@@ -1084,7 +1087,10 @@ void Scheduler::thermostat_state(double* dt, double* eta, double* eta_v) const {
 
 // ----- per-kernel timing -------------------------------------------------------
 // ----- autotuner ---------------------------------------------------------------
-void Scheduler::autotune(int* chosen, double* ms6) {
+// Sweeps lanes per atom {1, ..., 32} x neighbors per lane sweep {2, 4}
+// (only cfg.nbr_batch when that is fixed); ms12[6 * (batch == 4) + k] gets
+// the time of lanes 2^k, -1 where not measured.
+void Scheduler::autotune(int* chosen, int* chosen_batch, double* ms12) {
   TDMD_REQUIRE(uploaded_, "autotune before upload");
   if (n_ == 0) return;
   if (!initialized_) initial_forces();
@@ -1095,31 +1101,39 @@ void Scheduler::autotune(int* chosen, double* ms6) {
   TDMD_CU(cudaEventCreate(&e0));
   TDMD_CU(cudaEventCreate(&e1));
   const int cand[6] = {1, 2, 4, 8, 16, 32};
+  const int batches[2] = {2, 4};
   double best_ms = 1e300;
-  int best = lpa_;
-  for (int k = 0; k < 6; ++k) {
-    lpa_ = cand[k];
-    enqueue_force(false);  // warm
-    double m = 1e300;
-    for (int rep = 0; rep < 3; ++rep) {
-      TDMD_CU(cudaEventRecord(e0, stream_));
-      enqueue_force(false);
-      TDMD_CU(cudaEventRecord(e1, stream_));
-      TDMD_CU(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      TDMD_CU(cudaEventElapsedTime(&ms, e0, e1));
-      m = std::min(m, static_cast<double>(ms));
-    }
-    if (ms6) ms6[k] = m;
-    if (m < best_ms) {
-      best_ms = m;
-      best = cand[k];
+  int best = lpa_, best_u = nu_;
+  for (int b = 0; b < 2; ++b) {
+    for (int k = 0; k < 6; ++k) {
+      if (ms12) ms12[6 * b + k] = -1.0;
+      if (cfg_.nbr_batch > 0 && batches[b] != cfg_.nbr_batch) continue;
+      lpa_ = cand[k];
+      nu_ = batches[b];
+      enqueue_force(false);  // warm
+      double m = 1e300;
+      for (int rep = 0; rep < 3; ++rep) {
+        TDMD_CU(cudaEventRecord(e0, stream_));
+        enqueue_force(false);
+        TDMD_CU(cudaEventRecord(e1, stream_));
+        TDMD_CU(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        TDMD_CU(cudaEventElapsedTime(&ms, e0, e1));
+        m = std::min(m, static_cast<double>(ms));
+      }
+      if (ms12) ms12[6 * b + k] = m;
+      if (m < best_ms) {
+        best_ms = m;
+        best = cand[k];
+        best_u = batches[b];
+      }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  // The forces of the current state, summed in the chosen lanes' order.
+  // The forces of the current state, summed in the chosen shape's order.
   lpa_ = best;
+  nu_ = best_u;
   enqueue_force(false);
   TDMD_CU(cudaStreamSynchronize(stream_));
   launches_ = l0;  // tuning passes are not part of the run's kernel count
@@ -1127,6 +1141,7 @@ void Scheduler::autotune(int* chosen, double* ms6) {
   tuned_ = true;
   profiling_ = prof;
   if (chosen) *chosen = best;
+  if (chosen_batch) *chosen_batch = best_u;
 }
 
 void Scheduler::set_profiling(bool on) {
@@ -1190,6 +1205,8 @@ void Scheduler::stats(tdmd_fast_pipeline_stats* o) const {
   o->graph_launches = graph_launches_;
   o->nlist_retries = retries_;
   o->nlist_capacity = cap_;
+  o->lanes_per_atom = lpa_;
+  o->nbr_batch = nu_;
 }
 
 }  // namespace tdmd_b200
@@ -1356,11 +1373,13 @@ int32_t tdmd_sched_stream(const tdmd_sched* s, void** stream) {
 
 }  // extern "C"
 
-extern "C" int32_t tdmd_sched_autotune(tdmd_sched* s, int32_t* chosen_lanes, double* ms6) {
+extern "C" int32_t tdmd_sched_autotune(tdmd_sched* s, int32_t* chosen_lanes,
+                                       int32_t* chosen_batch, double* ms12) {
   return guarded([&] {
     TDMD_REQUIRE(s, "null handle");
-    int c = 0;
-    s->s->autotune(&c, ms6);
+    int c = 0, u = 0;
+    s->s->autotune(&c, &u, ms12);
     if (chosen_lanes) *chosen_lanes = c;
+    if (chosen_batch) *chosen_batch = u;
   });
 }

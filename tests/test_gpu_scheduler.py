@@ -268,12 +268,43 @@ def test_autotune_keeps_forces(cuda, precision):
     s, sysm, t = _eam_setup(precision, ncell=8)
     s.run_until(0)
     f0 = s.download().forces.astype(np.float64)
-    chosen, ms = s.autotune()
-    assert chosen in (1, 2, 4, 8, 16, 32) and all(v > 0 for v in ms.values())
+    chosen, nb, ms = s.autotune()
+    assert chosen in (1, 2, 4, 8, 16, 32) and nb in (2, 4)
+    assert f"{chosen}x{nb}" in ms and len(ms) == 12 and all(v > 0 for v in ms.values())
+    st = s.stats()
+    assert (st.lanes_per_atom, st.nbr_batch) == (chosen, nb)
     f1 = s.download().forces.astype(np.float64)
     assert rel_rms(f1, f0) < (1e-13 if precision == "fp64" else 1e-6)
     s.run_until(20)
     assert s.current_step() == 20
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_neighbor_batch_sizes(cuda, precision):
+    """Neighbors per lane sweep (2 or 4) only regroups a lane's loads: with
+    one lane per atom each lane still visits its row in order, so the two
+    sizes give bit-identical trajectories; with four lanes the per-lane sums
+    regroup and the forces agree to rounding.  A fixed size limits the
+    autotuner's sweep to it."""
+    runs = {}
+    for lanes in (1, 4):
+        for nb in (2, 4):
+            s, _, _ = _eam_setup(precision, ncell=6, lanes_per_atom=lanes, nbr_batch=nb)
+            s.run_until(0)
+            f = s.download().forces.astype(np.float64)
+            s.run_until(20)
+            st = s.download()
+            assert (s.stats().lanes_per_atom, s.stats().nbr_batch) == (lanes, nb)
+            runs[lanes, nb] = (f, st.positions, st.velocities)
+            s.close()
+    for k in range(3):
+        assert np.array_equal(runs[1, 2][k], runs[1, 4][k]), k
+    assert rel_rms(runs[4, 2][0], runs[4, 4][0]) < (1e-13 if precision == "fp64" else 1e-6)
+    s, _, _ = _eam_setup(precision, ncell=6, lanes_per_atom=4, nbr_batch=2)
+    s.run_until(0)
+    _, nb, ms = s.autotune()
+    assert nb == 2 and sorted(ms) == sorted(f"{1 << k}x2" for k in range(6))
+    s.close()
 
 
 @pytest.mark.parametrize("use_graphs", [True, False])
