@@ -64,3 +64,19 @@ def rel_rms(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def two_element_tables():
+    """Two elements, every function distinct: F_A = -sqrt(rho),
+    F_B = -1.7 sqrt(rho); f_A = exp(-1.1 r), f_B = 2.5 exp(-0.7 r);
+    r phi_AA = 0.4 exp(-2.1 r), r phi_AB = 0.9 exp(-1.95 r),
+    r phi_BB = 1.3 exp(-1.75 r); grids drho 0.01 x 500, dr 0.012 x 501
+    (cutoff 6.0)."""
+    from tdmd_claude_b200 import workloads as W
+    nrho, drho, nr, dr = 500, 0.01, 501, 0.012
+    rg = np.arange(nrho) * drho
+    r = np.arange(nr) * dr
+    F = np.stack([-np.sqrt(rg), -1.7 * np.sqrt(rg)])
+    rho = np.stack([np.exp(-1.1 * r), 2.5 * np.exp(-0.7 * r)])
+    rphi = np.stack([0.4 * np.exp(-2.1 * r), 0.9 * np.exp(-1.95 * r), 1.3 * np.exp(-1.75 * r)])
+    return W.EamTables(2, nrho, drho, nr, dr, 6.0, F, rho, rphi, ("A", "B"), (10.0, 20.0))

@@ -222,3 +222,29 @@ def test_standalone_banner_usage_and_argument_errors():
     assert out.returncode == 1 and "D,alpha,r0,rc" in out.stderr
     out = run("--precision", "fp16")
     assert out.returncode == 1
+
+
+def test_two_element_setfl_parses():
+    """A written two-element setfl reads back with ntypes 2, its cutoff and
+    the embedding and density splines passing through the tabulated values
+    (test_eam.cpp:163-170)."""
+    import os
+    import tempfile
+
+    from conftest import two_element_tables
+
+    from tdmd_claude_b200 import EamAlloy
+    from tdmd_claude_b200 import io as TIO
+    t = two_element_tables()
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "ab.eam.alloy")
+        TIO.write_setfl(p, t, comment="two-element test alloy")
+        eam = EamAlloy().read_setfl(p)
+    assert eam.ntypes() == 2 and abs(eam.cutoff() - 6.0) < 1e-12
+    # the a coefficients of F and rho are the tabulated values (phi is
+    # built from r phi / r, so it is not compared here)
+    for kind, tab in ((0, t.F), (1, t.rho)):
+        for k in range(2):
+            c = eam.coeffs(kind, k)
+            n = len(c) // 4
+            assert np.allclose(c[:n], tab[k][:n], rtol=1e-14, atol=1e-14), (kind, k)

@@ -53,6 +53,8 @@ def test_run0_eam_lammps(oracle):
     r = eam.forces(pos, np.ones(len(pos), np.int32), m["lo"], m["hi"], g["skin"])
     assert np.abs(r["forces"] - np.array(g["lammps_forces"])).max() < g["tolerance_fp64"]
     assert r["pe"] == g["reference_pe"]
+    # FCC bulk cohesive energy of this potential (test_eam.cpp:398-415)
+    assert abs(r["pe"] / len(pos) + 3.54) < 0.1
 
 
 def test_reference_morse_jitter(oracle):
