@@ -240,6 +240,18 @@ def path_roofline(value, pot, precision, K, n_cell, hbm_gbs, R=None):
             "model": "gather model, whole step + list build / R"}
 
 
+def shape_str(shapes):
+    """{"density": "<lanes>x<batch>" or None, "force": ...} of an autotune result."""
+    return {p: (f"{v[0]}x{v[1]}" if v else None) for p, v in shapes.items()}
+
+
+def stats_shapes(st):
+    """Launch shapes in use from a FastPipelineStats."""
+    return shape_str({"density": (st.density_lanes_per_atom, st.density_nbr_batch)
+                      if st.density_lanes_per_atom > 0 else None,
+                      "force": (st.lanes_per_atom, st.nbr_batch)})
+
+
 def timed_windows(sched, steps, warmup, flush, torch, dist=None):
     """Device ms per window (L2 flushed before each), max over ranks."""
     stream = torch.cuda.ExternalStream(sched.stream())
@@ -336,12 +348,12 @@ def cpu_baseline_sample(sysm, t, nsteps):
     return sec, kind
 
 
-def nve_drift(sysm, eam, precision, lanes, nsteps, every=100, nbr_batch=0):
+def nve_drift(sysm, eam, precision, nsteps, every=100):
     """Total-energy drift of an NVE run from the device energy log:
     least-squares slope of E_total/N against time (eV/atom/ns) and the
     largest |E_total - E_0|/N."""
-    s = make_sched(sysm, eam, precision, lanes_per_atom=lanes, nbr_batch=nbr_batch,
-                   energy_every=every, energy_log_capacity=nsteps // every + 1)
+    s = make_sched(sysm, eam, precision, energy_every=every,
+                   energy_log_capacity=nsteps // every + 1)
     s.run_until(nsteps)
     log = s.energy_log()
     s.close()
@@ -353,7 +365,7 @@ def nve_drift(sysm, eam, precision, lanes, nsteps, every=100, nbr_batch=0):
 
 
 def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=0, world=1,
-                lanes=None):
+                lanes=None, nbr_batch=None):
     """Batched replicas: 512 independent Cu FCC Morse systems (n^3 cells,
     n uniform 4..16, 100-1500 K), NVE, K = 10 steps per graph-replayed
     window; aggregate atom-steps/s and per-replica energy drift."""
@@ -368,7 +380,8 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
                      MorseParams.make(*W.MORSE_CU),
                      make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW, precision=precision,
                                  energy_every=WINDOW, energy_log_capacity=steps + warmup + 8,
-                                 **({"lanes_per_atom": lanes} if lanes else {})))
+                                 **({"lanes_per_atom": lanes} if lanes else {}),
+                                 **({"nbr_batch": nbr_batch} if nbr_batch else {})))
     b.upload(np.concatenate([s.positions for s in systems]),
              np.concatenate([s.velocities for s in systems]),
              np.concatenate([s.types for s in systems]), systems[0].masses)
@@ -376,7 +389,7 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
     ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, dist)
     steps_log, pk = b.energy_log()
     info = b.info()
-    info["nbr_batch"] = b.stats().nbr_batch
+    info["launch_shapes"] = stats_shapes(b.stats())
     natoms = np.array([s.n for s in systems], np.float64)
     etot = (pk[:, :, 0] + pk[:, :, 1]) / natoms          # eV/atom per window
     t_ns = steps_log * DT * 1e-3
@@ -393,7 +406,7 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
             "timesteps_per_s_each_replica": WINDOW * steps / (ms * 1e-3),
             "path_roofline": path_roofline(value, "morse", precision, K, occ, hbm),
             "replicas": 512, "atoms": int(atoms), "ranks": world, "precision": precision,
-            "lanes_per_atom": info["lanes_per_atom"], "nbr_batch": info["nbr_batch"],
+            "launch_shapes": info["launch_shapes"],
             "kernel_launches_timed": launches,
             "drift_ev_per_atom_per_ns": {"median_abs": float(np.median(np.abs(slopes))),
                                          "max_abs": float(np.max(np.abs(slopes))),
@@ -549,7 +562,7 @@ def batch_eam_bench(steps, warmup, flush, torch, eam, precision, nrep=8):
     b.run_until(0)
     ms, _, launches, _ = timed_windows(b, steps, warmup, flush, torch, None)
     info = b.info()
-    info["nbr_batch"] = b.stats().nbr_batch
+    info["launch_shapes"] = stats_shapes(b.stats())
     b.close()
     value = info["natoms"] * WINDOW * steps / (ms * 1e-3)
     hbm, _ = measured_peaks()
@@ -560,7 +573,7 @@ def batch_eam_bench(steps, warmup, flush, torch, eam, precision, nrep=8):
             "path_roofline": path_roofline(value, "eam", precision, fcc_neighbors(3.615, rl),
                                            cell_occupancy(s0.n, s0.hi[0] - s0.lo[0], rl), hbm),
             "ms_per_window": ms / steps, "replicas": nrep, "atoms": info["natoms"],
-            "lanes_per_atom": info["lanes_per_atom"], "nbr_batch": info["nbr_batch"],
+            "launch_shapes": info["launch_shapes"],
             "kernel_launches_timed": launches}
 
 
@@ -655,8 +668,12 @@ def main():
                          "FP64, or mixed NVT with energy/virial every step), or the 512 "
                          "Morse replicas")
     ap.add_argument("--lanes", type=int, default=None,
-                    help="lanes per atom for --kernels-only (EAM: default 2, no autotune; "
+                    help="lanes per atom for --kernels-only (EAM: default 4, no autotune; "
                          "Morse replicas: autotuned unless given)")
+    ap.add_argument("--nbr-batch", type=int, default=None,
+                    help="neighbors per lane sweep for --kernels-only (EAM: default 2, the "
+                         "autotuner's usual choice at 131,072 atoms; Morse replicas: autotuned "
+                         "unless given)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip timing the reference's own GPU scheduler")
     ap.add_argument("--no-fit", action="store_true",
@@ -697,14 +714,15 @@ def main():
         if args.case.startswith("morse-batch"):
             prec = "fp64" if args.case.endswith("fp64") else "mixed"
             batch_bench(args.steps, args.warmup, flush, torch, prec, dist, rank, world,
-                        args.lanes)
+                        args.lanes, args.nbr_batch)
         else:
             prec = "fp64" if args.case == "eam-fp64" else "mixed"
             kw = {}
             if args.case == "eam-nvt-ev":
                 kw = dict(t_target=300.0, t_period=0.1, nhc_length=3, energy_every=1,
                           energy_log_capacity=16)
-            s32 = make_sched(sysm, eam, prec, lanes_per_atom=args.lanes or 2, **kw)
+            s32 = make_sched(sysm, eam, prec, lanes_per_atom=args.lanes or 4,
+                             nbr_batch=args.nbr_batch or 2, **kw)
             s32.run_until(0)
             timed_windows(s32, args.steps, args.warmup, flush, torch, dist)
             s32.close()
@@ -718,8 +736,8 @@ def main():
     s32 = make_sched(sysm, eam, "mixed")
     s64.run_until(0)
     s32.run_until(0)
-    lanes32, nb32, tune32 = s32.autotune()
-    lanes64, nb64, tune64 = s64.autotune()
+    shapes32, tune32 = s32.autotune()
+    shapes64, tune64 = s64.autotune()
     f64 = s64.download().forces
     f32 = s32.download().forces.astype(np.float64)
     rel_err = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
@@ -748,8 +766,7 @@ def main():
     s64.set_profiling(False)
 
     # NVT (Nose-Hoover chain 3, tau 0.1 ps, 300 K), same protocol.
-    snvt = make_sched(sysm, eam, "mixed", lanes_per_atom=lanes32, nbr_batch=nb32,
-                      t_target=300.0,
+    snvt = make_sched(sysm, eam, "mixed", t_target=300.0,
                       t_period=0.1, nhc_length=3)
     snvt.run_until(0)
     ms_nvt, _, _, _ = timed_windows(snvt, args.steps, args.warmup, flush, torch, dist)
@@ -758,10 +775,8 @@ def main():
 
     drift = None
     if args.drift_steps > 0:
-        drift = {"mixed": nve_drift(sysm, eam, "mixed", lanes32, args.drift_steps,
-                                    nbr_batch=nb32),
-                 "fp64": nve_drift(sysm, eam, "fp64", lanes64, args.drift_steps,
-                                   nbr_batch=nb64)}
+        drift = {"mixed": nve_drift(sysm, eam, "mixed", args.drift_steps),
+                 "fp64": nve_drift(sysm, eam, "fp64", args.drift_steps)}
 
     batch = None
     if not args.no_batch:
@@ -829,10 +844,9 @@ def main():
                 "md_steps_per_bench_step": WINDOW, "parallelism": f"replicas x{world}",
                 "l2": "flushed (256 MiB write) before every bench step, outside its timing",
                 "mean_neighbors_K": K,
-                "lanes_per_atom": {"mixed": lanes32, "fp64": lanes64,
-                                   "nbr_batch": {"mixed": nb32, "fp64": nb64},
-                                   "autotune_ms_mixed": tune32, "autotune_ms_fp64": tune64,
-                                   "autotune_keys": "<lanes per atom>x<neighbors per lane sweep>"},
+                "launch_shapes": {"mixed": shape_str(shapes32), "fp64": shape_str(shapes64),
+                                  "autotune_ms_mixed": tune32, "autotune_ms_fp64": tune64,
+                                  "keys": "<pass> <lanes per atom>x<neighbors per lane sweep>"},
                 "timesteps_per_s": value / sysm.n,
                 "path_roofline": path_roofline(value, "eam", "mixed", K, occ, hbm),
                 "fp64": {"value": value64, "ms_per_step": ms_fp64 / args.steps,

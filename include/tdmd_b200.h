@@ -107,8 +107,12 @@ typedef struct tdmd_fast_pipeline_stats {
   int64_t graph_launches;
   int64_t nlist_retries;   /* windows re-run after a capacity overflow        */
   int64_t nlist_capacity;  /* neighbor slots per atom currently allocated     */
-  int32_t lanes_per_atom;  /* launch shape in use (after any autotuning)      */
+  /* Launch shapes in use (after any autotuning): the pair-force pass and,
+   * for EAM, the density pass (0 for Morse). */
+  int32_t lanes_per_atom;
   int32_t nbr_batch;
+  int32_t density_lanes_per_atom;
+  int32_t density_nbr_batch;
 } tdmd_fast_pipeline_stats;
 
 /* ------------------------------------------------------------------------ */
@@ -329,16 +333,17 @@ int32_t tdmd_sched_atom_order(const tdmd_sched* s, const int32_t** d_order);
 int32_t tdmd_sched_set_profiling(tdmd_sched* s, int32_t on);
 int32_t tdmd_sched_kernel_times(const tdmd_sched* s, double* avg_ms, int64_t* counts,
                                 int32_t ncat);
-/* Autotuner (no reference counterpart): times the scheduler's force passes
- * on its current state for 1, 2, 4, 8, 16 and 32 lanes per atom and 2 or 4
- * neighbors per lane sweep (only cfg.nbr_batch when that is fixed), keeps
- * the fastest pair and recomputes the forces with it.  ms12 (nullable)
- * receives the timings, ms12[6 * (batch == 4) + k] for 2^k lanes, -1 where
- * not measured.  Runs by itself on the first run_until when
+/* Autotuner (no reference counterpart): times each gather pass of the
+ * scheduler on its current state -- the EAM density pass, then the pair-force
+ * pass -- for 1, 2, 4, 8, 16 and 32 lanes per atom and 2 or 4 neighbors per
+ * lane sweep (only cfg.nbr_batch when that is fixed), keeps each pass's
+ * fastest shape and recomputes the forces with them.  lanes2 / batch2
+ * (nullable) get {density, force} (density 0 for Morse); ms24 (nullable)
+ * the timings, ms24[12 * pass + 6 * (batch == 4) + k] for 2^k lanes, -1
+ * where not measured.  Runs by itself on the first run_until when
  * cfg.lanes_per_atom == 0 and natoms >= 2048.  Results are bit-reproducible
- * for a fixed (lanes, batch) choice. */
-int32_t tdmd_sched_autotune(tdmd_sched* s, int32_t* chosen_lanes, int32_t* chosen_batch,
-                            double* ms12);
+ * for fixed shapes. */
+int32_t tdmd_sched_autotune(tdmd_sched* s, int32_t* lanes2, int32_t* batch2, double* ms24);
 /* Device time (ms) of the last run_until window: CUDA events recorded on the
  * scheduler's stream before its first and after its last enqueued kernel. */
 int32_t tdmd_sched_last_window_ms(const tdmd_sched* s, double* ms);
@@ -390,12 +395,10 @@ int32_t tdmd_batch_energy_log(const tdmd_batch* b, double* steps, double* pe_ke,
 int32_t tdmd_batch_stats(const tdmd_batch* b, tdmd_fast_pipeline_stats* out);
 int32_t tdmd_batch_info(const tdmd_batch* b, int32_t* nreplicas, int64_t* natoms_total,
                         int32_t* lanes_per_atom, int32_t* current_step);
-/* Times the batched force pass for 1..32 lanes per atom and 2 or 4
- * neighbors per lane sweep and keeps the fastest pair (ms12 as for
- * tdmd_sched_autotune; runs by itself on the first run_until when
- * cfg.lanes_per_atom is 0 and the batch has >= 2048 atoms). */
-int32_t tdmd_batch_autotune(tdmd_batch* b, int32_t* chosen_lanes, int32_t* chosen_batch,
-                            double* ms12);
+/* As tdmd_sched_autotune for the batched passes (runs by itself on the
+ * first run_until when cfg.lanes_per_atom is 0 and the batch has >= 2048
+ * atoms). */
+int32_t tdmd_batch_autotune(tdmd_batch* b, int32_t* lanes2, int32_t* batch2, double* ms24);
 /* Device time of the last run_until window (events on the batch's stream). */
 int32_t tdmd_batch_last_window_ms(const tdmd_batch* b, double* ms);
 int32_t tdmd_batch_stream(const tdmd_batch* b, void** stream);

@@ -75,7 +75,8 @@ class FastPipelineStats(C.Structure):
     _fields_ = [("ticks", C.c_int64), ("kernel_launches", C.c_int64), ("rebuilds", C.c_int64),
                 ("graph_launches", C.c_int64), ("nlist_retries", C.c_int64),
                 ("nlist_capacity", C.c_int64), ("lanes_per_atom", C.c_int32),
-                ("nbr_batch", C.c_int32)]
+                ("nbr_batch", C.c_int32), ("density_lanes_per_atom", C.c_int32),
+                ("density_nbr_batch", C.c_int32)]
 
 
 _p = C.c_void_p
@@ -153,7 +154,7 @@ SIGNATURES = {
     "tdmd_batch_energy_log": [_p, _p, _p, _i32, _pi32],
     "tdmd_batch_stats": [_p, C.POINTER(FastPipelineStats)],
     "tdmd_batch_info": [_p, _pi32, C.POINTER(C.c_int64), _pi32, _pi32],
-    "tdmd_batch_autotune": [_p, _pi32, _pi32, _p],
+    "tdmd_batch_autotune": [_p, _p, _p, _p],
     "tdmd_batch_last_window_ms": [_p, _pf64],
     "tdmd_batch_stream": [_p, _pp],
     "tdmd_fit_create": [_i32, _i32, C.POINTER(Box), _p, _p, _f64, _i32, _pp],
@@ -163,7 +164,7 @@ SIGNATURES = {
     "tdmd_fit_eam": [_p, _i32, _i32, _f64, _i32, _f64, _p, _p, _p, _p, _p, _p, _p, _p, _p],
     "tdmd_fit_info": [_p, C.POINTER(C.c_int64), _pi32],
     "tdmd_sched_set_profiling": [_p, _i32],
-    "tdmd_sched_autotune": [_p, _pi32, _pi32, _p],
+    "tdmd_sched_autotune": [_p, _p, _p, _p],
     "tdmd_sched_last_window_ms": [_p, _pf64],
     "tdmd_sched_kernel_times": [_p, _p, _p, _i32],
 }

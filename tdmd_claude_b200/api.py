@@ -62,11 +62,19 @@ def _i32(a):
 
 
 def _autotune(fn, handle):
-    c, u = C.c_int32(), C.c_int32()
-    ms = np.zeros(12, np.float64)
-    call(fn, handle, C.byref(c), C.byref(u), _ptr(ms))
-    return c.value, u.value, {f"{1 << k}x{b}": float(ms[6 * i + k])
-                              for i, b in enumerate((2, 4)) for k in range(6) if ms[6 * i + k] >= 0}
+    """Both passes' chosen shapes {"density": (lanes, batch) or None for
+    Morse, "force": (lanes, batch)} and the timings {"<pass> <lanes>x<batch>":
+    ms} of every shape measured."""
+    lanes = np.zeros(2, np.int32)
+    batch = np.zeros(2, np.int32)
+    ms = np.zeros(24, np.float64)
+    call(fn, handle, _ptr(lanes), _ptr(batch), _ptr(ms))
+    shapes = {"density": (int(lanes[0]), int(batch[0])) if lanes[0] > 0 else None,
+              "force": (int(lanes[1]), int(batch[1]))}
+    timings = {f"{p} {1 << k}x{b}": float(ms[12 * j + 6 * i + k])
+               for j, p in enumerate(("density", "force")) for i, b in enumerate((2, 4))
+               for k in range(6) if ms[12 * j + 6 * i + k] >= 0}
+    return shapes, timings
 
 
 def make_config(dt=0.001, r_skin=1.0, rebuild_every=10, precision="fp64", use_graphs=True,
@@ -283,8 +291,9 @@ class FastPipelineScheduler:
         return v.value
 
     def autotune(self):
-        """Pick lanes per atom and neighbors per lane sweep by timing the
-        force passes; returns (lanes, batch, {"<lanes>x<batch>": ms})."""
+        """Pick each gather pass's launch shape (lanes per atom, neighbors
+        per lane sweep) by timing it; returns (shapes, timings) as
+        _autotune describes."""
         return _autotune("tdmd_sched_autotune", self._h)
 
     def set_profiling(self, on: bool = True):

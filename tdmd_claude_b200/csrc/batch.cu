@@ -245,7 +245,7 @@ class Batch {
   void run_until(int target);
   void energies(double* pe, double* ke);
   void energy_log(double* steps, double* pe_ke, int cap, int* count) const;
-  void autotune(int* chosen, int* chosen_batch, double* ms12);
+  void autotune(int* lanes2, int* batch2, double* ms24);
   void stats(tdmd_fast_pipeline_stats* o) const {
     *o = tdmd_fast_pipeline_stats{};
     o->ticks = ticks_;
@@ -256,6 +256,8 @@ class Batch {
     o->nlist_capacity = cap_;
     o->lanes_per_atom = lpa_;
     o->nbr_batch = nu_;
+    o->density_lanes_per_atom = eam_ ? lpa_d_ : 0;
+    o->density_nbr_batch = eam_ ? nu_d_ : 0;
   }
   int nreplicas() const { return nrep_; }
   long long natoms() const { return n_; }
@@ -267,7 +269,9 @@ class Batch {
 
  private:
   void rebuild(int* status);
-  void force(bool kd = false, bool pe_atom = false);
+  // parts: which EAM passes (density, pair force); Morse has one pass.
+  static constexpr int kPassDensity = 1, kPassForce = 2, kPassBoth = 3;
+  void force(bool kd = false, bool pe_atom = false, int parts = kPassBoth);
   void rep_energy();
   void kick_drift(bool full);
   void half_kick();
@@ -294,6 +298,9 @@ class Batch {
   int ncells_ = 0;
   int lpa_ = 0;
   int nu_ = kU;  // neighbors per lane per sweep (2 or 4)
+  // launch shape of the EAM density pass (lpa_ / nu_: the pair-force pass)
+  int lpa_d_ = 0;
+  int nu_d_ = kU;
   int cap_ = 0;
   int n_types_ = 0;
   bool uploaded_ = false, initialized_ = false, tuned_ = false;
@@ -396,6 +403,8 @@ Batch::Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_mors
   TDMD_REQUIRE(cfg.nbr_batch == 0 || cfg.nbr_batch == 2 || cfg.nbr_batch == 4,
                "nbr_batch must be 0 (tuned), 2 or 4");
   nu_ = cfg.nbr_batch > 0 ? cfg.nbr_batch : kU;
+  lpa_d_ = lpa_;
+  nu_d_ = nu_;
   TDMD_CU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   TDMD_CU(cudaEventCreate(&win_ev_[0]));
   TDMD_CU(cudaEventCreate(&win_ev_[1]));
@@ -551,10 +560,12 @@ void Batch::rebuild(int* status) {
   ++rebuilds_;
 }
 
-void Batch::force(bool kd, bool pea) {
+void Batch::force(bool kd, bool pea, int parts) {
   cudaStream_t s = stream_;
   const NbrView nl = view();
   const int n = static_cast<int>(n_);
+  const Tune td{lpa_d_, nu_d_}, tf{lpa_, nu_};
+  const bool dens = parts & kPassDensity, pair = parts & kPassForce;
   TDMD_REQUIRE(!kd || (eam_ && mixed_), "fused kick-drift needs the mixed EAM batch");
   if (eam_) {
     // Density + embedding, then forces, over all replicas at once (the
@@ -563,36 +574,41 @@ void Batch::force(bool kd, bool pea) {
     if (mixed_) {
       const GeoQB g{q_.data(), rep_.data(), scales_.data()};
       const GeoQB gg{g_.data(), rep_.data(), scales_.data()};
-      launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), nullptr, nullptr,
-                                       g_.data(), false, nullptr, Tune{lpa_, nu_}, s,
-                                       pea ? pe_atom_.data() : nullptr);
+      if (dens)
+        launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), nullptr,
+                                         nullptr, g_.data(), false, nullptr, td, s,
+                                         pea ? pe_atom_.data() : nullptr);
       // kd: the next step's kick + drift in the same pass (the force pass
       // reads gather records only), each atom in its replica's box
       const KickDrift kdr{pos4_.data(), q_.data(), vel_.data(), types_.data(), inv_mm_.data(),
                           cfg_.dt, nullptr, DevBox{}, rep_.data(), reps_.data()};
-      launch_eam_force<GeoQB, true, float, float>(gg, nl, n, eam_->d32, types, fp32_.data(),
-                                                  f32_.data(), pea, nullptr, Tune{lpa_, nu_}, s,
-                                                  kd ? &kdr : nullptr,
-                                                  pea ? pe_atom_.data() : nullptr);
+      if (pair)
+        launch_eam_force<GeoQB, true, float, float>(gg, nl, n, eam_->d32, types, fp32_.data(),
+                                                    f32_.data(), pea, nullptr, tf, s,
+                                                    kd ? &kdr : nullptr,
+                                                    pea ? pe_atom_.data() : nullptr);
     } else {
       const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
-      launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), nullptr,
-                                         nullptr, nullptr, false, nullptr, Tune{lpa_, nu_}, s,
-                                         pea ? pe_atom_.data() : nullptr);
-      launch_eam_force<GeoD4B, false, double, double>(g, nl, n, eam_->d64, types, fp64_.data(),
-                                                      f64_.data(), pea, nullptr, Tune{lpa_, nu_}, s,
-                                                      nullptr, pea ? pe_atom_.data() : nullptr);
+      if (dens)
+        launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), nullptr,
+                                           nullptr, nullptr, false, nullptr, td, s,
+                                           pea ? pe_atom_.data() : nullptr);
+      if (pair)
+        launch_eam_force<GeoD4B, false, double, double>(g, nl, n, eam_->d64, types,
+                                                        fp64_.data(), f64_.data(), pea, nullptr,
+                                                        tf, s, nullptr,
+                                                        pea ? pe_atom_.data() : nullptr);
     }
-    launches_ += 2;
+    launches_ += (dens ? 1 : 0) + (pair ? 1 : 0);
     return;
   }
   if (mixed_) {
     const GeoQB g{q_.data(), rep_.data(), scales_.data()};
-    launch_morse(g, nl, n, m32_, f32_.data(), pea, nullptr, Tune{lpa_, nu_}, s,
+    launch_morse(g, nl, n, m32_, f32_.data(), pea, nullptr, tf, s,
                  pea ? pe_atom_.data() : nullptr);
   } else {
     const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
-    launch_morse(g, nl, n, m64_, f64_.data(), pea, nullptr, Tune{lpa_, nu_}, s,
+    launch_morse(g, nl, n, m64_, f64_.data(), pea, nullptr, tf, s,
                  pea ? pe_atom_.data() : nullptr);
   }
   ++launches_;
@@ -727,48 +743,66 @@ void Batch::initial_forces() {
   initialized_ = true;
 }
 
-// Sweeps lanes per atom {1, ..., 32} x neighbors per lane sweep {2, 4}
-// (only cfg.nbr_batch when that is fixed); ms12[6 * (batch == 4) + k] gets
-// the time of lanes 2^k, -1 where not measured.
-void Batch::autotune(int* chosen, int* chosen_batch, double* ms12) {
+// Sweeps the launch shape of each gather pass on its own, as
+// Scheduler::autotune does: lanes per atom {1, ..., 32} x neighbors per lane
+// sweep {2, 4} (only cfg.nbr_batch when that is fixed), the EAM density
+// pass first, then the pair-force pass; ms24 laid out as there.
+void Batch::autotune(int* lanes2, int* batch2, double* ms24) {
   TDMD_REQUIRE(uploaded_, "autotune before upload");
   if (n_ == 0) return;
   if (!initialized_) initial_forces();
   cudaStream_t s = stream_;
   const int cands[6] = {1, 2, 4, 8, 16, 32};
   const int batches[2] = {2, 4};
-  double best = 1e30;
-  int best_l = lpa_, best_u = nu_;
-  for (int b = 0; b < 2; ++b) {
-    for (int k = 0; k < 6; ++k) {
-      if (ms12) ms12[6 * b + k] = -1.0;
+  if (ms24)
+    for (int k = 0; k < 24; ++k) ms24[k] = -1.0;
+  auto sweep = [&](int pass) {
+    int& lanes = pass == 0 ? lpa_d_ : lpa_;
+    int& batch = pass == 0 ? nu_d_ : nu_;
+    const int parts = pass == 0 ? kPassDensity : kPassForce;
+    double best = 1e30;
+    int best_l = lanes, best_u = batch;
+    for (int b = 0; b < 2; ++b) {
       if (cfg_.nbr_batch > 0 && batches[b] != cfg_.nbr_batch) continue;
-      lpa_ = cands[k];
-      nu_ = batches[b];
-      force();  // warm
-      TDMD_CU(cudaEventRecord(win_ev_[0], s));
-      for (int rep = 0; rep < 5; ++rep) force();
-      TDMD_CU(cudaEventRecord(win_ev_[1], s));
-      TDMD_CU(cudaEventSynchronize(win_ev_[1]));
-      float ms = 0.f;
-      TDMD_CU(cudaEventElapsedTime(&ms, win_ev_[0], win_ev_[1]));
-      const double per = ms / 5.0;
-      if (ms12) ms12[6 * b + k] = per;
-      if (per < best) {
-        best = per;
-        best_l = cands[k];
-        best_u = batches[b];
+      for (int k = 0; k < 6; ++k) {
+        lanes = cands[k];
+        batch = batches[b];
+        force(false, false, parts);  // warm
+        TDMD_CU(cudaEventRecord(win_ev_[0], s));
+        for (int rep = 0; rep < 5; ++rep) force(false, false, parts);
+        TDMD_CU(cudaEventRecord(win_ev_[1], s));
+        TDMD_CU(cudaEventSynchronize(win_ev_[1]));
+        float ms = 0.f;
+        TDMD_CU(cudaEventElapsedTime(&ms, win_ev_[0], win_ev_[1]));
+        const double per = ms / 5.0;
+        if (ms24) ms24[12 * pass + 6 * b + k] = per;
+        if (per < best) {
+          best = per;
+          best_l = cands[k];
+          best_u = batches[b];
+        }
       }
     }
+    lanes = best_l;
+    batch = best_u;
+  };
+  if (eam_) {
+    sweep(0);
+    force(false, false, kPassDensity);  // the chosen density pass's output
   }
-  lpa_ = best_l;
-  nu_ = best_u;
+  sweep(1);
   clear_graphs();
-  force();  // forces of the current state with the chosen shape
+  force();  // forces of the current state with the chosen shapes
   TDMD_CU(cudaStreamSynchronize(s));
   tuned_ = true;
-  if (chosen) *chosen = lpa_;
-  if (chosen_batch) *chosen_batch = nu_;
+  if (lanes2) {
+    lanes2[0] = eam_ ? lpa_d_ : 0;
+    lanes2[1] = lpa_;
+  }
+  if (batch2) {
+    batch2[0] = eam_ ? nu_d_ : 0;
+    batch2[1] = nu_;
+  }
 }
 
 void Batch::run_until(int target) {
@@ -884,7 +918,7 @@ void Batch::reduce_energies(double* out) {
     if (mixed_) {
       const GeoQB g{q_.data(), rep_.data(), scales_.data()};
       launch_eam_density<GeoQB, float>(g, nl, n, eam_->d32, types, fp32_.data(), rho_.data(),
-                                       nullptr, g_.data(), false, nullptr, Tune{lpa_, nu_}, s);
+                                       nullptr, g_.data(), false, nullptr, Tune{lpa_d_, nu_d_}, s);
       TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(
           tn, {
             k_eam_atom_pe<GeoQB, L, U, V, M><<<nblk, kThreads, 0, s>>>(
@@ -893,7 +927,7 @@ void Batch::reduce_energies(double* out) {
     } else {
       const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
       launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), rho_.data(),
-                                         nullptr, nullptr, false, nullptr, Tune{lpa_, nu_}, s);
+                                         nullptr, nullptr, false, nullptr, Tune{lpa_d_, nu_d_}, s);
       TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(
           tn, {
             k_eam_atom_pe<GeoD4B, L, U, V, M><<<nblk, kThreads, 0, s>>>(
@@ -1049,11 +1083,15 @@ int32_t tdmd_batch_info(const tdmd_batch* b, int32_t* nreplicas, int64_t* natoms
   });
 }
 
-int32_t tdmd_batch_autotune(tdmd_batch* b, int32_t* chosen_lanes, int32_t* chosen_batch,
-                            double* ms12) {
+int32_t tdmd_batch_autotune(tdmd_batch* b, int32_t* lanes2, int32_t* batch2, double* ms24) {
   return guarded([&] {
     TDMD_REQUIRE(b, "null handle");
-    b->b.autotune(chosen_lanes, chosen_batch, ms12);
+    int l[2] = {0, 0}, u[2] = {0, 0};
+    b->b.autotune(l, u, ms24);
+    for (int k = 0; k < 2; ++k) {
+      if (lanes2) lanes2[k] = l[k];
+      if (batch2) batch2[k] = u[k];
+    }
   });
 }
 

@@ -89,7 +89,7 @@ class Scheduler {
   // Times the force passes for lanes-per-atom in {1,2,4,8,16,32} on the
   // current state, keeps the fastest, recomputes the forces with it.
   // ms6[k] = ms of candidate 2^k (nullable).
-  void autotune(int* chosen, int* chosen_batch, double* ms12);
+  void autotune(int* lanes2, int* batch2, double* ms24);
   int lanes_per_atom() const { return lpa_; }
   // Device time of the last run_until window (events on the stream around
   // its enqueued work), ms.
@@ -111,7 +111,9 @@ class Scheduler {
   void enqueue_rebuild();
   // kd: the force pass also applies the next step's full kick + drift
   // (mixed EAM, NVE; the force pass reads gather records, not positions).
-  void enqueue_force(bool ev, bool kd = false);
+  // parts: which EAM passes (density, pair force); Morse has one pass.
+  static constexpr int kPassDensity = 1, kPassForce = 2, kPassBoth = 3;
+  void enqueue_force(bool ev, bool kd = false, int parts = kPassBoth);
   bool can_fuse_kick() const { return mixed_ && kind_ == TDMD_POT_EAM && !thermo_; }
   template <class F>
   void enqueue_kick_drift_t(F* f, bool full, bool scale);
@@ -158,6 +160,9 @@ class Scheduler {
   bool mixed_ = false, nvt_ = false, thermo_ = false;
   int lpa_ = 8;
   int nu_ = kU;  // neighbors per lane per sweep (2 or 4)
+  // launch shape of the EAM density pass (lpa_ / nu_: the pair-force pass)
+  int lpa_d_ = 8;
+  int nu_d_ = kU;
   MorseP<double> m64_{};
   MorseP<float> m32_{};
   std::unique_ptr<EamDevTables> eam_;

@@ -402,6 +402,8 @@ void Scheduler::finish_setup() {
   TDMD_REQUIRE(cfg_.nbr_batch == 0 || cfg_.nbr_batch == 2 || cfg_.nbr_batch == 4,
                "nbr_batch must be 0 (tuned), 2 or 4");
   nu_ = cfg_.nbr_batch > 0 ? cfg_.nbr_batch : kU;
+  lpa_d_ = lpa_;
+  nu_d_ = nu_;
 }
 
 void Scheduler::upload(const double* x, const double* v, const void* f, const int* types,
@@ -594,64 +596,76 @@ void Scheduler::enqueue_rebuild() {
 }
 
 // ----- forces ---------------------------------------------------------------
-void Scheduler::enqueue_force(bool ev, bool kd) {
+void Scheduler::enqueue_force(bool ev, bool kd, int parts) {
   TDMD_REQUIRE(!kd || can_fuse_kick(), "fused kick-drift needs the mixed EAM NVE path");
   cudaStream_t s = stream_;
   const NbrView nl{nbr_.data(), nullptr, cnt_.data(), cap_};
-  const int nblk = force_blocks(n_, lpa_);
+  const int nblk = force_blocks(n_, lpa_);       // pair-force pass records
+  const int nblk_d = force_blocks(n_, lpa_d_);   // EAM density pass records
+  const Tune td{lpa_d_, nu_d_}, tf{lpa_, nu_};
   double* part = ev ? ev_part_.data() : nullptr;
   if (kind_ == TDMD_POT_MORSE) {
     prof_begin(kProfForce);
     if (mixed_) {
       const GeoQ g = make_geoq(q_.data(), box_);
-      launch_morse(g, nl, n_, m32_, f32_.data(), ev, part, Tune{lpa_, nu_}, s);
+      launch_morse(g, nl, n_, m32_, f32_.data(), ev, part, tf, s);
     } else {
       GeoD4 g{pos4_.data(), {box_.L[0], box_.L[1], box_.L[2]},
               {box_.halfL[0], box_.halfL[1], box_.halfL[2]},
               {box_.periodic[0], box_.periodic[1], box_.periodic[2]}};
-      launch_morse(g, nl, n_, m64_, f64_.data(), ev, part, Tune{lpa_, nu_}, s);
+      launch_morse(g, nl, n_, m64_, f64_.data(), ev, part, tf, s);
     }
     prof_end(kProfForce);
     launches_ += 1;
   } else {
     const int* types = eam_->ntypes > 1 ? types_.data() : nullptr;
-    double* part2 = ev ? part + static_cast<long long>(nblk) * kEvStride : nullptr;
+    double* part2 = ev ? part + static_cast<long long>(nblk_d) * kEvStride : nullptr;
     if (mixed_) {
       // Density reads the position records and writes {q, F'} gather
       // records; the force pass gathers those.
       const GeoQ g = make_geoq(q_.data(), box_);
       const GeoQ gg = make_geoq(g_.data(), box_);
-      prof_begin(kProfDensity);
-      launch_eam_density<GeoQ, float>(g, nl, n_, eam_->d32, types, fp32_.data(), nullptr,
-                                      nullptr, g_.data(), ev, part, Tune{lpa_, nu_}, s);
-      prof_end(kProfDensity);
-      prof_begin(kProfForce);
+      if (parts & kPassDensity) {
+        prof_begin(kProfDensity);
+        launch_eam_density<GeoQ, float>(g, nl, n_, eam_->d32, types, fp32_.data(), nullptr,
+                                        nullptr, g_.data(), ev, part, td, s);
+        prof_end(kProfDensity);
+      }
       const KickDrift kdr{pos4_.data(), q_.data(), vel_.data(), types_.data(), inv_mm_.data(),
                           cfg_.dt,
                           reinterpret_cast<long long*>(reinterpret_cast<char*>(ctl_.data()) +
                                                        offsetof(SchedCtl, step)),
                           box_, nullptr, nullptr};
-      launch_eam_force<GeoQ, true, float, float>(gg, nl, n_, eam_->d32, types, fp32_.data(),
-                                                 f32_.data(), ev, part2, Tune{lpa_, nu_}, s,
-                                                 kd ? &kdr : nullptr);
-      prof_end(kProfForce);
+      if (parts & kPassForce) {
+        prof_begin(kProfForce);
+        launch_eam_force<GeoQ, true, float, float>(gg, nl, n_, eam_->d32, types, fp32_.data(),
+                                                   f32_.data(), ev, part2, tf, s,
+                                                   kd ? &kdr : nullptr);
+        prof_end(kProfForce);
+      }
     } else {
       GeoD4 g{pos4_.data(), {box_.L[0], box_.L[1], box_.L[2]},
               {box_.halfL[0], box_.halfL[1], box_.halfL[2]},
               {box_.periodic[0], box_.periodic[1], box_.periodic[2]}};
-      prof_begin(kProfDensity);
-      launch_eam_density<GeoD4, double>(g, nl, n_, eam_->d64, types, fp64_.data(), nullptr,
-                                        nullptr, nullptr, ev, part, Tune{lpa_, nu_}, s);
-      prof_end(kProfDensity);
-      prof_begin(kProfForce);
-      launch_eam_force<GeoD4, false, double, double>(g, nl, n_, eam_->d64, types, fp64_.data(),
-                                                     f64_.data(), ev, part2, Tune{lpa_, nu_}, s);
-      prof_end(kProfForce);
+      if (parts & kPassDensity) {
+        prof_begin(kProfDensity);
+        launch_eam_density<GeoD4, double>(g, nl, n_, eam_->d64, types, fp64_.data(), nullptr,
+                                          nullptr, nullptr, ev, part, td, s);
+        prof_end(kProfDensity);
+      }
+      if (parts & kPassForce) {
+        prof_begin(kProfForce);
+        launch_eam_force<GeoD4, false, double, double>(g, nl, n_, eam_->d64, types,
+                                                       fp64_.data(), f64_.data(), ev, part2, tf,
+                                                       s);
+        prof_end(kProfForce);
+      }
     }
-    launches_ += 2;
+    launches_ += ((parts & kPassDensity) ? 1 : 0) + ((parts & kPassForce) ? 1 : 0);
   }
   if (ev) {
-    const int nrec = kind_ == TDMD_POT_EAM ? 2 * nblk : nblk;
+    TDMD_REQUIRE(parts == kPassBoth, "energy/virial needs both passes");
+    const int nrec = kind_ == TDMD_POT_EAM ? nblk_d + nblk : nblk;
     TDMD_CU(cudaMemsetAsync(ctl_ev(), 0, sizeof(double) * 7, s));
     k_reduce_partials<<<1, 256, 0, s>>>(ev_part_.data(), nrec, ctl_ev(),
                                         ctl_ev() + 1);
@@ -1087,10 +1101,13 @@ void Scheduler::thermostat_state(double* dt, double* eta, double* eta_v) const {
 
 // ----- per-kernel timing -------------------------------------------------------
 // ----- autotuner ---------------------------------------------------------------
-// Sweeps lanes per atom {1, ..., 32} x neighbors per lane sweep {2, 4}
-// (only cfg.nbr_batch when that is fixed); ms12[6 * (batch == 4) + k] gets
-// the time of lanes 2^k, -1 where not measured.
-void Scheduler::autotune(int* chosen, int* chosen_batch, double* ms12) {
+// Sweeps the launch shape of each gather pass on its own -- lanes per atom
+// {1, ..., 32} x neighbors per lane sweep {2, 4} (only cfg.nbr_batch when
+// that is fixed): the EAM density pass first, then the pair-force pass on
+// that density.  lanes2 / batch2 = {density, force} (density 0 for Morse);
+// ms24[12 * pass + 6 * (batch == 4) + k] = time of lanes 2^k, -1 where not
+// measured.
+void Scheduler::autotune(int* lanes2, int* batch2, double* ms24) {
   TDMD_REQUIRE(uploaded_, "autotune before upload");
   if (n_ == 0) return;
   if (!initialized_) initial_forces();
@@ -1100,48 +1117,66 @@ void Scheduler::autotune(int* chosen, int* chosen_batch, double* ms12) {
   cudaEvent_t e0, e1;
   TDMD_CU(cudaEventCreate(&e0));
   TDMD_CU(cudaEventCreate(&e1));
+  const bool eam = kind_ == TDMD_POT_EAM;
   const int cand[6] = {1, 2, 4, 8, 16, 32};
   const int batches[2] = {2, 4};
-  double best_ms = 1e300;
-  int best = lpa_, best_u = nu_;
-  for (int b = 0; b < 2; ++b) {
-    for (int k = 0; k < 6; ++k) {
-      if (ms12) ms12[6 * b + k] = -1.0;
+  if (ms24)
+    for (int k = 0; k < 24; ++k) ms24[k] = -1.0;
+  auto sweep = [&](int pass) {
+    int& lanes = pass == 0 ? lpa_d_ : lpa_;
+    int& batch = pass == 0 ? nu_d_ : nu_;
+    const int parts = pass == 0 ? kPassDensity : kPassForce;
+    double best_ms = 1e300;
+    int best_l = lanes, best_u = batch;
+    for (int b = 0; b < 2; ++b) {
       if (cfg_.nbr_batch > 0 && batches[b] != cfg_.nbr_batch) continue;
-      lpa_ = cand[k];
-      nu_ = batches[b];
-      enqueue_force(false);  // warm
-      double m = 1e300;
-      for (int rep = 0; rep < 3; ++rep) {
-        TDMD_CU(cudaEventRecord(e0, stream_));
-        enqueue_force(false);
-        TDMD_CU(cudaEventRecord(e1, stream_));
-        TDMD_CU(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        TDMD_CU(cudaEventElapsedTime(&ms, e0, e1));
-        m = std::min(m, static_cast<double>(ms));
-      }
-      if (ms12) ms12[6 * b + k] = m;
-      if (m < best_ms) {
-        best_ms = m;
-        best = cand[k];
-        best_u = batches[b];
+      for (int k = 0; k < 6; ++k) {
+        lanes = cand[k];
+        batch = batches[b];
+        enqueue_force(false, false, parts);  // warm
+        double m = 1e300;
+        for (int rep = 0; rep < 3; ++rep) {
+          TDMD_CU(cudaEventRecord(e0, stream_));
+          enqueue_force(false, false, parts);
+          TDMD_CU(cudaEventRecord(e1, stream_));
+          TDMD_CU(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          TDMD_CU(cudaEventElapsedTime(&ms, e0, e1));
+          m = std::min(m, static_cast<double>(ms));
+        }
+        if (ms24) ms24[12 * pass + 6 * b + k] = m;
+        if (m < best_ms) {
+          best_ms = m;
+          best_l = cand[k];
+          best_u = batches[b];
+        }
       }
     }
+    lanes = best_l;
+    batch = best_u;
+  };
+  if (eam) {
+    sweep(0);
+    enqueue_force(false, false, kPassDensity);  // the chosen density pass's output
   }
+  sweep(1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  // The forces of the current state, summed in the chosen shape's order.
-  lpa_ = best;
-  nu_ = best_u;
+  // The forces of the current state, summed in the chosen shapes' order.
   enqueue_force(false);
   TDMD_CU(cudaStreamSynchronize(stream_));
   launches_ = l0;  // tuning passes are not part of the run's kernel count
   clear_graphs();
   tuned_ = true;
   profiling_ = prof;
-  if (chosen) *chosen = best;
-  if (chosen_batch) *chosen_batch = best_u;
+  if (lanes2) {
+    lanes2[0] = eam ? lpa_d_ : 0;
+    lanes2[1] = lpa_;
+  }
+  if (batch2) {
+    batch2[0] = eam ? nu_d_ : 0;
+    batch2[1] = nu_;
+  }
 }
 
 void Scheduler::set_profiling(bool on) {
@@ -1207,6 +1242,8 @@ void Scheduler::stats(tdmd_fast_pipeline_stats* o) const {
   o->nlist_capacity = cap_;
   o->lanes_per_atom = lpa_;
   o->nbr_batch = nu_;
+  o->density_lanes_per_atom = kind_ == TDMD_POT_EAM ? lpa_d_ : 0;
+  o->density_nbr_batch = kind_ == TDMD_POT_EAM ? nu_d_ : 0;
 }
 
 }  // namespace tdmd_b200
@@ -1373,13 +1410,15 @@ int32_t tdmd_sched_stream(const tdmd_sched* s, void** stream) {
 
 }  // extern "C"
 
-extern "C" int32_t tdmd_sched_autotune(tdmd_sched* s, int32_t* chosen_lanes,
-                                       int32_t* chosen_batch, double* ms12) {
+extern "C" int32_t tdmd_sched_autotune(tdmd_sched* s, int32_t* lanes2, int32_t* batch2,
+                                       double* ms24) {
   return guarded([&] {
     TDMD_REQUIRE(s, "null handle");
-    int c = 0, u = 0;
-    s->s->autotune(&c, &u, ms12);
-    if (chosen_lanes) *chosen_lanes = c;
-    if (chosen_batch) *chosen_batch = u;
+    int l[2] = {0, 0}, u[2] = {0, 0};
+    s->s->autotune(l, u, ms24);
+    for (int k = 0; k < 2; ++k) {
+      if (lanes2) lanes2[k] = l[k];
+      if (batch2) batch2[k] = u[k];
+    }
   });
 }

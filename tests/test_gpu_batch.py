@@ -127,8 +127,10 @@ def test_batch_autotune_keeps_forces(cuda):
     b = _batch(systems, "mixed", lanes=0)
     b.run_until(0)
     _, _, f0 = b.download()
-    lanes, nb, ms = b.autotune()
-    assert f"{lanes}x{nb}" in ms and len(ms) == 12 and all(v > 0 for v in ms.values())
+    shapes, ms = b.autotune()
+    lanes, nb = shapes["force"]
+    assert shapes["density"] is None  # Morse: one pass
+    assert f"force {lanes}x{nb}" in ms and len(ms) == 12 and all(v > 0 for v in ms.values())
     st = b.stats()
     assert (st.lanes_per_atom, st.nbr_batch) == (lanes, nb)
     _, _, f1 = b.download()

@@ -268,11 +268,15 @@ def test_autotune_keeps_forces(cuda, precision):
     s, sysm, t = _eam_setup(precision, ncell=8)
     s.run_until(0)
     f0 = s.download().forces.astype(np.float64)
-    chosen, nb, ms = s.autotune()
-    assert chosen in (1, 2, 4, 8, 16, 32) and nb in (2, 4)
-    assert f"{chosen}x{nb}" in ms and len(ms) == 12 and all(v > 0 for v in ms.values())
+    shapes, ms = s.autotune()
+    for p in ("density", "force"):
+        lanes, nb = shapes[p]
+        assert lanes in (1, 2, 4, 8, 16, 32) and nb in (2, 4)
+        assert f"{p} {lanes}x{nb}" in ms
+    assert len(ms) == 24 and all(v > 0 for v in ms.values())
     st = s.stats()
-    assert (st.lanes_per_atom, st.nbr_batch) == (chosen, nb)
+    assert (st.density_lanes_per_atom, st.density_nbr_batch) == shapes["density"]
+    assert (st.lanes_per_atom, st.nbr_batch) == shapes["force"]
     f1 = s.download().forces.astype(np.float64)
     assert rel_rms(f1, f0) < (1e-13 if precision == "fp64" else 1e-6)
     s.run_until(20)
@@ -302,8 +306,9 @@ def test_neighbor_batch_sizes(cuda, precision):
     assert rel_rms(runs[4, 2][0], runs[4, 4][0]) < (1e-13 if precision == "fp64" else 1e-6)
     s, _, _ = _eam_setup(precision, ncell=6, lanes_per_atom=4, nbr_batch=2)
     s.run_until(0)
-    _, nb, ms = s.autotune()
-    assert nb == 2 and sorted(ms) == sorted(f"{1 << k}x2" for k in range(6))
+    shapes, ms = s.autotune()
+    assert shapes["density"][1] == 2 and shapes["force"][1] == 2
+    assert sorted(ms) == sorted(f"{p} {1 << k}x2" for p in ("density", "force") for k in range(6))
     s.close()
 
 
