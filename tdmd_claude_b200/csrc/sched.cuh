@@ -105,7 +105,7 @@ class Scheduler {
 
  private:
   void finish_setup();
-  void size_neighbor_list();
+  int size_neighbor_list();  // returns the cell-list kernels launched
   void grow_capacity(int max_count);
   void initial_forces();
   void enqueue_rebuild();
@@ -139,9 +139,8 @@ class Scheduler {
   // bin + scan + scatter + sort
   int cell_list_kernels() const { return 3 + device_scan_launches(cl_.ncells); }
   void reorder_by_cell();
-  void build_cells() {
-    build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, stream_, order_.data());
-  }
+  // Keyed cell list of the current positions; returns the kernels launched.
+  int build_cells();
   int* ctl_status() const {
     return reinterpret_cast<int*>(reinterpret_cast<char*>(ctl_.data()) +
                                   offsetof(SchedCtl, status));
@@ -174,6 +173,13 @@ class Scheduler {
   DevArray<double> f64_;
   DevArray<float> f32_;
   DevArray<int> types_, ids_;
+  // second buffers of the per-atom state: upload gathers into them and swaps
+  DevArray<double4> pos4_alt_;
+  DevArray<int4> q_alt_;
+  DevArray<double> vel_alt_, f64_alt_;
+  DevArray<float> f32_alt_;
+  DevArray<int> types_alt_, ids_alt_;
+  bool cells_from_upload_ = false;  // cl_ holds the cells of the reordered upload
   DevArray<double> masses_;
   DevArray<double> inv_mm_;  // 1 / (m mvv2e) per type: the kick factor per unit dt
   DevArray<int4> g_;         // mixed EAM: {qx, qy, qz, bits(F'(rho))} per atom
@@ -184,7 +190,6 @@ class Scheduler {
   // their members by that index, so every neighbor row lists the same atoms
   // in the same order as without the reordering.
   DevArray<int> order_;
-  DevArray<double4> perm_tmp_;
   int n_types_ = 0;
 
   // Neighbor list: padded rows of cap_ entries.

@@ -79,6 +79,33 @@ __global__ void k_gather(const T* __restrict__ src, const int* __restrict__ idx,
   if (i < n) dst[i] = src[idx[i]];
 }
 
+// The whole per-atom state into the cell order in one pass: dst[i] =
+// src[idx[i]] for positions, velocities, types, ids, fixed-point records
+// (nullable) and forces.
+template <class F>
+__global__ void k_gather_state(const int* __restrict__ idx, int n,
+                               const double4* __restrict__ p, double4* __restrict__ p_o,
+                               const D3* __restrict__ v, D3* __restrict__ v_o,
+                               const int* __restrict__ t, int* __restrict__ t_o,
+                               const int* __restrict__ id, int* __restrict__ id_o,
+                               const int4* __restrict__ q, int4* __restrict__ q_o,
+                               const F* __restrict__ f, F* __restrict__ f_o) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j = idx[i];
+  p_o[i] = p[j];
+  v_o[i] = v[j];
+  t_o[i] = t[j];
+  id_o[i] = id[j];
+  if (q) q_o[i] = q[j];
+  f_o[i] = f[j];
+}
+
+__global__ void k_iota(int* __restrict__ a, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+
 // dst[idx[i]] = src[i]
 template <class T>
 __global__ void k_scatter(const T* __restrict__ src, const int* __restrict__ idx, int n,
@@ -427,13 +454,9 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
     f64_.reserve(3 * n);
   }
   n_types_ = n_types;
+  uploaded_ = false;
+  cells_from_upload_ = false;
   if (n_ > 0) {
-    // Host types are checked: the kernels index masses[type] directly.
-    for (size_t i = 0; i < n; ++i)
-      TDMD_REQUIRE(types[i] >= 1 && types[i] < n_types, "atom type out of range of masses");
-    if (kind_ == TDMD_POT_EAM)
-      for (size_t i = 0; i < n; ++i)
-        TDMD_REQUIRE(types[i] <= eam_->ntypes, "atom type beyond the EAM element count");
     TDMD_CU(cudaMemcpyAsync(stage_.data(), x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     TDMD_CU(cudaMemcpyAsync(vel_.data(), v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     TDMD_CU(cudaMemcpyAsync(types_.data(), types, n * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -485,7 +508,16 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
     log_cap_ = cfg_.energy_log_capacity > 0 ? cfg_.energy_log_capacity : 1024;
     log_.reserve(static_cast<size_t>(log_cap_) * 9);
   }
+  // Host types are checked (the kernels index masses[type] directly) while
+  // the copies and the reordering run; nothing that indexes by type has
+  // been enqueued yet.
+  bool types_ok = true, types_in_eam = true;
+  for (size_t i = 0; i < n; ++i) types_ok &= types[i] >= 1 && types[i] < n_types;
+  if (kind_ == TDMD_POT_EAM)
+    for (size_t i = 0; i < n; ++i) types_in_eam &= types[i] <= eam_->ntypes;
   TDMD_CU(cudaStreamSynchronize(s));
+  TDMD_REQUIRE(types_ok, "atom type out of range of masses");
+  TDMD_REQUIRE(types_in_eam, "atom type beyond the EAM element count");
   uploaded_ = true;
   initialized_ = false;
   step_ = 0;
@@ -499,27 +531,43 @@ void Scheduler::reorder_by_cell() {
   const size_t n = static_cast<size_t>(n_);
   build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, s);
   order_.reserve(n);
-  perm_tmp_.reserve(n);
   TDMD_CU(cudaMemcpyAsync(order_.data(), cl_.cell_atoms.data(), n * sizeof(int),
                           cudaMemcpyDeviceToDevice, s));
+  // Gather into the second set of buffers, then swap them in.
+  pos4_alt_.reserve(n);
+  vel_alt_.reserve(3 * n);
+  types_alt_.reserve(n);
+  ids_alt_.reserve(n);
   const int nb = ceil_div(n_, kThreads);
-  auto permute = [&](auto* arr) {
-    using T = std::remove_pointer_t<decltype(arr)>;
-    T* tmp = reinterpret_cast<T*>(perm_tmp_.data());
-    k_gather<T><<<nb, kThreads, 0, s>>>(arr, order_.data(), n_, tmp);
-    TDMD_LAUNCH_CHECK();
-    TDMD_CU(cudaMemcpyAsync(arr, tmp, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
-  };
-  permute(pos4_.data());
-  permute(reinterpret_cast<D3*>(vel_.data()));
-  permute(types_.data());
-  permute(ids_.data());
   if (mixed_) {
-    permute(q_.data());
-    permute(reinterpret_cast<F3*>(f32_.data()));
+    q_alt_.reserve(n);
+    f32_alt_.reserve(3 * n);
+    k_gather_state<F3><<<nb, kThreads, 0, s>>>(
+        order_.data(), n_, pos4_.data(), pos4_alt_.data(),
+        reinterpret_cast<const D3*>(vel_.data()), reinterpret_cast<D3*>(vel_alt_.data()),
+        types_.data(), types_alt_.data(), ids_.data(), ids_alt_.data(), q_.data(),
+        q_alt_.data(), reinterpret_cast<const F3*>(f32_.data()),
+        reinterpret_cast<F3*>(f32_alt_.data()));
+    std::swap(q_, q_alt_);
+    std::swap(f32_, f32_alt_);
   } else {
-    permute(reinterpret_cast<D3*>(f64_.data()));
+    f64_alt_.reserve(3 * n);
+    k_gather_state<D3><<<nb, kThreads, 0, s>>>(
+        order_.data(), n_, pos4_.data(), pos4_alt_.data(),
+        reinterpret_cast<const D3*>(vel_.data()), reinterpret_cast<D3*>(vel_alt_.data()),
+        types_.data(), types_alt_.data(), ids_.data(), ids_alt_.data(), nullptr, nullptr,
+        reinterpret_cast<const D3*>(f64_.data()), reinterpret_cast<D3*>(f64_alt_.data()));
+    std::swap(f64_, f64_alt_);
   }
+  TDMD_LAUNCH_CHECK();
+  std::swap(pos4_, pos4_alt_);
+  std::swap(vel_, vel_alt_);
+  std::swap(types_, types_alt_);
+  std::swap(ids_, ids_alt_);
+  // The cells of the reordered atoms: same counts and starts, and each
+  // cell's members are consecutive indices in ID order -- the next
+  // build_cells only has to write the identity.
+  cells_from_upload_ = true;
 }
 
 void Scheduler::download(double* x, double* v, void* f, int* types, int* ids, int natoms) const {
@@ -557,9 +605,20 @@ void Scheduler::download(double* x, double* v, void* f, int* types, int* ids, in
 }
 
 // ----- neighbor list ------------------------------------------------------
-void Scheduler::size_neighbor_list() {
+int Scheduler::build_cells() {
+  if (cells_from_upload_) {
+    cells_from_upload_ = false;
+    k_iota<<<ceil_div(n_, kThreads), kThreads, 0, stream_>>>(cl_.cell_atoms.data(), n_);
+    TDMD_LAUNCH_CHECK();
+    return 1;
+  }
+  build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, stream_, order_.data());
+  return cell_list_kernels();
+}
+
+int Scheduler::size_neighbor_list() {
   cudaStream_t s = stream_;
-  build_cells();
+  const int kernels = build_cells();
   cnt_.reserve(static_cast<size_t>(n_));
   const double rl = cutoff_ + cfg_.r_skin;
   TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
@@ -569,6 +628,7 @@ void Scheduler::size_neighbor_list() {
   TDMD_CU(cudaMemcpyAsync(st, ctl_status(), sizeof(st), cudaMemcpyDeviceToHost, s));
   TDMD_CU(cudaStreamSynchronize(s));
   grow_capacity(st[1]);
+  return kernels;
 }
 
 void Scheduler::grow_capacity(int max_count) {
@@ -586,12 +646,12 @@ void Scheduler::grow_capacity(int max_count) {
 void Scheduler::enqueue_rebuild() {
   cudaStream_t s = stream_;
   prof_begin(kProfRebuild);
-  build_cells();
+  const int cell_kernels = build_cells();
   const double rl = cutoff_ + cfg_.r_skin;
   build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl * rl, nbr_.data(), nullptr,
                       cap_, cnt_.data(), ctl_status(), s);
   prof_end(kProfRebuild);
-  launches_ += cell_list_kernels() + 1;  // cell list + row build
+  launches_ += cell_kernels + 1;  // cell list + row build
   ++rebuilds_;
 }
 
@@ -905,13 +965,13 @@ void Scheduler::initial_forces() {
   // The first upload sizes the rows with a count pass; later uploads reuse
   // the capacity and fill directly, counting a second fill only when a row
   // did not fit.
-  int passes = 1;
+  int passes = 1, cell_kernels = 0;
   const bool reuse = cap_ > 0;
   if (reuse) {
-    build_cells();
+    cell_kernels = build_cells();
     cnt_.reserve(static_cast<size_t>(n_));
   } else {
-    size_neighbor_list();
+    cell_kernels = size_neighbor_list();
     ++passes;
   }
   TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
@@ -929,7 +989,7 @@ void Scheduler::initial_forces() {
       ++passes;
     }
   }
-  launches_ += cell_list_kernels() + passes;  // cell list + (count pass) + fill pass(es)
+  launches_ += cell_kernels + passes;  // cell list + (count pass) + fill pass(es)
   ++rebuilds_;
   since_rebuild_ = 0;
   enqueue_force(false);
