@@ -253,12 +253,18 @@ __device__ __forceinline__ void build_cell_rows(
           dz = min_image1(dz, Lz, hz, b.periodic[2]);
         }
         const float r2f = dx * dx + dy * dy + dz * dz;
-        bool pred = j != i && r2f < lo_f;
-        if (j != i && r2f >= lo_f && r2f <= hi_f) pred = exact_within(pos, i, j, rl2, b.L[0], b.L[1], b.L[2], b.halfL[0],
-                                         b.halfL[1], b.halfL[2], b.periodic[0], b.periodic[1],
-                                         b.periodic[2]);
-        const unsigned m = __ballot_sync(0xffffffffu, pred);
-        if (WRITE && pred) {
+        const bool other = j != i;
+        unsigned m = __ballot_sync(0xffffffffu, other && r2f < lo_f);
+        // Candidates inside the filter's band go to the exact FP64 test:
+        // rare, so the warp enters that path only when some lane needs it.
+        const bool band = other && r2f >= lo_f && r2f <= hi_f;
+        if (__any_sync(0xffffffffu, band)) {
+          const bool ok = band && exact_within(pos, i, j, rl2, b.L[0], b.L[1], b.L[2],
+                                               b.halfL[0], b.halfL[1], b.halfL[2],
+                                               b.periodic[0], b.periodic[1], b.periodic[2]);
+          m |= __ballot_sync(0xffffffffu, ok);
+        }
+        if (WRITE && ((m >> lane) & 1u)) {
           const int p = cnt + __popc(m & lt_mask);
           if (p < limit) nbr[base + p] = j;
         }
