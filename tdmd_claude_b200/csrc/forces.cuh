@@ -624,7 +624,15 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
           // FP64 work.
           T sx;
           const int idx = spline_fast(g.radius_fast(pr[u]), e, sx);
-          const int tj = MULTI ? __ldg(types + jj[u]) - 1 : 0;
+          // fixed-point position records carry the atom's 1-based type in
+          // their fourth word (the density pass always reads those)
+          int tj = 0;
+          if constexpr (MULTI) {
+            if constexpr (Geo::kRecords)
+              tj = pr[u].w - 1;
+            else
+              tj = __ldg(types + jj[u]) - 1;
+          }
           const auto cf = ldv4<T>(e.dtab + static_cast<long long>(idx) * e.ntypes + tj);
           rho.add(spl_val(cf, sx));
         }
