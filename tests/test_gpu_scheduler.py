@@ -264,6 +264,40 @@ def test_upload_rejects_bad_types(cuda):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("periodic", [(1, 1, 0), (0, 0, 0)])
+def test_eam_nonperiodic_matches_oracle(cuda, oracle, precision, periodic):
+    """A slab (vacuum along z) and a free cluster: with 8 A of vacuum on
+    each non-periodic axis, the neighbor rows take no image across those
+    axes and the trajectory follows the oracle's."""
+    from tdmd_claude_b200 import Box, EamAlloy, FastPipelineScheduler, make_config
+    from tdmd_claude_b200 import workloads as W
+    t = W.cu_eam_tables()
+    sysm = W.fcc_system(5, 3.615, 300.0, seed=33)
+    lo, hi = np.array(sysm.lo, float), np.array(sysm.hi, float)
+    for a in range(3):
+        if not periodic[a]:
+            lo[a] -= 8.0
+            hi[a] += 8.0
+    eam = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    s = FastPipelineScheduler(Box.make(lo, hi, periodic), sysm.n, eam,
+                              make_config(r_skin=0.3, precision=precision, lanes_per_atom=2))
+    s.upload(sysm.positions, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+    s.run_until(40)
+    st = s.download()
+    s.close()
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    r = oracle.md_run(sysm.positions, sysm.velocities, sysm.types, sysm.masses, lo, hi, 0.001,
+                      0.3, 10, [40], eam=oe, periodic=periodic)
+    d = _wrap_diff(st.positions, r["pos"], hi - lo)
+    if precision == "fp64":
+        assert np.abs(d).max() < 1e-10
+        assert rel_rms(st.forces, r["forces"]) < 1e-9
+    else:
+        assert np.abs(d).max() < 5e-4
+        assert rel_rms(st.forces, r["forces"]) < 1e-4
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_autotune_keeps_forces(cuda, precision):
     """The autotuner only reorders the per-atom sums: forces stay within
     rounding, the choice is one of the candidates, later steps still match."""
