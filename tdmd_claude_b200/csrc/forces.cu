@@ -234,11 +234,15 @@ void EamDevTables::upload(const tdmd_eam& e, cudaStream_t stream) {
   TDMD_CU(cudaStreamSynchronize(stream));
   ntypes = nt;
   cutoff = e.cutoff;
+  // type bits in the mixed gather records: ceil(log2(nt)) for 2..16 types
+  int tbits = 0;
+  if (nt > 1 && nt <= 16)
+    while ((1 << tbits) < nt) ++tbits;
   d64 = EamDev<double>{dtab64.data(), rtab64.data(), ftab.data(), nt, S, e.nr, e.nrho, e.dr,
-                       1.0 / e.dr, e.cutoff * e.cutoff, e.drho, e.dr};
+                       1.0 / e.dr, e.cutoff * e.cutoff, e.drho, e.dr, 0};
   d32 = EamDev<float>{dtab32.data(), rtab32.data(), ftab.data(), nt, S, e.nr, e.nrho,
                       static_cast<float>(e.dr), static_cast<float>(1.0 / e.dr),
-                      static_cast<float>(e.cutoff * e.cutoff), e.drho, e.dr};
+                      static_cast<float>(e.cutoff * e.cutoff), e.drho, e.dr, tbits};
 }
 
 // --------------------------------------------------------------------------

@@ -484,6 +484,11 @@ struct EamDev {
   T dr, inv_dr, rc_sq;
   double drho;
   double dr_d;
+  // Multi-type mixed path: the low tbits mantissa bits of the gather
+  // record's F'(rho) word hold the atom's 0-based type (a relative change of
+  // F' below 2^(tbits-23)), so the force pass gathers no type; 0 = types are
+  // gathered (one type, or more than 16).
+  int tbits;
 };
 
 __device__ __forceinline__ int phi_slot(int ti, int tj, int nt) {
@@ -655,6 +660,10 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
       if (gout) {
         int4 rec = g.record(o);
         rec.w = __float_as_int(static_cast<float>(dF));
+        if (MULTI && e.tbits) {
+          const int mask = (1 << e.tbits) - 1;
+          rec.w = (rec.w & ~mask) | ti;
+        }
         gout[i] = rec;
       }
     }
@@ -731,7 +740,15 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
     const long long row = nl.row(i);
     const int c = nl.count(i);
     const int ti = MULTI ? __ldg(types + i) - 1 : 0;
-    const T fpi = static_cast<T>(__ldg(fp + i));
+    // packed types (FPG, multi-type): F' of both atoms from the records with
+    // the type bits cleared, so the pair term stays symmetric
+    const bool packed = FPG && MULTI && e.tbits > 0;
+    const int tmask = packed ? (1 << e.tbits) - 1 : 0;
+    T fpi;
+    if constexpr (FPG && MULTI && Geo::kRecords)
+      fpi = packed ? __int_as_float(g.record(o).w & ~tmask) : static_cast<T>(__ldg(fp + i));
+    else
+      fpi = static_cast<T>(__ldg(fp + i));
     for (int base = U * sub; base < c; base += U * LPA) {
       int jj[U];
       nbr_batch<VEC>(nl, row, base, c, jj);
@@ -751,7 +768,11 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
           g.radius(o, pr[u], r, rinv, rd);
           const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
           const int j = jj[u];
-          const int tj = MULTI ? __ldg(types + j) - 1 : 0;
+          int tj = 0;
+          if constexpr (MULTI && FPG)
+            tj = packed ? (pr[u].w & tmask) : __ldg(types + j) - 1;
+          else if constexpr (MULTI)
+            tj = __ldg(types + j) - 1;
           const auto* rowp = e.rtab + static_cast<long long>(idx) * e.S;
           typename V4<T>::type cphi, crho;
           if constexpr (!MULTI && sizeof(T) == sizeof(float)) {
@@ -765,7 +786,7 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
           if (MULTI && tj != ti) dri = dspl_der(ldv4<T>(rowp + ti), sx);
           T fpj;
           if constexpr (FPG) {
-            fpj = __int_as_float(pr[u].w);
+            fpj = __int_as_float(pr[u].w & ~tmask);
           } else {
             fpj = static_cast<T>(__ldg(fp + j));
           }
