@@ -263,6 +263,30 @@ def test_upload_rejects_bad_types(cuda):
         s.run_until(3)     # nothing uploaded
 
 
+def test_ternary_scheduler_mixed_forces_vs_oracle(cuda, oracle):
+    """The scheduler's mixed multi-type path carries each atom's type in the
+    low mantissa bits of its F'(rho) gather word: its forces and energy stay
+    within the mixed bounds of the FP64 oracle, at the start and after 20
+    steps (oracle forces of the scheduler's own positions)."""
+    from tdmd_claude_b200 import Box, EamAlloy, FastPipelineScheduler, make_config
+    from tdmd_claude_b200 import workloads as W
+    t = W.ternary_eam_tables()
+    sysm = W.ternary(6, seed=3)
+    eam = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    s = FastPipelineScheduler(Box.make(sysm.lo, sysm.hi), sysm.n, eam,
+                              make_config(r_skin=0.3, precision="mixed", lanes_per_atom=2))
+    s.upload(sysm.positions, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    for step in (0, 20):
+        s.run_until(step)
+        st = s.download()
+        pe, _, _ = s.energies()
+        r = oe.forces(st.positions, sysm.types, sysm.lo, sysm.hi, 0.3)
+        assert rel_rms(st.forces, r["forces"]) < 1e-5, step
+        assert abs(pe - r["pe"]) / abs(r["pe"]) < 1e-6, step
+    s.close()
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("periodic", [(1, 1, 0), (0, 0, 0)])
 def test_eam_nonperiodic_matches_oracle(cuda, oracle, precision, periodic):
