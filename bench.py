@@ -457,7 +457,7 @@ def ternary_bench(steps, warmup, flush, torch, total_steps=2000):
                         "NVT NHC-3 1000 K, adaptive dt"}
 
 
-def fit_bench(torch, adam_steps=200, nsnap=64):
+def fit_bench(torch, adam_steps=200, nsnap=64, continue_morse=True):
     """Force matching: nsnap snapshots of a 10^3-cell Cu FCC (4,000 atoms)
     FP64 NVE run at 1200 K (one every 100 steps, config-1 EAM); targets from
     the FP64 forces of parameters perturbed by seeded 5 % Gaussian noise;
@@ -505,7 +505,7 @@ def fit_bench(torch, adam_steps=200, nsnap=64):
     # Net forces of a near-lattice constrain mostly the pair curvature at the
     # neighbor shells, which leaves a shallow D - r0 valley: an untimed
     # continuation with a decaying step size shows where the fit goes.
-    more = 10 * adam_steps
+    more = 10 * adam_steps if continue_morse else 1
     l2, sec2 = FT.adam_fit(lambda q: FT.morse_loss(q, fm), [p], steps=more, lr=5e-3,
                            lr_final=1e-5)
     pt = torch.tensor(true, dtype=torch.float64, device="cuda")
@@ -663,7 +663,7 @@ def main():
                     help="only the mixed timed windows (for profiler captures); no JSON line")
     ap.add_argument("--case", default="eam-mixed",
                     choices=["eam-mixed", "eam-fp64", "eam-nvt-ev", "morse-batch",
-                             "morse-batch-fp64"],
+                             "morse-batch-fp64", "fit"],
                     help="workload of --kernels-only: the 131,072-atom EAM system (mixed, "
                          "FP64, or mixed NVT with energy/virial every step), or the 512 "
                          "Morse replicas")
@@ -711,7 +711,9 @@ def main():
     eam = make_eam(t)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     if args.kernels_only:
-        if args.case.startswith("morse-batch"):
+        if args.case == "fit":
+            fit_bench(torch, adam_steps=args.steps, nsnap=64, continue_morse=False)
+        elif args.case.startswith("morse-batch"):
             prec = "fp64" if args.case.endswith("fp64") else "mixed"
             batch_bench(args.steps, args.warmup, flush, torch, prec, dist, rank, world,
                         args.lanes, args.nbr_batch)

@@ -419,7 +419,117 @@ __global__ void __launch_bounds__(kThreads) k_fm_eam_adjoint(
   }
 }
 
+// Single-element alloys: the same adjoint with the r-spline gradients
+// (phi, rho) of intervals [k0, k0 + W) accumulated in shared memory by each
+// block of a persistent grid and added to the global arrays once per block
+// at the end; intervals below k0 (pairs closer than k0 * dr) go straight to
+// global memory.  Shared layout: [phi, rho][coefficient 0..3][W].
+__device__ __forceinline__ void add_r(double* gl, double* sh, int ns, int k, int k0, int W,
+                                      int coef, double v) {
+  if (k >= k0) atomicAdd(sh + coef * W + (k - k0), v);
+  else atomicAdd(gl + coef * ns + k, v);
+}
+
+template <class Geo, int LPA>
+__global__ void __launch_bounds__(kThreads) k_fm_eam_adjoint_w(
+    Geo g, NbrView nl, int n, FitEam e, double rc_sq, const double* __restrict__ rho,
+    const double* __restrict__ fp, const double* __restrict__ fpp,
+    const double* __restrict__ G, int k0, int W) {
+  using T = typename Geo::T;
+  extern __shared__ double sg[];
+  double* const sphi = sg;
+  double* const srho = sg + 4 * W;
+  for (int k = threadIdx.x; k < 8 * W; k += blockDim.x) sg[k] = 0.0;
+  __syncthreads();
+  const int ns = e.nsr;
+  const int per_block = blockDim.x / LPA;
+  const int sub = threadIdx.x % LPA;
+  for (long long first = static_cast<long long>(blockIdx.x) * per_block; first < n;
+       first += static_cast<long long>(gridDim.x) * per_block) {
+    const long long ii = first + threadIdx.x / LPA;
+    const bool active = ii < n;
+    const int i = active ? static_cast<int>(ii) : 0;
+    double w = 0.0;
+    typename Geo::Own o{};
+    int cnt = 0;
+    long long row = 0;
+    if (active) {
+      o = g.own(i);
+      row = nl.row(i);
+      cnt = nl.count(i);
+      const double gix = G[3ll * i], giy = G[3ll * i + 1], giz = G[3ll * i + 2];
+      const double fpi = fp[i];
+      for (int k = sub; k < cnt; k += LPA) {
+        const int j = __ldg(nl.nbr + row + k);
+        typename Geo::Pair pr;
+        g.pair(o, j, pr);
+        if (pr.r2 < static_cast<T>(rc_sq)) {
+          T r, rinv;
+          double rd;
+          g.radius(o, pr, r, rinv, rd);
+          double dx;
+          const int kk = spl_seg(rd, e.dr, ns, dx);
+          const double ddx = pr.dx, ddy = pr.dy, ddz = pr.dz, rr = static_cast<double>(r);
+          const double q = (gix * ddx + giy * ddy + giz * ddz) / rr;
+          const double fpj = fp[j];
+          // phi' and rho' terms: d/dc of the derivative basis (b, 2c x, 3d x^2)
+          const double wp = -q, wr = -q * (fpi + fpj);
+          add_r(e.gphi, sphi, ns, kk, k0, W, 1, wp);
+          add_r(e.gphi, sphi, ns, kk, k0, W, 2, 2.0 * wp * dx);
+          add_r(e.gphi, sphi, ns, kk, k0, W, 3, 3.0 * wp * dx * dx);
+          add_r(e.grho, srho, ns, kk, k0, W, 1, wr);
+          add_r(e.grho, srho, ns, kk, k0, W, 2, 2.0 * wr * dx);
+          add_r(e.grho, srho, ns, kk, k0, W, 3, 3.0 * wr * dx * dx);
+          const double drj = spl_deriv<double>(e.rhos(0), kk, dx);
+          const double gdiff = (gix - G[3ll * j]) * ddx + (giy - G[3ll * j + 1]) * ddy +
+                               (giz - G[3ll * j + 2]) * ddz;
+          w -= drj * gdiff / rr;
+        }
+      }
+    }
+    w = lane_sum<double, LPA>(w);
+    if (active) {
+      if (sub == 0) {
+        double dx;
+        const int kk = spl_seg(rho[i], e.drho, e.nsf, dx);
+        add_deriv_basis(e.gF, e.nsf, kk, dx, w);
+      }
+      const double wf = w * fpp[i];
+      // rho values through rho_i: w_i F''_i * drho/dc at r_ij
+      for (int k = sub; k < cnt; k += LPA) {
+        const int j = __ldg(nl.nbr + row + k);
+        typename Geo::Pair pr;
+        g.pair(o, j, pr);
+        if (pr.r2 < static_cast<T>(rc_sq)) {
+          T r, rinv;
+          double rd;
+          g.radius(o, pr, r, rinv, rd);
+          double dx;
+          const int kk = spl_seg(rd, e.dr, ns, dx);
+          add_r(e.grho, srho, ns, kk, k0, W, 0, wf);
+          add_r(e.grho, srho, ns, kk, k0, W, 1, wf * dx);
+          add_r(e.grho, srho, ns, kk, k0, W, 2, wf * dx * dx);
+          add_r(e.grho, srho, ns, kk, k0, W, 3, wf * dx * dx * dx);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < 8 * W; k += blockDim.x) {
+    const double v = sg[k];
+    if (v != 0.0) {
+      const int sp = k / (4 * W), coef = (k / W) % 4, b = k % W;
+      atomicAdd((sp == 0 ? e.gphi : e.grho) + coef * ns + k0 + b, v);
+    }
+  }
+}
+
 }  // namespace
+
+// Intervals of the r splines whose gradients a block keeps in shared memory
+// (8 doubles each: 4 coefficients of phi and of rho): 1280 x 64 B = 80 KiB,
+// two blocks per SM.
+constexpr int kAdjointWindow = 1280;
 
 class Fit {
  public:
@@ -657,10 +767,22 @@ void Fit::eam(int ntypes, int nrho, double drho, int nr, double dr, const double
       k_fm_eam_force<Geo, L><<<nblk, kThreads, 0, s>>>(g, nl, m, types_.data(), e, rc_sq_,
                                                        fp_.data(), target_.data(), c, G_.data(),
                                                        d_forces, part_.data());
-      if (grad)
+      if (grad && ntypes == 1) {
+        // one element: shared-memory window of the r-spline gradients over
+        // the top W intervals, a persistent grid of two blocks per SM
+        const int W = std::min(nr - 1, kAdjointWindow);
+        const size_t smem = sizeof(double) * 8 * static_cast<size_t>(W);
+        auto kern = k_fm_eam_adjoint_w<Geo, L>;
+        TDMD_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        const int grid = std::min(2 * sm_count(), nblk);
+        kern<<<grid, kThreads, smem, s>>>(g, nl, m, e, rc_sq_, rho_.data(), fp_.data(),
+                                          fpp_.data(), G_.data(), (nr - 1) - W, W);
+      } else if (grad) {
         k_fm_eam_adjoint<Geo, L><<<nblk, kThreads, 0, s>>>(g, nl, m, types_.data(), e, rc_sq_,
                                                            rho_.data(), fp_.data(), fpp_.data(),
                                                            G_.data());
+      }
     });
   });
   TDMD_LAUNCH_CHECK();
