@@ -107,7 +107,9 @@ class Scheduler {
   void finish_setup();
   int size_neighbor_list();  // returns the cell-list kernels launched
   void grow_capacity(int max_count);
-  void initial_forces();
+  // defer_check: leave the list build's overflow flag for the window that
+  // follows (it keeps the flag, and its retry rebuilds and recomputes)
+  void initial_forces(bool defer_check = false);
   void enqueue_rebuild();
   // kd: the force pass also applies the next step's full kick + drift
   // (mixed EAM, NVE; the force pass reads gather records, not positions).
@@ -225,6 +227,7 @@ class Scheduler {
   long long prof_n_[kProfCount] = {0, 0, 0, 0, 0};
 
   bool uploaded_ = false, initialized_ = false, tuned_ = false;
+  bool init_check_pending_ = false;  // the first list's overflow flag awaits the window
   int step_ = 0, since_rebuild_ = 0;
   long long ticks_ = 0, launches_ = 0, rebuilds_ = 0, graph_launches_ = 0, retries_ = 0;
 };

@@ -957,7 +957,7 @@ std::vector<StepPlan> Scheduler::plan_steps(int target, int* since_out) const {
   return plan;
 }
 
-void Scheduler::initial_forces() {
+void Scheduler::initial_forces(bool defer_check) {
   const bool prof = profiling_;
   profiling_ = false;  // timing covers the steps of run_until windows only
   cudaStream_t s = stream_;
@@ -977,7 +977,9 @@ void Scheduler::initial_forces() {
   TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
   build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl2, nbr_.data(), nullptr,
                       cap_, cnt_.data(), ctl_status(), s);
-  if (reuse) {
+  if (reuse && defer_check) {
+    init_check_pending_ = true;
+  } else if (reuse) {
     int st[4];
     TDMD_CU(cudaMemcpyAsync(st, ctl_status(), sizeof(st), cudaMemcpyDeviceToHost, s));
     TDMD_CU(cudaStreamSynchronize(s));
@@ -1046,7 +1048,9 @@ void Scheduler::run_until(int target) {
     step_ = std::max(step_, target);
     return;
   }
-  if (!initialized_) initial_forces();
+  // With a window to run, the first list's overflow check is left to it:
+  // no host round trip between the upload and the window.
+  if (!initialized_) initial_forces(/*defer_check=*/step_ < target);
   // lanes_per_atom = 0: measure the candidates once on the first window of
   // a system large enough for the choice to matter.
   if (!tuned_ && cfg_.lanes_per_atom == 0 && n_ >= 2048) autotune(nullptr, nullptr, nullptr);
@@ -1058,7 +1062,9 @@ void Scheduler::run_until(int target) {
   for (int attempt = 0;; ++attempt) {
     TDMD_CU(cudaEventRecord(win_ev_[0], stream_));
     snapshot();
-    TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, stream_));
+    // a pending first-list overflow flag stays set for this window's check
+    if (attempt > 0 || !init_check_pending_)
+      TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, stream_));
     int since_end = 0;
     const std::vector<StepPlan> plan = plan_steps(target, &since_end);
     // Segments start at each rebuild step; at most 64 steps each.
@@ -1082,6 +1088,7 @@ void Scheduler::run_until(int target) {
       last_window_ms_ = ms;
     }
     prof_collect();
+    init_check_pending_ = false;
     if (!st[0]) {
       step_ = target;
       since_rebuild_ = since_end;
@@ -1095,11 +1102,14 @@ void Scheduler::run_until(int target) {
     restore();
     step_ = step0;
     since_rebuild_ = since0;
-    // The restored positions need a list built into the new capacity.
+    // The restored positions need a list built into the new capacity, and
+    // their forces again (those of the snapshot came from an overflowed
+    // list when the overflow was the first list's; otherwise the same bits).
     build_cells();
     build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_,
                         (cutoff_ + cfg_.r_skin) * (cutoff_ + cfg_.r_skin), nbr_.data(), nullptr,
                         cap_, cnt_.data(), nullptr, stream_);
+    enqueue_force(false);
   }
 }
 
