@@ -419,6 +419,33 @@ def test_reupload_reuses_or_grows_rows(cuda, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_reupload_overflow_caught_by_the_window(cuda, precision):
+    """After a re-upload the first list's overflow flag is checked by the
+    window that follows rather than before it: a denser state that no longer
+    fits the rows is caught there, the window is redone with grown rows and
+    recomputed initial forces, and the trajectory equals a fresh
+    scheduler's bit for bit."""
+    s, sysm, _ = _eam_setup(precision, ncell=6, lanes_per_atom=4)
+    s.run_until(0)
+    cap0 = s.stats().nlist_capacity
+    lo = np.array(sysm.lo)
+    dense = lo + 0.75 * (sysm.positions - lo)
+    s.upload(dense, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+    s.run_until(7)
+    st = s.stats()
+    assert st.nlist_capacity > cap0 and st.nlist_retries >= 1
+    fresh, _, _ = _eam_setup(precision, ncell=6, lanes_per_atom=4)
+    fresh.upload(dense, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+    fresh.run_until(7)
+    a, b = s.download(), fresh.download()
+    assert np.array_equal(a.positions, b.positions)
+    assert np.array_equal(a.velocities, b.velocities)
+    assert np.array_equal(a.forces, b.forces)
+    fresh.close()
+    s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_arbitrary_atom_order(cuda, oracle, precision):
     """A shuffled upload (held internally in cell order) gives the oracle's
     trajectory for that order atom for atom and downloads in the caller's
