@@ -417,6 +417,45 @@ def batch_bench(steps, warmup, flush, torch, precision="mixed", dist=None, rank=
             "_slopes": slopes}
 
 
+def morse256_bench(torch, nsteps=1000):
+    """The reference's CPU-runnable case: 4^3 Cu FCC (256 atoms), Morse
+    rc 6.0, skin 0.3, 300 K, NVE dt 1 fs, nsteps steps in windows of 10 (a
+    few microseconds of work per step: launch and graph-replay latency
+    bound).  timesteps/s from the device time of the windows, and the energy
+    drift of the run from the device energy log."""
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, MorseParams, make_config
+    from tdmd_claude_b200 import workloads as W
+    sysm = W.fcc_system(4, 3.615, 300.0, 4321)
+    out = {}
+    for prec in ("mixed", "fp64"):
+        s = FastPipelineScheduler(Box.make(sysm.lo, sysm.hi), sysm.n,
+                                  MorseParams.make(*W.MORSE_CU),
+                                  make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW,
+                                              precision=prec, energy_every=WINDOW,
+                                              energy_log_capacity=nsteps // WINDOW + 1))
+        s.upload(sysm.positions, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+        s.run_until(0)
+        for w in range(3):                  # warm-up windows (graphs captured)
+            s.run_until((w + 1) * WINDOW)
+        s.upload(sysm.positions, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+        s.run_until(0)
+        ms = 0.0
+        for w in range(nsteps // WINDOW):
+            s.run_until((w + 1) * WINDOW)
+            ms += s.last_window_ms()
+        log = s.energy_log()
+        s.close()
+        t_ns = log[:, 0] * DT * 1e-3
+        e = (log[:, 1] + log[:, 2]) / sysm.n
+        out[prec] = {"timesteps_per_s": nsteps / (ms * 1e-3),
+                     "atom_steps_per_s": sysm.n * nsteps / (ms * 1e-3),
+                     "drift_ev_per_atom_per_ns": float(np.polyfit(t_ns, e, 1)[0]),
+                     "steps": nsteps}
+    out["workload"] = ("Cu FCC 4^3 cells = 256 atoms, Morse (0.3429, 1.3588, 2.866, rc 6.0), "
+                       "skin 0.3, 300 K, NVE dt 1 fs, energy log every 10 steps")
+    return out
+
+
 def ternary_bench(steps, warmup, flush, torch, total_steps=2000):
     """Equiatomic random ternary FCC alloy, 100^3 cells = 4,000,000 atoms
     (a = 3.56 A), per-species analytic EAM, mixed precision, NVT
@@ -802,6 +841,7 @@ def main():
         beam["mixed_batched_over_plain_fp64"] = beam["mixed"]["value"] / value64
         beam["mixed_over_fp64_batched"] = beam["mixed"]["value"] / beam["fp64"]["value"]
     fitfig = None if args.no_fit else fit_bench(torch)
+    small = None if args.no_batch else morse256_bench(torch)
     ternary = None if args.no_ternary else ternary_bench(max(3, args.steps // 3), 3, flush,
                                                            torch)
 
@@ -862,6 +902,7 @@ def main():
                 "batched_replicas": batch,
                 "batched_eam_131k_x8": beam,
                 "ternary_4m_nvt_adaptive": ternary,
+                "morse_256_nve_1000": small,
                 "force_matching": fitfig,
                 "wall_s_timed_region": wall_mixed,
             },
