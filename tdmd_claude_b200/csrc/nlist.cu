@@ -128,6 +128,14 @@ __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __re
 //     < rl^2.
 // Accepted candidates are compacted with ballot/popc in candidate order, so
 // every row is the reference's per-atom list, bit for bit.
+//
+// Cell pruning (staged, no FP32 re-wrap): a candidate whose FP32 r^2 to the
+// bounding box of the center cell's own records exceeds the band's upper end
+// is dropped while staging (order kept).  Rounding is monotone, so the sweep's
+// r^2 to any center atom is at least that bound: every dropped candidate is
+// one the filter would reject for every center atom, and the rows do not
+// change.  About 30 % of a 27-cell neighborhood lies farther than r_list from
+// the center cell.
 // --------------------------------------------------------------------------
 constexpr int kRowThreads = 128;
 constexpr int kStageCap = 1536;  // staged candidate records (24 KiB)
@@ -156,7 +164,16 @@ struct RowSmem {
   float4 stage[kStageCap];
   int s_start[27], s_pre[28];
   int s_max[kRowThreads / 32];
+  int s_wcnt[kRowThreads / 32];  // kept candidates per warp (staging chunk)
+  float s_bb[6];                 // center cell's bounding box: min xyz, max xyz
+  int s_c0;                      // staged index of the center cell's first atom
 };
+
+// FP32 r^2 in one fixed order of round-to-nearest ops; the filter and the
+// pruning bound both use it (the bound relies on its monotonicity).
+__device__ __forceinline__ float r2_rn(float dx, float dy, float dz) {
+  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
 
 // Rows of the atoms of cell c of box b's grid; cell_start / cell_count index
 // that grid's cells, cell_atoms and the atom indices are global.
@@ -218,41 +235,99 @@ __device__ __forceinline__ void build_cell_rows(
                        __fmul_rn(__int2float_rn(encode_q(p.z, b.qlo[2], b.qinv[2]) - oz), s2),
                        __int_as_float(j));
   };
+  const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];  // center = slot 13
+  const unsigned lt_mask = (1u << lane) - 1u;
+  int kept = total;  // staged candidates (after pruning)
   if (staged) {
-    for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = record(k);
-    for (int k = total + threadIdx.x; k < padded; k += kRowThreads)
+    if (WRAP) {
+      for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = record(k);
+    } else {
+      if (warp == 0) {
+        float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int a = lane; a < ncen; a += 32) {
+          const float4 r = record(c0 + a);
+          mn[0] = fminf(mn[0], r.x), mn[1] = fminf(mn[1], r.y), mn[2] = fminf(mn[2], r.z);
+          mx[0] = fmaxf(mx[0], r.x), mx[1] = fmaxf(mx[1], r.y), mx[2] = fmaxf(mx[2], r.z);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+          }
+        }
+        if (lane == 0) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) sm.s_bb[d] = mn[d], sm.s_bb[3 + d] = mx[d];
+        }
+      }
+      __syncthreads();
+      const float bx0 = sm.s_bb[0], by0 = sm.s_bb[1], bz0 = sm.s_bb[2];
+      const float bx1 = sm.s_bb[3], by1 = sm.s_bb[4], bz1 = sm.s_bb[5];
+      kept = 0;
+      for (int k0 = 0; k0 < total; k0 += kRowThreads) {
+        const int k = k0 + threadIdx.x;
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool keep = false;
+        if (k < total) {
+          r = record(k);
+          const float ex = fmaxf(0.f, fmaxf(__fsub_rn(bx0, r.x), __fsub_rn(r.x, bx1)));
+          const float ey = fmaxf(0.f, fmaxf(__fsub_rn(by0, r.y), __fsub_rn(r.y, by1)));
+          const float ez = fmaxf(0.f, fmaxf(__fsub_rn(bz0, r.z), __fsub_rn(r.z, bz1)));
+          keep = (k >= c0 && k < c0 + ncen) || !(r2_rn(ex, ey, ez) > hi_f);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) sm.s_wcnt[warp] = __popc(m);
+        __syncthreads();
+        int off = kept, tot = kept;
+#pragma unroll
+        for (int w = 0; w < kRowThreads / 32; ++w) {
+          const int cw = sm.s_wcnt[w];
+          off += w < warp ? cw : 0;
+          tot += cw;
+        }
+        off += __popc(m & lt_mask);
+        if (keep) stage[off] = r;
+        if (k == c0 && ncen > 0) sm.s_c0 = off;
+        kept = tot;
+        __syncthreads();
+      }
+    }
+    for (int k = kept + threadIdx.x; k < ((kept + 31) & ~31); k += kRowThreads)
       stage[k] = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
   }
   __syncthreads();
   const float Lx = static_cast<float>(b.L[0]), Ly = static_cast<float>(b.L[1]),
               Lz = static_cast<float>(b.L[2]);
   const float hx = 0.5f * Lx, hy = 0.5f * Ly, hz = 0.5f * Lz;
-  const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];  // center = slot 13
-  const unsigned lt_mask = (1u << lane) - 1u;
+  // candidates swept and the center cell's first one
+  const int ncand = kept;
+  const int cbase = (staged && !WRAP && ncen > 0) ? sm.s_c0 : c0;
   int wmax = 0;  // lane 0: this warp's longest row
   // One sweep per candidate source: staged records (the hot path) or
   // records rebuilt on the fly, so the hot loop carries no second path.
   auto sweep = [&](auto cand, auto padded_tag) {
     constexpr bool kPadded = decltype(padded_tag)::value;
     for (int a = warp; a < ncen; a += kRowThreads / 32) {
-      const float4 ci = cand(c0 + a);
+      const float4 ci = cand(cbase + a);
       const int i = __float_as_int(ci.w);
       const long long base = row_off ? static_cast<long long>(row_off[i])
                                      : static_cast<long long>(i) * cap;
       const int limit = row_off ? INT_MAX : cap;
       int cnt = 0;
-      for (int k0 = 0; k0 < total; k0 += 32) {
+      for (int k0 = 0; k0 < ncand; k0 += 32) {
         const int k = k0 + lane;
         // past the end: a sentinel (staged) or atom i itself (rebuilt records)
-        const float4 cj = cand(kPadded ? k : (k < total ? k : c0 + a));
+        const float4 cj = cand(kPadded ? k : (k < ncand ? k : cbase + a));
         const int j = __float_as_int(cj.w);
-        float dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
+        float dx = __fsub_rn(cj.x, ci.x), dy = __fsub_rn(cj.y, ci.y), dz = __fsub_rn(cj.z, ci.z);
         if (WRAP) {
           dx = min_image1(dx, Lx, hx, b.periodic[0]);
           dy = min_image1(dy, Ly, hy, b.periodic[1]);
           dz = min_image1(dz, Lz, hz, b.periodic[2]);
         }
-        const float r2f = dx * dx + dy * dy + dz * dz;
+        const float r2f = r2_rn(dx, dy, dz);
         const bool other = j != i;
         unsigned m = __ballot_sync(0xffffffffu, other && r2f < lo_f);
         // Candidates inside the filter's band go to the exact FP64 test:
