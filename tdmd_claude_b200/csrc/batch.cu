@@ -391,6 +391,7 @@ Batch::Batch(int nrep, const tdmd_box* boxes, const int* natoms, const tdmd_mors
       m.halfL[a] = d.box.halfL[a];
       m.per[a] = d.box.periodic[a];
     }
+    s.iso = d.box.qstep[0] == d.box.qstep[1] && d.box.qstep[1] == d.box.qstep[2];
     atoms += natoms[r];
     cells += d.ncells;
     TDMD_REQUIRE(atoms < INT_MAX / 2 && cells < INT_MAX / 2, "batch too large");

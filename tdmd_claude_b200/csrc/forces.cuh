@@ -145,6 +145,22 @@ struct PairQ {
 // |r| and 1/|r| in FP32 and the FP64-refined radius from a PairQ: with
 // r = sqrt(r2) in FP32, r2d - r*r = res + (r2 - r*r), the second term exact
 // by FMA; one Newton step rd = r + (r2d - r*r) / (2r).
+// FP64 residual (exact r^2 of the fixed-point deltas) - r2.  When the
+// three axes share one step (iso), the squares are summed exactly in 64-bit
+// integers (|d| <= 2^31: each square <= 2^62, the sum < 2^64) and scaled
+// once; otherwise each axis is scaled in FP64.
+__device__ __forceinline__ float q_residual(int ix, int iy, int iz, int iso, double s2x,
+                                            double s2y, double s2z, float r2) {
+  if (iso) {
+    const unsigned long long q2 = static_cast<unsigned long long>(static_cast<long long>(ix) * ix) +
+                                  static_cast<unsigned long long>(static_cast<long long>(iy) * iy) +
+                                  static_cast<unsigned long long>(static_cast<long long>(iz) * iz);
+    return static_cast<float>(fma(__ull2double_rn(q2), s2x, -static_cast<double>(r2)));
+  }
+  const double x = ix, y = iy, z = iz;
+  return static_cast<float>(x * x * s2x + y * y * s2y + z * z * s2z - static_cast<double>(r2));
+}
+
 __device__ __forceinline__ void radius_q(float r2, float res, float& r, float& rinv, double& rd) {
   rinv = rsqrtf(r2);
   r = r2 * rinv;
@@ -265,6 +281,7 @@ struct GeoQ {
   const int4* q;
   float s[3];
   double s2[3];  // (Lq/2^32)^2 per axis
+  int iso;       // one step on all three axes
   __device__ __forceinline__ Own own(int i) const { return __ldg(q + i); }
   __device__ __forceinline__ int4 record(const Own& o) const { return o; }
   __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
@@ -275,9 +292,7 @@ struct GeoQ {
     pr.dy = __fmul_rn(__int2float_rn(iy), s[1]);
     pr.dz = __fmul_rn(__int2float_rn(iz), s[2]);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
-    const double x = ix, y = iy, z = iz;
-    pr.res = static_cast<float>(x * x * s2[0] + y * y * s2[1] + z * z * s2[2] -
-                                static_cast<double>(pr.r2));
+    pr.res = q_residual(ix, iy, iz, iso, s2[0], s2[1], s2[2], pr.r2);
   }
   __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
                                          double& rd) const {
@@ -289,7 +304,8 @@ struct GeoQ {
 __host__ inline GeoQ make_geoq(const int4* q, const DevBox& b) {
   return GeoQ{q,
               {b.qscale[0], b.qscale[1], b.qscale[2]},
-              {b.qstep[0] * b.qstep[0], b.qstep[1] * b.qstep[1], b.qstep[2] * b.qstep[2]}};
+              {b.qstep[0] * b.qstep[0], b.qstep[1] * b.qstep[1], b.qstep[2] * b.qstep[2]},
+              b.qstep[0] == b.qstep[1] && b.qstep[1] == b.qstep[2]};
 }
 
 __host__ inline GeoAoS32 make_geo_aos32(const double* p, const DevBox& b) {

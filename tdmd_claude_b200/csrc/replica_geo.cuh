@@ -24,6 +24,7 @@ struct GeoQB {
     int4 q;
     float s0, s1, s2;
     double t0, t1, t2;
+    int iso;
   };
   using Pair = PairQ;
   static constexpr bool kRecords = true;
@@ -41,6 +42,7 @@ struct GeoQB {
     o.t0 = __ldg(&p->s2[0]);
     o.t1 = __ldg(&p->s2[1]);
     o.t2 = __ldg(&p->s2[2]);
+    o.iso = __ldg(&p->iso);
     return o;
   }
   __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
@@ -51,9 +53,7 @@ struct GeoQB {
     pr.dy = __fmul_rn(__int2float_rn(iy), o.s1);
     pr.dz = __fmul_rn(__int2float_rn(iz), o.s2);
     pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
-    const double x = ix, y = iy, z = iz;
-    pr.res = static_cast<float>(x * x * o.t0 + y * y * o.t1 + z * z * o.t2 -
-                                static_cast<double>(pr.r2));
+    pr.res = q_residual(ix, iy, iz, o.iso, o.t0, o.t1, o.t2, pr.r2);
   }
   __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
                                          double& rd) const {
@@ -129,6 +129,7 @@ __host__ inline RepScale rep_scale(const DevBox& b) {
     s.s[a] = b.qscale[a];
     s.s2[a] = b.qstep[a] * b.qstep[a];
   }
+  s.iso = b.qstep[0] == b.qstep[1] && b.qstep[1] == b.qstep[2];
   return s;
 }
 

@@ -21,7 +21,7 @@ struct RepDesc {
 // Per-replica fixed-point decode scales of the mixed force path.
 struct RepScale {
   float s[3];
-  float pad;
+  int iso;       // one step on all three axes
   double s2[3];  // (Lq / 2^32)^2
   double pad2;
 };
