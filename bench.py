@@ -702,10 +702,10 @@ def main():
                     help="only the mixed timed windows (for profiler captures); no JSON line")
     ap.add_argument("--case", default="eam-mixed",
                     choices=["eam-mixed", "eam-fp64", "eam-nvt-ev", "morse-batch",
-                             "morse-batch-fp64", "fit"],
+                             "morse-batch-fp64", "fit", "ternary"],
                     help="workload of --kernels-only: the 131,072-atom EAM system (mixed, "
-                         "FP64, or mixed NVT with energy/virial every step), or the 512 "
-                         "Morse replicas")
+                         "FP64, or mixed NVT with energy/virial every step), the 512 "
+                         "Morse replicas, force matching, or the 4M-atom ternary NVT run")
     ap.add_argument("--lanes", type=int, default=None,
                     help="lanes per atom for --kernels-only (EAM: default 4, no autotune; "
                          "Morse replicas: autotuned unless given)")
@@ -752,6 +752,8 @@ def main():
     if args.kernels_only:
         if args.case == "fit":
             fit_bench(torch, adam_steps=args.steps, nsnap=64, continue_morse=False)
+        elif args.case == "ternary":
+            ternary_bench(args.steps, args.warmup, flush, torch, total_steps=0)
         elif args.case.startswith("morse-batch"):
             prec = "fp64" if args.case.endswith("fp64") else "mixed"
             batch_bench(args.steps, args.warmup, flush, torch, prec, dist, rank, world,

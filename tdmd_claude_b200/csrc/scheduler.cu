@@ -271,31 +271,63 @@ enum CtlMode : int {
   kCtlLog = 8,    // append an energy-log record
 };
 
-// One block: reduce (KE, v2max) partials in block order, run the chain and
-// the adaptive-dt rule, write the pending scale / next dt, optionally log.
-__global__ void k_control(SchedCtl* __restrict__ ctl, const double* __restrict__ partials, int nblk,
-                          CtlParams p, int mode, double* __restrict__ log, int log_cap) {
+// Threads of the single-block reducers below: 1024 above 4096 records (4 M
+// atoms: 15 625), else 256 (the extra warps cost more than they hide).
+constexpr int kCtlThreads = 1024;
+inline int ctl_threads(int nblk) { return nblk > 4096 ? kCtlThreads : 256; }
+
+// Sum of partials[2b] and max of partials[2b + 1] over b < nblk, for thread
+// 0 of one block: each thread keeps four independent (sum, max) pairs so
+// four loads are in flight (a 15 625-record reduction at 4 M atoms is
+// latency-bound otherwise), then the warp tree and the warps in order.  The
+// order depends only on nblk and the block size: bit-reproducible.
+__device__ __forceinline__ void reduce_ke_v2(const double* __restrict__ partials, int nblk,
+                                             double& ke, double& v2) {
   __shared__ double red[32 * 2];
-  double ke = 0.0, v2 = 0.0;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-    ke += partials[2ll * b];
-    v2 = fmax(v2, partials[2ll * b + 1]);
+  const int nt = blockDim.x;
+  double k4[4] = {0.0, 0.0, 0.0, 0.0}, m4[4] = {0.0, 0.0, 0.0, 0.0};
+  const double2* p2 = reinterpret_cast<const double2*>(partials);
+  int b = threadIdx.x;
+  for (; b + 3 * nt < nblk; b += 4 * nt) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double2 v = p2[b + u * nt];
+      k4[u] += v.x;
+      m4[u] = fmax(m4[u], v.y);
+    }
   }
-  ke = warp_sum(ke);
-  v2 = warp_max(v2);
+  for (; b < nblk; b += nt) {
+    const double2 v = p2[b];
+    k4[0] += v.x;
+    m4[0] = fmax(m4[0], v.y);
+  }
+  ke = warp_sum((k4[0] + k4[1]) + (k4[2] + k4[3]));
+  v2 = warp_max(fmax(fmax(m4[0], m4[1]), fmax(m4[2], m4[3])));
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
     red[2 * warp] = ke;
     red[2 * warp + 1] = v2;
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
   ke = 0.0;
   v2 = 0.0;
-  for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
-    ke += red[2 * w];
-    v2 = fmax(v2, red[2 * w + 1]);
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < (nt >> 5); ++w) {
+      ke += red[2 * w];
+      v2 = fmax(v2, red[2 * w + 1]);
+    }
   }
+}
+
+// One block: reduce (KE, v2max) partials in block order, run the chain and
+// the adaptive-dt rule, write the pending scale / next dt, optionally log.
+__global__ void __launch_bounds__(kCtlThreads) k_control(SchedCtl* __restrict__ ctl,
+                                                         const double* __restrict__ partials,
+                                                         int nblk, CtlParams p, int mode,
+                                                         double* __restrict__ log, int log_cap) {
+  double ke, v2;
+  reduce_ke_v2(partials, nblk, ke, v2);
+  if (threadIdx.x != 0) return;
   auto adapt = [&](double vmax2) {
     if (!p.adaptive) return;
     const double vmax = sqrt(vmax2);
@@ -338,18 +370,13 @@ __global__ void k_control(SchedCtl* __restrict__ ctl, const double* __restrict__
 }
 
 // NVE energy-log record: KE partials at integer time + the step's EV sums.
-__global__ void k_log_nve(SchedCtl* __restrict__ ctl, const double* __restrict__ partials, int nblk,
-                          double* __restrict__ log, int log_cap) {
-  __shared__ double red[32];
-  double ke = 0.0;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) ke += partials[2ll * b];
-  ke = warp_sum(ke);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) red[warp] = ke;
-  __syncthreads();
+__global__ void __launch_bounds__(kCtlThreads) k_log_nve(SchedCtl* __restrict__ ctl,
+                                                         const double* __restrict__ partials,
+                                                         int nblk, double* __restrict__ log,
+                                                         int log_cap) {
+  double ke, v2;
+  reduce_ke_v2(partials, nblk, ke, v2);
   if (threadIdx.x != 0) return;
-  ke = 0.0;
-  for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) ke += red[w];
   const int slot = ctl->log_count % (log_cap > 0 ? log_cap : 1);
   double* r = log + 9ll * slot;
   r[0] = static_cast<double>(ctl->step);
@@ -809,8 +836,9 @@ CtlParams Scheduler::ctl_params() const {
 
 void Scheduler::enqueue_control(int mode) {
   const CtlParams p = ctl_params();
-  k_control<<<1, 256, 0, stream_>>>(ctl_.data(), ke_part_.data(), ceil_div(n_, kThreads), p, mode,
-                                    log_.data(), log_cap_);
+  const int nb = ceil_div(n_, kThreads);
+  k_control<<<1, ctl_threads(nb), 0, stream_>>>(ctl_.data(), ke_part_.data(), nb, p, mode,
+                                                log_.data(), log_cap_);
   TDMD_LAUNCH_CHECK();
   launches_ += 1;
 }
@@ -834,7 +862,8 @@ void Scheduler::enqueue_log_nve() {
     k_ke_integer<<<nb, kThreads, 0, s>>>(vel_.data(), f64_.data(), types_.data(), masses_.data(), inv_mm_.data(),
                                          n_, cfg_.dt, ke_part_.data());
   TDMD_LAUNCH_CHECK();
-  k_log_nve<<<1, 256, 0, s>>>(ctl_.data(), ke_part_.data(), nb, log_.data(), log_cap_);
+  k_log_nve<<<1, ctl_threads(nb), 0, s>>>(ctl_.data(), ke_part_.data(), nb, log_.data(),
+                                          log_cap_);
   TDMD_LAUNCH_CHECK();
   launches_ += 2;
 }
