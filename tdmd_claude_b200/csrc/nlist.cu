@@ -139,6 +139,8 @@ __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __re
 // --------------------------------------------------------------------------
 constexpr int kRowThreads = 128;
 constexpr int kStageCap = 1536;  // staged candidate records (24 KiB)
+constexpr int kSlabMax = 128;    // center atoms handled as warp slabs
+constexpr int kIdxCap = 512;     // kept candidates per warp slab
 
 // The reference's decision for one pair (NeighborList::build,
 // neighbor_list.cpp:57-63): delta = r_j - r_i in FP64, minimum image,
@@ -169,6 +171,12 @@ struct RowSmem {
   int s_c0;                      // staged index of the center cell's first atom
 };
 
+// Shared memory of the warp-slab variant (4.3 KiB more per CTA).
+struct SlabSmem {
+  short s_order[kSlabMax];                          // center atoms by x
+  unsigned short s_idx[kRowThreads / 32][kIdxCap];  // each warp's kept candidates
+};
+
 // FP32 r^2 in one fixed order of round-to-nearest ops; the filter and the
 // pruning bound both use it (the bound relies on its monotonicity).
 __device__ __forceinline__ float r2_rn(float dx, float dy, float dz) {
@@ -177,9 +185,9 @@ __device__ __forceinline__ float r2_rn(float dx, float dy, float dz) {
 
 // Rows of the atoms of cell c of box b's grid; cell_start / cell_count index
 // that grid's cells, cell_atoms and the atom indices are global.
-template <class Load, bool WRAP, bool WRITE>
+template <class Load, bool WRAP, bool WRITE, bool SLAB>
 __device__ __forceinline__ void build_cell_rows(
-    RowSmem& sm, Load pos, const DevBox& b, int c, const int* __restrict__ cell_start,
+    RowSmem& sm, SlabSmem* ss, Load pos, const DevBox& b, int c, const int* __restrict__ cell_start,
     const int* __restrict__ cell_count, const int* __restrict__ cell_atoms, double rl2,
     float lo_f, float hi_f, int* __restrict__ nbr, const int* __restrict__ row_off, int cap,
     int* __restrict__ counts, int* __restrict__ status) {
@@ -237,124 +245,199 @@ __device__ __forceinline__ void build_cell_rows(
   };
   const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];  // center = slot 13
   const unsigned lt_mask = (1u << lane) - 1u;
-  int kept = total;  // staged candidates (after pruning)
-  if (staged) {
-    if (WRAP) {
-      for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = record(k);
-    } else {
-      if (warp == 0) {
-        float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int a = lane; a < ncen; a += 32) {
-          const float4 r = record(c0 + a);
-          mn[0] = fminf(mn[0], r.x), mn[1] = fminf(mn[1], r.y), mn[2] = fminf(mn[2], r.z);
-          mx[0] = fmaxf(mx[0], r.x), mx[1] = fmaxf(mx[1], r.y), mx[2] = fmaxf(mx[2], r.z);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
-            mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
-          }
-        }
-        if (lane == 0) {
-#pragma unroll
-          for (int d = 0; d < 3; ++d) sm.s_bb[d] = mn[d], sm.s_bb[3 + d] = mx[d];
-        }
-      }
-      __syncthreads();
-      const float bx0 = sm.s_bb[0], by0 = sm.s_bb[1], bz0 = sm.s_bb[2];
-      const float bx1 = sm.s_bb[3], by1 = sm.s_bb[4], bz1 = sm.s_bb[5];
-      kept = 0;
-      for (int k0 = 0; k0 < total; k0 += kRowThreads) {
-        const int k = k0 + threadIdx.x;
-        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
-        bool keep = false;
-        if (k < total) {
-          r = record(k);
-          const float ex = fmaxf(0.f, fmaxf(__fsub_rn(bx0, r.x), __fsub_rn(r.x, bx1)));
-          const float ey = fmaxf(0.f, fmaxf(__fsub_rn(by0, r.y), __fsub_rn(r.y, by1)));
-          const float ez = fmaxf(0.f, fmaxf(__fsub_rn(bz0, r.z), __fsub_rn(r.z, bz1)));
-          keep = (k >= c0 && k < c0 + ncen) || !(r2_rn(ex, ey, ez) > hi_f);
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) sm.s_wcnt[warp] = __popc(m);
-        __syncthreads();
-        int off = kept, tot = kept;
-#pragma unroll
-        for (int w = 0; w < kRowThreads / 32; ++w) {
-          const int cw = sm.s_wcnt[w];
-          off += w < warp ? cw : 0;
-          tot += cw;
-        }
-        off += __popc(m & lt_mask);
-        if (keep) stage[off] = r;
-        if (k == c0 && ncen > 0) sm.s_c0 = off;
-        kept = tot;
-        __syncthreads();
-      }
-    }
-    for (int k = kept + threadIdx.x; k < ((kept + 31) & ~31); k += kRowThreads)
-      stage[k] = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
-  }
-  __syncthreads();
   const float Lx = static_cast<float>(b.L[0]), Ly = static_cast<float>(b.L[1]),
               Lz = static_cast<float>(b.L[2]);
   const float hx = 0.5f * Lx, hy = 0.5f * Ly, hz = 0.5f * Lz;
-  // candidates swept and the center cell's first one
-  const int ncand = kept;
-  const int cbase = (staged && !WRAP && ncen > 0) ? sm.s_c0 : c0;
   int wmax = 0;  // lane 0: this warp's longest row
-  // One sweep per candidate source: staged records (the hot path) or
-  // records rebuilt on the fly, so the hot loop carries no second path.
-  auto sweep = [&](auto cand, auto padded_tag) {
+  // The row of one center atom (record ci, candidate index self_k) over
+  // candidates cand(0 .. nloop): padded sources carry sentinels up to whole
+  // sweeps; otherwise lanes past the end read atom i itself (j == i,
+  // rejected).
+  auto row = [&](const float4 ci, int self_k, auto cand, int nloop, auto padded_tag) {
     constexpr bool kPadded = decltype(padded_tag)::value;
-    for (int a = warp; a < ncen; a += kRowThreads / 32) {
-      const float4 ci = cand(cbase + a);
-      const int i = __float_as_int(ci.w);
-      const long long base = row_off ? static_cast<long long>(row_off[i])
-                                     : static_cast<long long>(i) * cap;
-      const int limit = row_off ? INT_MAX : cap;
-      int cnt = 0;
-      for (int k0 = 0; k0 < ncand; k0 += 32) {
-        const int k = k0 + lane;
-        // past the end: a sentinel (staged) or atom i itself (rebuilt records)
-        const float4 cj = cand(kPadded ? k : (k < ncand ? k : cbase + a));
-        const int j = __float_as_int(cj.w);
-        float dx = __fsub_rn(cj.x, ci.x), dy = __fsub_rn(cj.y, ci.y), dz = __fsub_rn(cj.z, ci.z);
-        if (WRAP) {
-          dx = min_image1(dx, Lx, hx, b.periodic[0]);
-          dy = min_image1(dy, Ly, hy, b.periodic[1]);
-          dz = min_image1(dz, Lz, hz, b.periodic[2]);
-        }
-        const float r2f = r2_rn(dx, dy, dz);
-        const bool other = j != i;
-        unsigned m = __ballot_sync(0xffffffffu, other && r2f < lo_f);
-        // Candidates inside the filter's band go to the exact FP64 test:
-        // rare, so the warp enters that path only when some lane needs it.
-        const bool band = other && r2f >= lo_f && r2f <= hi_f;
-        if (__any_sync(0xffffffffu, band)) {
-          const bool ok = band && exact_within(pos, i, j, rl2, b.L[0], b.L[1], b.L[2],
-                                               b.halfL[0], b.halfL[1], b.halfL[2],
-                                               b.periodic[0], b.periodic[1], b.periodic[2]);
-          m |= __ballot_sync(0xffffffffu, ok);
-        }
-        if (WRITE && ((m >> lane) & 1u)) {
-          const int p = cnt + __popc(m & lt_mask);
-          if (p < limit) nbr[base + p] = j;
-        }
-        cnt += __popc(m);
+    const int i = __float_as_int(ci.w);
+    const long long base = row_off ? static_cast<long long>(row_off[i])
+                                   : static_cast<long long>(i) * cap;
+    const int limit = row_off ? INT_MAX : cap;
+    int cnt = 0;
+    for (int k0 = 0; k0 < nloop; k0 += 32) {
+      const int k = k0 + lane;
+      const float4 cj = cand(kPadded ? k : (k < nloop ? k : self_k));
+      const int j = __float_as_int(cj.w);
+      float dx = __fsub_rn(cj.x, ci.x), dy = __fsub_rn(cj.y, ci.y), dz = __fsub_rn(cj.z, ci.z);
+      if (WRAP) {
+        dx = min_image1(dx, Lx, hx, b.periodic[0]);
+        dy = min_image1(dy, Ly, hy, b.periodic[1]);
+        dz = min_image1(dz, Lz, hz, b.periodic[2]);
       }
-      if (lane == 0) {
-        counts[i] = cnt;
-        wmax = cnt > wmax ? cnt : wmax;
+      const float r2f = r2_rn(dx, dy, dz);
+      const bool other = j != i;
+      unsigned m = __ballot_sync(0xffffffffu, other && r2f < lo_f);
+      // Candidates inside the filter's band go to the exact FP64 test:
+      // rare, so the warp enters that path only when some lane needs it.
+      const bool band = other && r2f >= lo_f && r2f <= hi_f;
+      if (__any_sync(0xffffffffu, band)) {
+        const bool ok = band && exact_within(pos, i, j, rl2, b.L[0], b.L[1], b.L[2],
+                                             b.halfL[0], b.halfL[1], b.halfL[2],
+                                             b.periodic[0], b.periodic[1], b.periodic[2]);
+        m |= __ballot_sync(0xffffffffu, ok);
       }
+      if (WRITE && ((m >> lane) & 1u)) {
+        const int p = cnt + __popc(m & lt_mask);
+        if (p < limit) nbr[base + p] = j;
+      }
+      cnt += __popc(m);
+    }
+    if (lane == 0) {
+      counts[i] = cnt;
+      wmax = cnt > wmax ? cnt : wmax;
     }
   };
-  if (staged)
-    sweep([&](int k) { return stage[k]; }, std::true_type{});
-  else
-    sweep(record, std::false_type{});
+  const float4 sentinel = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
+  if (SLAB && !WRAP && total < kStageCap && ncen <= kSlabMax) {
+    // Warp slabs: all candidates staged once (one sentinel after them); the
+    // center atoms ranked by x and cut into one contiguous slab per warp;
+    // each warp keeps, in candidate order, the candidates within the band
+    // of its slab's bounding box (an index list), and sweeps only those.
+    for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = record(k);
+    if (threadIdx.x == 0) stage[total] = sentinel;
+    __syncthreads();
+    for (int t = threadIdx.x; t < ncen; t += kRowThreads) {
+      const float xt = stage[c0 + t].x;
+      int rank = 0;
+      for (int u = 0; u < ncen; ++u) {
+        const float xu = stage[c0 + u].x;
+        rank += (xu < xt || (xu == xt && u < t)) ? 1 : 0;
+      }
+      ss->s_order[rank] = static_cast<short>(t);
+    }
+    __syncthreads();
+    constexpr int kWarps = kRowThreads / 32;
+    const int rlo = warp * ncen / kWarps, rhi = (warp + 1) * ncen / kWarps;
+    if (rlo < rhi) {
+      float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (int r = rlo + lane; r < rhi; r += 32) {
+        const float4 q = stage[c0 + ss->s_order[r]];
+        mn[0] = fminf(mn[0], q.x), mn[1] = fminf(mn[1], q.y), mn[2] = fminf(mn[2], q.z);
+        mx[0] = fmaxf(mx[0], q.x), mx[1] = fmaxf(mx[1], q.y), mx[2] = fmaxf(mx[2], q.z);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+          mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+      }
+      unsigned short* const idx = ss->s_idx[warp];
+      int cnt = 0;
+      for (int k0 = 0; k0 < total; k0 += 32) {
+        const int k = k0 + lane;
+        bool keep = false;
+        if (k < total) {
+          const float4 q = stage[k];
+          const float ex = fmaxf(0.f, fmaxf(__fsub_rn(mn[0], q.x), __fsub_rn(q.x, mx[0])));
+          const float ey = fmaxf(0.f, fmaxf(__fsub_rn(mn[1], q.y), __fsub_rn(q.y, mx[1])));
+          const float ez = fmaxf(0.f, fmaxf(__fsub_rn(mn[2], q.z), __fsub_rn(q.z, mx[2])));
+          keep = !(r2_rn(ex, ey, ez) > hi_f);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        const int p = cnt + __popc(m & lt_mask);
+        if (keep && p < kIdxCap) idx[p] = static_cast<unsigned short>(k);
+        cnt += __popc(m);
+      }
+      const int npad = (cnt + 31) & ~31;
+      const bool fits = npad <= kIdxCap;
+      if (fits)
+        for (int p = cnt + lane; p < npad; p += 32) idx[p] = static_cast<unsigned short>(total);
+      __syncwarp();
+      if (fits) {
+        for (int r = rlo; r < rhi; ++r) {
+          const int self = c0 + ss->s_order[r];
+          row(stage[self], self, [&](int k) { return stage[idx[k]]; }, cnt, std::true_type{});
+        }
+      } else {  // more kept candidates than the index list holds: all of them
+        for (int r = rlo; r < rhi; ++r) {
+          const int self = c0 + ss->s_order[r];
+          row(stage[self], self, [&](int k) { return stage[k]; }, total, std::false_type{});
+        }
+      }
+    }
+  } else {
+    int kept = total;  // staged candidates (after pruning)
+    if (staged) {
+      if (WRAP) {
+        for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = record(k);
+      } else {
+        if (warp == 0) {
+          float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+          for (int a = lane; a < ncen; a += 32) {
+            const float4 r = record(c0 + a);
+            mn[0] = fminf(mn[0], r.x), mn[1] = fminf(mn[1], r.y), mn[2] = fminf(mn[2], r.z);
+            mx[0] = fmaxf(mx[0], r.x), mx[1] = fmaxf(mx[1], r.y), mx[2] = fmaxf(mx[2], r.z);
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+              mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+            }
+          }
+          if (lane == 0) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) sm.s_bb[d] = mn[d], sm.s_bb[3 + d] = mx[d];
+          }
+        }
+        __syncthreads();
+        const float bx0 = sm.s_bb[0], by0 = sm.s_bb[1], bz0 = sm.s_bb[2];
+        const float bx1 = sm.s_bb[3], by1 = sm.s_bb[4], bz1 = sm.s_bb[5];
+        kept = 0;
+        for (int k0 = 0; k0 < total; k0 += kRowThreads) {
+          const int k = k0 + threadIdx.x;
+          float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+          bool keep = false;
+          if (k < total) {
+            r = record(k);
+            const float ex = fmaxf(0.f, fmaxf(__fsub_rn(bx0, r.x), __fsub_rn(r.x, bx1)));
+            const float ey = fmaxf(0.f, fmaxf(__fsub_rn(by0, r.y), __fsub_rn(r.y, by1)));
+            const float ez = fmaxf(0.f, fmaxf(__fsub_rn(bz0, r.z), __fsub_rn(r.z, bz1)));
+            keep = (k >= c0 && k < c0 + ncen) || !(r2_rn(ex, ey, ez) > hi_f);
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, keep);
+          if (lane == 0) sm.s_wcnt[warp] = __popc(m);
+          __syncthreads();
+          int off = kept, tot = kept;
+#pragma unroll
+          for (int w = 0; w < kRowThreads / 32; ++w) {
+            const int cw = sm.s_wcnt[w];
+            off += w < warp ? cw : 0;
+            tot += cw;
+          }
+          off += __popc(m & lt_mask);
+          if (keep) stage[off] = r;
+          if (k == c0 && ncen > 0) sm.s_c0 = off;
+          kept = tot;
+          __syncthreads();
+        }
+      }
+      for (int k = kept + threadIdx.x; k < ((kept + 31) & ~31); k += kRowThreads)
+        stage[k] = sentinel;
+    }
+    __syncthreads();
+    // candidates swept and the center cell's first one
+    const int ncand = kept;
+    const int cbase = (staged && !WRAP && ncen > 0) ? sm.s_c0 : c0;
+    // staged records (the hot path) or records rebuilt on the fly
+    if (staged) {
+      for (int a = warp; a < ncen; a += kRowThreads / 32)
+        row(stage[cbase + a], cbase + a, [&](int k) { return stage[k]; }, ncand,
+            std::true_type{});
+    } else {
+      for (int a = warp; a < ncen; a += kRowThreads / 32)
+        row(record(cbase + a), cbase + a, record, ncand, std::false_type{});
+    }
+  }
   // Status: one atomic per CTA, and only when something needs reporting --
   // the maximum for a sizing (count-only) pass, the overflow flag when a
   // padded row is too short.
@@ -379,8 +462,9 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
     const int* __restrict__ row_off, int cap, int* __restrict__ counts,
     int* __restrict__ status) {
   __shared__ RowSmem sm;
-  build_cell_rows<Load, WRAP, WRITE>(sm, pos, b, blockIdx.x, cell_start, cell_count, cell_atoms,
-                                     rl2, lo_f, hi_f, nbr, row_off, cap, counts, status);
+  build_cell_rows<Load, WRAP, WRITE, false>(sm, nullptr, pos, b, blockIdx.x, cell_start,
+                                            cell_count, cell_atoms, rl2, lo_f, hi_f, nbr,
+                                            row_off, cap, counts, status);
 }
 
 // Batched replicas: one CTA per cell of any replica (cells of replica r are
@@ -393,18 +477,21 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells_batch(
     const int* __restrict__ cell_atoms, double rl2, int* __restrict__ nbr, int cap,
     int* __restrict__ counts, int* __restrict__ status) {
   __shared__ RowSmem sm;
+  __shared__ SlabSmem ss;
   __shared__ RepDesc d;
   const int gc = blockIdx.x;
   if (threadIdx.x == 0) d = reps[__ldg(cell_rep + gc)];
   __syncthreads();
   if (d.wrap)
-    build_cell_rows<LoadD4, true, WRITE>(sm, pos, d.box, gc - d.cell0, cell_start + d.cell0,
-                                  cell_count + d.cell0, cell_atoms, rl2, d.lo_f, d.hi_f, nbr,
-                                  nullptr, cap, counts, status);
+    build_cell_rows<LoadD4, true, WRITE, true>(sm, &ss, pos, d.box, gc - d.cell0,
+                                               cell_start + d.cell0, cell_count + d.cell0,
+                                               cell_atoms, rl2, d.lo_f, d.hi_f, nbr, nullptr,
+                                               cap, counts, status);
   else
-    build_cell_rows<LoadD4, false, WRITE>(sm, pos, d.box, gc - d.cell0, cell_start + d.cell0,
-                                   cell_count + d.cell0, cell_atoms, rl2, d.lo_f, d.hi_f, nbr,
-                                   nullptr, cap, counts, status);
+    build_cell_rows<LoadD4, false, WRITE, true>(sm, &ss, pos, d.box, gc - d.cell0,
+                                                cell_start + d.cell0, cell_count + d.cell0,
+                                                cell_atoms, rl2, d.lo_f, d.hi_f, nbr, nullptr,
+                                                cap, counts, status);
 }
 
 // Batched binning: the replica of atom i is rep[i]; its cell is the
