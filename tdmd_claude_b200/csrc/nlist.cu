@@ -163,7 +163,6 @@ __device__ __noinline__ bool exact_within(Load pos, int i, int j, double rl2, do
 
 // Shared memory of one row-building CTA.
 struct RowSmem {
-  float4 stage[kStageCap];
   int s_start[27], s_pre[28];
   int s_max[kRowThreads / 32];
   int s_wcnt[kRowThreads / 32];  // kept candidates per warp (staging chunk)
@@ -187,11 +186,11 @@ __device__ __forceinline__ float r2_rn(float dx, float dy, float dz) {
 // that grid's cells, cell_atoms and the atom indices are global.
 template <class Load, bool WRAP, bool WRITE, bool SLAB>
 __device__ __forceinline__ void build_cell_rows(
-    RowSmem& sm, SlabSmem* ss, Load pos, const DevBox& b, int c, const int* __restrict__ cell_start,
+    RowSmem& sm, float4* stage, int stage_cap, SlabSmem* ss, Load pos, const DevBox& b, int c,
+    const int* __restrict__ cell_start,
     const int* __restrict__ cell_count, const int* __restrict__ cell_atoms, double rl2,
     float lo_f, float hi_f, int* __restrict__ nbr, const int* __restrict__ row_off, int cap,
     int* __restrict__ counts, int* __restrict__ status) {
-  float4* const stage = sm.stage;
   int* const s_start = sm.s_start;
   int* const s_pre = sm.s_pre;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -223,7 +222,7 @@ __device__ __forceinline__ void build_cell_rows(
   // far outside any box (their r^2 overflows to +inf and fails both the
   // filter and the band), so the staged sweep needs no bounds select.
   const int padded = (total + 31) & ~31;
-  const bool staged = padded <= kStageCap;
+  const bool staged = padded <= stage_cap;
   // Fixed-point lower corner of the center cell.
   const int ox = encode_q(b.lo[0] + ix * b.cs[0], b.qlo[0], b.qinv[0]);
   const int oy = encode_q(b.lo[1] + iy * b.cs[1], b.qlo[1], b.qinv[1]);
@@ -294,7 +293,7 @@ __device__ __forceinline__ void build_cell_rows(
     }
   };
   const float4 sentinel = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
-  if (SLAB && !WRAP && total < kStageCap && ncen <= kSlabMax) {
+  if (SLAB && !WRAP && total < stage_cap && ncen <= kSlabMax) {
     // Warp slabs: all candidates staged once (one sentinel after them); the
     // center atoms ranked by x and cut into one contiguous slab per warp;
     // each warp keeps, in candidate order, the candidates within the band
@@ -460,11 +459,14 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
     Load pos, DevBox b, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const int* __restrict__ cell_atoms, double rl2, float lo_f, float hi_f, int* __restrict__ nbr,
     const int* __restrict__ row_off, int cap, int* __restrict__ counts,
-    int* __restrict__ status) {
+    int* __restrict__ status, int stage_cap) {
+  // The stage is dynamic shared memory of stage_cap records (sized by the
+  // launch from the mean cell occupancy, so that more CTAs fit on an SM).
+  extern __shared__ float4 stage[];
   __shared__ RowSmem sm;
-  build_cell_rows<Load, WRAP, WRITE, false>(sm, nullptr, pos, b, blockIdx.x, cell_start,
-                                            cell_count, cell_atoms, rl2, lo_f, hi_f, nbr,
-                                            row_off, cap, counts, status);
+  build_cell_rows<Load, WRAP, WRITE, false>(sm, stage, stage_cap, nullptr, pos, b, blockIdx.x,
+                                            cell_start, cell_count, cell_atoms, rl2, lo_f, hi_f,
+                                            nbr, row_off, cap, counts, status);
 }
 
 // Batched replicas: one CTA per cell of any replica (cells of replica r are
@@ -476,6 +478,7 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells_batch(
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const int* __restrict__ cell_atoms, double rl2, int* __restrict__ nbr, int cap,
     int* __restrict__ counts, int* __restrict__ status) {
+  __shared__ float4 stage[kStageCap];
   __shared__ RowSmem sm;
   __shared__ SlabSmem ss;
   __shared__ RepDesc d;
@@ -483,12 +486,13 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells_batch(
   if (threadIdx.x == 0) d = reps[__ldg(cell_rep + gc)];
   __syncthreads();
   if (d.wrap)
-    build_cell_rows<LoadD4, true, WRITE, true>(sm, &ss, pos, d.box, gc - d.cell0,
+    build_cell_rows<LoadD4, true, WRITE, true>(sm, stage, kStageCap, &ss, pos, d.box, gc - d.cell0,
                                                cell_start + d.cell0, cell_count + d.cell0,
                                                cell_atoms, rl2, d.lo_f, d.hi_f, nbr, nullptr,
                                                cap, counts, status);
   else
-    build_cell_rows<LoadD4, false, WRITE, true>(sm, &ss, pos, d.box, gc - d.cell0,
+    build_cell_rows<LoadD4, false, WRITE, true>(sm, stage, kStageCap, &ss, pos, d.box,
+                                                gc - d.cell0,
                                                 cell_start + d.cell0, cell_count + d.cell0,
                                                 cell_atoms, rl2, d.lo_f, d.hi_f, nbr, nullptr,
                                                 cap, counts, status);
@@ -615,6 +619,15 @@ void build_neighbor_rows_batch(const CellListDev& cl, const double4* pos, const 
   TDMD_LAUNCH_CHECK();
 }
 
+// Staged records per row-building CTA: twice the mean 27-cell neighborhood,
+// 768 to 1536 records (12 to 24 KiB); denser cells build their rows from
+// records made on the fly.
+static int stage_capacity(long long n, int ncells) {
+  const double mean = ncells > 0 ? static_cast<double>(n) / ncells : 0.0;
+  const int want = (static_cast<int>(std::ceil(54.0 * mean)) + 31) & ~31;
+  return std::min(kStageCap, std::max(768, want));
+}
+
 void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout layout,
                          long long n, const DevBox& box, double r_list_sq, int* nbr,
                          const int* row_off, int cap, int* counts, int* status,
@@ -623,16 +636,18 @@ void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout lay
   float lo_f = 0.f, hi_f = 0.f;
   int wrap = 0;
   row_filter_band(box, r_list_sq, &lo_f, &hi_f, &wrap);
+  const int scap = stage_capacity(n, cl.ncells);
+  const size_t smem = sizeof(float4) * static_cast<size_t>(scap);
   auto go = [&](auto load, auto wrap_tag) {
     constexpr bool W = decltype(wrap_tag)::value;
     if (nbr)
-      k_build_cells<decltype(load), W, true><<<cl.ncells, kRowThreads, 0, stream>>>(
+      k_build_cells<decltype(load), W, true><<<cl.ncells, kRowThreads, smem, stream>>>(
           load, box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
-          lo_f, hi_f, nbr, row_off, cap, counts, status);
+          lo_f, hi_f, nbr, row_off, cap, counts, status, scap);
     else
-      k_build_cells<decltype(load), W, false><<<cl.ncells, kRowThreads, 0, stream>>>(
+      k_build_cells<decltype(load), W, false><<<cl.ncells, kRowThreads, smem, stream>>>(
           load, box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
-          lo_f, hi_f, nullptr, row_off, cap, counts, status);
+          lo_f, hi_f, nullptr, row_off, cap, counts, status, scap);
   };
   if (layout == PosLayout::AoS3) {
     const LoadAoS3 ld{static_cast<const double*>(d_pos)};
