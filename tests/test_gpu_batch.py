@@ -75,6 +75,33 @@ def test_batch_replicas_equal_single_schedulers(cuda, precision):
     assert st.ticks == 25 and st.rebuilds == 3 and st.graph_launches > 0
 
 
+def test_batch_dense_replica_equals_single_scheduler(cuda):
+    """A replica at twice the FCC density (a = 2.87 A, 2 916 atoms, 4 cells
+    per axis, ~45 atoms per cell): its list build keeps more candidates per
+    warp slab than the slab's index list holds and sweeps all staged
+    candidates instead; forces and two steps stay bit-identical to a single
+    scheduler's (whose list build takes the cell-pruned path)."""
+    from tdmd_claude_b200 import workloads as W
+    systems = [W.fcc_system(9, 2.87, 300.0, 61), W.fcc_system(5, 3.615, 300.0, 62)]
+    for precision in ("fp64", "mixed"):
+        b = _batch(systems, precision)
+        b.run_until(0)
+        _, _, f0 = b.download()
+        b.run_until(2)
+        pos, vel, frc = b.download()
+        for r, s in enumerate(systems):
+            sc = _single(s, precision)
+            sc.run_until(0)
+            assert np.array_equal(b.replica(f0, r), sc.download().forces), (precision, r)
+            sc.run_until(2)
+            st = sc.download()
+            assert np.array_equal(b.replica(pos, r), st.positions), (precision, r)
+            assert np.array_equal(b.replica(vel, r), st.velocities), (precision, r)
+            assert np.array_equal(b.replica(frc, r), st.forces), (precision, r)
+            sc.close()
+        b.close()
+
+
 def test_batch_graphs_equal_direct_launches(cuda):
     systems = _systems(SPECS[:3], seed=40)
     a = _batch(systems, "mixed", use_graphs=True)

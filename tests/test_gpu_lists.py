@@ -36,9 +36,15 @@ def _cases():
     # a box that is not cubic and has a 3-cell axis
     q = rng.uniform(0, 1, size=(900, 3)) * [16.0, 30.0, 41.0] + [-3.0, 2.0, 5.0]
     yield "orthorhombic", q, (-3.0, 2.0, 5.0), (13.0, 32.0, 46.0), 5.0, 0.5
+    # a dense blob in a dilute gas: the mean occupancy sizes the shared-memory
+    # stage for ~100 candidates, the blob's cells have ~1000, so their rows
+    # come from records made on the fly
+    blob = rng.uniform(23.0, 37.0, size=(1000, 3))
+    gas = rng.uniform(0.0, 60.0, size=(300, 3))
+    yield "dense_blob", np.concatenate([blob, gas]), (0, 0, 0), (60, 60, 60), 5.0, 0.3
 
 
-@pytest.mark.parametrize("case", list(range(5)))
+@pytest.mark.parametrize("case", list(range(6)))
 def test_cell_list_bit_exact(cuda, oracle, case):
     from tdmd_claude_b200 import DeviceCellList
     name, pos, lo, hi, rc, skin = list(_cases())[case]
@@ -54,7 +60,7 @@ def test_cell_list_bit_exact(cuda, oracle, case):
     assert np.array_equal(acell, eac), name
 
 
-@pytest.mark.parametrize("case", list(range(5)))
+@pytest.mark.parametrize("case", list(range(6)))
 def test_full_neighbor_list_bit_exact(cuda, oracle, case):
     from tdmd_claude_b200 import DeviceNeighborList
     name, pos, lo, hi, rc, skin = list(_cases())[case]
