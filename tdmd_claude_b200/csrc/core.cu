@@ -138,6 +138,32 @@ __global__ void k_scan_single(const int* __restrict__ in, int* __restrict__ out,
   if (threadIdx.x == 0 && total_out) *total_out = carry;
 }
 
+// One-pass single-block scan of up to kScanThreads * kScanWide items: each
+// thread holds kScanWide consecutive items (all loads issued at once), one
+// block scan.  out may alias in.
+constexpr int kScanWide = 16;
+__global__ void __launch_bounds__(kScanThreads) k_scan_wide(const int* __restrict__ in,
+                                                            int* __restrict__ out, int n,
+                                                            int* __restrict__ total_out) {
+  __shared__ int smem[32];
+  const int b0 = threadIdx.x * kScanWide;
+  int v[kScanWide];
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanWide; ++k) {
+    v[k] = b0 + k < n ? in[b0 + k] : 0;
+    s += v[k];
+  }
+  int total;
+  int pre = block_exclusive_scan(s, smem, &total);
+#pragma unroll
+  for (int k = 0; k < kScanWide; ++k) {
+    if (b0 + k < n) out[b0 + k] = pre;
+    pre += v[k];
+  }
+  if (threadIdx.x == 0 && total_out) *total_out = total;
+}
+
 __global__ void k_scan_apply(const int* __restrict__ in, int* __restrict__ out, long long n,
                              const int* __restrict__ block_prefix) {
   __shared__ int smem[32];
@@ -174,6 +200,11 @@ void device_exclusive_scan(const int* in, int* out, long long n, int* total, Dev
     return;
   }
   const long long nblocks = (n + kScanTile - 1) / kScanTile;
+  if (n <= static_cast<long long>(kScanThreads) * kScanWide) {
+    k_scan_wide<<<1, kScanThreads, 0, stream>>>(in, out, static_cast<int>(n), total);
+    TDMD_LAUNCH_CHECK();
+    return;
+  }
   // Up to kScanSingleTiles tiles one block walking the tiles beats three
   // launches; beyond that, reduce -> scan of block sums -> apply.
   if (nblocks <= kScanSingleTiles) {
