@@ -72,10 +72,12 @@ __global__ void k_scatter_atoms(const int* __restrict__ atom_cell, int n,
 }
 
 // Restores ID-ascending order inside each cell: one warp per cell, rank
-// sort through shuffles for cells of up to 32 atoms (a lane's rank is the
-// number of smaller ids), lane-0 insertion sort beyond that.  key (nullable)
-// gives each array index its ID when the arrays are held in another order
-// than the caller's (the scheduler's cell-ordered layout); keys are unique.
+// sort through shuffles for cells of up to 32 * kSortPerLane atoms (lane l
+// holds entries l, l + 32, ...; an entry's rank is the number of smaller
+// ids), lane-0 insertion sort beyond that.  key (nullable) gives each array
+// index its ID when the arrays are held in another order than the caller's
+// (the scheduler's cell-ordered layout); keys are unique.
+constexpr int kSortPerLane = 4;
 __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __restrict__ cell_count,
                              int ncells, int* __restrict__ cell_atoms,
                              const int* __restrict__ key) {
@@ -92,6 +94,31 @@ __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __re
 #pragma unroll
     for (int k = 0; k < 32; ++k) rank += __shfl_sync(0xffffffffu, kv, k) < kv ? 1 : 0;
     if (lane < m) a[rank] = v;
+    return;
+  }
+  if (m <= 32 * kSortPerLane) {
+    int v[kSortPerLane], kv[kSortPerLane], rank[kSortPerLane];
+#pragma unroll
+    for (int r = 0; r < kSortPerLane; ++r) {
+      const int e = lane + 32 * r;
+      v[r] = e < m ? a[e] : INT_MAX;
+      kv[r] = e < m ? (key ? __ldg(key + v[r]) : v[r]) : INT_MAX;
+      rank[r] = 0;
+    }
+    // every read is in registers before the first write: the shuffles
+    // below synchronise the warp
+#pragma unroll
+    for (int q = 0; q < kSortPerLane; ++q) {
+      if (32 * q >= m) break;  // uniform
+      for (int k = 0; k < 32; ++k) {
+        const int o = __shfl_sync(0xffffffffu, kv[q], k);
+#pragma unroll
+        for (int r = 0; r < kSortPerLane; ++r) rank[r] += o < kv[r] ? 1 : 0;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kSortPerLane; ++r)
+      if (lane + 32 * r < m) a[rank[r]] = v[r];
     return;
   }
   if (lane == 0) {
