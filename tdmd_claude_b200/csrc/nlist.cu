@@ -17,9 +17,12 @@
 //    with an FP32 filter and fall back to the reference's exact FP64
 //    expression (round-to-nearest ops, no FMA contraction) only within 1e-5
 //    of r_list^2, so the lists match the CPU reference bit for bit; a
-//    ballot/popc compaction writes accepted neighbors in stencil order.  One
-//    pass: rows are padded to a fixed capacity and an overflow flag replaces
-//    the reference's count pass + 8-byte D2H sync.
+//    ballot/popc compaction writes accepted neighbors in stencil order.
+//    Candidates that cannot be within r_list of any center atom (FP32 r^2 to
+//    the center atoms' bounding box above the band) are dropped while
+//    staging, in order; the replica kernel keeps one such list per warp
+//    slab of center atoms.  One pass: rows are padded to a fixed capacity and
+//    an overflow flag replaces the reference's count pass + 8-byte D2H sync.
 #include <algorithm>
 #include <climits>
 #include <cmath>
