@@ -95,9 +95,14 @@ void build_cell_list(CellListDev& cl, const void* d_pos, PosLayout layout, long 
 //   row_off != nullptr: dense CSR rows at nbr[row_off[i] + k].
 //   nbr == nullptr:     count only.
 // counts[i] always gets the full count; status[1] = max count (atomicMax).
+// max_cell: the largest cell occupancy seen (sizes the shared-memory stage;
+// <= 0 = unknown, the full stage).
 void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout layout,
                          long long n, const DevBox& box, double r_list_sq, int* nbr,
                          const int* row_off, int cap, int* counts, int* status,
-                         cudaStream_t stream);
+                         cudaStream_t stream, int max_cell = 0);
+
+// *d_out = the largest cell occupancy of a built cell list (one launch).
+void cell_count_max(const CellListDev& cl, int* d_out, cudaStream_t stream);
 
 }  // namespace tdmd_b200

@@ -649,24 +649,47 @@ void build_neighbor_rows_batch(const CellListDev& cl, const double4* pos, const 
   TDMD_LAUNCH_CHECK();
 }
 
-// Staged records per row-building CTA: twice the mean 27-cell neighborhood,
-// 768 to 1536 records (12 to 24 KiB); denser cells build their rows from
-// records made on the fly.
-static int stage_capacity(long long n, int ncells) {
-  const double mean = ncells > 0 ? static_cast<double>(n) / ncells : 0.0;
-  const int want = (static_cast<int>(std::ceil(54.0 * mean)) + 31) & ~31;
+// Staged records per row-building CTA from the largest cell occupancy seen
+// (27 cells of it, plus a quarter for atoms that move in later): 768 to 1536
+// records (12 to 24 KiB); unknown (<= 0): 1536.  Cells with more candidates
+// build their rows from records made on the fly.
+static int stage_capacity(int max_cell) {
+  if (max_cell <= 0) return kStageCap;
+  const int want = (static_cast<int>(std::ceil(27.0 * 1.25 * max_cell)) + 31) & ~31;
   return std::min(kStageCap, std::max(768, want));
+}
+
+namespace {
+// Largest cell occupancy, one block.
+__global__ void k_max_count(const int* __restrict__ count, int ncells, int* __restrict__ out) {
+  __shared__ int red[32];
+  int m = 0;
+  for (int c = threadIdx.x; c < ncells; c += blockDim.x) m = max(m, count[c]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = max(m, red[w]);
+    *out = m;
+  }
+}
+}  // namespace
+
+void cell_count_max(const CellListDev& cl, int* d_out, cudaStream_t stream) {
+  k_max_count<<<1, 1024, 0, stream>>>(cl.cell_count.data(), cl.ncells, d_out);
+  TDMD_LAUNCH_CHECK();
 }
 
 void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout layout,
                          long long n, const DevBox& box, double r_list_sq, int* nbr,
                          const int* row_off, int cap, int* counts, int* status,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, int max_cell) {
   if (n == 0) return;
   float lo_f = 0.f, hi_f = 0.f;
   int wrap = 0;
   row_filter_band(box, r_list_sq, &lo_f, &hi_f, &wrap);
-  const int scap = stage_capacity(n, cl.ncells);
+  const int scap = stage_capacity(max_cell);
   const size_t smem = sizeof(float4) * static_cast<size_t>(scap);
   auto go = [&](auto load, auto wrap_tag) {
     constexpr bool W = decltype(wrap_tag)::value;

@@ -193,6 +193,12 @@ class Scheduler {
   // in the same order as without the reordering.
   DevArray<int> order_;
   int n_types_ = 0;
+  // Largest cell occupancy of the upload (sizes the list build's stage):
+  // written by the device into pinned host memory, read after the upload's
+  // stream synchronisation.
+  DevArray<int> cellmax_;
+  int* h_cellmax_ = nullptr;
+  int max_cell_ = 0;
 
   // Neighbor list: padded rows of cap_ entries.
   CellListDev cl_;

@@ -416,6 +416,7 @@ Scheduler::Scheduler(const tdmd_box& box, int natoms, const tdmd_fast_pipeline_c
 
 Scheduler::~Scheduler() {
   clear_graphs();
+  if (h_cellmax_) cudaFreeHost(h_cellmax_);
   for (auto& pe : prof_pending_) {
     cudaEventDestroy(pe.second.first);
     cudaEventDestroy(pe.second.second);
@@ -543,6 +544,7 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
   if (kind_ == TDMD_POT_EAM)
     for (size_t i = 0; i < n; ++i) types_in_eam &= types[i] <= eam_->ntypes;
   TDMD_CU(cudaStreamSynchronize(s));
+  max_cell_ = (n_ > 0 && h_cellmax_) ? *h_cellmax_ : 0;
   TDMD_REQUIRE(types_ok, "atom type out of range of masses");
   TDMD_REQUIRE(types_in_eam, "atom type beyond the EAM element count");
   uploaded_ = true;
@@ -557,6 +559,11 @@ void Scheduler::reorder_by_cell() {
   cudaStream_t s = stream_;
   const size_t n = static_cast<size_t>(n_);
   build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, s);
+  cellmax_.reserve(1);
+  if (!h_cellmax_) TDMD_CU(cudaMallocHost(reinterpret_cast<void**>(&h_cellmax_), sizeof(int)));
+  *h_cellmax_ = 0;
+  cell_count_max(cl_, cellmax_.data(), s);
+  TDMD_CU(cudaMemcpyAsync(h_cellmax_, cellmax_.data(), sizeof(int), cudaMemcpyDeviceToHost, s));
   order_.reserve(n);
   TDMD_CU(cudaMemcpyAsync(order_.data(), cl_.cell_atoms.data(), n * sizeof(int),
                           cudaMemcpyDeviceToDevice, s));
@@ -650,7 +657,7 @@ int Scheduler::size_neighbor_list() {
   const double rl = cutoff_ + cfg_.r_skin;
   TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
   build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl * rl, nullptr, nullptr, 0,
-                      cnt_.data(), ctl_status(), s);
+                      cnt_.data(), ctl_status(), s, max_cell_);
   int st[4];
   TDMD_CU(cudaMemcpyAsync(st, ctl_status(), sizeof(st), cudaMemcpyDeviceToHost, s));
   TDMD_CU(cudaStreamSynchronize(s));
@@ -676,7 +683,7 @@ void Scheduler::enqueue_rebuild() {
   const int cell_kernels = build_cells();
   const double rl = cutoff_ + cfg_.r_skin;
   build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl * rl, nbr_.data(), nullptr,
-                      cap_, cnt_.data(), ctl_status(), s);
+                      cap_, cnt_.data(), ctl_status(), s, max_cell_);
   prof_end(kProfRebuild);
   launches_ += cell_kernels + 1;  // cell list + row build
   ++rebuilds_;
@@ -1005,7 +1012,7 @@ void Scheduler::initial_forces(bool defer_check) {
   }
   TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
   build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl2, nbr_.data(), nullptr,
-                      cap_, cnt_.data(), ctl_status(), s);
+                      cap_, cnt_.data(), ctl_status(), s, max_cell_);
   if (reuse && defer_check) {
     init_check_pending_ = true;
   } else if (reuse) {
@@ -1016,7 +1023,7 @@ void Scheduler::initial_forces(bool defer_check) {
       grow_capacity(st[1]);
       TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, s));
       build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_, rl2, nbr_.data(), nullptr,
-                          cap_, cnt_.data(), ctl_status(), s);
+                          cap_, cnt_.data(), ctl_status(), s, max_cell_);
       ++passes;
     }
   }
@@ -1137,7 +1144,7 @@ void Scheduler::run_until(int target) {
     build_cells();
     build_neighbor_rows(cl_, pos4_.data(), PosLayout::D4, n_, box_,
                         (cutoff_ + cfg_.r_skin) * (cutoff_ + cfg_.r_skin), nbr_.data(), nullptr,
-                        cap_, cnt_.data(), nullptr, stream_);
+                        cap_, cnt_.data(), nullptr, stream_, max_cell_);
     enqueue_force(false);
   }
 }
