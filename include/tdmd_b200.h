@@ -209,8 +209,10 @@ int32_t tdmd_morse_compute(const double* d_positions, void* d_forces, int32_t pr
  *    the scratch itself needs no zeroing;
  *  - two calls in flight on one device at the same time share the scratch
  *    and race: order them on one stream;
- *  - the first call on each device (made with that device current) looks
- *    up the scratch address; make it before any stream capture begins. */
+ *  - the first call on each device (made with that device current) that
+ *    asks for an energy or a virial looks up the scratch address; make it
+ *    before any stream capture begins.  Force-only and natoms == 0 calls
+ *    use no scratch and do no look-up. */
 #define TDMD_MORSE_NOALLOC_MAX_ATOMS 524288
 int32_t tdmd_morse_compute_noalloc(const double* d_positions, void* d_forces, int32_t precision,
                                    const int32_t* d_neighbors, const int32_t* d_offsets,

@@ -45,17 +45,29 @@ class OrcPotential(C.Structure):
                 ("r0", C.c_double), ("rc", C.c_double), ("eam", C.c_void_p)]
 
 
+def reference_tree() -> str | None:
+    """The reference checkout: $TDMD_REFERENCE_TREE when set, else a
+    directory named `reference` beside this repository; None when neither
+    holds the reference's `src/` (the tests that need it then skip)."""
+    env = os.environ.get("TDMD_REFERENCE_TREE")
+    cand = env if env else os.path.join(os.path.dirname(os.path.dirname(_HERE)), "reference")
+    return cand if os.path.isdir(os.path.join(cand, "src")) else None
+
+
 def build(ref: bool | None = None) -> None:
     """Compile liboracle.so (and, when the reference tree exists, _ref/: its
     CPU path for the oracle's pins and the CPU baseline, and its GPU
     scheduler in both precision builds for the same-box comparison)."""
     targets = ["all"]
-    ref_tree = os.environ.get("TDMD_REFERENCE_TREE", "/root/reference")
+    ref_tree = reference_tree()
     if ref is None:
-        ref = os.path.isdir(os.path.join(ref_tree, "src"))
+        ref = ref_tree is not None
     if ref:
+        if ref_tree is None:
+            raise RuntimeError("reference tree not found: set TDMD_REFERENCE_TREE")
         targets += ["ref", "refgpu"]
-    subprocess.run(["make", "-s", "-C", _HERE, f"REF={ref_tree}", *targets], check=True)
+    args = [f"REF={ref_tree}"] if ref_tree else []
+    subprocess.run(["make", "-s", "-C", _HERE, *args, *targets], check=True)
 
 
 _lib = None

@@ -1,4 +1,5 @@
 // core.cu -- error state, device box set-up and the fixed-order device scan.
+#include <atomic>
 #include <cmath>
 #include <string>
 
@@ -20,14 +21,21 @@ int32_t fail(int32_t code, const std::string& msg) {
   return code;
 }
 
+// SM count per device ordinal, cached; concurrent first calls from several
+// host threads may both query the attribute, but they store the same value.
 int sm_count() {
-  static int cached = 0;
-  if (cached == 0) {
-    int dev = 0;
-    TDMD_CU(cudaGetDevice(&dev));
-    TDMD_CU(cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev));
+  constexpr int kMaxCachedDevices = 64;
+  static std::atomic<int> cached[kMaxCachedDevices];
+  int dev = 0;
+  TDMD_CU(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < kMaxCachedDevices) {
+    const int c = cached[dev].load(std::memory_order_relaxed);
+    if (c > 0) return c;
   }
-  return cached;
+  int v = 0;
+  TDMD_CU(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+  if (dev >= 0 && dev < kMaxCachedDevices) cached[dev].store(v, std::memory_order_relaxed);
+  return v;
 }
 
 DevBox make_devbox(const tdmd_box& b, double r_list) {

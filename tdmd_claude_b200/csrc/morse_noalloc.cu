@@ -13,15 +13,20 @@
 //    TDMD_ERR_INVALID_ARGUMENT before anything is launched;
 //  * the scratch holds at most kMaxBlocks partial records (1 MiB); every
 //    block of the force kernel overwrites its own record before the
-//    reduction reads it, so the scratch needs no zeroing;
+//    reduction reads it, so the scratch needs no zeroing.  The launch uses
+//    tdmd_morse_compute's lanes per atom, halved while its blocks would
+//    exceed kMaxBlocks (never at the default choice on a B200, whose lanes
+//    give 16384 blocks at the atom limit; one lane per atom always fits);
 //  * d_energy / d_virial are ADDED to, as in tdmd_morse_compute: zero them
 //    first to get this call's totals alone; d_forces is overwritten;
 //  * there is one scratch per device, so two calls in flight on the same
 //    device at once (different streams, or different host threads without
 //    ordering between them) race on it; order them on one stream;
-//  * the first call on each device looks up the scratch's device address
-//    (cudaGetSymbolAddress, which may load this module); make that first
-//    call before any stream capture begins on that device.
+//  * the first call on each device that asks for an energy or a virial
+//    looks up the scratch's device address (cudaGetSymbolAddress, which may
+//    load this module); make that first call before any stream capture
+//    begins on that device.  Force-only and empty calls need no scratch and
+//    do no look-up.
 #include <mutex>
 
 #include "common.cuh"
@@ -34,6 +39,15 @@ namespace {
 
 constexpr int kMaxBlocks = 16384;
 constexpr int kMaxDevices = 64;
+
+// One lane per atom fits at the atom limit, so halving the lanes always
+// ends inside the scratch; the default 8 lanes of large inputs fit too.
+static_assert(static_cast<long long>(TDMD_MORSE_NOALLOC_MAX_ATOMS) <=
+                  static_cast<long long>(kMaxBlocks) * kForceThreads,
+              "one lane per atom must fit the scratch at the atom limit");
+static_assert(static_cast<long long>(TDMD_MORSE_NOALLOC_MAX_ATOMS) * 8 <=
+                  static_cast<long long>(kMaxBlocks) * kForceThreads,
+              "the default lanes of large inputs must fit the scratch at the atom limit");
 
 // Per-block {energy, virial[6], pad} records of the force kernel.
 static __device__ __align__(256) double g_morse_partials[kMaxBlocks * kEvStride];
@@ -73,17 +87,17 @@ extern "C" int32_t tdmd_morse_compute_noalloc(const double* d_positions, void* d
     TDMD_REQUIRE(natoms <= TDMD_MORSE_NOALLOC_MAX_ATOMS,
                  "natoms exceeds TDMD_MORSE_NOALLOC_MAX_ATOMS (fixed scratch size)");
     TDMD_REQUIRE(precision == TDMD_FP64 || precision == TDMD_MIXED, "unknown precision");
-    double* scratch = scratch_for_current_device();
     if (natoms == 0) return;
     TDMD_REQUIRE(d_positions && d_forces && d_offsets && d_counts, "null device array");
     cudaStream_t s = as_stream(stream);
     const DevBox b = make_devbox(*box, 0.0);
     const NbrView nl{d_neighbors, d_offsets, d_counts, 0};
     const bool ev = d_energy || d_virial;
-    const int lpa = default_lpa(natoms);
+    int lpa = default_lpa(natoms);
+    while (lpa > 1 && force_blocks(natoms, lpa) > kMaxBlocks) lpa >>= 1;
     const int nblk = force_blocks(natoms, lpa);
     TDMD_REQUIRE(nblk <= kMaxBlocks, "partial records exceed the fixed scratch");
-    double* part = ev ? scratch : nullptr;
+    double* part = ev ? scratch_for_current_device() : nullptr;
     if (precision == TDMD_FP64) {
       GeoAoS64 g{d_positions, {b.L[0], b.L[1], b.L[2]}, {b.halfL[0], b.halfL[1], b.halfL[2]},
                  {b.periodic[0], b.periodic[1], b.periodic[2]}};

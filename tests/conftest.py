@@ -14,7 +14,9 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REF_TREE = os.environ.get("TDMD_REFERENCE_TREE", "/root/reference")
+from oracle.oracle import reference_tree  # noqa: E402
+
+REF_TREE = reference_tree()
 
 
 def pytest_configure(config):
@@ -43,7 +45,29 @@ def ref_lib(oracle):
     return R
 
 
+def golden_file(name: str, tmp_dir: str) -> str:
+    """Path of a golden fixture; a `.xz` one is decompressed into tmp_dir."""
+    import lzma
+    src = os.path.join(GOLDEN, name)
+    if not name.endswith(".xz"):
+        return src
+    dst = os.path.join(tmp_dir, name[:-3])
+    if not os.path.exists(dst):
+        with lzma.open(src, "rb") as f, open(dst, "wb") as o:
+            o.write(f.read())
+    return dst
+
+
+@pytest.fixture(scope="session")
+def mishin_setfl(tmp_path_factory):
+    """The reference's Mishin Cu setfl (tests/data/Cu_mishin1.eam.alloy)."""
+    g = golden("run0_eam_256.json")
+    return golden_file(g["potential_file"], str(tmp_path_factory.mktemp("golden")))
+
+
 def reference_file(rel: str) -> str:
+    if REF_TREE is None:
+        pytest.skip(f"reference tree not found (set TDMD_REFERENCE_TREE); {rel} unavailable")
     p = os.path.join(REF_TREE, rel)
     if not os.path.exists(p):
         pytest.skip(f"reference file {rel} not available here")

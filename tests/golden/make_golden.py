@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference.
 
-Run where the reference tree is available (default /root/reference, or
-$TDMD_REFERENCE_TREE) after `make -C oracle all ref`:
+Run where the reference tree is available ($TDMD_REFERENCE_TREE, or a
+checkout named `reference` beside this repository) after
+`make -C oracle all ref`:
 
     python tests/golden/make_golden.py
 
@@ -13,9 +14,12 @@ Sources of truth, all from the reference itself:
                               forces_morse.dump) + the lattice of
                               tests/data/cu_fcc_256.data + the reference CPU
                               path's PE/forces on it
-  * run0_eam_256.json      -- same for the Mishin Cu EAM dump (forces_eam.dump);
-                              the potential file itself is not copied, so the
-                              tests that need it run only where it exists
+  * run0_eam_256.json      -- same for the Mishin Cu EAM dump (forces_eam.dump)
+  * Cu_mishin1.eam.alloy.xz -- the reference's test potential
+                              (tests/data/Cu_mishin1.eam.alloy, Mishin et al.
+                              PRB 63, 224106 (2001)), xz-compressed byte for
+                              byte, so the EAM run-0 tests run where the
+                              reference tree is absent
   * ref_*.json             -- outputs of the reference's CPU path (compiled
                               from its sources into oracle/_ref/) on the
                               seeded synthetic inputs of tdmd_claude_b200.workloads
@@ -24,6 +28,7 @@ from __future__ import annotations
 
 import ctypes as C
 import json
+import lzma
 import os
 import sys
 import tempfile
@@ -38,7 +43,9 @@ from oracle import oracle as O  # noqa: E402
 from tdmd_claude_b200 import io as TIO  # noqa: E402
 from tdmd_claude_b200 import workloads as W  # noqa: E402
 
-REF = os.environ.get("TDMD_REFERENCE_TREE", "/root/reference")
+REF = O.reference_tree()
+if REF is None:
+    sys.exit("reference tree not found: set TDMD_REFERENCE_TREE")
 PER = np.ones(3, np.int32)
 
 
@@ -96,6 +103,11 @@ def main():
         reference_pe=pe, reference_forces=arr(f),
         tolerance_fp64=1e-12, tolerance_mixed=5e-5))
     mishin = os.path.join(REF, "tests/data/Cu_mishin1.eam.alloy")
+    with open(mishin, "rb") as f:
+        raw = f.read()
+    with open(os.path.join(HERE, "Cu_mishin1.eam.alloy.xz"), "wb") as f:
+        f.write(lzma.compress(raw, preset=9 | lzma.PRESET_EXTREME))
+    print("wrote Cu_mishin1.eam.alloy.xz")
     h = R.ref_eam_load(mishin.encode())
     fe = np.zeros((N, 3))
     pe_e = R.ref_eam_forces(h, pos.reshape(-1), ty, N, lo, hi, PER, 1.0, fe.reshape(-1))
@@ -104,7 +116,7 @@ def main():
     dump("run0_eam_256.json", dict(
         source=["tests/data/Cu_mishin1.eam.alloy",
                 "verifylab/cases/run0-force-match/forces_eam.dump"],
-        potential_file="tests/data/Cu_mishin1.eam.alloy", skin=1.0,
+        potential_file="Cu_mishin1.eam.alloy.xz", skin=1.0,
         lammps_forces=arr(fle), lammps_pe=-906.29591, reference_pe=pe_e,
         reference_forces=arr(fe), tolerance_fp64=1e-12, tolerance_mixed=1e-4))
     R.ref_eam_free(h)

@@ -10,7 +10,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import golden, reference_file, rel_rms
+from conftest import golden, rel_rms
 
 pytestmark = pytest.mark.gpu
 
@@ -175,11 +175,11 @@ def test_eam_setfl_reader_matches_oracle(cuda, oracle, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_eam_mishin_run0_lammps(cuda, precision):
+def test_eam_mishin_run0_lammps(cuda, mishin_setfl, precision):
     from tdmd_claude_b200 import EamAlloy
     g = golden("run0_eam_256.json")
     m = golden("run0_morse_256.json")
-    eam = EamAlloy().read_setfl(reference_file(g["potential_file"]))
+    eam = EamAlloy().read_setfl(mishin_setfl)
     pos = np.array(m["positions"])
     f, e, *_ = _eam_gpu(cuda, eam, pos, np.ones(256, np.int32), m["lo"], m["hi"], g["skin"],
                         precision)

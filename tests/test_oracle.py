@@ -9,7 +9,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import golden, reference_file
+from conftest import golden
 
 
 def test_two_atoms_morse_analytic(oracle):
@@ -45,9 +45,9 @@ def test_run0_morse_lammps(oracle):
     assert abs(pe - g["lammps_pe"]) / abs(g["lammps_pe"]) < 1e-7
 
 
-def test_run0_eam_lammps(oracle):
+def test_run0_eam_lammps(oracle, mishin_setfl):
     g = golden("run0_eam_256.json")
-    eam = oracle.OracleEam.from_setfl(reference_file(g["potential_file"]))
+    eam = oracle.OracleEam.from_setfl(mishin_setfl)
     m = golden("run0_morse_256.json")
     pos = np.array(m["positions"])
     r = eam.forces(pos, np.ones(len(pos), np.int32), m["lo"], m["hi"], g["skin"])
