@@ -283,8 +283,9 @@ def timed_windows(sched, steps, warmup, flush, torch, dist=None):
     return total, wall, launches, ms
 
 
-def e2e_windows(sysm, eam, steps, warmup, torch):
-    """upload (pinned host) + run_until(WINDOW) + download (pinned host), wall."""
+def e2e_windows(sysm, eam, steps, warmup, torch, dist=None):
+    """upload (pinned host) + run_until(WINDOW) + download (pinned host), wall
+    (a barrier on both sides of the timed steps under a process group)."""
     from tdmd_claude_b200 import Box, FastPipelineScheduler, make_config
     s = FastPipelineScheduler(Box.make(sysm.lo, sysm.hi), sysm.n, eam,
                               make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW,
@@ -308,11 +309,15 @@ def e2e_windows(sysm, eam, steps, warmup, torch):
     for _ in range(warmup):
         one()
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
         one()
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
+    if dist is not None:
+        dist.barrier()
     s.close()
     return wall, h2d, d2h
 
@@ -616,11 +621,42 @@ def batch_eam_bench(steps, warmup, flush, torch, eam, precision, nrep=8):
             "kernel_launches_timed": launches}
 
 
-def reference_gpu_sample(sysm, t, windows=10, warm=5):
+def batch_eam_drift(eam, precision, nsteps=10000, nrep=8, every=100):
+    """Per-replica NVE energy drift of the nrep x 131,072-atom EAM batch:
+    nsteps steps in windows of `every` (the energy log writes each replica's
+    PE and KE at every window's end, on the device); least-squares slope of
+    E_total/N against time per replica, eV/atom/ns.  Untimed."""
+    from tdmd_claude_b200 import Box, ReplicaBatch, make_config
+    from tdmd_claude_b200 import workloads as W
+    systems = [W.fcc_system(NCELL, 3.615, 300.0, 5000 + r) for r in range(nrep)]
+    b = ReplicaBatch([Box.make(s.lo, s.hi) for s in systems], [s.n for s in systems], eam,
+                     make_config(dt=DT, r_skin=SKIN, rebuild_every=WINDOW, precision=precision,
+                                 energy_every=every, energy_log_capacity=nsteps // every + 4))
+    b.upload(np.concatenate([s.positions for s in systems]),
+             np.concatenate([s.velocities for s in systems]),
+             np.concatenate([s.types for s in systems]), systems[0].masses)
+    b.run_until(0)
+    for k in range(every, nsteps + 1, every):
+        b.run_until(k)
+    steps_log, pk = b.energy_log()
+    b.close()
+    natoms = np.array([s.n for s in systems], np.float64)
+    etot = (pk[:, :, 0] + pk[:, :, 1]) / natoms
+    t_ns = steps_log * DT * 1e-3
+    slopes = np.atleast_1d(np.polyfit(t_ns, etot, 1)[0])
+    return {"steps": nsteps, "ns": nsteps * DT * 1e-3, "replicas": nrep,
+            "slope_ev_per_atom_per_ns": slopes.tolist(),
+            "max_abs_slope": float(np.abs(slopes).max()),
+            "max_abs_dev_ev_per_atom": float(np.abs(etot - etot[0]).max())}
+
+
+def reference_gpu_sample(sysm, t, windows=50, warm=5, repeats=3):
     """The reference's own GPU FastPipelineScheduler (oracle/_ref, compiled
     from its sources, FP64 and mixed builds) on the same system: host wall
-    clock around whole run_until windows (it synchronizes the host inside a
-    rebuild).  None where those libraries or a GPU are absent."""
+    clock around `windows` whole run_until windows (it synchronizes the host
+    inside a rebuild), after `warm` untimed ones, repeated `repeats` times
+    with a fresh scheduler each; median and range of the repeats.  None
+    where those libraries or a GPU are absent."""
     import ctypes as C
     out = {}
     try:
@@ -642,21 +678,31 @@ def reference_gpu_sample(sysm, t, windows=10, warm=5):
         L.refgpu_run_eam.argtypes = [C.c_char_p, f64p, f64p, i32p, f64p, C.c_int32, C.c_int32,
                                      f64p, f64p, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                      C.c_int32, C.c_int32]
+        secs = []
         with tempfile.TemporaryDirectory() as d:
             setfl = os.path.join(d, "cu.eam.alloy")
             TIO.write_setfl(setfl, t)
-            sec = L.refgpu_run_eam(setfl.encode(), np.ascontiguousarray(sysm.positions),
-                                   np.ascontiguousarray(sysm.velocities),
-                                   np.ascontiguousarray(sysm.types, dtype=np.int32),
-                                   np.ascontiguousarray(sysm.masses), sysm.masses.size, sysm.n,
-                                   np.array(sysm.lo, np.float64), np.array(sysm.hi, np.float64),
-                                   DT, SKIN, WINDOW, WINDOW, warm, windows)
-        if sec <= 0:
+            for _ in range(repeats):
+                sec = L.refgpu_run_eam(setfl.encode(), np.ascontiguousarray(sysm.positions),
+                                       np.ascontiguousarray(sysm.velocities),
+                                       np.ascontiguousarray(sysm.types, dtype=np.int32),
+                                       np.ascontiguousarray(sysm.masses), sysm.masses.size,
+                                       sysm.n, np.array(sysm.lo, np.float64),
+                                       np.array(sysm.hi, np.float64), DT, SKIN, WINDOW, WINDOW,
+                                       warm, windows)
+                if sec <= 0:
+                    break
+                secs.append(sec)
+        if not secs:
             out[prec] = {"error": L.refgpu_last_error().decode()}
             continue
-        out[prec] = {"value": sysm.n * WINDOW * windows / sec, "unit": "atom-steps/s",
-                     "ms_per_window": 1e3 * sec / windows,
-                     "timing": "host wall clock around run_until windows"}
+        vals = sorted(sysm.n * WINDOW * windows / x for x in secs)
+        out[prec] = {"value": float(np.median(vals)), "min": vals[0], "max": vals[-1],
+                     "samples": vals, "unit": "atom-steps/s",
+                     "ms_per_window_median": float(np.median([1e3 * x / windows for x in secs])),
+                     "windows_per_sample": windows, "warmup_windows": warm,
+                     "timing": "host wall clock around run_until windows (median of "
+                               f"{len(secs)} samples, fresh scheduler each)"}
     return out or None
 
 
@@ -714,7 +760,7 @@ def main():
                          "autotuner's usual choice at 131,072 atoms; Morse replicas: autotuned "
                          "unless given)")
     ap.add_argument("--no-ref-gpu", action="store_true",
-                    help="reference arm: skip timing the reference's own GPU scheduler")
+                    help="skip timing the reference's own GPU scheduler (same-run context)")
     ap.add_argument("--no-fit", action="store_true",
                     help="skip the force-matching (adjoint + Adam) figure")
     ap.add_argument("--no-ternary", action="store_true",
@@ -792,7 +838,7 @@ def main():
                                                         dist)
     clk = clocks.stop()
     # Plain FP64 path, same protocol.
-    ms_fp64, _, _, _ = timed_windows(s64, args.steps, args.warmup, flush, torch, dist)
+    ms_fp64, wall_fp64, _, _ = timed_windows(s64, args.steps, args.warmup, flush, torch, dist)
 
     units = world * sysm.n * WINDOW * args.steps
     value = units / (ms_mixed * 1e-3)
@@ -842,6 +888,9 @@ def main():
                 for p in ("mixed", "fp64")}
         beam["mixed_batched_over_plain_fp64"] = beam["mixed"]["value"] / value64
         beam["mixed_over_fp64_batched"] = beam["mixed"]["value"] / beam["fp64"]["value"]
+        if args.drift_steps > 0:
+            nd = min(args.drift_steps, 10000)
+            beam["nve_drift"] = {p: batch_eam_drift(eam, p, nsteps=nd) for p in ("mixed", "fp64")}
     fitfig = None if args.no_fit else fit_bench(torch)
     small = None if args.no_batch else morse256_bench(torch)
     ternary = None if args.no_ternary else ternary_bench(max(3, args.steps // 3), 3, flush,
@@ -855,17 +904,43 @@ def main():
     dens_bytes = sysm.n * (40 + 20 * K)
     force_ms = kt["force"][0]
     achieved = force_bytes / (force_ms * 1e-3) / 1e9 if force_ms > 0 else None
-    traffic = None
+    # traffic is a recorded figure (an ncu capture of this kernel on this
+    # workload, summarised in profiles/), not measured by this run
+    traffic, traffic_src = None, None
     prof_json = os.path.join(ROOT, "profiles", "eam_force_mixed_131k.json")
     if os.path.exists(prof_json):
         with open(prof_json) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            rec = json.load(f)
+        traffic = rec.get("dram_bytes_per_launch")
+        traffic_src = {"recorded": "profiles/eam_force_mixed_131k.json",
+                       "captured": rec.get("captured"), "kernel": rec.get("kernel"),
+                       "command": rec.get("command")}
 
-    e2e_wall, h2d, d2h = (None, 0, 0)
-    if rank == 0 or world > 1:
-        e2e_wall, h2d, d2h = e2e_windows(sysm, eam, max(3, args.steps // 3), 2, torch)
+    # e2e: every rank times its own steps; the job's time is the slowest rank's
+    from tdmd_claude_b200.replicas import max_over_ranks
     e2e_steps = max(3, args.steps // 3)
-    e2e_value = sysm.n * WINDOW * e2e_steps / e2e_wall * world
+    e2e_wall, h2d, d2h = e2e_windows(sysm, eam, e2e_steps, 2, torch, dist)
+    e2e_wall = max_over_ranks(e2e_wall, dist, "cuda")
+    e2e_value = world * sysm.n * WINDOW * e2e_steps / e2e_wall
+
+    # Same-run context: the reference's own GPU scheduler on this system and
+    # GPU (host wall clock, as it synchronizes inside rebuilds), against this
+    # run's host-wall windows and e2e figure.
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_sample(sysm, t)
+        if ref_gpu:
+            ours = {"mixed_host_wall": units / wall_mixed, "fp64_host_wall": units / wall_fp64,
+                    "e2e": e2e_value}
+            ratios = {}
+            for prec in ("mixed", "fp64"):
+                ref_v = (ref_gpu.get(prec) or {}).get("value")
+                if ref_v:
+                    ratios[f"ours_{prec}_host_wall_over_ref_{prec}"] = \
+                        ours[f"{prec}_host_wall"] / ref_v
+                    ratios[f"ours_e2e_over_ref_{prec}"] = e2e_value / ref_v
+            ref_gpu = {"reference": ref_gpu, "ours_same_run": ours, "ratios_vs_median": ratios,
+                       "note": "host wall includes the L2-flush writes between windows"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -907,9 +982,14 @@ def main():
                 "morse_256_nve_1000": small,
                 "force_matching": fitfig,
                 "wall_s_timed_region": wall_mixed,
+                "reference_gpu_same_run": ref_gpu,
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                         "traffic_source": traffic_src,
+                         "ms_source": "CUDA events around each force launch on the "
+                                      "scheduler's stream, ungraphed windows of the same "
+                                      "system (the graph-replayed windows give value)",
                          "kernel": "k_eam_force<GeoQ> (mixed)", "peak_source": peak_kind,
                          "bytes_per_launch": force_bytes, "ms_per_launch": force_ms,
                          "model": "gather model n*(48+24K) B, K = mean full-list length, "

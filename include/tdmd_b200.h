@@ -39,7 +39,8 @@ typedef enum tdmd_status {
   TDMD_ERR_STATE = 5,          /* call order (e.g. run_until before upload) */
   TDMD_ERR_NLIST_OVERFLOW = 6, /* neighbor capacity exceeded, retry failed  */
   TDMD_ERR_TIMEOUT = 7,        /* a bounded device-side wait gave up        */
-  TDMD_ERR_UNSUPPORTED = 8
+  TDMD_ERR_UNSUPPORTED = 8,
+  TDMD_ERR_IO = 9              /* a file could not be opened or written     */
 } tdmd_status;
 
 /* Arithmetic of the force path.  FP64: everything double (the reference's
@@ -220,6 +221,58 @@ int32_t tdmd_morse_compute_noalloc(const double* d_positions, void* d_forces, in
                                    const tdmd_morse_params* params, double* d_energy,
                                    double* d_virial, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* File formats (host only).                                                */
+/* ------------------------------------------------------------------------ */
+/* read_lammps_data, src/io/lammps_data_reader.cpp:33-204: a LAMMPS
+ * `atomic` data file into a host SystemState (ids 1-based, atom with id k
+ * at index k-1, velocities 0 without a Velocities section, masses
+ * [ntypes+1] with 1.0 where Masses gives none, periodic box).  Parse errors
+ * return TDMD_ERR_PARSE; so does an atom id outside 1..N or a Masses type
+ * outside 1..ntypes (where the reference would index out of its arrays). */
+typedef struct tdmd_system tdmd_system;
+int32_t tdmd_read_lammps_data(const char* path, tdmd_system** out);
+int32_t tdmd_system_destroy(tdmd_system* s);
+/* The arrays of a read SystemState (owned by it): positions and velocities
+ * double[3n], types and ids int32[n], masses double[ntypes+1].  Any output
+ * may be null. */
+int32_t tdmd_system_get(const tdmd_system* s, int64_t* natoms, int32_t* ntypes, tdmd_box* box,
+                        const double** positions, const double** velocities,
+                        const int32_t** types, const int32_t** ids, const double** masses);
+/* No reference counterpart (the reference reads data files only): writes
+ * a data file that read_lammps_data reads back exactly (17 significant
+ * digits): title line, counts, box, Masses (masses[ntypes+1], nullable:
+ * 1.0), "Atoms # atomic", and Velocities when velocities is non-null;
+ * ids nullable (1..N). */
+int32_t tdmd_write_lammps_data(const char* path, const char* title, int64_t natoms,
+                               int32_t ntypes, const tdmd_box* box, const double* positions,
+                               const double* velocities, const int32_t* types,
+                               const int32_t* ids, const double* masses);
+/* read_lammps_dump, src/io/dump_reader.cpp:15-55: a `dump custom id type x
+ * y z fx fy fz` file, records sorted by id.  *natoms gets the count; with
+ * every array null nothing else is read (size query), otherwise capacity
+ * must be >= the count; each array may be null. */
+int32_t tdmd_read_force_dump(const char* path, int64_t* natoms, int64_t capacity, int32_t* ids,
+                             int32_t* types, double* positions, double* forces);
+/* write_lammps_force_dump, src/drivers/tdmd_main.cpp:65-95: TIMESTEP,
+ * NUMBER OF ATOMS, BOX BOUNDS pp pp pp, ATOMS id type x y z fx fy fz with
+ * 17 significant digits; forces double[3n] (TDMD_FP64) or float[3n]
+ * (TDMD_MIXED); ids nullable (1..N). */
+int32_t tdmd_write_force_dump(const char* path, int64_t step, int64_t natoms,
+                              const tdmd_box* box, const int32_t* ids, const int32_t* types,
+                              const double* positions, const void* forces,
+                              int32_t force_precision);
+/* No reference counterpart (the reference reads setfl only): writes the
+ * raw tables of an EAM in the setfl layout EamAlloy::read_setfl
+ * (src/potentials/eam_alloy.cpp:90-192) reads, values with 17 significant
+ * digits, so reading the file back gives the same tables and spline
+ * coefficients bit for bit.  A table read from a setfl keeps its comment
+ * and element header lines unless comment / masses (double[ntypes],
+ * nullable) are given; elements (nullable) replaces the element names with
+ * a space-separated list. */
+int32_t tdmd_write_setfl(const char* path, const tdmd_eam* eam, const char* comment,
+                         const double* masses, const char* elements);
+
 /* DeviceEam, src/potentials/device_eam.cuh:26-75: device copy of the
  * tables plus rho/fp scratch. */
 typedef struct tdmd_device_eam tdmd_device_eam;
@@ -327,6 +380,15 @@ int32_t tdmd_sched_device_state(tdmd_sched* s, void** d_pos4, double** d_vel, vo
  * rows and results are those of the caller's order (cells list their atoms
  * by the caller's index); upload and download convert. */
 int32_t tdmd_sched_atom_order(const tdmd_sched* s, const int32_t** d_order);
+/* No reference counterpart (the reference keeps its scheduler's
+ * DeviceNeighborList private).  Copies the scheduler's current neighbor
+ * list to host memory in the caller's atom order as dense CSR: counts[n]
+ * (required), then, when neighbors is non-null, the rows back to back
+ * (row i starts at the sum of counts[0..i)); *total (nullable) gets the
+ * number of entries.  Needs a list (after run_until); synchronises the
+ * scheduler's stream; TDMD_ERR_INVALID_ARGUMENT when capacity < total. */
+int32_t tdmd_sched_neighbor_list(const tdmd_sched* s, int32_t* counts, int32_t* neighbors,
+                                 int64_t capacity, int64_t* total);
 /* Per-kernel timing (no reference counterpart; the reference profiles only
  * from outside with nsys/ncu).  While on, windows run without graph replay
  * and CUDA events on the scheduler's stream bracket each phase; averages in

@@ -94,6 +94,31 @@ struct Box {
   }
 };
 
+// --- src/core/system_state.hpp: the host SoA state of a simulation ----------
+struct SystemState {
+  i64 natoms{0};
+  Box box;
+  std::vector<PositionVec> positions;
+  std::vector<VelocityVec> velocities;
+  std::vector<ForceVec> forces;
+  std::vector<i32> types;
+  std::vector<i32> ids;
+  std::vector<real> masses;  // indexed by the 1-based type: size ntypes + 1
+  std::vector<std::string> type_names;
+  i64 step{0};
+  real time{0};
+
+  void resize(i64 n) {
+    natoms = n;
+    const size_t k = static_cast<size_t>(n);
+    positions.resize(k);
+    velocities.resize(k);
+    forces.resize(k);
+    types.resize(k);
+    ids.resize(k);
+  }
+};
+
 // --- src/potentials -----------------------------------------------------------
 namespace potentials {
 
@@ -190,6 +215,94 @@ class DeviceEam {
 };
 
 }  // namespace potentials
+
+// --- src/io: LAMMPS data files and force dumps, setfl ------------------------
+namespace io {
+
+// lammps_data_reader.hpp / .cpp:33-204
+inline SystemState read_lammps_data(const std::string& filename) {
+  tdmd_system* h = nullptr;
+  detail::check(tdmd_read_lammps_data(filename.c_str(), &h));
+  struct Owner {
+    tdmd_system* h;
+    ~Owner() { tdmd_system_destroy(h); }
+  } own{h};
+  int64_t n = 0;
+  int32_t nt = 0;
+  tdmd_box b{};
+  const double *p = nullptr, *v = nullptr, *m = nullptr;
+  const int32_t *t = nullptr, *id = nullptr;
+  detail::check(tdmd_system_get(h, &n, &nt, &b, &p, &v, &t, &id, &m));
+  SystemState s;
+  s.box.lo = Vec3D{b.lo[0], b.lo[1], b.lo[2]};
+  s.box.hi = Vec3D{b.hi[0], b.hi[1], b.hi[2]};
+  s.resize(n);
+  for (i64 i = 0; i < n; ++i) {
+    const size_t k = static_cast<size_t>(i);
+    s.positions[k] = PositionVec{p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+    s.velocities[k] = VelocityVec{v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+    s.forces[k] = ForceVec{0, 0, 0};
+    s.types[k] = t[i];
+    s.ids[k] = id[i];
+  }
+  s.masses.assign(m, m + nt + 1);
+  s.type_names.resize(static_cast<size_t>(nt) + 1);
+  return s;
+}
+
+// dump_reader.hpp:14-26
+struct DumpAtom {
+  i32 id;
+  i32 type;
+  PositionVec pos;
+  ForceVec force;
+};
+
+inline std::vector<DumpAtom> read_lammps_dump(const std::string& filename) {
+  int64_t n = 0;
+  detail::check(tdmd_read_force_dump(filename.c_str(), &n, 0, nullptr, nullptr, nullptr,
+                                     nullptr));
+  const size_t k = static_cast<size_t>(n);
+  std::vector<int32_t> id(k), ty(k);
+  std::vector<double> p(3 * k), f(3 * k);
+  detail::check(tdmd_read_force_dump(filename.c_str(), &n, n, id.data(), ty.data(), p.data(),
+                                     f.data()));
+  std::vector<DumpAtom> out(k);
+  for (size_t i = 0; i < k; ++i)
+    out[i] = DumpAtom{id[i], ty[i], PositionVec{p[3 * i], p[3 * i + 1], p[3 * i + 2]},
+                      ForceVec{static_cast<force_t>(f[3 * i]), static_cast<force_t>(f[3 * i + 1]),
+                               static_cast<force_t>(f[3 * i + 2])}};
+  return out;
+}
+
+// No reference counterpart (the reference only reads data files).
+inline void write_lammps_data(const SystemState& s, const std::string& path,
+                              const std::string& title = "tdmd_claude_b200 data") {
+  const tdmd_box b = s.box.to_c();
+  std::vector<double> m(s.masses.begin(), s.masses.end());
+  const int32_t nt = s.masses.empty() ? 1 : static_cast<int32_t>(s.masses.size()) - 1;
+  detail::check(tdmd_write_lammps_data(
+      path.c_str(), title.c_str(), s.natoms, nt, &b,
+      reinterpret_cast<const double*>(s.positions.data()),
+      reinterpret_cast<const double*>(s.velocities.data()), s.types.data(), s.ids.data(),
+      m.empty() ? nullptr : m.data()));
+}
+
+// tdmd_main.cpp:65-95 (the reference driver's dump writer)
+inline void write_lammps_force_dump(const SystemState& s, const std::string& path) {
+  const tdmd_box b = s.box.to_c();
+  detail::check(tdmd_write_force_dump(path.c_str(), s.step, s.natoms, &b, s.ids.data(),
+                                      s.types.data(),
+                                      reinterpret_cast<const double*>(s.positions.data()),
+                                      s.forces.data(), kForcePrecision));
+}
+
+// No reference counterpart (the reference only reads setfl).
+inline void write_setfl(const potentials::EamAlloy& eam, const std::string& path) {
+  detail::check(tdmd_write_setfl(path.c_str(), eam.handle(), nullptr, nullptr, nullptr));
+}
+
+}  // namespace io
 
 // --- src/domain/device_cell_list.cuh:16-60 -------------------------------------
 namespace domain {

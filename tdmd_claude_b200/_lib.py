@@ -20,7 +20,7 @@ TDMD_POT_EAM = 1
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "OUT_OF_MEMORY", 4: "PARSE", 5: "STATE",
-    6: "NLIST_OVERFLOW", 7: "TIMEOUT", 8: "UNSUPPORTED",
+    6: "NLIST_OVERFLOW", 7: "TIMEOUT", 8: "UNSUPPORTED", 9: "IO",
 }
 
 
@@ -97,6 +97,13 @@ SIGNATURES = {
     "tdmd_eam_create": [_i32, _i32, _f64, _i32, _f64, _f64, _p, _p, _p, _pp],
     "tdmd_eam_destroy": [_p],
     "tdmd_eam_info": [_p, _pi32, _pi32, _pf64, _pi32, _pf64, _pf64],
+    "tdmd_read_lammps_data": [C.c_char_p, _pp],
+    "tdmd_system_destroy": [_p],
+    "tdmd_system_get": [_p, C.POINTER(_i64), _pi32, _p, _pp, _pp, _pp, _pp, _pp],
+    "tdmd_write_lammps_data": [C.c_char_p, C.c_char_p, _i64, _i32, _p, _p, _p, _p, _p, _p],
+    "tdmd_read_force_dump": [C.c_char_p, C.POINTER(_i64), _i64, _p, _p, _p, _p],
+    "tdmd_write_force_dump": [C.c_char_p, _i64, _i64, _p, _p, _p, _p, _p, _i32],
+    "tdmd_write_setfl": [C.c_char_p, _p, C.c_char_p, _p, C.c_char_p],
     "tdmd_eam_coeffs": [_p, _i32, _i32, _p],
     "tdmd_cell_list_create": [_pp],
     "tdmd_cell_list_destroy": [_p],
@@ -142,6 +149,7 @@ SIGNATURES = {
     "tdmd_sched_thermostat_state": [_p, _pf64, _p, _p],
     "tdmd_sched_device_state": [_p, _pp, _pp, _pp],
     "tdmd_sched_atom_order": [_p, _pp],
+    "tdmd_sched_neighbor_list": [_p, _p, _p, _i64, _p],
     "tdmd_sched_stream": [_p, _pp],
     "tdmd_batch_create_morse": [_i32, C.POINTER(Box), _p, C.POINTER(MorseParams),
                                 C.POINTER(FastPipelineConfig), _pp],

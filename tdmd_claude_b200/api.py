@@ -313,6 +313,19 @@ class FastPipelineScheduler:
         call("tdmd_sched_stream", self._h, C.byref(s))
         return s.value or 0
 
+    def neighbor_list(self):
+        """(counts, offsets, neighbors) of the scheduler's current list, in
+        the caller's atom order (dense CSR on the host)."""
+        n = self.natoms
+        cnt = np.zeros(n, np.int32)
+        tot = C.c_int64()
+        call("tdmd_sched_neighbor_list", self._h, _ptr(cnt), None, 0, C.byref(tot))
+        nb = np.zeros(max(tot.value, 1), np.int32)
+        call("tdmd_sched_neighbor_list", self._h, _ptr(cnt), _ptr(nb), tot.value, C.byref(tot))
+        off = np.zeros(n, np.int32)
+        off[1:] = np.cumsum(cnt)[:-1]
+        return cnt, off, nb[:tot.value]
+
 
 # ---------------------------------------------------------------------------
 # Batched replicas (no reference counterpart; see tdmd_batch_* in the header)

@@ -22,6 +22,10 @@ struct tdmd_eam {
   double dr = 0.0;
   double cutoff = 0.0;
   std::vector<std::string> elements;
+  // setfl text kept for writing the tables back out: the 3 comment lines
+  // and each element's header line (empty for tables built from arrays)
+  std::vector<std::string> comments;
+  std::vector<std::string> headers;
   std::vector<double> F;     // [ntypes][nrho] raw F(rho)
   std::vector<double> rho;   // [ntypes][nr]   raw rho(r)
   std::vector<double> rphi;  // [npairs][nr]   raw r*phi(r)

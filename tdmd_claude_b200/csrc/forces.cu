@@ -143,8 +143,12 @@ static void read_setfl(const std::string& path, tdmd_eam& e) {
   std::ifstream f(path);
   if (!f.is_open()) throw Error{TDMD_ERR_PARSE, "cannot open EAM file: " + path};
   std::string line;
-  for (int k = 0; k < 3; ++k)
+  e.comments.clear();
+  for (int k = 0; k < 3; ++k) {
     if (!std::getline(f, line)) throw Error{TDMD_ERR_PARSE, "premature end of EAM file"};
+    if (!line.empty() && line.back() == '\r') line.pop_back();
+    e.comments.push_back(line);
+  }
   if (!std::getline(f, line)) throw Error{TDMD_ERR_PARSE, "premature end of EAM file"};
   {
     std::istringstream is(line);
@@ -167,8 +171,11 @@ static void read_setfl(const std::string& path, tdmd_eam& e) {
   e.rho.assign(static_cast<size_t>(nt) * e.nr, 0.0);
   e.rphi.assign(static_cast<size_t>(npairs) * e.nr, 0.0);
   SetflReader r{f};
+  e.headers.assign(static_cast<size_t>(nt), std::string());
   for (int t = 0; t < nt; ++t) {
-    (void)r.header();
+    std::string h = r.header();
+    while (!h.empty() && (h.back() == '\r' || h.back() == ' ')) h.pop_back();
+    e.headers[static_cast<size_t>(t)] = h;
     r.values(e.nrho, e.F.data() + static_cast<size_t>(t) * e.nrho, "F(rho)");
     r.values(e.nr, e.rho.data() + static_cast<size_t>(t) * e.nr, "rho(r)");
   }

@@ -253,11 +253,26 @@ __device__ __forceinline__ void build_cell_rows(
   // filter and the band), so the staged sweep needs no bounds select.
   const int padded = (total + 31) & ~31;
   const bool staged = padded <= stage_cap;
-  // Fixed-point lower corner of the center cell.
-  const int ox = encode_q(b.lo[0] + ix * b.cs[0], b.qlo[0], b.qinv[0]);
-  const int oy = encode_q(b.lo[1] + iy * b.cs[1], b.qlo[1], b.qinv[1]);
-  const int oz = encode_q(b.lo[2] + iz * b.cs[2], b.qlo[2], b.qinv[2]);
+  // Lower corner of the center cell: fixed point (periodic axes) and FP64.
+  const double cx = b.lo[0] + ix * b.cs[0], cy = b.lo[1] + iy * b.cs[1],
+               cz = b.lo[2] + iz * b.cs[2];
+  const int ox = encode_q(cx, b.qlo[0], b.qinv[0]);
+  const int oy = encode_q(cy, b.qlo[1], b.qinv[1]);
+  const int oz = encode_q(cz, b.qlo[2], b.qinv[2]);
   const float s0 = b.qscale[0], s1 = b.qscale[1], s2 = b.qscale[2];
+  // One coordinate of a record.  Periodic axis: the exact int32 fixed-point
+  // difference (its wrap is the minimum image).  Non-periodic axis: the FP64
+  // difference rounded once to FP32 -- the fixed-point difference would wrap
+  // for an atom more than 2L from the corner (the cell list clamps atoms
+  // outside the box into its edge cells); a coordinate farther than four
+  // cells from the corner (outside the filter's error analysis) becomes NaN,
+  // which sends every pair of that record to the exact FP64 test.
+  auto coord = [](double x, double c, double qlo, double qinv, int oq, float sc, int per,
+                  double cs) -> float {
+    if (per) return __fmul_rn(__int2float_rn(encode_q(x, qlo, qinv) - oq), sc);
+    const float r = __double2float_rn(__dsub_rn(x, c));
+    return fabsf(r) <= static_cast<float>(4.0 * cs) ? r : __int_as_float(0x7fc00000);
+  };
   // Candidate record k (cell t with s_pre[t] <= k < s_pre[t+1]).
   auto record = [&](int k) -> float4 {
     int lo = 0, hi = 27;
@@ -267,9 +282,9 @@ __device__ __forceinline__ void build_cell_rows(
     }
     const int j = __ldg(cell_atoms + s_start[lo] + (k - s_pre[lo]));
     const double3 p = pos(j);
-    return make_float4(__fmul_rn(__int2float_rn(encode_q(p.x, b.qlo[0], b.qinv[0]) - ox), s0),
-                       __fmul_rn(__int2float_rn(encode_q(p.y, b.qlo[1], b.qinv[1]) - oy), s1),
-                       __fmul_rn(__int2float_rn(encode_q(p.z, b.qlo[2], b.qinv[2]) - oz), s2),
+    return make_float4(coord(p.x, cx, b.qlo[0], b.qinv[0], ox, s0, b.periodic[0], b.cs[0]),
+                       coord(p.y, cy, b.qlo[1], b.qinv[1], oy, s1, b.periodic[1], b.cs[1]),
+                       coord(p.z, cz, b.qlo[2], b.qinv[2], oz, s2, b.periodic[2], b.cs[2]),
                        __int_as_float(j));
   };
   const int c0 = s_pre[13], ncen = s_pre[14] - s_pre[13];  // center = slot 13
@@ -304,7 +319,9 @@ __device__ __forceinline__ void build_cell_rows(
       unsigned m = __ballot_sync(0xffffffffu, other && r2f < lo_f);
       // Candidates inside the filter's band go to the exact FP64 test:
       // rare, so the warp enters that path only when some lane needs it.
-      const bool band = other && r2f >= lo_f && r2f <= hi_f;
+      // (Written with negations so that a NaN r^2 -- a far record -- lands
+      // in the band.)
+      const bool band = other && !(r2f < lo_f) && !(r2f > hi_f);
       if (__any_sync(0xffffffffu, band)) {
         const bool ok = band && exact_within(pos, i, j, rl2, b.L[0], b.L[1], b.L[2],
                                              b.halfL[0], b.halfL[1], b.halfL[2],
@@ -331,11 +348,13 @@ __device__ __forceinline__ void build_cell_rows(
     for (int k = threadIdx.x; k < total; k += kRowThreads) stage[k] = record(k);
     if (threadIdx.x == 0) stage[total] = sentinel;
     __syncthreads();
+    // (a far record's NaN x ranks as +inf, so the ranks stay a permutation)
+    auto xkey = [](float x) { return x == x ? x : INFINITY; };
     for (int t = threadIdx.x; t < ncen; t += kRowThreads) {
-      const float xt = stage[c0 + t].x;
+      const float xt = xkey(stage[c0 + t].x);
       int rank = 0;
       for (int u = 0; u < ncen; ++u) {
-        const float xu = stage[c0 + u].x;
+        const float xu = xkey(stage[c0 + u].x);
         rank += (xu < xt || (xu == xt && u < t)) ? 1 : 0;
       }
       ss->s_order[rank] = static_cast<short>(t);
@@ -345,8 +364,10 @@ __device__ __forceinline__ void build_cell_rows(
     const int rlo = warp * ncen / kWarps, rhi = (warp + 1) * ncen / kWarps;
     if (rlo < rhi) {
       float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      bool far = false;
       for (int r = rlo + lane; r < rhi; r += 32) {
         const float4 q = stage[c0 + ss->s_order[r]];
+        far = far || !(q.x == q.x && q.y == q.y && q.z == q.z);
         mn[0] = fminf(mn[0], q.x), mn[1] = fminf(mn[1], q.y), mn[2] = fminf(mn[2], q.z);
         mx[0] = fmaxf(mx[0], q.x), mx[1] = fmaxf(mx[1], q.y), mx[2] = fmaxf(mx[2], q.z);
       }
@@ -357,6 +378,11 @@ __device__ __forceinline__ void build_cell_rows(
           mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
           mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
         }
+      }
+      // a far center atom: no bounding box, every candidate is kept
+      if (__any_sync(0xffffffffu, far)) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) mn[d] = -INFINITY, mx[d] = INFINITY;
       }
       unsigned short* const idx = ss->s_idx[warp];
       int cnt = 0;
@@ -400,8 +426,10 @@ __device__ __forceinline__ void build_cell_rows(
       } else {
         if (warp == 0) {
           float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+          bool far = false;
           for (int a = lane; a < ncen; a += 32) {
             const float4 r = record(c0 + a);
+            far = far || !(r.x == r.x && r.y == r.y && r.z == r.z);
             mn[0] = fminf(mn[0], r.x), mn[1] = fminf(mn[1], r.y), mn[2] = fminf(mn[2], r.z);
             mx[0] = fmaxf(mx[0], r.x), mx[1] = fmaxf(mx[1], r.y), mx[2] = fmaxf(mx[2], r.z);
           }
@@ -412,6 +440,11 @@ __device__ __forceinline__ void build_cell_rows(
               mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
               mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
             }
+          }
+          // a far center atom: no bounding box, every candidate is kept
+          if (__any_sync(0xffffffffu, far)) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) mn[d] = -INFINITY, mx[d] = INFINITY;
           }
           if (lane == 0) {
 #pragma unroll

@@ -96,6 +96,10 @@ class Scheduler {
   double last_window_ms() const { return last_window_ms_; }
   void kernel_times(double* avg_ms, long long* counts, int ncat) const;
   const int* atom_order() const { return order_.data(); }
+  // The current neighbor list in the caller's atom order, as dense CSR on
+  // the host (inspection; synchronises the stream).  counts[n] always;
+  // neighbors (capacity entries, nullable) the rows back to back.
+  void neighbor_list(int* counts, int* neighbors, long long capacity, long long* total) const;
   void device_state(void** pos4, double** vel, void** forces) {
     if (pos4) *pos4 = pos4_.data();
     if (vel) *vel = vel_.data();

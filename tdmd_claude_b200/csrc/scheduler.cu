@@ -604,6 +604,37 @@ void Scheduler::reorder_by_cell() {
   cells_from_upload_ = true;
 }
 
+void Scheduler::neighbor_list(int* counts, int* neighbors, long long capacity,
+                              long long* total) const {
+  TDMD_REQUIRE(initialized_, "no neighbor list yet: call run_until first");
+  TDMD_REQUIRE(counts, "counts is null");
+  const size_t n = static_cast<size_t>(n_);
+  std::vector<int> cnt(n), ord(n), rows(n * static_cast<size_t>(cap_));
+  TDMD_CU(cudaMemcpyAsync(cnt.data(), cnt_.data(), n * sizeof(int), cudaMemcpyDeviceToHost,
+                          stream_));
+  TDMD_CU(cudaMemcpyAsync(ord.data(), order_.data(), n * sizeof(int), cudaMemcpyDeviceToHost,
+                          stream_));
+  if (neighbors && !rows.empty())
+    TDMD_CU(cudaMemcpyAsync(rows.data(), nbr_.data(), rows.size() * sizeof(int),
+                            cudaMemcpyDeviceToHost, stream_));
+  TDMD_CU(cudaStreamSynchronize(stream_));
+  // internal atom k is the caller's atom ord[k]; its row holds internal indices
+  std::vector<long long> off(n + 1, 0);
+  for (size_t k = 0; k < n; ++k) {
+    TDMD_REQUIRE(cnt[k] <= cap_, "neighbor rows overflowed their capacity");
+    counts[ord[k]] = cnt[k];
+  }
+  for (size_t i = 0; i < n; ++i) off[i + 1] = off[i] + counts[i];
+  if (total) *total = off[n];
+  if (!neighbors) return;
+  TDMD_REQUIRE(capacity >= off[n], "neighbor capacity too small");
+  for (size_t k = 0; k < n; ++k) {
+    const int* row = rows.data() + k * static_cast<size_t>(cap_);
+    int* out = neighbors + off[static_cast<size_t>(ord[k])];
+    for (int t = 0; t < cnt[k]; ++t) out[t] = ord[static_cast<size_t>(row[t])];
+  }
+}
+
 void Scheduler::download(double* x, double* v, void* f, int* types, int* ids, int natoms) const {
   TDMD_REQUIRE(uploaded_, "download before upload");
   TDMD_REQUIRE(natoms >= 0 && natoms <= n_, "natoms out of range");
@@ -1472,6 +1503,16 @@ int32_t tdmd_sched_atom_order(const tdmd_sched* s, const int32_t** d_order) {
   return guarded([&] {
     TDMD_REQUIRE(s && d_order, "null argument");
     *d_order = s->s->atom_order();
+  });
+}
+
+int32_t tdmd_sched_neighbor_list(const tdmd_sched* s, int32_t* counts, int32_t* neighbors,
+                                 int64_t capacity, int64_t* total) {
+  return guarded([&] {
+    TDMD_REQUIRE(s, "null handle");
+    long long t = 0;
+    s->s->neighbor_list(counts, neighbors, capacity, &t);
+    if (total) *total = t;
   });
 }
 

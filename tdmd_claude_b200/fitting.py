@@ -96,6 +96,88 @@ class ForceMatch:
         return f.cpu().numpy().reshape(self.nsnap, self.natoms, 3)
 
 
+def snapshot_shard(nsnap: int, rank: int, world: int) -> range:
+    """The contiguous, balanced slice of snapshot indices that `rank` of
+    `world` owns (the first nsnap % world ranks take one more)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    base, extra = divmod(int(nsnap), world)
+    start = rank * base + min(rank, extra)
+    return range(start, start + base + (1 if rank < extra else 0))
+
+
+class ShardedForceMatch:
+    """Force matching sharded by snapshot over a process group.
+
+    Each rank evaluates the loss and gradient of its own snapshots (a
+    ForceMatch, or any object with the same morse / eam methods, on the
+    rank's shard).  The loss is a mean over all atoms of all snapshots, so
+    the global loss and gradient are the shard values weighted by
+    w_r = nsnap_r / nsnap, summed over ranks: one all_reduce(sum) of the
+    packed vector w_r [L_r, gradient_r] per evaluation (NCCL on GPUs, gloo
+    on CPU tensors).  Predicted forces stay per shard.  The morse / eam
+    methods take the same arguments as ForceMatch's, so MorseLoss / EamLoss
+    (and adam_fit) run unchanged on top of it; every rank must make the same
+    calls in the same order.
+
+    No reference counterpart (the reference computes no gradients); its
+    only multi-rank reduction is the scalar MPI_Allreduce of the distributed
+    scheduler (src/scheduler/distributed_pipeline_scheduler.cu:432,453)."""
+
+    def __init__(self, local, nsnap_local: int, nsnap_total: int, dist=None, group=None):
+        self.local = local
+        self.nsnap_local = int(nsnap_local)
+        self.nsnap_total = int(nsnap_total)
+        self.weight = self.nsnap_local / self.nsnap_total
+        self.dist = dist
+        self.group = group
+
+    @classmethod
+    def from_snapshots(cls, positions, types, box: Box, cutoff: float, precision="fp64",
+                       dist=None, group=None):
+        """All ranks pass the same snapshots[nsnap, n, 3] (and types); each
+        builds a ForceMatch on its own shard only."""
+        pos = np.asarray(positions, np.float64)
+        nsnap, n = pos.shape[0], pos.shape[1]
+        rank = dist.get_rank(group) if dist is not None else 0
+        world = dist.get_world_size(group) if dist is not None else 1
+        sh = snapshot_shard(nsnap, rank, world)
+        if len(sh) == 0:
+            raise ValueError("more ranks than snapshots")
+        typ = np.asarray(types, np.int32).reshape(-1, n)
+        typ = typ[sh.start:sh.stop] if typ.shape[0] == nsnap else typ
+        fm = ForceMatch(pos[sh.start:sh.stop], typ, box, cutoff, precision)
+        return cls(fm, len(sh), nsnap, dist, group)
+
+    def set_targets(self, targets_local):
+        """Targets of this rank's snapshots only ([nsnap_local, n, 3])."""
+        self.local.set_targets(targets_local)
+
+    def _reduce(self, loss, grads):
+        import torch
+        parts = [loss.reshape(-1)] + [g.reshape(-1) for g in grads if g is not None]
+        buf = torch.cat(parts) * self.weight
+        if self.dist is not None:
+            self.dist.all_reduce(buf, op=self.dist.ReduceOp.SUM, group=self.group)
+        off = 0
+        for t in [loss] + [g for g in grads if g is not None]:
+            k = t.numel()
+            t.copy_(buf[off:off + k].reshape(t.shape))
+            off += k
+
+    def morse(self, params, loss, grad=None, forces=None):
+        self.local.morse(params, loss, grad, forces)
+        self._reduce(loss, [grad])
+
+    def eam(self, tables: dict, F, rho, phi, loss, gF=None, grho=None, gphi=None, forces=None):
+        self.local.eam(tables, F, rho, phi, loss, gF, grho, gphi, forces)
+        self._reduce(loss, [gF, grho, gphi])
+
+    def close(self):
+        if hasattr(self.local, "close"):
+            self.local.close()
+
+
 def _autograd():
     import torch
 

@@ -1,133 +1,102 @@
-"""File formats around the path: LAMMPS `atomic` data files and setfl.
+"""File formats around the path, through the library's native readers and
+writers (tdmd_read_lammps_data, tdmd_write_lammps_data,
+tdmd_read_force_dump, tdmd_write_force_dump, tdmd_write_setfl):
 
-* write_lammps_data / read_lammps_data follow read_lammps_data
-  (src/io/lammps_data_reader.cpp:33-204): header counts and box, Masses,
-  Atoms (id type x y z, stored at index id-1), optional Velocities.
-* write_setfl writes the DYNAMO setfl layout that EamAlloy::read_setfl
-  (src/potentials/eam_alloy.cpp:90-192) reads: 3 comment lines, element
-  line, grid line, per element a header + F + rho, then r*phi per pair i<=j.
-* write_force_dump writes `dump custom id type x y z fx fy fz`
-  (src/drivers/tdmd_main.cpp:65-95).
+* read_lammps_data / write_lammps_data: LAMMPS `atomic` data files as
+  read_lammps_data (src/io/lammps_data_reader.cpp:33-204) reads them --
+  header counts and box, Masses, Atoms (id type x y z, stored at index
+  id-1), optional Velocities.
+* write_setfl: the DYNAMO setfl layout EamAlloy::read_setfl
+  (src/potentials/eam_alloy.cpp:90-192) reads.
+* write_force_dump / read_force_dump: `dump custom id type x y z fx fy fz`
+  (src/drivers/tdmd_main.cpp:65-95, src/io/dump_reader.cpp:15-55).
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 
+from ._lib import TDMD_FP64, TDMD_MIXED, Box, call, lib
 from .workloads import EamTables, System
 
 
+def _cptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
 def write_setfl(path: str, t: EamTables, comment: str = "analytic EAM") -> None:
-    with open(path, "w") as f:
-        f.write(f"# {comment}\n# generated by tdmd_claude_b200.io.write_setfl\n#\n")
-        f.write(f"{t.ntypes} " + " ".join(t.elements) + "\n")
-        f.write(f"{t.nrho} {t.drho:.17g} {t.nr} {t.dr:.17g} {t.cutoff:.17g}\n")
+    from .api import EamAlloy
+    e = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    masses = np.ascontiguousarray(t.masses, np.float64)
+    call("tdmd_write_setfl", path.encode(), e.handle, comment.encode(), _cptr(masses),
+         " ".join(t.elements).encode())
 
-        def block(vals):
-            for k in range(0, len(vals), 5):
-                f.write(" ".join(f"{v:.17g}" for v in vals[k:k + 5]) + "\n")
 
-        for i in range(t.ntypes):
-            f.write(f"{i + 1} {t.masses[i]:.6f} 0.0 fcc\n")
-            block(t.F[i])
-            block(t.rho[i])
-        for p in range(t.rphi.shape[0]):
-            block(t.rphi[p])
+def write_eam_setfl(path: str, eam, comment: str | None = None) -> None:
+    """An EamAlloy's tables (a setfl read keeps its own comment and element
+    header lines unless comment is given)."""
+    call("tdmd_write_setfl", path.encode(), eam.handle, comment.encode() if comment else None,
+         None, None)
 
 
 def write_lammps_data(path: str, s: System, title: str = "tdmd_claude_b200 data") -> None:
     ntypes = s.masses.size - 1
-    with open(path, "w") as f:
-        f.write(f"{title}\n\n{s.n} atoms\n{ntypes} atom types\n\n")
-        for a, (lo, hi) in enumerate(zip(s.lo, s.hi)):
-            ax = "xyz"[a]
-            f.write(f"{lo:.17g} {hi:.17g} {ax}lo {ax}hi\n")
-        f.write("\nMasses\n\n")
-        for t in range(1, ntypes + 1):
-            f.write(f"{t} {s.masses[t]:.17g}\n")
-        f.write("\nAtoms # atomic\n\n")
-        for i in range(s.n):
-            x, y, z = s.positions[i]
-            f.write(f"{s.ids[i]} {s.types[i]} {x:.17g} {y:.17g} {z:.17g}\n")
-        f.write("\nVelocities\n\n")
-        for i in range(s.n):
-            vx, vy, vz = s.velocities[i]
-            f.write(f"{s.ids[i]} {vx:.17g} {vy:.17g} {vz:.17g}\n")
+    pos = np.ascontiguousarray(s.positions, np.float64)
+    vel = np.ascontiguousarray(s.velocities, np.float64) if s.velocities is not None else None
+    typ = np.ascontiguousarray(s.types, np.int32)
+    ids = np.ascontiguousarray(s.ids, np.int32)
+    m = np.ascontiguousarray(s.masses, np.float64)
+    box = Box.make(s.lo, s.hi)
+    call("tdmd_write_lammps_data", path.encode(), title.encode(), int(s.n), int(ntypes),
+         C.byref(box), _cptr(pos), _cptr(vel), _cptr(typ), _cptr(ids), _cptr(m))
 
 
 def read_lammps_data(path: str) -> System:
-    with open(path) as f:
-        lines = f.read().splitlines()
-    natoms = ntypes = 0
-    lo = [0.0] * 3
-    hi = [0.0] * 3
-    k = 1
-    while k < len(lines):
-        t = lines[k].strip()
-        if t in ("Atoms", "Velocities", "Masses") or t.startswith("Atoms "):
-            break
-        if "atom types" in t:
-            ntypes = int(t.split()[0])
-        elif "atoms" in t:
-            natoms = int(t.split()[0])
-        for a, ax in enumerate("xyz"):
-            if f"{ax}lo {ax}hi" in t:
-                p = t.split()
-                lo[a], hi[a] = float(p[0]), float(p[1])
-        k += 1
-    if natoms <= 0:
-        raise ValueError("no atoms in data file")
-    pos = np.zeros((natoms, 3))
-    vel = np.zeros((natoms, 3))
-    types = np.zeros(natoms, np.int32)
-    ids = np.zeros(natoms, np.int32)
-    masses = np.ones(ntypes + 1)
-    while k < len(lines):
-        sec = lines[k].split("#")[0].strip()
-        k += 1
-        if sec not in ("Masses", "Atoms", "Velocities"):
-            continue
-        count = ntypes if sec == "Masses" else natoms
-        got = 0
-        while got < count and k < len(lines):
-            p = lines[k].split()
-            k += 1
-            if not p:
-                continue
-            if sec == "Masses":
-                masses[int(p[0])] = float(p[1])
-            elif sec == "Atoms":
-                i = int(p[0]) - 1
-                ids[i], types[i] = int(p[0]), int(p[1])
-                pos[i] = [float(p[2]), float(p[3]), float(p[4])]
-            else:
-                i = int(p[0]) - 1
-                vel[i] = [float(p[1]), float(p[2]), float(p[3])]
-            got += 1
-    return System(pos, vel, types, ids, masses, tuple(lo), tuple(hi))
+    h = C.c_void_p()
+    call("tdmd_read_lammps_data", path.encode(), C.byref(h))
+    try:
+        n, nt, box = C.c_int64(), C.c_int32(), Box()
+        pp = [C.c_void_p() for _ in range(5)]
+        call("tdmd_system_get", h, C.byref(n), C.byref(nt), C.byref(box),
+             *[C.byref(p) for p in pp])
+        N, T = n.value, nt.value
+
+        def arr(p, count, ct, dtype):
+            return np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), shape=(count,)).astype(dtype)
+
+        pos = arr(pp[0], 3 * N, C.c_double, np.float64).reshape(N, 3)
+        vel = arr(pp[1], 3 * N, C.c_double, np.float64).reshape(N, 3)
+        typ = arr(pp[2], N, C.c_int32, np.int32)
+        ids = arr(pp[3], N, C.c_int32, np.int32)
+        mas = arr(pp[4], T + 1, C.c_double, np.float64)
+        return System(pos, vel, typ, ids, mas, tuple(box.lo), tuple(box.hi))
+    finally:
+        lib().tdmd_system_destroy(h)
 
 
 def write_force_dump(path: str, s: System, forces: np.ndarray, step: int = 0) -> None:
-    with open(path, "w") as f:
-        f.write(f"ITEM: TIMESTEP\n{step}\nITEM: NUMBER OF ATOMS\n{s.n}\n")
-        f.write("ITEM: BOX BOUNDS pp pp pp\n")
-        for lo, hi in zip(s.lo, s.hi):
-            f.write(f"{lo:.17g} {hi:.17g}\n")
-        f.write("ITEM: ATOMS id type x y z fx fy fz\n")
-        for i in range(s.n):
-            x, y, z = s.positions[i]
-            fx, fy, fz = forces[i]
-            f.write(f"{s.ids[i]} {s.types[i]} {x:.17g} {y:.17g} {z:.17g} "
-                    f"{fx:.17g} {fy:.17g} {fz:.17g}\n")
+    f = np.ascontiguousarray(forces)
+    prec = TDMD_MIXED if f.dtype == np.float32 else TDMD_FP64
+    f = f if prec == TDMD_MIXED else f.astype(np.float64)
+    pos = np.ascontiguousarray(s.positions, np.float64)
+    typ = np.ascontiguousarray(s.types, np.int32)
+    ids = np.ascontiguousarray(s.ids, np.int32)
+    box = Box.make(s.lo, s.hi)
+    call("tdmd_write_force_dump", path.encode(), int(step), int(s.n), C.byref(box), _cptr(ids),
+         _cptr(typ), _cptr(pos), _cptr(f), prec)
 
 
 def read_force_dump(path: str):
-    """(ids, types, positions, forces) of a `id type x y z fx fy fz` dump."""
-    with open(path) as f:
-        lines = f.read().splitlines()
-    k = lines.index("ITEM: NUMBER OF ATOMS") + 1
-    n = int(lines[k])
-    start = next(i for i, l in enumerate(lines) if l.startswith("ITEM: ATOMS")) + 1
-    rows = np.array([[float(x) for x in l.split()] for l in lines[start:start + n]])
-    order = np.argsort(rows[:, 0])
-    rows = rows[order]
-    return rows[:, 0].astype(np.int32), rows[:, 1].astype(np.int32), rows[:, 2:5], rows[:, 5:8]
+    """(ids, types, positions, forces) of a `id type x y z fx fy fz` dump,
+    sorted by id."""
+    n = C.c_int64()
+    call("tdmd_read_force_dump", path.encode(), C.byref(n), 0, None, None, None, None)
+    N = n.value
+    ids = np.zeros(N, np.int32)
+    typ = np.zeros(N, np.int32)
+    pos = np.zeros((N, 3), np.float64)
+    frc = np.zeros((N, 3), np.float64)
+    call("tdmd_read_force_dump", path.encode(), C.byref(n), N, _cptr(ids), _cptr(typ),
+         _cptr(pos), _cptr(frc))
+    return ids, typ, pos, frc

@@ -49,3 +49,24 @@ def sum_over_ranks(value: float, dist=None, device=None) -> float:
                      device=device if device is not None else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def gather_by_replica(local_values, mine, nrep: int, dist=None) -> list:
+    """Per-replica results of every rank, back in replica order: rank r
+    holds local_values[k] for replica mine[k] (its LPT shard); returns the
+    list of all nrep results (one all_gather_object of the (index, value)
+    pairs; the local list itself without a process group)."""
+    pairs = list(zip([int(i) for i in mine], local_values))
+    if dist is not None:
+        allp = [None] * dist.get_world_size()
+        dist.all_gather_object(allp, pairs)
+        pairs = [pv for part in allp for pv in part]
+    out = [None] * int(nrep)
+    for i, v in pairs:
+        if out[i] is not None:
+            raise ValueError(f"replica {i} reported twice")
+        out[i] = v
+    if any(v is None for v in out):
+        raise ValueError("a replica is missing from the shards")
+    return out
+

@@ -8,6 +8,7 @@ import os
 import shutil
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import golden
@@ -39,8 +40,12 @@ def test_cpp_layer_host_calls(tmp_path, define, precision):
     from tdmd_claude_b200 import workloads as W
     setfl = str(tmp_path / "cu.eam.alloy")
     TIO.write_setfl(setfl, W.cu_eam_tables())
+    s = W.morse_256()
+    data = str(tmp_path / "c0.data")
+    TIO.write_lammps_data(data, s)
     exe = _build(tmp_path, define)
-    out = subprocess.run([exe, setfl], check=True, capture_output=True, text=True).stdout
+    out = subprocess.run([exe, setfl, data, str(tmp_path / "out")], check=True,
+                         capture_output=True, text=True).stdout
     kv = dict(line.split(" ", 1) for line in out.strip().splitlines())
     assert int(kv["precision"]) == precision
     assert int(kv["rebuild"]) == 10 and abs(float(kv["skin"]) - 0.3) < 1e-7
@@ -49,4 +54,11 @@ def test_cpp_layer_host_calls(tmp_path, define, precision):
     tol = 0.0 if precision == 0 else 1e-7  # the mixed build returns a float
     assert abs(float(kv["scale0"]) - ref) <= tol
     assert float(kv["t_target"]) == 400.0
+    # masses are `real` as in the reference's SystemState: float in the mixed build
+    m1 = float(s.masses[1]) if precision == 0 else float(np.float32(s.masses[1]))
+    assert int(kv["natoms"]) == 256 and float(kv["mass1"]) == m1
+    assert float(kv["x0"]) == float(s.positions[0, 0])
+    assert int(kv["data_roundtrip"]) == 1
+    assert int(kv["dump_n"]) == 256 and float(kv["dump_fx0"]) == 1.5 and int(kv["dump_id0"]) == 1
+    assert abs(float(kv["setfl_cutoff"]) - 5.0) < 1e-6
     assert int(kv["error"]) != 0

@@ -117,6 +117,19 @@ def test_eam_trajectory_matches_oracle(cuda, oracle, precision):
     else:
         assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < 5e-4
         assert rel_rms(st.forces, r["forces"]) < 1e-4
+        # the force error itself, at the mixed path's own positions
+        ro = oe.forces(st.positions, sysm.types, sysm.lo, sysm.hi, 0.3)
+        assert rel_rms(st.forces, ro["forces"]) <= 1e-5
+
+
+def test_eam_mixed_step0_forces_vs_oracle(cuda, oracle):
+    """Mixed EAM forces at step 0 within the 1e-5 RMS bound of the FP64 oracle."""
+    s, sysm, t = _eam_setup("mixed")
+    s.run_until(0)
+    st = s.download()
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    r = oe.forces(sysm.positions, sysm.types, sysm.lo, sysm.hi, 0.3)
+    assert rel_rms(st.forces, r["forces"]) <= 1e-5
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -319,6 +332,100 @@ def test_eam_nonperiodic_matches_oracle(cuda, oracle, precision, periodic):
     else:
         assert np.abs(d).max() < 5e-4
         assert rel_rms(st.forces, r["forces"]) < 1e-4
+
+
+def _slab_with_far_atoms(ncell=5):
+    """ncell^3 Cu slab (z non-periodic, 8 A of vacuum) plus atoms far past the
+    z faces, where the cell list clamps them into the edge cells: one 2 Lz
+    out, a dimer (2.5 A apart) 3.3 Lz out, and one 4 Lz - 1 A above a
+    surface atom (a fixed-point frame of width 4 Lz would wrap it onto a
+    point 1 A from that atom)."""
+    from tdmd_claude_b200 import workloads as W
+    sysm = W.fcc_system(ncell, 3.615, 300.0, seed=34)
+    lo, hi = np.array(sysm.lo, float), np.array(sysm.hi, float)
+    lo[2] -= 8.0
+    hi[2] += 8.0
+    Lz = hi[2] - lo[2]
+    top = int(np.argmax(sysm.positions[:, 2]))
+    extra = np.array([[5.0, 6.0, hi[2] + 2.0 * Lz],
+                      [9.0, 9.0, hi[2] + 3.3 * Lz],
+                      [9.0, 9.0, hi[2] + 3.3 * Lz + 2.5],
+                      [sysm.positions[top, 0], sysm.positions[top, 1],
+                       sysm.positions[top, 2] + 4.0 * Lz - 1.0],
+                      [4.0, 3.0, lo[2] - 2.2 * Lz]])
+    pos = np.concatenate([sysm.positions, extra])
+    vel = np.concatenate([sysm.velocities, np.zeros_like(extra)])
+    types = np.ones(len(pos), np.int32)
+    return pos, vel, types, sysm.masses, lo, hi
+
+
+@pytest.mark.parametrize("ncell", [5, 6])
+def test_far_atoms_nonperiodic_lists_bit_exact(cuda, oracle, ncell):
+    """Atoms far outside a non-periodic axis: the free-function cell and
+    neighbor lists equal the oracle's (neighbor_list.cpp:50-64 takes every
+    delta in FP64), including the far dimer's pair and no pair for the atom
+    whose wrapped fixed-point position would sit 1 A from a surface atom.
+    ncell 5 gives 3-cell periodic axes (minimum image re-applied in FP32),
+    6 gives 4 cells (staging with the bounding-box pruning)."""
+    from tdmd_claude_b200 import Box, DeviceCellList, DeviceNeighborList
+    pos, vel, types, masses, lo, hi = _slab_with_far_atoms(ncell)
+    per = (1, 1, 0)
+    d = cuda.as_tensor(pos, dtype=cuda.float64, device="cuda")
+    box = Box.make(lo, hi, per)
+    cl = DeviceCellList()
+    cl.build(d, len(pos), box, 5.3)
+    nc, atoms, offs, cnts, acell = cl.arrays()
+    enc, ecc, eco, eca, eac = oracle.cell_list(pos, lo, hi, 5.3, per)
+    assert np.array_equal(cnts, ecc) and np.array_equal(atoms, eca)
+    assert np.array_equal(acell, eac)
+    nl = DeviceNeighborList()
+    nl.build(d, len(pos), box, 5.0, 0.3)
+    c, o, nb = nl.host_csr()
+    ec, eo, enb = oracle.neighbor_list(pos, lo, hi, 5.0, 0.3, half=False, periodic=per)
+    assert np.array_equal(c, ec) and np.array_equal(o, eo) and np.array_equal(nb, enb)
+    n0 = len(pos) - 5
+    assert c[n0] == 0 and c[n0 + 3] == 0 and c[n0 + 4] == 0
+    assert list(nb[o[n0 + 1]:o[n0 + 1] + c[n0 + 1]]) == [n0 + 2]
+
+
+@pytest.mark.parametrize("ncell", [5, 6])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_far_atoms_nonperiodic_trajectory(cuda, oracle, precision, ncell):
+    """The same system through the scheduler: lists bit-exact at step 0 and
+    after two rebuilds, forces and a 20-step trajectory against the oracle."""
+    from tdmd_claude_b200 import Box, EamAlloy, FastPipelineScheduler, make_config
+    from tdmd_claude_b200 import workloads as W
+    pos, vel, types, masses, lo, hi = _slab_with_far_atoms(ncell)
+    per = (1, 1, 0)
+    t = W.cu_eam_tables()
+    eam = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    s = FastPipelineScheduler(Box.make(lo, hi, per), len(pos), eam,
+                              make_config(r_skin=0.3, precision=precision, lanes_per_atom=2))
+    s.upload(pos, vel, None, types, None, masses)
+    oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    s.run_until(0)
+    c, o, nb = s.neighbor_list()
+    ec, eo, enb = oracle.neighbor_list(pos, lo, hi, 5.0, 0.3, half=False, periodic=per)
+    assert np.array_equal(c, ec) and np.array_equal(nb, enb)
+    r0 = oe.forces(pos, types, lo, hi, 0.3, periodic=per)
+    tol = 1e-10 if precision == "fp64" else 1e-5
+    assert rel_rms(s.download().forces, r0["forces"]) <= tol
+    s.run_until(20)
+    st = s.download()
+    c, o, nb = s.neighbor_list()
+    ec, eo, enb = oracle.neighbor_list(st.positions, lo, hi, 5.0, 0.3, half=False, periodic=per)
+    assert np.array_equal(c, ec) and np.array_equal(nb, enb)
+    r = oracle.md_run(pos, vel, types, masses, lo, hi, 0.001, 0.3, 10, [20], eam=oe,
+                      periodic=per)
+    d = _wrap_diff(st.positions, r["pos"], hi - lo)
+    if precision == "fp64":
+        assert np.abs(d).max() < 1e-10
+        assert rel_rms(st.forces, r["forces"]) < 1e-9
+    else:
+        assert np.abs(d).max() < 5e-4
+        ro = oe.forces(st.positions, types, lo, hi, 0.3, periodic=per)
+        assert rel_rms(st.forces, ro["forces"]) <= 1e-5
+    s.close()
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

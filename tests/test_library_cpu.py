@@ -248,3 +248,160 @@ def test_two_element_setfl_parses():
             c = eam.coeffs(kind, k)
             n = len(c) // 4
             assert np.allclose(c[:n], tab[k][:n], rtol=1e-14, atol=1e-14), (kind, k)
+
+
+# ---------------------------------------------------------------------------
+# Native file formats (tdmd_read_lammps_data & co.) against the reference's
+# own readers, compiled from its sources into oracle/_ref.
+# ---------------------------------------------------------------------------
+def _ref_read(ref_lib, path):
+    import ctypes as C
+    n, nt = C.c_int64(), C.c_int32()
+    lo, hi = np.zeros(3), np.zeros(3)
+    assert ref_lib.ref_read_data(path.encode(), C.byref(n), C.byref(nt), lo, hi, None, None,
+                                 None, None, None) == 0
+    N = n.value
+    pos, vel = np.zeros((N, 3)), np.zeros((N, 3))
+    ty, ids, m = np.zeros(N, np.int32), np.zeros(N, np.int32), np.zeros(nt.value + 1)
+    assert ref_lib.ref_read_data(path.encode(), C.byref(n), C.byref(nt), lo, hi,
+                                 pos.ctypes.data, vel.ctypes.data, ty.ctypes.data,
+                                 ids.ctypes.data, m.ctypes.data) == 0
+    return pos, vel, ty, ids, m, lo, hi
+
+
+def _data_files(tmp):
+    """The reference's own data fixtures (where its tree is present) and a
+    file written here with velocities, blank lines inside sections and a
+    comment after the Atoms keyword."""
+    from conftest import REF_TREE
+    out = []
+    if REF_TREE is not None:
+        for f in ("tests/data/cu_fcc_256.data", "tests/data/cu_fcc_32.data",
+                  "tests/data/4atoms.data"):
+            p = os.path.join(REF_TREE, f)
+            if os.path.exists(p):
+                out.append(p)
+    p = os.path.join(tmp, "odd.data")
+    with open(p, "w") as f:
+        f.write("odd layout\n\n3 atoms\n2 atom types\n\n0 10 xlo xhi\n-1 9 ylo yhi\n"
+                "0.5 7.5 zlo zhi\n\nMasses\n\n1 63.546\n\n2 58.69\n\nAtoms # atomic\n\n"
+                "3 2 1.25 2.5 3.75\n1 1 0.1 0.2 0.3\n\n2 1 4 5 6\n\nVelocities\n\n"
+                "2 0.5 -0.5 0.25\n1 1e-3 2e-3 3e-3\n3 -1 -2 -3\n")
+    out.append(p)
+    return out
+
+
+def test_native_data_reader_equals_reference(L, ref_lib, tmp_path):
+    """tdmd_read_lammps_data gives the reference read_lammps_data's arrays
+    (lammps_data_reader.cpp:33-204), bit for bit."""
+    from tdmd_claude_b200 import io as TIO
+    for p in _data_files(str(tmp_path)):
+        s = TIO.read_lammps_data(p)
+        pos, vel, ty, ids, m, lo, hi = _ref_read(ref_lib, p)
+        assert np.array_equal(s.positions, pos), p
+        assert np.array_equal(s.velocities, vel), p
+        assert np.array_equal(s.types, ty) and np.array_equal(s.ids, ids), p
+        assert np.array_equal(s.masses, m), p
+        assert np.array_equal(s.lo, lo) and np.array_equal(s.hi, hi), p
+
+
+def test_native_data_roundtrip_and_reference_reads_it(L, ref_lib, tmp_path):
+    from tdmd_claude_b200 import io as TIO
+    from tdmd_claude_b200 import workloads as W
+    s = W.ternary(3, seed=5)
+    p = str(tmp_path / "t.data")
+    TIO.write_lammps_data(p, s)
+    r = TIO.read_lammps_data(p)
+    for a, b in ((r.positions, s.positions), (r.velocities, s.velocities), (r.types, s.types),
+                 (r.ids, s.ids), (r.masses, s.masses)):
+        assert np.array_equal(a, b)
+    pos, vel, ty, ids, m, lo, hi = _ref_read(ref_lib, p)
+    assert np.array_equal(pos, s.positions) and np.array_equal(vel, s.velocities)
+    assert np.array_equal(ty, s.types) and np.array_equal(m, s.masses)
+
+
+@pytest.mark.parametrize("body,what", [
+    ("t\n\n2 atoms\n1 atom types\n0 1 xlo xhi\n0 1 ylo yhi\n\nAtoms\n\n1 1 0 0 0\n2 1 0 0 0\n",
+     "incomplete box"),
+    ("t\n\n2 atoms\n1 atom types\n0 1 xlo xhi\n0 1 ylo yhi\n0 1 zlo zhi\n\nAtoms\n\n1 1 0 0 0\n",
+     "premature end"),
+    ("t\n\n2 atoms\n1 atom types\n0 1 xlo xhi\n0 1 ylo yhi\n0 1 zlo zhi\n\nAtoms\n\n"
+     "1 1 0 0 0\n2 1 0 x 0\n", "bad Atoms line"),
+    ("t\n\n2 atoms\n1 atom types\n0 1 xlo xhi\n0 1 ylo yhi\n0 1 zlo zhi\n\nAtoms\n\n"
+     "1 1 0 0 0\n7 1 0 0 0\n", "out of range"),
+    ("t\n\n2 atoms\n1 atom types\n0 1 xlo xhi\n0 1 ylo yhi\n0 1 zlo zhi\n\nMasses\n\n1 2.0\n",
+     "no Atoms section"),
+    ("t\n\n0 atoms\n", "invalid atom count"),
+])
+def test_native_data_reader_rejects_malformed(L, tmp_path, body, what):
+    from tdmd_claude_b200 import TdmdError
+    from tdmd_claude_b200 import io as TIO
+    p = str(tmp_path / "bad.data")
+    with open(p, "w") as f:
+        f.write(body)
+    with pytest.raises(TdmdError) as ei:
+        TIO.read_lammps_data(p)
+    assert ei.value.code == 4 and what in str(ei.value)
+
+
+def test_native_force_dump_roundtrip_and_reference_dump(L, tmp_path):
+    """Dumps written natively read back exactly (17 digits; float forces
+    widened exactly); the reference's committed LAMMPS dump reads into the
+    values of the golden fixture made from it."""
+    from conftest import REF_TREE
+    from tdmd_claude_b200 import io as TIO
+    from tdmd_claude_b200 import workloads as W
+    s = W.morse_256()
+    rng = np.random.default_rng(1)
+    for dt in (np.float64, np.float32):
+        f = rng.standard_normal((s.n, 3)).astype(dt)
+        p = str(tmp_path / f"d_{np.dtype(dt).name}.dump")
+        # shuffled ids: the reader sorts by id
+        perm = rng.permutation(s.n)
+        sp = W.System(s.positions[perm], s.velocities[perm], s.types[perm], s.ids[perm],
+                      s.masses, s.lo, s.hi)
+        TIO.write_force_dump(p, sp, f[perm], step=42)
+        ids, ty, pos, fr = TIO.read_force_dump(p)
+        assert np.array_equal(ids, s.ids) and np.array_equal(ty, s.types)
+        assert np.array_equal(pos, s.positions) and np.array_equal(fr, f.astype(np.float64))
+        with open(p) as fh:
+            assert fh.read().startswith("ITEM: TIMESTEP\n42\nITEM: NUMBER OF ATOMS\n256\n")
+    if REF_TREE is not None:
+        p = os.path.join(REF_TREE, "verifylab/cases/run0-force-match/forces_morse.dump")
+        if os.path.exists(p):
+            ids, ty, pos, fr = TIO.read_force_dump(p)
+            assert np.array_equal(fr, np.array(golden("run0_morse_256.json")["lammps_forces"]))
+
+
+def test_native_setfl_writer_roundtrip(L, mishin_setfl, tmp_path):
+    """A read setfl written back natively reads again to the same tables and
+    spline coefficients (the Mishin Cu file), and the reference's
+    EamAlloy::read_setfl reads the written file to the same forces."""
+    from tdmd_claude_b200 import EamAlloy
+    from tdmd_claude_b200 import io as TIO
+    a = EamAlloy().read_setfl(mishin_setfl)
+    p = str(tmp_path / "again.eam.alloy")
+    TIO.write_eam_setfl(p, a)
+    b = EamAlloy().read_setfl(p)
+    assert a.info() == b.info()
+    for kind in (0, 1, 2):
+        assert np.array_equal(a.coeffs(kind, 0), b.coeffs(kind, 0))
+    with open(p) as f, open(mishin_setfl) as g:
+        assert f.readline() == g.readline()      # comment lines kept
+    from oracle import oracle as O
+    R = O.ref()
+    if R is not None:
+        import ctypes as C
+        m = golden("run0_morse_256.json")
+        pos = np.array(m["positions"])
+        out = []
+        for path in (mishin_setfl, p):
+            h = R.ref_eam_load(path.encode())
+            f = np.zeros_like(pos)
+            pe = R.ref_eam_forces(h, pos.reshape(-1), np.ones(256, np.int32), 256,
+                                  np.array(m["lo"]), np.array(m["hi"]), np.ones(3, np.int32),
+                                  1.0, f.reshape(-1))
+            R.ref_eam_free(h)
+            out.append((pe, f))
+        assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
+        _ = C
