@@ -60,6 +60,10 @@ using ForceVec = Vec3D;
 constexpr int32_t kForcePrecision = TDMD_FP64;
 #endif
 
+// --- src/core/constants.hpp:15,28 (metal units) -----------------------------
+inline constexpr real kBoltzmann = real{8.617333262e-5};
+inline constexpr real kMvv2e = real{1.0364269e-4};
+
 // --- src/core/error.hpp -----------------------------------------------------
 class Error : public std::runtime_error {
  public:

@@ -65,7 +65,7 @@ def build(ref: bool | None = None) -> None:
     if ref:
         if ref_tree is None:
             raise RuntimeError("reference tree not found: set TDMD_REFERENCE_TREE")
-        targets += ["ref", "refgpu"]
+        targets += ["ref", "refgpu", "dropin"]
     args = [f"REF={ref_tree}"] if ref_tree else []
     subprocess.run(["make", "-s", "-C", _HERE, *args, *targets], check=True)
 

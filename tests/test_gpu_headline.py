@@ -9,9 +9,9 @@
   (test_device_neighbor_list.cu:16-128); FP64 forces, energy and virial
   agree to 1e-10 relative (test_device_eam.cu:24-92 with the FP64
   tolerance); mixed forces to 1e-5 RMS relative and energy to 1e-6, against
-  the oracle's FP64 values, not this library's FP64 path.  One 10-step
-  window (a rebuild, the fused kick + drift of the mixed path) follows the
-  oracle's scheduler loop.
+  the oracle's FP64 values, not this library's FP64 path.  A 10-step
+  window (the fused kick + drift of the mixed path) and the next step (the
+  first rebuild) follow the oracle's scheduler loop.
 * An equiatomic random ternary, 20^3 cells = 32 000 atoms, with the
   three-species analytic EAM of the 4 M-atom workload: the same checks.
 
@@ -115,15 +115,18 @@ def test_headline_scheduler_step0(cuda, headline, precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_headline_scheduler_window(cuda, oracle, headline, precision):
-    """One bench window (10 steps, the rebuild after the 10th drift) against
-    the oracle's restatement of the scheduler loop; the list of the rebuilt
-    state is compared too (the oracle's list of the scheduler's positions)."""
+    """One bench window of 10 steps, then the next step, whose drift is
+    followed by the first rebuild (maybe_rebuild_nlist: steps since the last
+    build reach rebuild_every), against the oracle's restatement of the
+    scheduler loop; the rebuilt list equals the oracle's list of the
+    scheduler's positions at that step."""
     s, t, oe, _, _ = headline
     sch = _sched(s, t, precision)
     sch.run_until(10)
+    sch.run_until(11)
     st = sch.download()
     r = oracle.md_run(s.positions, s.velocities, s.types, s.masses, s.lo, s.hi, 0.001, SKIN, 10,
-                      [10], eam=oe)
+                      [10, 11], eam=oe)
     L = np.array(s.hi) - np.array(s.lo)
     dx = np.abs(_wrap_diff(st.positions, r["pos"], L)).max()
     if precision == "fp64":
