@@ -221,6 +221,21 @@ int32_t tdmd_morse_compute_noalloc(const double* d_positions, void* d_forces, in
                                    const tdmd_morse_params* params, double* d_energy,
                                    double* d_virial, void* stream);
 
+/* The ID-ordered energy mode, the run-time form of the reference's
+ * TDMD_DETERMINISTIC_REDUCE build (src/core/determinism.hpp:20-24, ADR
+ * 0010; sum_per_atom_kernel, src/potentials/device_morse.cu:16-30).
+ * Process-wide, off by default.  While on, tdmd_morse_compute and
+ * tdmd_device_eam_compute in TDMD_FP64 that ask for an energy or a virial
+ * compute each atom's energy with the reference's per-atom arithmetic in
+ * neighbor-row order and add the atoms' energies to *d_energy one after
+ * another in atom-ID order (EAM: the embedding energies, then the pair
+ * halves), the virial likewise: the energies equal the reference's
+ * deterministic build bit for bit.  Slower (one thread per atom, one-thread
+ * sums).  Mixed precision and the scheduler keep their fixed-order block
+ * reductions, which are reproducible run to run. */
+int32_t tdmd_set_deterministic_reduce(int32_t on);
+int32_t tdmd_get_deterministic_reduce(int32_t* on);
+
 /* ------------------------------------------------------------------------ */
 /* File formats (host only).                                                */
 /* ------------------------------------------------------------------------ */

@@ -81,6 +81,18 @@ inline void check(int32_t rc) {
 inline void* stream_ptr(cudaStream_t s) { return reinterpret_cast<void*>(s); }
 }  // namespace detail
 
+// --- src/core/determinism.hpp:20-24 ----------------------------------------
+// The reference selects ID-ordered energy sums at build time
+// (kDeterministicReduce); here it is a process-wide run-time switch.
+inline void set_deterministic_reduce(bool on) {
+  detail::check(tdmd_set_deterministic_reduce(on ? 1 : 0));
+}
+inline bool deterministic_reduce() {
+  int32_t on = 0;
+  detail::check(tdmd_get_deterministic_reduce(&on));
+  return on != 0;
+}
+
 // --- src/core/box.hpp -------------------------------------------------------
 struct Box {
   Vec3D lo{0, 0, 0};

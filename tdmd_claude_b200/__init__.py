@@ -11,7 +11,8 @@ from .api import (DeviceCellList, DeviceEam, DeviceNeighborList, EamAlloy,  # no
                   device_compute_ke,
                   device_compute_vmax, device_drift, device_fused_full_kick_drift,
                   device_fused_half_kick_drift, device_half_kick, device_scale_velocities,
-                  device_zero_forces, make_config)
+                  device_zero_forces, deterministic_reduce, make_config,
+                  set_deterministic_reduce)
 from ._lib import (TDMD_FP64, TDMD_MIXED, TDMD_POT_EAM, TDMD_POT_MORSE, Box,  # noqa: F401
                    FastPipelineConfig, FastPipelineStats, MorseParams, TdmdError)
 
@@ -21,5 +22,6 @@ __all__ = [
     "compute_morse_gpu", "device_half_kick", "device_drift", "device_fused_half_kick_drift",
     "device_fused_full_kick_drift", "device_zero_forces", "device_compute_ke",
     "device_compute_vmax", "device_scale_velocities", "NoseHooverChain", "make_config",
+    "set_deterministic_reduce", "deterministic_reduce",
     "TDMD_FP64", "TDMD_MIXED", "TDMD_POT_MORSE", "TDMD_POT_EAM",
 ]

@@ -97,6 +97,8 @@ SIGNATURES = {
     "tdmd_eam_create": [_i32, _i32, _f64, _i32, _f64, _f64, _p, _p, _p, _pp],
     "tdmd_eam_destroy": [_p],
     "tdmd_eam_info": [_p, _pi32, _pi32, _pf64, _pi32, _pf64, _pf64],
+    "tdmd_set_deterministic_reduce": [_i32],
+    "tdmd_get_deterministic_reduce": [_pi32],
     "tdmd_read_lammps_data": [C.c_char_p, _pp],
     "tdmd_system_destroy": [_p],
     "tdmd_system_get": [_p, C.POINTER(_i64), _pi32, _p, _pp, _pp, _pp, _pp, _pp],

@@ -528,6 +528,18 @@ class DeviceNeighborList:
                 _dev_to_numpy(pn, tot, np.int32))
 
 
+def set_deterministic_reduce(on: bool = True) -> None:
+    """The ID-ordered energy mode (the reference's TDMD_DETERMINISTIC_REDUCE
+    build, src/core/determinism.hpp:20-24), process-wide."""
+    call("tdmd_set_deterministic_reduce", 1 if on else 0)
+
+
+def deterministic_reduce() -> bool:
+    v = C.c_int32()
+    call("tdmd_get_deterministic_reduce", C.byref(v))
+    return bool(v.value)
+
+
 def compute_morse_gpu(d_positions, d_forces, d_neighbors, d_offsets, d_counts, natoms, box: Box,
                       params: MorseParams, d_energy=None, d_virial=None, precision="fp64",
                       stream=None):

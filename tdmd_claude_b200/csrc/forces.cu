@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "eam_tables.cuh"
 #include "forces.cuh"
+#include "determinism.cuh"
 #include "launch.cuh"
 
 namespace tdmd_b200 {
@@ -296,6 +297,11 @@ struct tdmd_device_eam {
   EamDevTables tabs;
   DevArray<float> fp32;
   DevArray<double> fp64;
+  // the reference's flat layout, for the ID-ordered energy mode (built on
+  // its first use)
+  RefEamTables ref;
+  bool ref_ready = false;
+  tdmd_eam copy;  // the host tables, kept for the ID-ordered mode
 };
 
 namespace {
@@ -402,9 +408,15 @@ int32_t tdmd_morse_compute(const double* d_positions, void* d_forces, int32_t pr
     if (natoms == 0) return;
     TDMD_REQUIRE(d_positions && d_forces && d_offsets && d_counts, "null device array");
     cudaStream_t s = as_stream(stream);
+    const bool ev = d_energy || d_virial;
+    if (ev && precision == TDMD_FP64 && deterministic_reduce()) {
+      TDMD_REQUIRE(d_neighbors || natoms == 0, "null device array");
+      morse_id_ordered(d_positions, static_cast<double*>(d_forces), d_neighbors, d_offsets,
+                       d_counts, natoms, *box, *params, d_energy, d_virial, s);
+      return;
+    }
     const DevBox b = make_devbox(*box, 0.0);
     const NbrView nl = make_view(d_neighbors, d_offsets, d_counts);
-    const bool ev = d_energy || d_virial;
     const int lpa = default_lpa(natoms);
     const int nblk = force_blocks(natoms, lpa);
     Partials part(ev ? nblk : 0, s);
@@ -433,6 +445,7 @@ int32_t tdmd_device_eam_create(const tdmd_eam* eam, tdmd_device_eam** out) {
     auto* de = new tdmd_device_eam();
     try {
       de->tabs.upload(*eam, nullptr);
+      de->copy = *eam;
     } catch (...) {
       delete de;
       throw;
@@ -459,9 +472,18 @@ int32_t tdmd_device_eam_compute(tdmd_device_eam* de, const double* d_positions, 
     TDMD_REQUIRE(d_positions && d_forces && d_offsets && d_counts && d_types,
                  "null device array");
     cudaStream_t s = as_stream(stream);
+    const bool ev = d_energy || d_virial;
+    if (ev && precision == TDMD_FP64 && deterministic_reduce()) {
+      if (!de->ref_ready) {
+        de->ref.upload(de->copy);
+        de->ref_ready = true;
+      }
+      eam_id_ordered(de->ref, d_positions, static_cast<double*>(d_forces), d_types, d_neighbors,
+                     d_offsets, d_counts, natoms, *box, d_energy, d_virial, d_rho, d_fp, s);
+      return;
+    }
     const DevBox b = make_devbox(*box, 0.0);
     const NbrView nl = make_view(d_neighbors, d_offsets, d_counts);
-    const bool ev = d_energy || d_virial;
     const int lpa = default_lpa(natoms);
     const int nblk = force_blocks(natoms, lpa);
     // Density records [0, nblk) and force records [nblk, 2*nblk).
