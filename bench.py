@@ -759,9 +759,6 @@ def main():
                     help="neighbors per lane sweep for --kernels-only (EAM: default 2, the "
                          "autotuner's usual choice at 131,072 atoms; Morse replicas: autotuned "
                          "unless given)")
-    ap.add_argument("--pair-coeffs", type=int, default=0, choices=[0, 1, 2],
-                    help="single-type EAM passes for --kernels-only: 0 autotuned form "
-                         "(plain when the shape is fixed), 1 plain, 2 pair coefficients")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip timing the reference's own GPU scheduler (same-run context)")
     ap.add_argument("--no-fit", action="store_true",
@@ -814,7 +811,7 @@ def main():
                 kw = dict(t_target=300.0, t_period=0.1, nhc_length=3, energy_every=1,
                           energy_log_capacity=16)
             s32 = make_sched(sysm, eam, prec, lanes_per_atom=args.lanes or 4,
-                             nbr_batch=args.nbr_batch or 2, pair_coeffs=args.pair_coeffs, **kw)
+                             nbr_batch=args.nbr_batch or 2, **kw)
             s32.run_until(0)
             timed_windows(s32, args.steps, args.warmup, flush, torch, dist)
             s32.close()

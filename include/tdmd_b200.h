@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define TDMD_B200_ABI_VERSION 3
+#define TDMD_B200_ABI_VERSION 2
 
 typedef enum tdmd_status {
   TDMD_OK = 0,
@@ -97,13 +97,6 @@ typedef struct tdmd_fast_pipeline_config {
    * the autotuner (4 when it does not run), else 2 or 4.  Results are
    * bit-reproducible for a fixed (lanes_per_atom, nbr_batch) pair. */
   int32_t nbr_batch;
-  /* Single-type EAM: the density pass also stores each listed pair's
-   * phi'(r)/r and rho'(r)/r beside its neighbor index, and the force pass
-   * combines them with F' of both atoms instead of evaluating splines again
-   * ("pair coefficients").  0 = the autotuner times both forms and keeps
-   * the faster (the plain form when it does not run), 1 = plain, 2 = pair
-   * coefficients. */
-  int32_t pair_coeffs;
 } tdmd_fast_pipeline_config;
 
 /* FastPipelineStats, src/scheduler/fast_pipeline_scheduler.cuh:49-53, plus
@@ -121,7 +114,6 @@ typedef struct tdmd_fast_pipeline_stats {
   int32_t nbr_batch;
   int32_t density_lanes_per_atom;
   int32_t density_nbr_batch;
-  int32_t pair_coeffs;     /* 1 while the EAM passes use pair coefficients    */
 } tdmd_fast_pipeline_stats;
 
 /* ------------------------------------------------------------------------ */

@@ -571,7 +571,6 @@ struct FastPipelineConfig {
   i32 energy_every{0};
   i32 energy_log_capacity{0};
   i32 nbr_batch{0};  // neighbors per lane sweep: 0 = autotuned, else 2 or 4
-  i32 pair_coeffs{0};  // single-type EAM pair coefficients: 0 auto, 1 off, 2 on
 
   tdmd_fast_pipeline_config to_c() const {
     tdmd_fast_pipeline_config c;
@@ -592,7 +591,6 @@ struct FastPipelineConfig {
     c.energy_every = energy_every;
     c.energy_log_capacity = energy_log_capacity;
     c.nbr_batch = nbr_batch;
-    c.pair_coeffs = pair_coeffs;
     return c;
   }
 };

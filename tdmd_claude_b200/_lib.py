@@ -67,7 +67,7 @@ class FastPipelineConfig(C.Structure):
                 ("t_period", C.c_double), ("nhc_length", C.c_int32), ("adaptive_dt", C.c_int32),
                 ("dt_min", C.c_double), ("dt_max", C.c_double), ("c2", C.c_double),
                 ("energy_every", C.c_int32), ("energy_log_capacity", C.c_int32),
-                ("nbr_batch", C.c_int32), ("pair_coeffs", C.c_int32)]
+                ("nbr_batch", C.c_int32)]
 
 
 class FastPipelineStats(C.Structure):
@@ -76,7 +76,7 @@ class FastPipelineStats(C.Structure):
                 ("graph_launches", C.c_int64), ("nlist_retries", C.c_int64),
                 ("nlist_capacity", C.c_int64), ("lanes_per_atom", C.c_int32),
                 ("nbr_batch", C.c_int32), ("density_lanes_per_atom", C.c_int32),
-                ("density_nbr_batch", C.c_int32), ("pair_coeffs", C.c_int32)]
+                ("density_nbr_batch", C.c_int32)]
 
 
 _p = C.c_void_p

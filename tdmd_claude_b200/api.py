@@ -80,7 +80,7 @@ def _autotune(fn, handle):
 def make_config(dt=0.001, r_skin=1.0, rebuild_every=10, precision="fp64", use_graphs=True,
                 lanes_per_atom=0, t_target=0.0, t_period=0.1, nhc_length=3, adaptive_dt=False,
                 dt_min=0.0001, dt_max=0.002, c2=0.05, energy_every=0,
-                energy_log_capacity=0, nbr_batch=0, pair_coeffs=0) -> FastPipelineConfig:
+                energy_log_capacity=0, nbr_batch=0) -> FastPipelineConfig:
     """FastPipelineConfig{dt, r_skin, rebuild_every} plus this library's knobs."""
     cfg = FastPipelineConfig()
     lib().tdmd_fast_pipeline_config_default(C.byref(cfg))
@@ -93,7 +93,6 @@ def make_config(dt=0.001, r_skin=1.0, rebuild_every=10, precision="fp64", use_gr
     cfg.dt_min, cfg.dt_max, cfg.c2 = float(dt_min), float(dt_max), float(c2)
     cfg.energy_every, cfg.energy_log_capacity = int(energy_every), int(energy_log_capacity)
     cfg.nbr_batch = int(nbr_batch)
-    cfg.pair_coeffs = int(pair_coeffs)
     return cfg
 
 

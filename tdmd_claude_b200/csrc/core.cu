@@ -266,8 +266,6 @@ void tdmd_fast_pipeline_config_default(tdmd_fast_pipeline_config* cfg) {
   cfg->c2 = 0.05;
   cfg->energy_every = 0;
   cfg->energy_log_capacity = 0;
-  cfg->nbr_batch = 0;
-  cfg->pair_coeffs = 0;
 }
 
 }  // extern "C"

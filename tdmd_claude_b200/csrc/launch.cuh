@@ -5,7 +5,6 @@
 
 #include "common.cuh"
 #include "forces.cuh"
-#include "forces_pc.cuh"
 
 namespace tdmd_b200 {
 
@@ -139,52 +138,6 @@ void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typen
           g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
     }
   })));
-  TDMD_LAUNCH_CHECK();
-}
-
-// Single-type EAM with pair coefficients (forces_pc.cuh): padded rows only.
-template <class Geo, class FP>
-void launch_eam_density_pc(const Geo& g, const NbrView& nl, int n,
-                           const EamDev<typename Geo::T>& e, FP* fp, int4* gout,
-                           typename PcPair<typename Geo::T>::type* pc, bool ev, double* partials,
-                           Tune tn, cudaStream_t s) {
-  TDMD_REQUIRE(vec_rows(nl), "pair coefficients need padded rows");
-  const int nblk = force_blocks(n, tn.lpa);
-  TDMD_TUNE_DISPATCH(tn, {
-    if (ev)
-      k_eam_density_pc<Geo, L, U, true, FP><<<nblk, kForceThreads, 0, s>>>(g, nl, n, e, fp, gout,
-                                                                          pc, partials);
-    else
-      k_eam_density_pc<Geo, L, U, false, FP><<<nblk, kForceThreads, 0, s>>>(g, nl, n, e, fp,
-                                                                           gout, pc, nullptr);
-  });
-  TDMD_LAUNCH_CHECK();
-}
-
-template <class Geo, class F>
-void launch_eam_force_pc(const Geo& g, const NbrView& nl, int n,
-                         const typename PcPair<typename Geo::T>::type* pc,
-                         const typename Geo::T* fp, F* forces, bool ev, double* partials, Tune tn,
-                         cudaStream_t s, const KickDrift* kd = nullptr) {
-  TDMD_REQUIRE(vec_rows(nl), "pair coefficients need padded rows");
-  const int nblk = force_blocks(n, tn.lpa);
-  TDMD_TUNE_DISPATCH(tn, {
-    if (ev) {
-      k_eam_force_pc<Geo, L, U, 1, false, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, pc, fp, ForceOut<F>{forces}, partials, KickDrift{});
-    } else if constexpr (Geo::kRecords && sizeof(F) == sizeof(float)) {
-      if (kd)
-        k_eam_force_pc<Geo, L, U, 0, true, F><<<nblk, kForceThreads, 0, s>>>(
-            g, nl, n, pc, fp, ForceOut<F>{forces}, nullptr, *kd);
-      else
-        k_eam_force_pc<Geo, L, U, 0, false, F><<<nblk, kForceThreads, 0, s>>>(
-            g, nl, n, pc, fp, ForceOut<F>{forces}, nullptr, KickDrift{});
-    } else {
-      TDMD_REQUIRE(kd == nullptr, "fused kick-drift needs the mixed gather-record pass");
-      k_eam_force_pc<Geo, L, U, 0, false, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, pc, fp, ForceOut<F>{forces}, nullptr, KickDrift{});
-    }
-  });
   TDMD_LAUNCH_CHECK();
 }
 

@@ -208,13 +208,6 @@ class Scheduler {
   CellListDev cl_;
   DevArray<int> nbr_, cnt_;
   int cap_ = 0;
-  // Single-type EAM pair coefficients (phi'/r, rho'/r) in the rows' layout,
-  // written by the density pass, read by the force pass (forces_pc.cuh).
-  bool pc_ = false;
-  DevArray<float2> pc32_;
-  DevArray<double2> pc64_;
-  bool pc_eligible() const { return kind_ == TDMD_POT_EAM && eam_ && eam_->ntypes == 1; }
-  void reserve_pc();
 
   // Scratch.
   DevArray<float> fp32_;

@@ -459,10 +459,6 @@ void Scheduler::finish_setup() {
   nu_ = cfg_.nbr_batch > 0 ? cfg_.nbr_batch : kU;
   lpa_d_ = lpa_;
   nu_d_ = nu_;
-  TDMD_REQUIRE(cfg_.pair_coeffs >= 0 && cfg_.pair_coeffs <= 2,
-               "pair_coeffs must be 0 (tuned), 1 (off) or 2 (on)");
-  // Until (unless) the autotuner decides: on only when asked for.
-  pc_ = cfg_.pair_coeffs == 2 && pc_eligible();
 }
 
 void Scheduler::upload(const double* x, const double* v, const void* f, const int* types,
@@ -708,18 +704,8 @@ void Scheduler::grow_capacity(int max_count) {
   if (want > cap_) {
     cap_ = static_cast<int>(want);
     nbr_.reserve(static_cast<size_t>(cap_) * static_cast<size_t>(std::max(n_, 1)));
-    if (pc_) reserve_pc();
     clear_graphs();
   }
-}
-
-// Coefficient slots for every row slot (outside any capture: it may allocate).
-void Scheduler::reserve_pc() {
-  const size_t slots = static_cast<size_t>(cap_) * static_cast<size_t>(std::max(n_, 1));
-  if (mixed_)
-    pc32_.reserve(slots);
-  else
-    pc64_.reserve(slots);
 }
 
 void Scheduler::enqueue_rebuild() {
@@ -766,12 +752,8 @@ void Scheduler::enqueue_force(bool ev, bool kd, int parts) {
       const GeoQ gg = make_geoq(g_.data(), box_);
       if (parts & kPassDensity) {
         prof_begin(kProfDensity);
-        if (pc_)
-          launch_eam_density_pc<GeoQ, float>(g, nl, n_, eam_->d32, fp32_.data(), g_.data(),
-                                             pc32_.data(), ev, part, td, s);
-        else
-          launch_eam_density<GeoQ, float>(g, nl, n_, eam_->d32, types, fp32_.data(), nullptr,
-                                          nullptr, g_.data(), ev, part, td, s);
+        launch_eam_density<GeoQ, float>(g, nl, n_, eam_->d32, types, fp32_.data(), nullptr,
+                                        nullptr, g_.data(), ev, part, td, s);
         prof_end(kProfDensity);
       }
       const KickDrift kdr{pos4_.data(), q_.data(), vel_.data(), types_.data(), inv_mm_.data(),
@@ -781,13 +763,9 @@ void Scheduler::enqueue_force(bool ev, bool kd, int parts) {
                           box_, nullptr, nullptr};
       if (parts & kPassForce) {
         prof_begin(kProfForce);
-        if (pc_)
-          launch_eam_force_pc<GeoQ, float>(gg, nl, n_, pc32_.data(), nullptr, f32_.data(), ev,
-                                           part2, tf, s, kd ? &kdr : nullptr);
-        else
-          launch_eam_force<GeoQ, true, float, float>(gg, nl, n_, eam_->d32, types,
-                                                     fp32_.data(), f32_.data(), ev, part2, tf,
-                                                     s, kd ? &kdr : nullptr);
+        launch_eam_force<GeoQ, true, float, float>(gg, nl, n_, eam_->d32, types, fp32_.data(),
+                                                   f32_.data(), ev, part2, tf, s,
+                                                   kd ? &kdr : nullptr);
         prof_end(kProfForce);
       }
     } else {
@@ -796,23 +774,15 @@ void Scheduler::enqueue_force(bool ev, bool kd, int parts) {
               {box_.periodic[0], box_.periodic[1], box_.periodic[2]}};
       if (parts & kPassDensity) {
         prof_begin(kProfDensity);
-        if (pc_)
-          launch_eam_density_pc<GeoD4, double>(g, nl, n_, eam_->d64, fp64_.data(), nullptr,
-                                               pc64_.data(), ev, part, td, s);
-        else
-          launch_eam_density<GeoD4, double>(g, nl, n_, eam_->d64, types, fp64_.data(), nullptr,
-                                            nullptr, nullptr, ev, part, td, s);
+        launch_eam_density<GeoD4, double>(g, nl, n_, eam_->d64, types, fp64_.data(), nullptr,
+                                          nullptr, nullptr, ev, part, td, s);
         prof_end(kProfDensity);
       }
       if (parts & kPassForce) {
         prof_begin(kProfForce);
-        if (pc_)
-          launch_eam_force_pc<GeoD4, double>(g, nl, n_, pc64_.data(), fp64_.data(),
-                                             f64_.data(), ev, part2, tf, s);
-        else
-          launch_eam_force<GeoD4, false, double, double>(g, nl, n_, eam_->d64, types,
-                                                         fp64_.data(), f64_.data(), ev, part2,
-                                                         tf, s);
+        launch_eam_force<GeoD4, false, double, double>(g, nl, n_, eam_->d64, types,
+                                                       fp64_.data(), f64_.data(), ev, part2, tf,
+                                                       s);
         prof_end(kProfForce);
       }
     }
@@ -1289,7 +1259,7 @@ void Scheduler::autotune(int* lanes2, int* batch2, double* ms24) {
   const int batches[2] = {2, 4};
   if (ms24)
     for (int k = 0; k < 24; ++k) ms24[k] = -1.0;
-  auto sweep = [&](int pass) -> double {
+  auto sweep = [&](int pass) {
     int& lanes = pass == 0 ? lpa_d_ : lpa_;
     int& batch = pass == 0 ? nu_d_ : nu_;
     const int parts = pass == 0 ? kPassDensity : kPassForce;
@@ -1321,38 +1291,12 @@ void Scheduler::autotune(int* lanes2, int* batch2, double* ms24) {
     }
     lanes = best_l;
     batch = best_u;
-    return best_ms;
   };
-  // Both EAM forms when the pair-coefficient one applies (cfg.pair_coeffs
-  // 0: the faster pair of passes; 2: pair coefficients only).
-  const bool try_pc = pc_eligible() && cfg_.pair_coeffs != 1;
-  const bool plain_too = !(try_pc && cfg_.pair_coeffs == 2);
-  double t_plain = 1e300, t_pc = 1e300;
-  int plain_shape[4] = {lpa_d_, nu_d_, lpa_, nu_};
-  std::vector<double> plain_ms(ms24 ? 24 : 0);
-  if (plain_too) {
-    pc_ = false;
-    t_plain = 0.0;
-    if (eam) {
-      t_plain += sweep(0);
-      enqueue_force(false, false, kPassDensity);  // the chosen density pass's output
-    }
-    t_plain += sweep(1);
-    plain_shape[0] = lpa_d_, plain_shape[1] = nu_d_, plain_shape[2] = lpa_, plain_shape[3] = nu_;
-    if (ms24) std::copy(ms24, ms24 + 24, plain_ms.begin());
+  if (eam) {
+    sweep(0);
+    enqueue_force(false, false, kPassDensity);  // the chosen density pass's output
   }
-  if (try_pc) {
-    pc_ = true;
-    reserve_pc();
-    t_pc = sweep(0);
-    enqueue_force(false, false, kPassDensity);
-    t_pc += sweep(1);
-    if (plain_too && t_plain <= t_pc) {
-      pc_ = false;
-      lpa_d_ = plain_shape[0], nu_d_ = plain_shape[1], lpa_ = plain_shape[2], nu_ = plain_shape[3];
-      if (ms24) std::copy(plain_ms.begin(), plain_ms.end(), ms24);
-    }
-  }
+  sweep(1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   // The forces of the current state, summed in the chosen shapes' order.
@@ -1437,7 +1381,6 @@ void Scheduler::stats(tdmd_fast_pipeline_stats* o) const {
   o->nbr_batch = nu_;
   o->density_lanes_per_atom = kind_ == TDMD_POT_EAM ? lpa_d_ : 0;
   o->density_nbr_batch = kind_ == TDMD_POT_EAM ? nu_d_ : 0;
-  o->pair_coeffs = pc_ ? 1 : 0;
 }
 
 }  // namespace tdmd_b200

@@ -15,9 +15,7 @@
 * An equiatomic random ternary, 20^3 cells = 32 000 atoms, with the
   three-species analytic EAM of the 4 M-atom workload: the same checks.
 
-Both forms of the single-type EAM passes are checked: plain, and pair
-coefficients (pair_coeffs = 2).  The oracle needs ~0.5 s per 131 072-atom
-force evaluation (one host core)."""
+The oracle needs ~0.5 s per 131 072-atom force evaluation (one host core)."""
 from __future__ import annotations
 
 import numpy as np
@@ -57,11 +55,11 @@ def ternary(oracle):
     return s, t, oe, ref, lists
 
 
-def _sched(s, t, precision, **cfg):
+def _sched(s, t, precision):
     from tdmd_claude_b200 import Box, EamAlloy, FastPipelineScheduler, make_config
     eam = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
     sch = FastPipelineScheduler(Box.make(s.lo, s.hi), s.n, eam,
-                                make_config(r_skin=SKIN, precision=precision, **cfg))
+                                make_config(r_skin=SKIN, precision=precision))
     sch.upload(s.positions, s.velocities, None, s.types, s.ids, s.masses)
     return sch
 
@@ -105,30 +103,25 @@ def test_headline_free_function_lists_bit_exact(cuda, oracle, headline):
     assert np.array_equal(c, ec) and np.array_equal(o, eo) and np.array_equal(nb, enb)
 
 
-@pytest.mark.parametrize("pair_coeffs", [1, 2])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_headline_scheduler_step0(cuda, headline, precision, pair_coeffs):
-    """Both forms of the EAM passes: plain, and pair coefficients (the
-    density pass stores phi'/r and rho'/r per listed pair)."""
+def test_headline_scheduler_step0(cuda, headline, precision):
     s, t, _, ref, lists = headline
-    sch = _sched(s, t, precision, pair_coeffs=pair_coeffs)
+    sch = _sched(s, t, precision)
     sch.run_until(0)
-    assert sch.stats().pair_coeffs == (1 if pair_coeffs == 2 else 0)
     _check_lists(sch, lists)
     _check_forces(sch, ref, precision)
     sch.close()
 
 
-@pytest.mark.parametrize("pair_coeffs", [1, 2])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_headline_scheduler_window(cuda, oracle, headline, precision, pair_coeffs):
+def test_headline_scheduler_window(cuda, oracle, headline, precision):
     """One bench window of 10 steps, then the next step, whose drift is
     followed by the first rebuild (maybe_rebuild_nlist: steps since the last
     build reach rebuild_every), against the oracle's restatement of the
     scheduler loop; the rebuilt list equals the oracle's list of the
     scheduler's positions at that step."""
     s, t, oe, _, _ = headline
-    sch = _sched(s, t, precision, pair_coeffs=pair_coeffs)
+    sch = _sched(s, t, precision)
     sch.run_until(10)
     sch.run_until(11)
     st = sch.download()

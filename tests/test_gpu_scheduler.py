@@ -102,10 +102,9 @@ def _eam_setup(precision, ncell=6, **cfg):
     return s, sysm, t
 
 
-@pytest.mark.parametrize("pair_coeffs", [1, 2])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_eam_trajectory_matches_oracle(cuda, oracle, precision, pair_coeffs):
-    s, sysm, t = _eam_setup(precision, pair_coeffs=pair_coeffs)
+def test_eam_trajectory_matches_oracle(cuda, oracle, precision):
+    s, sysm, t = _eam_setup(precision)
     s.run_until(50)
     st = s.download()
     oe = oracle.OracleEam(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
@@ -133,10 +132,9 @@ def test_eam_mixed_step0_forces_vs_oracle(cuda, oracle):
     assert rel_rms(st.forces, r["forces"]) <= 1e-5
 
 
-@pytest.mark.parametrize("pair_coeffs", [1, 2])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_energies_and_virial(cuda, oracle, precision, pair_coeffs):
-    s, sysm, t = _eam_setup(precision, pair_coeffs=pair_coeffs)
+def test_energies_and_virial(cuda, oracle, precision):
+    s, sysm, t = _eam_setup(precision)
     s.run_until(7)
     pe, ke, w = s.energies()
     st = s.download()

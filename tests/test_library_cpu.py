@@ -35,7 +35,7 @@ def test_exports_every_declared_symbol(L):
     for s in syms:
         assert hasattr(L, s), s
     assert set(syms) == set(_lib.SIGNATURES), set(syms) ^ set(_lib.SIGNATURES)
-    assert L.tdmd_abi_version() == 3
+    assert L.tdmd_abi_version() == 2
 
 
 def test_config_defaults_follow_reference(L):
