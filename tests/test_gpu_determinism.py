@@ -148,14 +148,16 @@ def test_eam_energy_bits_equal_reference_deterministic_build(cuda, refdet, det_m
 
 
 def test_default_mode_agrees_with_deterministic_mode(cuda, mishin_setfl):
+    """Jittered positions (on the perfect lattice the forces are rounding
+    noise of ~1e-15 and no relative comparison means anything)."""
     from tdmd_claude_b200 import EamAlloy, set_deterministic_reduce
-    m = golden("run0_morse_256.json")
-    pos = np.array(m["positions"])
+    g = golden("ref_morse_256.json")
+    pos = np.array(g["positions"])
     eam = EamAlloy().read_setfl(mishin_setfl)
-    base = _ours_eam(cuda, eam, pos, np.ones(256, np.int32), m["lo"], m["hi"], 1.0)[0]
+    base = _ours_eam(cuda, eam, pos, np.ones(256, np.int32), g["lo"], g["hi"], 0.3)[0]
     set_deterministic_reduce(True)
     try:
-        det = _ours_eam(cuda, eam, pos, np.ones(256, np.int32), m["lo"], m["hi"], 1.0)[0]
+        det = _ours_eam(cuda, eam, pos, np.ones(256, np.int32), g["lo"], g["hi"], 0.3)[0]
     finally:
         set_deterministic_reduce(False)
     assert abs(base[0] - det[0]) <= 1e-12 * abs(det[0])
