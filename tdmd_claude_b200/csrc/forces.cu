@@ -247,10 +247,11 @@ void EamDevTables::upload(const tdmd_eam& e, cudaStream_t stream) {
   if (nt > 1 && nt <= 16)
     while ((1 << tbits) < nt) ++tbits;
   d64 = EamDev<double>{dtab64.data(), rtab64.data(), ftab.data(), nt, S, e.nr, e.nrho, e.dr,
-                       1.0 / e.dr, e.cutoff * e.cutoff, e.drho, e.dr, 0};
-  d32 = EamDev<float>{dtab32.data(), rtab32.data(), ftab.data(), nt, S, e.nr, e.nrho,
-                      static_cast<float>(e.dr), static_cast<float>(1.0 / e.dr),
-                      static_cast<float>(e.cutoff * e.cutoff), e.drho, e.dr, tbits};
+                       1.0 / e.dr, e.cutoff * e.cutoff, e.drho, e.dr, 0.0, 0};
+  const float dr32 = static_cast<float>(e.dr);
+  d32 = EamDev<float>{dtab32.data(), rtab32.data(), ftab.data(), nt, S, e.nr, e.nrho, dr32,
+                      static_cast<float>(1.0 / e.dr), static_cast<float>(e.cutoff * e.cutoff),
+                      e.drho, e.dr, static_cast<float>(e.dr - static_cast<double>(dr32)), tbits};
 }
 
 // --------------------------------------------------------------------------

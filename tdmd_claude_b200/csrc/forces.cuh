@@ -168,17 +168,6 @@ __device__ __forceinline__ void radius_q(float r2, float res, float& r, float& r
   rd = static_cast<double>(r) + static_cast<double>(corr);
 }
 
-// |r| from an FP32 r^2 with one Newton step on the rsqrt estimate (the
-// residual r2 - r*r is exact by FMA).  r2 * rsqrtf(r2) alone errs by up to
-// ~2 ulp with one sign more often than the other; summed over an atom's
-// density and through F(rho) that bias reached ~1.4e-6 of the potential
-// energy (32 000-atom ternary); the corrected radius rounds symmetrically.
-__device__ __forceinline__ float radius_nr(float r2) {
-  const float rinv = rsqrtf(r2);
-  const float r = r2 * rinv;
-  return fmaf(fmaf(-r, r, r2), 0.5f * rinv, r);
-}
-
 __device__ __forceinline__ void radius_f(float r2, double r2d, float& r, float& rinv, double& rd) {
   rinv = rsqrtf(r2);
   r = r2 * rinv;
@@ -213,7 +202,6 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
     rd = r;
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
-  __device__ __forceinline__ T radius_ev(const Pair& pr) const { return sqrt(pr.r2); }
 };
 
 struct GeoAoS64 {  // FP64, reference Vec3D AoS
@@ -243,7 +231,6 @@ struct GeoAoS64 {  // FP64, reference Vec3D AoS
     rd = r;
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
-  __device__ __forceinline__ T radius_ev(const Pair& pr) const { return sqrt(pr.r2); }
 };
 
 // Mixed on the reference layout (free functions): the delta is formed in
@@ -279,7 +266,6 @@ struct GeoAoS32 {
     radius_f(pr.r2, pr.r2d, r, rinv, rd);
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
-  __device__ __forceinline__ T radius_ev(const Pair& pr) const { return radius_nr(pr.r2); }
 };
 
 // Mixed, scheduler layout: fixed-point int4 records {qx,qy,qz,w}.  The
@@ -313,7 +299,6 @@ struct GeoQ {
     radius_q(pr.r2, pr.res, r, rinv, rd);
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
-  __device__ __forceinline__ T radius_ev(const Pair& pr) const { return radius_nr(pr.r2); }
 };
 
 __host__ inline GeoQ make_geoq(const int4* q, const DevBox& b) {
@@ -515,6 +500,11 @@ struct EamDev {
   T dr, inv_dr, rc_sq;
   double drho;
   double dr_d;
+  // FP32 path: dr_d - dr (the knot spacing's rounding), so that the
+  // spline offset r - idx*dr carries no error proportional to idx (the
+  // same sign for every pair of a neighbor shell, which summed into a
+  // bias of the embedding energy).
+  T dr_lo;
   // Multi-type mixed path: the low tbits mantissa bits of the gather
   // record's F'(rho) word hold the atom's 0-based type (a relative change of
   // F' below 2^(tbits-23)), so the force pass gathers no type; 0 = types are
@@ -562,7 +552,8 @@ template <class T>
 __device__ __forceinline__ int spline_fast(float r, const EamDev<T>& e, float& sx) {
   int idx = static_cast<int>(r * e.inv_dr);
   idx = idx < 0 ? 0 : (idx > e.nr - 2 ? e.nr - 2 : idx);
-  sx = fmaf(-static_cast<float>(idx), e.dr, r);
+  const float fi = static_cast<float>(idx);
+  sx = fmaf(-fi, e.dr_lo, fmaf(-fi, e.dr, r));
   return idx;
 }
 
@@ -657,10 +648,9 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
           // No FP64-refined radius here: in the mixed path the density's
           // FP32 radius error is a few percent of the total force error
           // (the force pass's radius dominates), so it is not worth the
-          // FP64 work.  Energy steps take the Newton-corrected FP32 radius
-          // (radius_nr), whose rounding carries no bias into F(rho).
+          // FP64 work.
           T sx;
-          const int idx = spline_fast(EV ? g.radius_ev(pr[u]) : g.radius_fast(pr[u]), e, sx);
+          const int idx = spline_fast(g.radius_fast(pr[u]), e, sx);
           // fixed-point position records carry the atom's 1-based type in
           // their fourth word (the density pass always reads those)
           int tj = 0;

@@ -60,7 +60,6 @@ struct GeoQB {
     radius_q(pr.r2, pr.res, r, rinv, rd);
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
-  __device__ __forceinline__ T radius_ev(const Pair& pr) const { return radius_nr(pr.r2); }
 };
 
 // FP64: double4 positions, per-replica minimum image.
@@ -112,7 +111,6 @@ struct GeoD4B {
     rd = r;
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
-  __device__ __forceinline__ T radius_ev(const Pair& pr) const { return sqrt(pr.r2); }
 };
 
 __host__ inline RepImg rep_img(const DevBox& b) {
