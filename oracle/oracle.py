@@ -67,7 +67,8 @@ def build(ref: bool | None = None) -> None:
             raise RuntimeError("reference tree not found: set TDMD_REFERENCE_TREE")
         targets += ["ref", "refgpu", "dropin"]
     args = [f"REF={ref_tree}"] if ref_tree else []
-    subprocess.run(["make", "-s", "-C", _HERE, *args, *targets], check=True)
+    jobs = str(max(1, min(8, os.cpu_count() or 1)))
+    subprocess.run(["make", "-s", "-j", jobs, "-C", _HERE, *args, *targets], check=True)
 
 
 _lib = None

@@ -298,11 +298,8 @@ struct tdmd_device_eam {
   EamDevTables tabs;
   DevArray<float> fp32;
   DevArray<double> fp64;
-  // the reference's flat layout, for the ID-ordered energy mode (built on
-  // its first use)
+  // the reference's flat layout, for the ID-ordered energy mode
   RefEamTables ref;
-  bool ref_ready = false;
-  tdmd_eam copy;  // the host tables, kept for the ID-ordered mode
 };
 
 namespace {
@@ -446,7 +443,7 @@ int32_t tdmd_device_eam_create(const tdmd_eam* eam, tdmd_device_eam** out) {
     auto* de = new tdmd_device_eam();
     try {
       de->tabs.upload(*eam, nullptr);
-      de->copy = *eam;
+      de->ref.upload(*eam);
     } catch (...) {
       delete de;
       throw;
@@ -475,10 +472,6 @@ int32_t tdmd_device_eam_compute(tdmd_device_eam* de, const double* d_positions, 
     cudaStream_t s = as_stream(stream);
     const bool ev = d_energy || d_virial;
     if (ev && precision == TDMD_FP64 && deterministic_reduce()) {
-      if (!de->ref_ready) {
-        de->ref.upload(de->copy);
-        de->ref_ready = true;
-      }
       eam_id_ordered(de->ref, d_positions, static_cast<double*>(d_forces), d_types, d_neighbors,
                      d_offsets, d_counts, natoms, *box, d_energy, d_virial, d_rho, d_fp, s);
       return;
