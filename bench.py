@@ -353,6 +353,55 @@ def cpu_baseline_sample(sysm, t, nsteps):
     return sec, kind
 
 
+def host_cores(cap=64):
+    """Host cores this process may use: its CPU affinity, bounded by a
+    cgroup CPU quota where one is set, at most `cap`."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as f:
+            quota, period = f.read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(int(quota) // int(period))))
+    except (OSError, ValueError):
+        pass
+    return max(1, min(n, cap))
+
+
+_CPU_BARRIER = None
+
+
+def _cpu_worker_init(barrier):
+    global _CPU_BARRIER
+    _CPU_BARRIER = barrier
+    os.environ["OMP_NUM_THREADS"] = "1"
+
+
+def _cpu_worker(nsteps):
+    """One process of the multi-core CPU baseline: the workload's system
+    rebuilt here (same seed), then, once every worker is ready, the
+    reference CPU loop (or the oracle port) for nsteps MD steps."""
+    sysm, t = workload()
+    _CPU_BARRIER.wait()
+    return cpu_baseline_sample(sysm, t, nsteps)
+
+
+def cpu_baseline_parallel(nsteps, cores):
+    """The reference's CPU path is single-threaded; to use every host core
+    it runs as `cores` independent processes, each advancing its own copy
+    of the 131,072-atom system by nsteps, started together behind a
+    barrier (processes spawned, never forked).  Returns (atom-steps/s of
+    the whole job = cores * n * nsteps / the slowest process's loop time,
+    that slowest time, the per-process times, kind)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(cores)
+    with ctx.Pool(cores, initializer=_cpu_worker_init, initargs=(barrier,)) as pool:
+        res = pool.map(_cpu_worker, [nsteps] * cores, chunksize=1)
+    secs = [r[0] for r in res]
+    n = NCELL ** 3 * 4
+    return cores * n * nsteps / max(secs), max(secs), secs, res[0][1]
+
+
 def nve_drift(sysm, eam, precision, nsteps, every=100):
     """Total-energy drift of an NVE run from the device energy log:
     least-squares slope of E_total/N against time (eV/atom/ns) and the
@@ -713,8 +762,12 @@ def run_reference(args, rank, world):
     sysm, t = workload()
     warm = max(1, min(args.warmup, 2))
     cpu_baseline_sample(sysm, t, warm)          # warm caches/pages (untimed)
-    sec, kind = cpu_baseline_sample(sysm, t, args.steps)
-    value = sysm.n * args.steps / sec
+    cores = args.cpu_cores or host_cores()
+    if cores > 1:
+        value, sec, secs, kind = cpu_baseline_parallel(args.steps, cores)
+    else:
+        sec, kind = cpu_baseline_sample(sysm, t, args.steps)
+        value, secs = sysm.n * args.steps / sec, [sec]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "atom-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -722,10 +775,14 @@ def run_reference(args, rank, world):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "eam_cu_fcc_131072", "atoms": sysm.n, "precision": "fp64 (CPU)",
                    "dt_fs": 1.0, "skin": SKIN, "rebuild_every": WINDOW,
-                   "step": "one MD timestep of the whole system"},
-        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": 1, "kind": kind,
-                         "sample": f"{args.steps} MD steps of the 131,072-atom EAM system "
-                                   "(single-threaded reference CPU loop, rebuild every 10)"},
+                   "step": "one MD timestep of every process's copy of the system",
+                   "processes": cores,
+                   "per_process_loop_s": secs},
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": kind,
+                         "sample": f"{args.steps} MD steps of the 131,072-atom EAM system in "
+                                   f"each of {cores} concurrent single-threaded processes "
+                                   "(the reference CPU loop has no threads; rebuild every 10); "
+                                   "value = all processes' atom-steps / the slowest loop"},
         "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -743,6 +800,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=10, help="reference CPU sample size")
+    ap.add_argument("--cpu-cores", type=int, default=0,
+                    help="processes of the CPU baseline / reference arm (0: every usable host "
+                         "core, at most 64)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the mixed timed windows (for profiler captures); no JSON line")
@@ -950,11 +1010,17 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sec, kind = cpu_baseline_sample(sysm, t, args.cpu_steps)
-        cpu = {"value": sysm.n * args.cpu_steps / sec, "unit": "atom-steps/s", "cores": 1,
-               "kind": kind,
+        cores = args.cpu_cores or host_cores()
+        sec1, kind = cpu_baseline_sample(sysm, t, args.cpu_steps)
+        if cores > 1:
+            value_c, _, _, kind = cpu_baseline_parallel(args.cpu_steps, cores)
+        else:
+            value_c = sysm.n * args.cpu_steps / sec1
+        cpu = {"value": value_c, "unit": "atom-steps/s", "cores": cores, "kind": kind,
+               "one_core": sysm.n * args.cpu_steps / sec1,
                "sample": f"{args.cpu_steps} MD steps (rebuild every 10) of the same 131,072-atom "
-                         "EAM system, single-threaded reference CPU loop"}
+                         f"EAM system in each of {cores} concurrent single-threaded processes "
+                         "(the reference CPU loop has no threads); one_core: one process alone"}
 
     if rank == 0:
         line = {

@@ -209,3 +209,71 @@ def test_eam_batch_replicas_equal_single_schedulers(cuda, precision, ternary):
         assert abs(pe_b[r] - pe) <= 1e-12 * abs(pe), r
         assert abs(ke_b[r] - ke) <= 1e-12 * abs(ke), r
         sc.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_far_atoms_nonperiodic_replica(cuda, precision):
+    """A slab replica (z non-periodic, 7 FCC cells across so its grid has 4
+    cells per axis and the batch list build takes the warp-slab path) with
+    atoms 2 to 4 box lengths outside its z faces, between two periodic
+    replicas: the slab's trajectory equals a single scheduler's bit for
+    bit (the list build's far records take the exact FP64 test)."""
+    from test_gpu_scheduler import _slab_with_far_atoms
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, ReplicaBatch, make_config
+    from tdmd_claude_b200 import workloads as W
+    pos, vel, types, masses, lo, hi = _slab_with_far_atoms(7)
+    per = (1, 1, 0)
+    a = W.fcc_system(4, 3.615, 300.0, seed=41)
+    c = W.fcc_system(5, 3.615, 700.0, seed=42)
+    boxes = [Box.make(a.lo, a.hi), Box.make(lo, hi, per), Box.make(c.lo, c.hi)]
+    cfg = make_config(dt=0.001, r_skin=0.3, rebuild_every=10, precision=precision,
+                      lanes_per_atom=4)
+    b = ReplicaBatch(boxes, [a.n, len(pos), c.n], _morse(), cfg)
+    b.upload(np.concatenate([a.positions, pos, c.positions]),
+             np.concatenate([a.velocities, vel, c.velocities]),
+             np.concatenate([a.types, types, c.types]), masses)
+    b.run_until(21)
+    bp, bv, bf = b.download()
+    sc = FastPipelineScheduler(Box.make(lo, hi, per), len(pos), _morse(), cfg)
+    sc.upload(pos, vel, None, types, None, masses)
+    sc.run_until(21)
+    st = sc.download()
+    assert np.array_equal(b.replica(bp, 1), st.positions)
+    assert np.array_equal(b.replica(bv, 1), st.velocities)
+    assert np.array_equal(b.replica(bf, 1), st.forces)
+    # the far dimer (the second and third added atoms) interacts
+    assert np.abs(st.forces[-4]).max() > 1e-3
+    sc.close()
+    b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_lpt_sharded_batches_equal_unsharded(cuda, precision):
+    """The replica workload split over two ranks by LPT, run here as two
+    batches one after the other on the one GPU: every replica's state and
+    logged energies equal the unsharded batch's bit for bit, gathered back
+    in replica order (replicas.gather_by_replica)."""
+    from tdmd_claude_b200 import workloads as W
+    from tdmd_claude_b200.replicas import gather_by_replica, lpt_partition
+    systems = W.replica_set(10, seed=13, nmin=4, nmax=6)
+    full = _batch(systems, precision, energy_every=10, energy_log_capacity=8)
+    full.run_until(20)
+    fp, fv, _ = full.download()
+    _, fpk = full.energy_log()
+    shards = lpt_partition([s.n for s in systems], 2)
+    pos_r, pk_r = [], []
+    for mine in shards:
+        sub = [systems[i] for i in mine]
+        b = _batch(sub, precision, energy_every=10, energy_log_capacity=8)
+        b.run_until(20)
+        p, v, _ = b.download()
+        _, pk = b.energy_log()
+        pos_r.append([b.replica(p, k) for k in range(len(sub))])
+        pk_r.append([pk[:, k, :] for k in range(len(sub))])
+        b.close()
+    pos_all = gather_by_replica(pos_r[0] + pos_r[1], shards[0] + shards[1], len(systems))
+    pk_all = gather_by_replica(pk_r[0] + pk_r[1], shards[0] + shards[1], len(systems))
+    for r in range(len(systems)):
+        assert np.array_equal(pos_all[r], full.replica(fp, r)), r
+        assert np.array_equal(pk_all[r], fpk[:, r, :]), r
+    full.close()

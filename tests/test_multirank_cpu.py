@@ -226,7 +226,7 @@ def test_reference_arm_prints_its_line():
     """bench.py --impl reference on rank 0: one JSON line with the arm's
     contract keys (the reference CPU loop, a bounded sample)."""
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                          "--steps", "1", "--warmup", "3"],
+                          "--steps", "1", "--warmup", "3", "--cpu-cores", "2"],
                          capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
@@ -234,4 +234,5 @@ def test_reference_arm_prints_its_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["unit"] == "atom-steps/s" and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
-    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] == 2
+    assert d["config"]["processes"] == 2 and len(d["config"]["per_process_loop_s"]) == 2
