@@ -146,30 +146,68 @@ __global__ void k_scan_single(const int* __restrict__ in, int* __restrict__ out,
   if (threadIdx.x == 0 && total_out) *total_out = carry;
 }
 
-// One-pass single-block scan of up to kScanThreads * kScanWide items: each
-// thread holds kScanWide consecutive items (all loads issued at once), one
-// block scan.  out may alias in.
+// One-pass single-block scan of up to kScanThreads * kScanWide items, all
+// loads and stores coalesced: thread t holds items t + k * kScanThreads
+// (k < kScanWide), i.e. column t of kScanWide rows; the kScanWide row scans
+// run side by side (warp shuffles, then the warps' totals of each row, then
+// the rows' totals), so item (k, t)'s prefix is rows_before(k) +
+// warps_before(k, t) + lanes_before(k, t).  out may alias in.
 constexpr int kScanWide = 16;
 __global__ void __launch_bounds__(kScanThreads) k_scan_wide(const int* __restrict__ in,
                                                             int* __restrict__ out, int n,
                                                             int* __restrict__ total_out) {
-  __shared__ int smem[32];
-  const int b0 = threadIdx.x * kScanWide;
-  int v[kScanWide];
-  int s = 0;
+  __shared__ int wsum[kScanWide][kScanThreads / 32];  // row k: per-warp totals -> prefixes
+  __shared__ int rsum[kScanWide + 1];                 // rows' exclusive prefixes, total
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  int v[kScanWide], incl[kScanWide];
 #pragma unroll
   for (int k = 0; k < kScanWide; ++k) {
-    v[k] = b0 + k < n ? in[b0 + k] : 0;
-    s += v[k];
+    const int i = k * kScanThreads + t;
+    v[k] = i < n ? in[i] : 0;
+    incl[k] = v[k];
   }
-  int total;
-  int pre = block_exclusive_scan(s, smem, &total);
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < kScanWide; ++k) {
+      const int y = __shfl_up_sync(0xffffffffu, incl[k], o);
+      if (lane >= o) incl[k] += y;
+    }
+  }
+  if (lane == 31) {
+#pragma unroll
+    for (int k = 0; k < kScanWide; ++k) wsum[k][warp] = incl[k];
+  }
+  __syncthreads();
+  // warp k scans row k's warp totals (kScanThreads / 32 = 32 of them)
+  if (warp < kScanWide) {
+    const int x = wsum[warp][lane];
+    int y = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int z = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += z;
+    }
+    wsum[warp][lane] = y - x;  // exclusive
+    if (lane == 31) rsum[warp] = y;
+  }
+  __syncthreads();
+  if (t == 0) {
+    int c = 0;
+    for (int k = 0; k < kScanWide; ++k) {
+      const int r = rsum[k];
+      rsum[k] = c;
+      c += r;
+    }
+    rsum[kScanWide] = c;
+  }
+  __syncthreads();
 #pragma unroll
   for (int k = 0; k < kScanWide; ++k) {
-    if (b0 + k < n) out[b0 + k] = pre;
-    pre += v[k];
+    const int i = k * kScanThreads + t;
+    if (i < n) out[i] = rsum[k] + wsum[k][warp] + incl[k] - v[k];
   }
-  if (threadIdx.x == 0 && total_out) *total_out = total;
+  if (t == 0 && total_out) *total_out = rsum[kScanWide];
 }
 
 __global__ void k_scan_apply(const int* __restrict__ in, int* __restrict__ out, long long n,
