@@ -66,7 +66,37 @@ def build(verbose: bool = False, force: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_driver()
     return LIB
+
+
+DRIVER_SRC = os.path.join(PKG, "driver", "tdmd_standalone.cpp")
+DRIVER_DIR = os.path.join(PKG, "bin", "native")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+
+def build_driver() -> dict:
+    """The native tdmd_standalone, once per precision as the reference builds
+    it (bin/native/tdmd_standalone: FP64, bin/native/tdmd_standalone_mixed),
+    compiled with the host C++ compiler against include/tdmd_b200.hpp and
+    linked to the library (rpath relative to the binary)."""
+    os.makedirs(DRIVER_DIR, exist_ok=True)
+    gxx = os.environ.get("CXX", "g++")
+    deps = max(os.path.getmtime(DRIVER_SRC), _headers_mtime(), os.path.getmtime(LIB))
+    out = {}
+    for name, define in (("tdmd_standalone", "TDMD_PRECISION_FP64"),
+                         ("tdmd_standalone_mixed", "TDMD_PRECISION_MIXED")):
+        exe = os.path.join(DRIVER_DIR, name)
+        out[name] = exe
+        if os.path.exists(exe) and os.path.getmtime(exe) >= deps:
+            continue
+        cmd = [gxx, "-std=c++20", "-O2", "-Wall", "-Wextra", "-Werror", f"-D{define}=1",
+               "-I", INCLUDE, "-I", os.path.join(CUDA_HOME, "include"), DRIVER_SRC, "-o", exe,
+               LIB, "-Wl,-rpath,$ORIGIN/../.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
+    return out
 
 
 if __name__ == "__main__":

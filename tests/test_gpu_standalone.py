@@ -1,8 +1,11 @@
-"""The GPU-backed tdmd_standalone (tdmd_claude_b200/bin) run as a VerifyLab
-script runs the reference binary: a subprocess with the reference's flags,
-thermo lines parsed with a "Step N  PE  KE  TE  T" pattern, the step-0 force
-dump read back.  Step-0 PE and forces equal the reference's (FP64 1e-10
-relative, mixed 1e-5 RMS); NVE total energy stays flat."""
+"""The GPU-backed tdmd_standalone run as a VerifyLab script runs the
+reference binary: a subprocess with the reference's flags, thermo lines
+parsed with a "Step N  PE  KE  TE  T" pattern, the step-0 force dump read
+back.  Two drivers: the native C++ one (tdmd_claude_b200/bin/native, built
+against include/tdmd_b200.hpp per precision as the reference's binary is)
+and the Python one (tdmd_claude_b200/bin).  Step-0 PE and forces equal the
+reference's (FP64 1e-10 relative, mixed 1e-5 RMS); NVE total energy stays
+flat; both drivers print the same thermo lines and dumps."""
 from __future__ import annotations
 
 import os
@@ -18,9 +21,24 @@ from conftest import golden, rel_rms
 pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-BIN = {"fp64": os.path.join(ROOT, "tdmd_claude_b200", "bin", "tdmd_standalone"),
-       "mixed": os.path.join(ROOT, "tdmd_claude_b200", "bin", "tdmd_standalone_mixed")}
+BIN = {("python", "fp64"): [sys.executable,
+                            os.path.join(ROOT, "tdmd_claude_b200", "bin", "tdmd_standalone")],
+       ("python", "mixed"): [sys.executable,
+                             os.path.join(ROOT, "tdmd_claude_b200", "bin",
+                                          "tdmd_standalone_mixed")],
+       ("native", "fp64"): [os.path.join(ROOT, "tdmd_claude_b200", "bin", "native",
+                                         "tdmd_standalone")],
+       ("native", "mixed"): [os.path.join(ROOT, "tdmd_claude_b200", "bin", "native",
+                                          "tdmd_standalone_mixed")]}
 THERMO = re.compile(r"^Step\s+(\d+)\s+PE\s+(\S+)\s+KE\s+(\S+)\s+TE\s+(\S+)\s+T\s+(\S+)", re.M)
+
+
+def _run(driver, precision, args):
+    cmd = BIN[(driver, precision)]
+    assert os.path.exists(cmd[-1]), f"{cmd[-1]} missing: build the library first"
+    out = subprocess.run(cmd + args, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    return out.stdout
 
 
 def _data_file(tmp_path):
@@ -35,19 +53,18 @@ def _data_file(tmp_path):
     return path, g
 
 
+@pytest.mark.parametrize("driver", ["native", "python"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_standalone_cli_matches_reference(cuda, tmp_path, precision):
+def test_standalone_cli_matches_reference(cuda, tmp_path, driver, precision):
     from tdmd_claude_b200 import io as TIO
     data, g = _data_file(tmp_path)
     dump = str(tmp_path / "f0.dump")
     final = str(tmp_path / "final.dump")
     morse = ",".join(str(x) for x in g["morse"])
-    out = subprocess.run([sys.executable, BIN[precision], "--data", data, "--nsteps", "200",
-                          "--thermo", "50", "--morse", morse, "--skin", str(g["skin"]),
-                          "--dump-forces", dump, "--dump-final", final],
-                         capture_output=True, text=True, timeout=600)
-    assert out.returncode == 0, out.stderr
-    rows = [tuple(float(x) for x in m) for m in THERMO.findall(out.stdout)]
+    stdout = _run(driver, precision, ["--data", data, "--nsteps", "200", "--thermo", "50",
+                                      "--morse", morse, "--skin", str(g["skin"]),
+                                      "--dump-forces", dump, "--dump-final", final])
+    rows = [tuple(float(x) for x in m) for m in THERMO.findall(stdout)]
     steps = [int(r[0]) for r in rows]
     assert steps[:5] == [0, 50, 100, 150, 200] and steps[-1] == 200   # + the "Final:" line
     pe0 = rows[0][1]
@@ -61,5 +78,29 @@ def test_standalone_cli_matches_reference(cuda, tmp_path, precision):
                                                                  else 1e-5)
     ids, _, pos_final, _ = TIO.read_force_dump(final)
     assert pos_final.shape == (256, 3)
-    assert "Neighbor list rebuilds:" in out.stdout
+    assert "Neighbor list rebuilds:" in stdout
 
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_native_and_python_drivers_agree_eam(cuda, tmp_path, precision):
+    """Ternary EAM (864 atoms, three element types): the native and the
+    Python driver print the same thermo lines and write the same dumps."""
+    from tdmd_claude_b200 import io as TIO
+    from tdmd_claude_b200 import workloads as W
+    s = W.ternary(6)
+    data = str(tmp_path / "ternary.data")
+    setfl = str(tmp_path / "ternary.eam.alloy")
+    TIO.write_lammps_data(data, s)
+    TIO.write_setfl(setfl, W.ternary_eam_tables())
+    res = {}
+    for driver in ("native", "python"):
+        d0, d1 = str(tmp_path / f"{driver}0.dump"), str(tmp_path / f"{driver}1.dump")
+        stdout = _run(driver, precision, ["--data", data, "--eam", setfl, "--nsteps", "60",
+                                          "--thermo", "20", "--skin", "0.5",
+                                          "--dump-forces", d0, "--dump-final", d1])
+        res[driver] = (THERMO.findall(stdout), TIO.read_force_dump(d0), TIO.read_force_dump(d1))
+    (tn, f0n, f1n), (tp, f0p, f1p) = res["native"], res["python"]
+    assert len(tn) == 5 and tn == tp  # steps 0, 20, 40, 60 and the "Final:" line
+    for a, b in ((f0n, f0p), (f1n, f1p)):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
