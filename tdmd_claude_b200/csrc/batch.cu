@@ -45,6 +45,7 @@ template <class Geo, int LPA, int U, bool VEC>
 __global__ void __launch_bounds__(kThreads) k_morse_atom_pe(Geo g, NbrView nl, int n,
                                                             MorseP<typename Geo::T> mp,
                                                             double* __restrict__ pe_atom) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;
@@ -86,6 +87,7 @@ __global__ void __launch_bounds__(kThreads) k_eam_atom_pe(Geo g, NbrView nl, int
                                                           const int* __restrict__ types,
                                                           const double* __restrict__ rho,
                                                           double* __restrict__ pe_atom) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;
@@ -134,6 +136,7 @@ __global__ void __launch_bounds__(kThreads) k_rep_energy(const double* __restric
                                                          const double* __restrict__ masses,
                                                          const RepDesc* __restrict__ reps,
                                                          double* __restrict__ out) {
+  dependent_launch_prologue();
   __shared__ double red[32 * 2];
   const int r = blockIdx.x;
   const int a0 = reps[r].atom0, na = reps[r].natoms;
@@ -154,6 +157,7 @@ __global__ void __launch_bounds__(kThreads) k_rep_energy(const double* __restric
 __global__ void k_pack_batch(const double* __restrict__ x, const int* __restrict__ types,
                              const int* __restrict__ rep, const RepDesc* __restrict__ reps,
                              int n, double4* __restrict__ pos4, int4* __restrict__ q) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double px = x[3ll * i], py = x[3ll * i + 1], pz = x[3ll * i + 2];
@@ -167,6 +171,7 @@ __global__ void k_pack_batch(const double* __restrict__ x, const int* __restrict
 }
 
 __global__ void k_unpack_batch(const double4* __restrict__ pos4, int n, double* __restrict__ x) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 p = pos4[i];
@@ -183,6 +188,7 @@ __global__ void __launch_bounds__(kThreads) k_kick_drift_batch(
     double4* __restrict__ pos4, int4* __restrict__ q, double* __restrict__ v,
     const F* __restrict__ f, const int* __restrict__ types, const int* __restrict__ rep,
     const RepDesc* __restrict__ reps, const double* __restrict__ inv_mm, int n, double dt) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double kick_dt = FULL ? dt : 0.5 * dt;
@@ -212,6 +218,7 @@ __global__ void __launch_bounds__(kThreads) k_half_kick_batch(double* __restrict
                                                               const int* __restrict__ types,
                                                               const double* __restrict__ inv_mm,
                                                               int n, double dt) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double factor = 0.5 * dt * inv_mm[types[i]];
@@ -494,9 +501,9 @@ void Batch::upload(const double* x, const double* v, const int* types, const dou
     TDMD_CU(cudaMemcpyAsync(stage_.data(), x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     TDMD_CU(cudaMemcpyAsync(vel_.data(), v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     TDMD_CU(cudaMemcpyAsync(types_.data(), types, n * sizeof(int), cudaMemcpyHostToDevice, s));
-    k_pack_batch<<<ceil_div(n_, kThreads), kThreads, 0, s>>>(
-        stage_.data(), types_.data(), rep_.data(), reps_.data(), static_cast<int>(n_),
-        pos4_.data(), mixed_ ? q_.data() : nullptr);
+    launch(k_pack_batch, ceil_div(n_, kThreads), kThreads, 0, s, stage_.data(), types_.data(),
+           rep_.data(), reps_.data(), static_cast<int>(n_), pos4_.data(),
+           mixed_ ? q_.data() : nullptr);
     TDMD_LAUNCH_CHECK();
   }
   masses_.reserve(static_cast<size_t>(n_types));
@@ -524,9 +531,8 @@ void Batch::download(double* x, double* v, void* f) const {
   cudaStream_t s = stream_;
   const size_t n = static_cast<size_t>(n_);
   if (x) {
-    k_unpack_batch<<<ceil_div(n_, kThreads), kThreads, 0, s>>>(pos4_.data(),
-                                                              static_cast<int>(n_),
-                                                              stage_.data());
+    launch(k_unpack_batch, ceil_div(n_, kThreads), kThreads, 0, s, pos4_.data(),
+           static_cast<int>(n_), stage_.data());
     TDMD_LAUNCH_CHECK();
     TDMD_CU(cudaMemcpyAsync(x, stage_.data(), 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
@@ -621,22 +627,22 @@ void Batch::kick_drift(bool full) {
   const int nb = ceil_div(n_, kThreads);
   if (mixed_) {
     if (full)
-      k_kick_drift_batch<float, true><<<nb, kThreads, 0, s>>>(
-          pos4_.data(), q_.data(), vel_.data(), f32_.data(), types_.data(), rep_.data(),
-          reps_.data(), inv_mm_.data(), n, cfg_.dt);
+      launch(k_kick_drift_batch<float, true>, nb, kThreads, 0, s, pos4_.data(), q_.data(),
+             vel_.data(), f32_.data(), types_.data(), rep_.data(), reps_.data(), inv_mm_.data(), n,
+             cfg_.dt);
     else
-      k_kick_drift_batch<float, false><<<nb, kThreads, 0, s>>>(
-          pos4_.data(), q_.data(), vel_.data(), f32_.data(), types_.data(), rep_.data(),
-          reps_.data(), inv_mm_.data(), n, cfg_.dt);
+      launch(k_kick_drift_batch<float, false>, nb, kThreads, 0, s, pos4_.data(), q_.data(),
+             vel_.data(), f32_.data(), types_.data(), rep_.data(), reps_.data(), inv_mm_.data(), n,
+             cfg_.dt);
   } else {
     if (full)
-      k_kick_drift_batch<double, true><<<nb, kThreads, 0, s>>>(
-          pos4_.data(), nullptr, vel_.data(), f64_.data(), types_.data(), rep_.data(),
-          reps_.data(), inv_mm_.data(), n, cfg_.dt);
+      launch(k_kick_drift_batch<double, true>, nb, kThreads, 0, s, pos4_.data(), nullptr,
+             vel_.data(), f64_.data(), types_.data(), rep_.data(), reps_.data(), inv_mm_.data(), n,
+             cfg_.dt);
     else
-      k_kick_drift_batch<double, false><<<nb, kThreads, 0, s>>>(
-          pos4_.data(), nullptr, vel_.data(), f64_.data(), types_.data(), rep_.data(),
-          reps_.data(), inv_mm_.data(), n, cfg_.dt);
+      launch(k_kick_drift_batch<double, false>, nb, kThreads, 0, s, pos4_.data(), nullptr,
+             vel_.data(), f64_.data(), types_.data(), rep_.data(), reps_.data(), inv_mm_.data(), n,
+             cfg_.dt);
   }
   TDMD_LAUNCH_CHECK();
   ++launches_;
@@ -647,11 +653,11 @@ void Batch::half_kick() {
   const int n = static_cast<int>(n_);
   const int nb = ceil_div(n_, kThreads);
   if (mixed_)
-    k_half_kick_batch<float><<<nb, kThreads, 0, s>>>(vel_.data(), f32_.data(), types_.data(),
-                                                     inv_mm_.data(), n, cfg_.dt);
+    launch(k_half_kick_batch<float>, nb, kThreads, 0, s, vel_.data(), f32_.data(), types_.data(),
+           inv_mm_.data(), n, cfg_.dt);
   else
-    k_half_kick_batch<double><<<nb, kThreads, 0, s>>>(vel_.data(), f64_.data(), types_.data(),
-                                                      inv_mm_.data(), n, cfg_.dt);
+    launch(k_half_kick_batch<double>, nb, kThreads, 0, s, vel_.data(), f64_.data(), types_.data(),
+           inv_mm_.data(), n, cfg_.dt);
   TDMD_LAUNCH_CHECK();
   ++launches_;
 }
@@ -922,8 +928,8 @@ void Batch::reduce_energies(double* out) {
                                        nullptr, g_.data(), false, nullptr, Tune{lpa_d_, nu_d_}, s);
       TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(
           tn, {
-            k_eam_atom_pe<GeoQB, L, U, V, M><<<nblk, kThreads, 0, s>>>(
-                g, nl, n, eam_->d32, types, rho_.data(), pe_atom_.data());
+            launch(k_eam_atom_pe<GeoQB, L, U, V, M>, nblk, kThreads, 0, s, g, nl, n,
+                   eam_->d32, types, rho_.data(), pe_atom_.data());
           })));
     } else {
       const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
@@ -931,8 +937,8 @@ void Batch::reduce_energies(double* out) {
                                          nullptr, nullptr, false, nullptr, Tune{lpa_d_, nu_d_}, s);
       TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(
           tn, {
-            k_eam_atom_pe<GeoD4B, L, U, V, M><<<nblk, kThreads, 0, s>>>(
-                g, nl, n, eam_->d64, types, rho_.data(), pe_atom_.data());
+            launch(k_eam_atom_pe<GeoD4B, L, U, V, M>, nblk, kThreads, 0, s, g, nl, n,
+                   eam_->d64, types, rho_.data(), pe_atom_.data());
           })));
     }
     TDMD_LAUNCH_CHECK();
@@ -940,11 +946,11 @@ void Batch::reduce_energies(double* out) {
   } else {
     TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
       if (mixed_)
-        k_morse_atom_pe<GeoQB, L, U, V><<<nblk, kThreads, 0, s>>>(
-            GeoQB{q_.data(), rep_.data(), scales_.data()}, nl, n, m32_, pe_atom_.data());
+        launch(k_morse_atom_pe<GeoQB, L, U, V>, nblk, kThreads, 0, s,
+               GeoQB{q_.data(), rep_.data(), scales_.data()}, nl, n, m32_, pe_atom_.data());
       else
-        k_morse_atom_pe<GeoD4B, L, U, V><<<nblk, kThreads, 0, s>>>(
-            GeoD4B{pos4_.data(), rep_.data(), imgs_.data()}, nl, n, m64_, pe_atom_.data());
+        launch(k_morse_atom_pe<GeoD4B, L, U, V>, nblk, kThreads, 0, s,
+               GeoD4B{pos4_.data(), rep_.data(), imgs_.data()}, nl, n, m64_, pe_atom_.data());
     }));
     TDMD_LAUNCH_CHECK();
   }
@@ -957,8 +963,8 @@ void Batch::reduce_energies(double* out) {
 
 // Per-replica (PE, KE) from pe_atom_ and the velocities, into eout_.
 void Batch::rep_energy() {
-  k_rep_energy<<<nrep_, kThreads, 0, stream_>>>(pe_atom_.data(), vel_.data(), types_.data(),
-                                                masses_.data(), reps_.data(), eout_.data());
+  launch(k_rep_energy, nrep_, kThreads, 0, stream_, pe_atom_.data(), vel_.data(), types_.data(),
+         masses_.data(), reps_.data(), eout_.data());
   TDMD_LAUNCH_CHECK();
   ++launches_;
 }

@@ -177,10 +177,13 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* smem) {
   }
 }
 
-// One read-only 32-byte record (32-byte aligned) in one 256-bit load.
+// One read-only 32-byte record (32-byte aligned) in one 256-bit load.  The
+// inline-asm loads here and in forces.cuh are volatile so that the compiler
+// keeps them after grid_dependency_wait() (also a volatile asm): a load
+// without a memory operand could otherwise be hoisted above the wait.
 __device__ __forceinline__ double4 ld_d4(const double4* p) {
   double4 v;
-  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
       : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
       : "l"(p));
   return v;
@@ -193,5 +196,48 @@ int sm_count();
 
 // Stream from the C ABI's void*.
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// --------------------------------------------------------------------------
+// Programmatic dependent launch.  A kernel started by launch() may become
+// resident while the kernel before it in the stream (or graph) drains: its
+// blocks park in griddepcontrol.wait, which returns once every prerequisite
+// grid has completed and its memory operations are visible.  So a kernel
+// launched this way calls grid_dependency_wait() before its first global
+// memory access, read or write; release_dependents() then lets the next
+// launch be scheduled as this grid's blocks finish.  Both are no-ops in a
+// kernel launched without the attribute (or after a copy or memset).
+// --------------------------------------------------------------------------
+__device__ __forceinline__ void grid_dependency_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void release_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+// At the top of a kernel.  The next launch is released implicitly as this
+// grid's blocks exit: releasing it at the top measured slower, the parked
+// blocks of the next pass sharing the SMs with this pass's last wave.
+__device__ __forceinline__ void dependent_launch_prologue() { grid_dependency_wait(); }
+
+// Whether launch() sets the programmatic-serialization attribute (environment
+// TDMD_PDL=0 turns it off; read once per process).
+bool programmatic_launch();
+
+template <class... P, class... A>
+void launch(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+            A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  if (programmatic_launch()) {
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  TDMD_CU(cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...));
+}
 
 }  // namespace tdmd_b200

@@ -1,6 +1,7 @@
 // core.cu -- error state, device box set-up and the fixed-order device scan.
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 
 #include "buffers.cuh"
@@ -36,6 +37,14 @@ int sm_count() {
   TDMD_CU(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
   if (dev >= 0 && dev < kMaxCachedDevices) cached[dev].store(v, std::memory_order_relaxed);
   return v;
+}
+
+bool programmatic_launch() {
+  static const bool on = [] {
+    const char* v = std::getenv("TDMD_PDL");
+    return !(v && v[0] == '0');
+  }();
+  return on;
 }
 
 DevBox make_devbox(const tdmd_box& b, double r_list) {
@@ -105,6 +114,7 @@ __device__ int block_exclusive_scan(int v, int* smem, int* total) {
 }
 
 __global__ void k_scan_reduce(const int* __restrict__ in, long long n, int* __restrict__ sums) {
+  dependent_launch_prologue();
   __shared__ int smem[32];
   const long long base = static_cast<long long>(blockIdx.x) * kScanTile;
   int s = 0;
@@ -122,6 +132,7 @@ __global__ void k_scan_reduce(const int* __restrict__ in, long long n, int* __re
 // block).  out may alias in.  *total gets the overall sum when non-null.
 __global__ void k_scan_single(const int* __restrict__ in, int* __restrict__ out, long long n,
                               int* __restrict__ total_out) {
+  dependent_launch_prologue();
   __shared__ int smem[32];
   int carry = 0;
   for (long long base = 0; base < n; base += kScanTile) {
@@ -156,6 +167,7 @@ constexpr int kScanWide = 16;
 __global__ void __launch_bounds__(kScanThreads) k_scan_wide(const int* __restrict__ in,
                                                             int* __restrict__ out, int n,
                                                             int* __restrict__ total_out) {
+  dependent_launch_prologue();
   __shared__ int wsum[kScanWide][kScanThreads / 32];  // row k: per-warp totals -> prefixes
   __shared__ int rsum[kScanWide + 1];                 // rows' exclusive prefixes, total
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -212,6 +224,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_wide(const int* __restric
 
 __global__ void k_scan_apply(const int* __restrict__ in, int* __restrict__ out, long long n,
                              const int* __restrict__ block_prefix) {
+  dependent_launch_prologue();
   __shared__ int smem[32];
   const long long base = static_cast<long long>(blockIdx.x) * kScanTile;
   int v[kScanItems];
@@ -247,24 +260,24 @@ void device_exclusive_scan(const int* in, int* out, long long n, int* total, Dev
   }
   const long long nblocks = (n + kScanTile - 1) / kScanTile;
   if (n <= static_cast<long long>(kScanThreads) * kScanWide) {
-    k_scan_wide<<<1, kScanThreads, 0, stream>>>(in, out, static_cast<int>(n), total);
+    launch(k_scan_wide, 1, kScanThreads, 0, stream, in, out, static_cast<int>(n), total);
     TDMD_LAUNCH_CHECK();
     return;
   }
   // Up to kScanSingleTiles tiles one block walking the tiles beats three
   // launches; beyond that, reduce -> scan of block sums -> apply.
   if (nblocks <= kScanSingleTiles) {
-    k_scan_single<<<1, kScanThreads, 0, stream>>>(in, out, n, total);
+    launch(k_scan_single, 1, kScanThreads, 0, stream, in, out, n, total);
     TDMD_LAUNCH_CHECK();
     return;
   }
   tmp.reserve(static_cast<size_t>(nblocks));
-  k_scan_reduce<<<static_cast<unsigned>(nblocks), kScanThreads, 0, stream>>>(in, n, tmp.data());
+  launch(k_scan_reduce, static_cast<unsigned>(nblocks), kScanThreads, 0, stream, in, n, tmp.data());
   TDMD_LAUNCH_CHECK();
-  k_scan_single<<<1, kScanThreads, 0, stream>>>(tmp.data(), tmp.data(), nblocks, total);
+  launch(k_scan_single, 1, kScanThreads, 0, stream, tmp.data(), tmp.data(), nblocks, total);
   TDMD_LAUNCH_CHECK();
-  k_scan_apply<<<static_cast<unsigned>(nblocks), kScanThreads, 0, stream>>>(in, out, n,
-                                                                            tmp.data());
+  launch(k_scan_apply, static_cast<unsigned>(nblocks), kScanThreads, 0, stream, in, out, n,
+         tmp.data());
   TDMD_LAUNCH_CHECK();
 }
 

@@ -125,6 +125,7 @@ __global__ void k_morse_idorder(const double* __restrict__ pos, double* __restri
                                 const int* __restrict__ cnt, int n, IdBox b, double D,
                                 double alpha, double r0, double rc_sq,
                                 double* __restrict__ e_atom, double* __restrict__ w_atom) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double xi = pos[3ll * i], yi = pos[3ll * i + 1], zi = pos[3ll * i + 2];
@@ -165,6 +166,7 @@ __global__ void k_eam_density_idorder(const double* __restrict__ pos,
                                       const RefSpline* __restrict__ dens,
                                       const double* __restrict__ coeff,
                                       double* __restrict__ rho) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double xi = pos[3ll * i], yi = pos[3ll * i + 1], zi = pos[3ll * i + 2];
@@ -189,6 +191,7 @@ __global__ void k_eam_embed_idorder(const int* __restrict__ types, int n,
                                     const double* __restrict__ coeff,
                                     const double* __restrict__ rho, double* __restrict__ fp,
                                     double* __restrict__ e_atom) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int ti = types[i] - 1;
@@ -216,6 +219,7 @@ __global__ void k_eam_force_idorder(const double* __restrict__ pos, double* __re
                                     const double* __restrict__ coeff,
                                     const double* __restrict__ fp, double* __restrict__ e_atom,
                                     double* __restrict__ w_atom) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double xi = pos[3ll * i], yi = pos[3ll * i + 1], zi = pos[3ll * i + 2];
@@ -256,6 +260,7 @@ __global__ void k_eam_force_idorder(const double* __restrict__ pos, double* __re
 // v[6i + k].
 __global__ void k_sum_in_id_order(const double* __restrict__ v, int n, int stride,
                                   double* __restrict__ out) {
+  dependent_launch_prologue();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int k = 0; k < stride; ++k) {
     double s = out[k];
@@ -313,16 +318,15 @@ void morse_id_ordered(const double* pos, double* forces, const int* nbr, const i
                       double* energy, double* virial, cudaStream_t s) {
   Scratch e_atom(static_cast<size_t>(n), s);
   Scratch w_atom(virial ? 6 * static_cast<size_t>(n) : 0, s);
-  k_morse_idorder<<<ceil_div(n, kThreads), kThreads, 0, s>>>(
-      pos, forces, nbr, off, cnt, n, id_box(box), p.d, p.alpha, p.r0, p.rc_sq, e_atom.p,
-      virial ? w_atom.p : nullptr);
+  launch(k_morse_idorder, ceil_div(n, kThreads), kThreads, 0, s, pos, forces, nbr, off, cnt, n,
+         id_box(box), p.d, p.alpha, p.r0, p.rc_sq, e_atom.p, virial ? w_atom.p : nullptr);
   TDMD_LAUNCH_CHECK();
   if (energy) {
-    k_sum_in_id_order<<<1, 1, 0, s>>>(e_atom.p, n, 1, energy);
+    launch(k_sum_in_id_order, 1, 1, 0, s, e_atom.p, n, 1, energy);
     TDMD_LAUNCH_CHECK();
   }
   if (virial) {
-    k_sum_in_id_order<<<1, 1, 0, s>>>(w_atom.p, n, 6, virial);
+    launch(k_sum_in_id_order, 1, 1, 0, s, w_atom.p, n, 6, virial);
     TDMD_LAUNCH_CHECK();
   }
 }
@@ -341,26 +345,25 @@ void eam_id_ordered(const RefEamTables& t, const double* pos, double* forces, co
   const RefSpline* dens = emb + nt;
   const RefSpline* phi = emb + 2 * nt;
   const int nb = ceil_div(n, kThreads);
-  k_eam_density_idorder<<<nb, kThreads, 0, s>>>(pos, types, nbr, off, cnt, n, b, rc_sq, dens,
-                                                 t.coeff.data(), rho.p);
+  launch(k_eam_density_idorder, nb, kThreads, 0, s, pos, types, nbr, off, cnt, n, b, rc_sq, dens,
+         t.coeff.data(), rho.p);
   TDMD_LAUNCH_CHECK();
-  k_eam_embed_idorder<<<nb, kThreads, 0, s>>>(types, n, emb, t.coeff.data(), rho.p, fp.p,
-                                               e_atom.p);
+  launch(k_eam_embed_idorder, nb, kThreads, 0, s, types, n, emb, t.coeff.data(), rho.p, fp.p,
+         e_atom.p);
   TDMD_LAUNCH_CHECK();
   if (energy) {
-    k_sum_in_id_order<<<1, 1, 0, s>>>(e_atom.p, n, 1, energy);
+    launch(k_sum_in_id_order, 1, 1, 0, s, e_atom.p, n, 1, energy);
     TDMD_LAUNCH_CHECK();
   }
-  k_eam_force_idorder<<<nb, kThreads, 0, s>>>(pos, forces, types, nbr, off, cnt, n, nt, b, rc_sq,
-                                               dens, phi, t.coeff.data(), fp.p, e_atom.p,
-                                               virial ? w_atom.p : nullptr);
+  launch(k_eam_force_idorder, nb, kThreads, 0, s, pos, forces, types, nbr, off, cnt, n, nt, b,
+         rc_sq, dens, phi, t.coeff.data(), fp.p, e_atom.p, virial ? w_atom.p : nullptr);
   TDMD_LAUNCH_CHECK();
   if (energy) {
-    k_sum_in_id_order<<<1, 1, 0, s>>>(e_atom.p, n, 1, energy);
+    launch(k_sum_in_id_order, 1, 1, 0, s, e_atom.p, n, 1, energy);
     TDMD_LAUNCH_CHECK();
   }
   if (virial) {
-    k_sum_in_id_order<<<1, 1, 0, s>>>(w_atom.p, n, 6, virial);
+    launch(k_sum_in_id_order, 1, 1, 0, s, w_atom.p, n, 6, virial);
     TDMD_LAUNCH_CHECK();
   }
   if (rho_out)

@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(kThreads) k_fm_morse_force(
     Geo g, NbrView nl, int n, const double* __restrict__ prm, double rc_sq,
     const double* __restrict__ target, double c, double* __restrict__ G,
     double* __restrict__ fout, double* __restrict__ part) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA, sub = tid % LPA;
@@ -197,6 +198,7 @@ __global__ void __launch_bounds__(kThreads) k_fm_morse_grad(Geo g, NbrView nl, i
                                                             double rc_sq,
                                                             const double* __restrict__ G,
                                                             double* __restrict__ part) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA, sub = tid % LPA;
@@ -237,6 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_fm_morse_grad(Geo g, NbrView nl, i
 // out[0..nv) = column sums.
 __global__ void k_fm_sum(const double* __restrict__ part, int nblk, int nv,
                          double* __restrict__ out) {
+  dependent_launch_prologue();
   __shared__ double red[32 * kPart];
   double v[kPart] = {0.0, 0.0, 0.0, 0.0};
   for (int b = threadIdx.x; b < nblk; b += blockDim.x)
@@ -253,6 +256,7 @@ template <class Geo, int LPA>
 __global__ void __launch_bounds__(kThreads) k_fm_eam_density(
     Geo g, NbrView nl, int n, const int* __restrict__ types, FitEam e, double rc_sq,
     double* __restrict__ rho_out, double* __restrict__ fp_out, double* __restrict__ fpp_out) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA, sub = tid % LPA;
@@ -294,6 +298,7 @@ __global__ void __launch_bounds__(kThreads) k_fm_eam_force(
     Geo g, NbrView nl, int n, const int* __restrict__ types, FitEam e, double rc_sq,
     const double* __restrict__ fp, const double* __restrict__ target, double c,
     double* __restrict__ G, double* __restrict__ fout, double* __restrict__ part) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA, sub = tid % LPA;
@@ -351,6 +356,7 @@ __global__ void __launch_bounds__(kThreads) k_fm_eam_adjoint(
     Geo g, NbrView nl, int n, const int* __restrict__ types, FitEam e, double rc_sq,
     const double* __restrict__ rho, const double* __restrict__ fp,
     const double* __restrict__ fpp, const double* __restrict__ G) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA, sub = tid % LPA;
@@ -435,6 +441,7 @@ __global__ void __launch_bounds__(kThreads) k_fm_eam_adjoint_w(
     Geo g, NbrView nl, int n, FitEam e, double rc_sq, const double* __restrict__ rho,
     const double* __restrict__ fp, const double* __restrict__ fpp,
     const double* __restrict__ G, int k0, int W) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   extern __shared__ double sg[];
   double* const sphi = sg;
@@ -713,24 +720,23 @@ void Fit::morse(const double* d_prm, double* d_loss, double* d_grad, double* d_f
   with_geo([&](auto g) {
     using Geo = decltype(g);
     TDMD_LPA_DISPATCH(lpa_, {
-      k_fm_morse_force<Geo, L><<<nblk, kThreads, 0, s>>>(g, nl, m, d_prm, rc_sq_,
-                                                         target_.data(), c, G_.data(), d_forces,
-                                                         part_.data());
+      launch(k_fm_morse_force<Geo, L>, nblk, kThreads, 0, s, g, nl, m, d_prm, rc_sq_,
+             target_.data(), c, G_.data(), d_forces, part_.data());
     });
   });
   TDMD_LAUNCH_CHECK();
-  k_fm_sum<<<1, kThreads, 0, s>>>(part_.data(), nblk, 1, d_loss);
+  launch(k_fm_sum, 1, kThreads, 0, s, part_.data(), nblk, 1, d_loss);
   TDMD_LAUNCH_CHECK();
   if (!d_grad) return;
   with_geo([&](auto g) {
     using Geo = decltype(g);
     TDMD_LPA_DISPATCH(lpa_, {
-      k_fm_morse_grad<Geo, L><<<nblk, kThreads, 0, s>>>(g, nl, m, d_prm, rc_sq_, G_.data(),
-                                                        part_.data());
+      launch(k_fm_morse_grad<Geo, L>, nblk, kThreads, 0, s, g, nl, m, d_prm, rc_sq_, G_.data(),
+             part_.data());
     });
   });
   TDMD_LAUNCH_CHECK();
-  k_fm_sum<<<1, kThreads, 0, s>>>(part_.data(), nblk, 3, d_grad);
+  launch(k_fm_sum, 1, kThreads, 0, s, part_.data(), nblk, 3, d_grad);
   TDMD_LAUNCH_CHECK();
 }
 
@@ -762,11 +768,10 @@ void Fit::eam(int ntypes, int nrho, double drho, int nr, double dr, const double
   with_geo([&](auto g) {
     using Geo = decltype(g);
     TDMD_LPA_DISPATCH(lpa_, {
-      k_fm_eam_density<Geo, L><<<nblk, kThreads, 0, s>>>(g, nl, m, types_.data(), e, rc_sq_,
-                                                         rho_.data(), fp_.data(), fpp_.data());
-      k_fm_eam_force<Geo, L><<<nblk, kThreads, 0, s>>>(g, nl, m, types_.data(), e, rc_sq_,
-                                                       fp_.data(), target_.data(), c, G_.data(),
-                                                       d_forces, part_.data());
+      launch(k_fm_eam_density<Geo, L>, nblk, kThreads, 0, s, g, nl, m, types_.data(), e, rc_sq_,
+             rho_.data(), fp_.data(), fpp_.data());
+      launch(k_fm_eam_force<Geo, L>, nblk, kThreads, 0, s, g, nl, m, types_.data(), e, rc_sq_,
+             fp_.data(), target_.data(), c, G_.data(), d_forces, part_.data());
       if (grad && ntypes == 1) {
         // one element: shared-memory window of the r-spline gradients over
         // the top W intervals, a persistent grid of two blocks per SM
@@ -776,17 +781,16 @@ void Fit::eam(int ntypes, int nrho, double drho, int nr, double dr, const double
         TDMD_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         const int grid = std::min(2 * sm_count(), nblk);
-        kern<<<grid, kThreads, smem, s>>>(g, nl, m, e, rc_sq_, rho_.data(), fp_.data(),
-                                          fpp_.data(), G_.data(), (nr - 1) - W, W);
+        launch(kern, grid, kThreads, smem, s, g, nl, m, e, rc_sq_, rho_.data(), fp_.data(),
+               fpp_.data(), G_.data(), (nr - 1) - W, W);
       } else if (grad) {
-        k_fm_eam_adjoint<Geo, L><<<nblk, kThreads, 0, s>>>(g, nl, m, types_.data(), e, rc_sq_,
-                                                           rho_.data(), fp_.data(), fpp_.data(),
-                                                           G_.data());
+        launch(k_fm_eam_adjoint<Geo, L>, nblk, kThreads, 0, s, g, nl, m, types_.data(), e, rc_sq_,
+               rho_.data(), fp_.data(), fpp_.data(), G_.data());
       }
     });
   });
   TDMD_LAUNCH_CHECK();
-  k_fm_sum<<<1, kThreads, 0, s>>>(part_.data(), nblk, 1, d_loss);
+  launch(k_fm_sum, 1, kThreads, 0, s, part_.data(), nblk, 1, d_loss);
   TDMD_LAUNCH_CHECK();
 }
 

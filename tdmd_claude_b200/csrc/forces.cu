@@ -259,6 +259,7 @@ void EamDevTables::upload(const tdmd_eam& e, cudaStream_t stream) {
 // --------------------------------------------------------------------------
 __global__ void k_reduce_partials(const double* __restrict__ partials, int nblk,
                                   double* __restrict__ energy, double* __restrict__ virial) {
+  dependent_launch_prologue();
   __shared__ double red[32 * 7];
   double v[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
@@ -431,7 +432,7 @@ int32_t tdmd_morse_compute(const double* d_positions, void* d_forces, int32_t pr
       launch_morse(g, nl, natoms, mp, static_cast<float*>(d_forces), ev, part.p, lpa, s);
     }
     if (ev) {
-      k_reduce_partials<<<1, 256, 0, s>>>(part.p, nblk, d_energy, d_virial);
+      launch(k_reduce_partials, 1, 256, 0, s, part.p, nblk, d_energy, d_virial);
       TDMD_LAUNCH_CHECK();
     }
   });
@@ -497,7 +498,7 @@ int32_t tdmd_device_eam_compute(tdmd_device_eam* de, const double* d_positions, 
                  static_cast<float*>(d_forces), ev, part.p, lpa, s);
     }
     if (ev) {
-      k_reduce_partials<<<1, 256, 0, s>>>(part.p, 2 * nblk, d_energy, d_virial);
+      launch(k_reduce_partials, 1, 256, 0, s, part.p, 2 * nblk, d_energy, d_virial);
       TDMD_LAUNCH_CHECK();
     }
   });

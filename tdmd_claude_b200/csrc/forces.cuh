@@ -65,14 +65,14 @@ struct NbrView {
 // (no_allocate), so they do not push rows and position records out.
 __device__ __forceinline__ float4 ld_keep(const float4* p) {
   float4 v;
-  asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+  asm volatile("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
       : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
       : "l"(p));
   return v;
 }
 __device__ __forceinline__ int4 ld_stream(const int4* p) {
   int4 v;
-  asm("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+  asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
       : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
       : "l"(p));
   return v;
@@ -85,7 +85,9 @@ constexpr int kU = 4;
 
 __device__ __forceinline__ int2 ld_stream2(const int2* p) {
   int2 v;
-  asm("ld.global.nc.L1::no_allocate.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.v2.s32 {%0, %1}, [%2];"
+               : "=r"(v.x), "=r"(v.y)
+               : "l"(p));
   return v;
 }
 
@@ -414,6 +416,7 @@ __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
                                                MorseP<typename Geo::T> mp, ForceOut<F> out,
                                                double* __restrict__ partials,
                                                double* __restrict__ pe_atom) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;
@@ -591,7 +594,7 @@ __device__ __forceinline__ float4 ldv4<float>(const float4* p) {
 // on a 32-byte boundary (one sector), in one 256-bit load: one L1 request per
 // pair instead of two.
 __device__ __forceinline__ void ld_rows2(const float4* p, float4& a, float4& b) {
-  asm("ld.global.nc.L1::evict_last.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+  asm volatile("ld.global.nc.L1::evict_last.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
       : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
       : "l"(p));
 }
@@ -620,6 +623,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
                                                      int4* __restrict__ gout,
                                                      double* __restrict__ partials,
                                                      double* __restrict__ e_out) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;
@@ -749,6 +753,7 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
                                                    double* __restrict__ partials,
                                                    KickDrift kd = {},
                                                    double* __restrict__ pe_atom = nullptr) {
+  dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / LPA;

@@ -22,6 +22,7 @@ template <class F>
 __global__ void k_half_kick(double* __restrict__ v, const F* __restrict__ f,
                             const int* __restrict__ types, const double* __restrict__ masses,
                             int n, double half_dt) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double factor = half_dt / (masses[types[i]] * kMvv2e);
@@ -31,6 +32,7 @@ __global__ void k_half_kick(double* __restrict__ v, const F* __restrict__ f,
 
 __global__ void k_drift(double* __restrict__ x, const double* __restrict__ v, int n, double dt,
                         DevBox b) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
 #pragma unroll
@@ -44,6 +46,7 @@ template <class F, bool FULL>
 __global__ void k_fused_kick_drift(double* __restrict__ v, double* __restrict__ x,
                                    const F* __restrict__ f, const int* __restrict__ types,
                                    const double* __restrict__ masses, int n, double dt, DevBox b) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double kick_dt = FULL ? dt : 0.5 * dt;
@@ -58,11 +61,13 @@ __global__ void k_fused_kick_drift(double* __restrict__ v, double* __restrict__ 
 
 template <class F>
 __global__ void k_zero(F* __restrict__ f, long long m) {
+  dependent_launch_prologue();
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < m) f[i] = F(0);
 }
 
 __global__ void k_scale(double* __restrict__ v, long long m, double s) {
+  dependent_launch_prologue();
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < m) v[i] *= s;
 }
@@ -73,6 +78,7 @@ __global__ void k_scale(double* __restrict__ v, long long m, double s) {
 __global__ void k_ke_vmax_partials(const double* __restrict__ v, const int* __restrict__ types,
                                    const double* __restrict__ masses, int n,
                                    double* __restrict__ partials) {
+  dependent_launch_prologue();
   __shared__ double red[32 * 2];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0.0, v2 = 0.0;
@@ -106,6 +112,7 @@ __global__ void k_ke_vmax_partials(const double* __restrict__ v, const int* __re
 // out[1] = max |v|^2.
 __global__ void k_ke_vmax_finish(const double* __restrict__ partials, int nblk,
                                  double* __restrict__ out) {
+  dependent_launch_prologue();
   __shared__ double red[32 * 2];
   double ke = 0.0, v2 = 0.0;
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
@@ -173,9 +180,9 @@ void ke_vmax(const double* v, const int* types, const double* masses, int n, dou
   const int nblk = ceil_div(n, kThreads);
   double* buf = nullptr;
   TDMD_CU(cudaMallocAsync(reinterpret_cast<void**>(&buf), sizeof(double) * (2ll * nblk + 2), s));
-  k_ke_vmax_partials<<<nblk, kThreads, 0, s>>>(v, types, masses, n, buf);
+  launch(k_ke_vmax_partials, nblk, kThreads, 0, s, v, types, masses, n, buf);
   cudaError_t e1 = cudaGetLastError();
-  k_ke_vmax_finish<<<1, 256, 0, s>>>(buf, nblk, buf + 2ll * nblk);
+  launch(k_ke_vmax_finish, 1, 256, 0, s, buf, nblk, buf + 2ll * nblk);
   cudaError_t e2 = cudaGetLastError();
   cudaError_t e3 = cudaMemcpyAsync(h2, buf + 2ll * nblk, 2 * sizeof(double),
                                    cudaMemcpyDeviceToHost, s);
@@ -198,8 +205,9 @@ int32_t tdmd_vv_half_kick(double* d_velocities, const void* d_forces, int32_t fo
     if (natoms == 0) return;
     TDMD_REQUIRE(d_velocities && d_forces && d_types && d_masses, "null device array");
     with_forces(force_precision, d_forces, [&](auto f) {
-      k_half_kick<<<ceil_div(natoms, kThreads), kThreads, 0, as_stream(stream)>>>(
-          d_velocities, f, d_types, d_masses, natoms, 0.5 * dt);
+      using F = std::remove_cv_t<std::remove_pointer_t<decltype(f)>>;
+      launch(k_half_kick<F>, ceil_div(natoms, kThreads), kThreads, 0, as_stream(stream),
+             d_velocities, f, d_types, d_masses, natoms, 0.5 * dt);
       TDMD_LAUNCH_CHECK();
       return 0;
     });
@@ -212,8 +220,8 @@ int32_t tdmd_vv_drift(double* d_positions, const double* d_velocities, int32_t n
     TDMD_REQUIRE(box && natoms >= 0, "bad arguments");
     if (natoms == 0) return;
     TDMD_REQUIRE(d_positions && d_velocities, "null device array");
-    k_drift<<<ceil_div(natoms, kThreads), kThreads, 0, as_stream(stream)>>>(
-        d_positions, d_velocities, natoms, dt, make_devbox(*box, 0.0));
+    launch(k_drift, ceil_div(natoms, kThreads), kThreads, 0, as_stream(stream), d_positions,
+           d_velocities, natoms, dt, make_devbox(*box, 0.0));
     TDMD_LAUNCH_CHECK();
   });
 }
@@ -231,11 +239,11 @@ int32_t tdmd_vv_fused_kick_drift(double* d_velocities, double* d_positions, cons
     with_forces(force_precision, d_forces, [&](auto f) {
       using F = std::remove_cv_t<std::remove_pointer_t<decltype(f)>>;
       if (full_kick)
-        k_fused_kick_drift<F, true><<<ceil_div(natoms, kThreads), kThreads, 0, as_stream(stream)>>>(
-            d_velocities, d_positions, f, d_types, d_masses, natoms, dt, b);
+        launch(k_fused_kick_drift<F, true>, ceil_div(natoms, kThreads), kThreads, 0,
+               as_stream(stream), d_velocities, d_positions, f, d_types, d_masses, natoms, dt, b);
       else
-        k_fused_kick_drift<F, false><<<ceil_div(natoms, kThreads), kThreads, 0, as_stream(stream)>>>(
-            d_velocities, d_positions, f, d_types, d_masses, natoms, dt, b);
+        launch(k_fused_kick_drift<F, false>, ceil_div(natoms, kThreads), kThreads, 0,
+               as_stream(stream), d_velocities, d_positions, f, d_types, d_masses, natoms, dt, b);
       TDMD_LAUNCH_CHECK();
       return 0;
     });
@@ -250,11 +258,11 @@ int32_t tdmd_vv_zero_forces(void* d_forces, int32_t force_precision, int32_t nat
     TDMD_REQUIRE(d_forces, "null device array");
     const long long m = 3ll * natoms;
     if (force_precision == TDMD_FP64)
-      k_zero<<<ceil_div(m, kThreads), kThreads, 0, as_stream(stream)>>>(
-          static_cast<double*>(d_forces), m);
+      launch(k_zero<double>, ceil_div(m, kThreads), kThreads, 0, as_stream(stream),
+             static_cast<double*>(d_forces), m);
     else
-      k_zero<<<ceil_div(m, kThreads), kThreads, 0, as_stream(stream)>>>(
-          static_cast<float*>(d_forces), m);
+      launch(k_zero<float>, ceil_div(m, kThreads), kThreads, 0, as_stream(stream),
+             static_cast<float*>(d_forces), m);
     TDMD_LAUNCH_CHECK();
   });
 }
@@ -306,7 +314,7 @@ int32_t tdmd_scale_velocities(double* d_velocities, int32_t natoms, double facto
     if (natoms == 0) return;
     TDMD_REQUIRE(d_velocities, "null device array");
     const long long m = 3ll * natoms;
-    k_scale<<<ceil_div(m, kThreads), kThreads, 0, as_stream(stream)>>>(d_velocities, m, factor);
+    launch(k_scale, ceil_div(m, kThreads), kThreads, 0, as_stream(stream), d_velocities, m, factor);
     TDMD_LAUNCH_CHECK();
   });
 }

@@ -75,14 +75,14 @@ void launch_morse(const Geo& g, const NbrView& nl, int n, const MorseP<typename 
   const int nblk = force_blocks(n, tn.lpa);
   TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
     if (ev && !partials && pe_atom)  // per-atom energies only
-      k_morse<Geo, L, U, 2, V, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, mp, ForceOut<F>{forces}, nullptr, pe_atom);
+      launch(k_morse<Geo, L, U, 2, V, F>, nblk, kForceThreads, 0, s, g, nl, n, mp,
+             ForceOut<F>{forces}, nullptr, pe_atom);
     else if (ev)
-      k_morse<Geo, L, U, 1, V, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, mp, ForceOut<F>{forces}, partials, pe_atom);
+      launch(k_morse<Geo, L, U, 1, V, F>, nblk, kForceThreads, 0, s, g, nl, n, mp,
+             ForceOut<F>{forces}, partials, pe_atom);
     else
-      k_morse<Geo, L, U, 0, V, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, mp, ForceOut<F>{forces}, nullptr, nullptr);
+      launch(k_morse<Geo, L, U, 0, V, F>, nblk, kForceThreads, 0, s, g, nl, n, mp,
+             ForceOut<F>{forces}, nullptr, nullptr);
   }));
   TDMD_LAUNCH_CHECK();
 }
@@ -98,11 +98,11 @@ void launch_eam_density(const Geo& g, const NbrView& nl, int n,
   const int nblk = force_blocks(n, tn.lpa);
   TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
     if (ev)
-      k_eam_density<Geo, L, U, true, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, e, types, fp, rho_out, fpd_out, gout, partials, e_out);
+      launch(k_eam_density<Geo, L, U, true, V, M, FP>, nblk, kForceThreads, 0, s, g, nl, n, e,
+             types, fp, rho_out, fpd_out, gout, partials, e_out);
     else
-      k_eam_density<Geo, L, U, false, V, M, FP><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, e, types, fp, rho_out, fpd_out, gout, nullptr, e_out);
+      launch(k_eam_density<Geo, L, U, false, V, M, FP>, nblk, kForceThreads, 0, s, g, nl, n, e,
+             types, fp, rho_out, fpd_out, gout, nullptr, e_out);
   })));
   TDMD_LAUNCH_CHECK();
 }
@@ -120,22 +120,22 @@ void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typen
   const int nblk = force_blocks(n, tn.lpa);
   TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
     if (ev && !partials && pe_atom)  // per-atom energies only
-      k_eam_force<Geo, L, U, 2, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr, KickDrift{}, pe_atom);
+      launch(k_eam_force<Geo, L, U, 2, FPG, V, M, FP, F>, nblk, kForceThreads, 0, s, g, nl, n, e,
+             types, fp, ForceOut<F>{forces}, nullptr, KickDrift{}, pe_atom);
     else if (ev)
-      k_eam_force<Geo, L, U, 1, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, e, types, fp, ForceOut<F>{forces}, partials, KickDrift{}, pe_atom);
+      launch(k_eam_force<Geo, L, U, 1, FPG, V, M, FP, F>, nblk, kForceThreads, 0, s, g, nl, n, e,
+             types, fp, ForceOut<F>{forces}, partials, KickDrift{}, pe_atom);
     else if constexpr (FPG && sizeof(F) == sizeof(float)) {
       if (kd)
-        k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F, true><<<nblk, kForceThreads, 0, s>>>(
-            g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr, *kd);
+        launch(k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F, true>, nblk, kForceThreads, 0, s, g, nl,
+               n, e, types, fp, ForceOut<F>{forces}, nullptr, *kd, nullptr);
       else
-        k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
-            g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
+        launch(k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F>, nblk, kForceThreads, 0, s, g, nl, n, e,
+               types, fp, ForceOut<F>{forces}, nullptr, KickDrift{}, nullptr);
     } else {
       TDMD_REQUIRE(kd == nullptr, "fused kick-drift needs the mixed gather-record pass");
-      k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F><<<nblk, kForceThreads, 0, s>>>(
-          g, nl, n, e, types, fp, ForceOut<F>{forces}, nullptr);
+      launch(k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F>, nblk, kForceThreads, 0, s, g, nl, n, e,
+             types, fp, ForceOut<F>{forces}, nullptr, KickDrift{}, nullptr);
     }
   })));
   TDMD_LAUNCH_CHECK();

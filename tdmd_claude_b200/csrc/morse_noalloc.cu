@@ -110,7 +110,7 @@ extern "C" int32_t tdmd_morse_compute_noalloc(const double* d_positions, void* d
       launch_morse(g, nl, natoms, mp, static_cast<float*>(d_forces), ev, part, lpa, s);
     }
     if (ev) {
-      k_reduce_partials<<<1, 256, 0, s>>>(part, nblk, d_energy, d_virial);
+      launch(k_reduce_partials, 1, 256, 0, s, part, nblk, d_energy, d_virial);
       TDMD_LAUNCH_CHECK();
     }
   });

@@ -55,6 +55,7 @@ struct LoadD4 {
 template <class Load>
 __global__ void k_bin_atoms(Load pos, int n, DevBox b, int* __restrict__ atom_cell,
                             int* __restrict__ cell_count) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double3 p = pos(i);
@@ -68,6 +69,7 @@ __global__ void k_bin_atoms(Load pos, int n, DevBox b, int* __restrict__ atom_ce
 
 __global__ void k_scatter_atoms(const int* __restrict__ atom_cell, int n,
                                 int* __restrict__ cursor, int* __restrict__ cell_atoms) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int slot = atomicAdd(&cursor[atom_cell[i]], 1);
@@ -84,6 +86,7 @@ constexpr int kSortPerLane = 4;
 __global__ void k_sort_cells(const int* __restrict__ cell_start, const int* __restrict__ cell_count,
                              int ncells, int* __restrict__ cell_atoms,
                              const int* __restrict__ key) {
+  dependent_launch_prologue();
   const long long gw = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (gw >= ncells) return;  // uniform per warp
@@ -523,6 +526,7 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells(
     const int* __restrict__ cell_atoms, double rl2, float lo_f, float hi_f, int* __restrict__ nbr,
     const int* __restrict__ row_off, int cap, int* __restrict__ counts,
     int* __restrict__ status, int stage_cap) {
+  dependent_launch_prologue();
   // The stage is dynamic shared memory of stage_cap records (sized by the
   // launch from the mean cell occupancy, so that more CTAs fit on an SM).
   extern __shared__ float4 stage[];
@@ -541,6 +545,7 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells_batch(
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const int* __restrict__ cell_atoms, double rl2, int* __restrict__ nbr, int cap,
     int* __restrict__ counts, int* __restrict__ status) {
+  dependent_launch_prologue();
   __shared__ float4 stage[kStageCap];
   __shared__ RowSmem sm;
   __shared__ SlabSmem ss;
@@ -566,6 +571,7 @@ __global__ void __launch_bounds__(kRowThreads) k_build_cells_batch(
 __global__ void k_bin_atoms_batch(LoadD4 pos, const int* __restrict__ rep,
                                   const RepDesc* __restrict__ reps, int n,
                                   int* __restrict__ atom_cell, int* __restrict__ cell_count) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const RepDesc* d = reps + __ldg(rep + i);
@@ -600,25 +606,21 @@ void build_cell_list(CellListDev& cl, const void* d_pos, PosLayout layout, long 
   TDMD_CU(cudaMemsetAsync(cl.cell_count.data(), 0, sizeof(int) * ncells, stream));
   const int nb = ceil_div(n, 256);
   if (layout == PosLayout::AoS3)
-    k_bin_atoms<<<nb, 256, 0, stream>>>(LoadAoS3{static_cast<const double*>(d_pos)},
-                                        static_cast<int>(n), box, cl.atom_cell.data(),
-                                        cl.cell_count.data());
+    launch(k_bin_atoms<LoadAoS3>, nb, 256, 0, stream, LoadAoS3{static_cast<const double*>(d_pos)},
+           static_cast<int>(n), box, cl.atom_cell.data(), cl.cell_count.data());
   else
-    k_bin_atoms<<<nb, 256, 0, stream>>>(LoadD4{static_cast<const double4*>(d_pos)},
-                                        static_cast<int>(n), box, cl.atom_cell.data(),
-                                        cl.cell_count.data());
+    launch(k_bin_atoms<LoadD4>, nb, 256, 0, stream, LoadD4{static_cast<const double4*>(d_pos)},
+           static_cast<int>(n), box, cl.atom_cell.data(), cl.cell_count.data());
   TDMD_LAUNCH_CHECK();
   device_exclusive_scan(cl.cell_count.data(), cl.cell_start.data(), ncells, nullptr, cl.scan_tmp,
                         stream);
   TDMD_CU(cudaMemcpyAsync(cl.cursor.data(), cl.cell_start.data(), sizeof(int) * ncells,
                           cudaMemcpyDeviceToDevice, stream));
-  k_scatter_atoms<<<nb, 256, 0, stream>>>(cl.atom_cell.data(), static_cast<int>(n),
-                                          cl.cursor.data(), cl.cell_atoms.data());
+  launch(k_scatter_atoms, nb, 256, 0, stream, cl.atom_cell.data(), static_cast<int>(n),
+         cl.cursor.data(), cl.cell_atoms.data());
   TDMD_LAUNCH_CHECK();
-  k_sort_cells<<<ceil_div(ncells * 32, 256), 256, 0, stream>>>(cl.cell_start.data(),
-                                                                cl.cell_count.data(),
-                                                                static_cast<int>(ncells),
-                                                                cl.cell_atoms.data(), key);
+  launch(k_sort_cells, ceil_div(ncells * 32, 256), 256, 0, stream, cl.cell_start.data(),
+         cl.cell_count.data(), static_cast<int>(ncells), cl.cell_atoms.data(), key);
   TDMD_LAUNCH_CHECK();
 }
 
@@ -652,18 +654,18 @@ void build_cell_list_batch(CellListDev& cl, const double4* pos, const int* rep,
   if (n == 0) return;
   TDMD_CU(cudaMemsetAsync(cl.cell_count.data(), 0, sizeof(int) * ncells_total, stream));
   const int nb = ceil_div(n, 256);
-  k_bin_atoms_batch<<<nb, 256, 0, stream>>>(LoadD4{pos}, rep, reps, static_cast<int>(n),
-                                            cl.atom_cell.data(), cl.cell_count.data());
+  launch(k_bin_atoms_batch, nb, 256, 0, stream, LoadD4{pos}, rep, reps, static_cast<int>(n),
+         cl.atom_cell.data(), cl.cell_count.data());
   TDMD_LAUNCH_CHECK();
   device_exclusive_scan(cl.cell_count.data(), cl.cell_start.data(), ncells_total, nullptr,
                         cl.scan_tmp, stream);
   TDMD_CU(cudaMemcpyAsync(cl.cursor.data(), cl.cell_start.data(), sizeof(int) * ncells_total,
                           cudaMemcpyDeviceToDevice, stream));
-  k_scatter_atoms<<<nb, 256, 0, stream>>>(cl.atom_cell.data(), static_cast<int>(n),
-                                          cl.cursor.data(), cl.cell_atoms.data());
+  launch(k_scatter_atoms, nb, 256, 0, stream, cl.atom_cell.data(), static_cast<int>(n),
+         cl.cursor.data(), cl.cell_atoms.data());
   TDMD_LAUNCH_CHECK();
-  k_sort_cells<<<ceil_div(1ll * ncells_total * 32, 256), 256, 0, stream>>>(
-      cl.cell_start.data(), cl.cell_count.data(), ncells_total, cl.cell_atoms.data(), nullptr);
+  launch(k_sort_cells, ceil_div(1ll * ncells_total * 32, 256), 256, 0, stream, cl.cell_start.data(),
+         cl.cell_count.data(), ncells_total, cl.cell_atoms.data(), nullptr);
   TDMD_LAUNCH_CHECK();
 }
 
@@ -672,13 +674,13 @@ void build_neighbor_rows_batch(const CellListDev& cl, const double4* pos, const 
                                int* counts, int* status, cudaStream_t stream) {
   if (cl.natoms == 0 || cl.ncells == 0) return;
   if (nbr)
-    k_build_cells_batch<true><<<cl.ncells, kRowThreads, 0, stream>>>(
-        LoadD4{pos}, reps, cell_rep, cl.cell_start.data(), cl.cell_count.data(),
-        cl.cell_atoms.data(), r_list_sq, nbr, cap, counts, status);
+    launch(k_build_cells_batch<true>, cl.ncells, kRowThreads, 0, stream, LoadD4{pos}, reps,
+           cell_rep, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
+           nbr, cap, counts, status);
   else
-    k_build_cells_batch<false><<<cl.ncells, kRowThreads, 0, stream>>>(
-        LoadD4{pos}, reps, cell_rep, cl.cell_start.data(), cl.cell_count.data(),
-        cl.cell_atoms.data(), r_list_sq, nullptr, cap, counts, status);
+    launch(k_build_cells_batch<false>, cl.ncells, kRowThreads, 0, stream, LoadD4{pos}, reps,
+           cell_rep, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
+           nullptr, cap, counts, status);
   TDMD_LAUNCH_CHECK();
 }
 
@@ -695,6 +697,7 @@ static int stage_capacity(int max_cell) {
 namespace {
 // Largest cell occupancy, one block.
 __global__ void k_max_count(const int* __restrict__ count, int ncells, int* __restrict__ out) {
+  dependent_launch_prologue();
   __shared__ int red[32];
   int m = 0;
   for (int c = threadIdx.x; c < ncells; c += blockDim.x) m = max(m, count[c]);
@@ -710,7 +713,7 @@ __global__ void k_max_count(const int* __restrict__ count, int ncells, int* __re
 }  // namespace
 
 void cell_count_max(const CellListDev& cl, int* d_out, cudaStream_t stream) {
-  k_max_count<<<1, 1024, 0, stream>>>(cl.cell_count.data(), cl.ncells, d_out);
+  launch(k_max_count, 1, 1024, 0, stream, cl.cell_count.data(), cl.ncells, d_out);
   TDMD_LAUNCH_CHECK();
 }
 
@@ -727,13 +730,13 @@ void build_neighbor_rows(const CellListDev& cl, const void* d_pos, PosLayout lay
   auto go = [&](auto load, auto wrap_tag) {
     constexpr bool W = decltype(wrap_tag)::value;
     if (nbr)
-      k_build_cells<decltype(load), W, true><<<cl.ncells, kRowThreads, smem, stream>>>(
-          load, box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
-          lo_f, hi_f, nbr, row_off, cap, counts, status, scap);
+      launch(k_build_cells<decltype(load), W, true>, cl.ncells, kRowThreads, smem, stream, load,
+             box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq, lo_f,
+             hi_f, nbr, row_off, cap, counts, status, scap);
     else
-      k_build_cells<decltype(load), W, false><<<cl.ncells, kRowThreads, smem, stream>>>(
-          load, box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq,
-          lo_f, hi_f, nullptr, row_off, cap, counts, status, scap);
+      launch(k_build_cells<decltype(load), W, false>, cl.ncells, kRowThreads, smem, stream, load,
+             box, cl.cell_start.data(), cl.cell_count.data(), cl.cell_atoms.data(), r_list_sq, lo_f,
+             hi_f, nullptr, row_off, cap, counts, status, scap);
   };
   if (layout == PosLayout::AoS3) {
     const LoadAoS3 ld{static_cast<const double*>(d_pos)};

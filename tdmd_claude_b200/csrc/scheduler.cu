@@ -53,6 +53,7 @@ constexpr int kThreads = 256;
 __global__ void k_pack_positions(const double* __restrict__ x, const int* __restrict__ types,
                                  int n, DevBox b, double4* __restrict__ pos4,
                                  int4* __restrict__ q) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double px = x[3ll * i], py = x[3ll * i + 1], pz = x[3ll * i + 2];
@@ -75,6 +76,7 @@ struct F3 {
 template <class T>
 __global__ void k_gather(const T* __restrict__ src, const int* __restrict__ idx, int n,
                          T* __restrict__ dst) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) dst[i] = src[idx[i]];
 }
@@ -90,6 +92,7 @@ __global__ void k_gather_state(const int* __restrict__ idx, int n,
                                const int* __restrict__ id, int* __restrict__ id_o,
                                const int4* __restrict__ q, int4* __restrict__ q_o,
                                const F* __restrict__ f, F* __restrict__ f_o) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int j = idx[i];
@@ -102,6 +105,7 @@ __global__ void k_gather_state(const int* __restrict__ idx, int n,
 }
 
 __global__ void k_iota(int* __restrict__ a, int n) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i;
 }
@@ -110,12 +114,14 @@ __global__ void k_iota(int* __restrict__ a, int n) {
 template <class T>
 __global__ void k_scatter(const T* __restrict__ src, const int* __restrict__ idx, int n,
                           T* __restrict__ dst) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) dst[idx[i]] = src[i];
 }
 
 __global__ void k_scatter_positions(const double4* __restrict__ pos4, const int* __restrict__ idx,
                                     int n, double* __restrict__ x) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 p = pos4[i];
@@ -138,6 +144,7 @@ __global__ void __launch_bounds__(kThreads) k_kick_drift(double4* __restrict__ p
                                                          const double* __restrict__ inv_mm, int n,
                                                          double dt_arg, SchedCtl* __restrict__ ctl,
                                                          int ctl_dt, DevBox b) {
+  dependent_launch_prologue();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) ctl->step += 1;
   if (i >= n) return;
@@ -180,6 +187,7 @@ __global__ void __launch_bounds__(kThreads) k_half_kick_s(double* __restrict__ v
                                                           const SchedCtl* __restrict__ ctl,
                                                           int ctl_dt,
                                                           double* __restrict__ partials) {
+  dependent_launch_prologue();
   __shared__ double red[32 * 2];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0.0, v2 = 0.0;
@@ -231,6 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_ke_integer(const double* __restric
                                                          const double* __restrict__ inv_mm,
                                                          int n, double dt,
                                                          double* __restrict__ partials) {
+  dependent_launch_prologue();
   __shared__ double red[32 * 2];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0.0, v2 = 0.0;
@@ -325,6 +334,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_control(SchedCtl* __restrict__ 
                                                          const double* __restrict__ partials,
                                                          int nblk, CtlParams p, int mode,
                                                          double* __restrict__ log, int log_cap) {
+  dependent_launch_prologue();
   double ke, v2;
   reduce_ke_v2(partials, nblk, ke, v2);
   if (threadIdx.x != 0) return;
@@ -374,6 +384,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_log_nve(SchedCtl* __restrict__ 
                                                          const double* __restrict__ partials,
                                                          int nblk, double* __restrict__ log,
                                                          int log_cap) {
+  dependent_launch_prologue();
   double ke, v2;
   reduce_ke_v2(partials, nblk, ke, v2);
   if (threadIdx.x != 0) return;
@@ -387,6 +398,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_log_nve(SchedCtl* __restrict__ 
 }
 
 __global__ void k_apply_scale(double* __restrict__ v, long long m, const SchedCtl* __restrict__ ctl) {
+  dependent_launch_prologue();
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < m) v[i] *= ctl->scale;
 }
@@ -498,8 +510,8 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
       TDMD_CU(cudaMemcpyAsync(fd, f, fb, cudaMemcpyHostToDevice, s));
     else
       TDMD_CU(cudaMemsetAsync(fd, 0, fb, s));
-    k_pack_positions<<<ceil_div(n_, kThreads), kThreads, 0, s>>>(
-        stage_.data(), types_.data(), n_, box_, pos4_.data(), mixed_ ? q_.data() : nullptr);
+    launch(k_pack_positions, ceil_div(n_, kThreads), kThreads, 0, s, stage_.data(), types_.data(),
+           n_, box_, pos4_.data(), mixed_ ? q_.data() : nullptr);
     TDMD_LAUNCH_CHECK();
     reorder_by_cell();
   }
@@ -576,21 +588,20 @@ void Scheduler::reorder_by_cell() {
   if (mixed_) {
     q_alt_.reserve(n);
     f32_alt_.reserve(3 * n);
-    k_gather_state<F3><<<nb, kThreads, 0, s>>>(
-        order_.data(), n_, pos4_.data(), pos4_alt_.data(),
-        reinterpret_cast<const D3*>(vel_.data()), reinterpret_cast<D3*>(vel_alt_.data()),
-        types_.data(), types_alt_.data(), ids_.data(), ids_alt_.data(), q_.data(),
-        q_alt_.data(), reinterpret_cast<const F3*>(f32_.data()),
-        reinterpret_cast<F3*>(f32_alt_.data()));
+    launch(k_gather_state<F3>, nb, kThreads, 0, s, order_.data(), n_, pos4_.data(),
+           pos4_alt_.data(), reinterpret_cast<const D3*>(vel_.data()),
+           reinterpret_cast<D3*>(vel_alt_.data()), types_.data(), types_alt_.data(), ids_.data(),
+           ids_alt_.data(), q_.data(), q_alt_.data(), reinterpret_cast<const F3*>(f32_.data()),
+           reinterpret_cast<F3*>(f32_alt_.data()));
     std::swap(q_, q_alt_);
     std::swap(f32_, f32_alt_);
   } else {
     f64_alt_.reserve(3 * n);
-    k_gather_state<D3><<<nb, kThreads, 0, s>>>(
-        order_.data(), n_, pos4_.data(), pos4_alt_.data(),
-        reinterpret_cast<const D3*>(vel_.data()), reinterpret_cast<D3*>(vel_alt_.data()),
-        types_.data(), types_alt_.data(), ids_.data(), ids_alt_.data(), nullptr, nullptr,
-        reinterpret_cast<const D3*>(f64_.data()), reinterpret_cast<D3*>(f64_alt_.data()));
+    launch(k_gather_state<D3>, nb, kThreads, 0, s, order_.data(), n_, pos4_.data(),
+           pos4_alt_.data(), reinterpret_cast<const D3*>(vel_.data()),
+           reinterpret_cast<D3*>(vel_alt_.data()), types_.data(), types_alt_.data(), ids_.data(),
+           ids_alt_.data(), nullptr, nullptr, reinterpret_cast<const D3*>(f64_.data()),
+           reinterpret_cast<D3*>(f64_alt_.data()));
     std::swap(f64_, f64_alt_);
   }
   TDMD_LAUNCH_CHECK();
@@ -646,14 +657,14 @@ void Scheduler::download(double* x, double* v, void* f, int* types, int* ids, in
   const int nb = ceil_div(n_, kThreads);
   const int* ord = order_.data();
   if (x) {
-    k_scatter_positions<<<nb, kThreads, 0, s>>>(pos4_.data(), ord, n_, stage_.data());
+    launch(k_scatter_positions, nb, kThreads, 0, s, pos4_.data(), ord, n_, stage_.data());
     TDMD_LAUNCH_CHECK();
     TDMD_CU(cudaMemcpyAsync(x, stage_.data(), 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
   auto unpermute = [&](const auto* arr, void* out) {
     using T = std::remove_const_t<std::remove_pointer_t<decltype(arr)>>;
     T* tmp = reinterpret_cast<T*>(stage_.data());
-    k_scatter<T><<<nb, kThreads, 0, s>>>(arr, ord, n_, tmp);
+    launch(k_scatter<T>, nb, kThreads, 0, s, arr, ord, n_, tmp);
     TDMD_LAUNCH_CHECK();
     TDMD_CU(cudaMemcpyAsync(out, tmp, n * sizeof(T), cudaMemcpyDeviceToHost, s));
   };
@@ -673,7 +684,7 @@ void Scheduler::download(double* x, double* v, void* f, int* types, int* ids, in
 int Scheduler::build_cells() {
   if (cells_from_upload_) {
     cells_from_upload_ = false;
-    k_iota<<<ceil_div(n_, kThreads), kThreads, 0, stream_>>>(cl_.cell_atoms.data(), n_);
+    launch(k_iota, ceil_div(n_, kThreads), kThreads, 0, stream_, cl_.cell_atoms.data(), n_);
     TDMD_LAUNCH_CHECK();
     return 1;
   }
@@ -792,8 +803,7 @@ void Scheduler::enqueue_force(bool ev, bool kd, int parts) {
     TDMD_REQUIRE(parts == kPassBoth, "energy/virial needs both passes");
     const int nrec = kind_ == TDMD_POT_EAM ? nblk_d + nblk : nblk;
     TDMD_CU(cudaMemsetAsync(ctl_ev(), 0, sizeof(double) * 7, s));
-    k_reduce_partials<<<1, 256, 0, s>>>(ev_part_.data(), nrec, ctl_ev(),
-                                        ctl_ev() + 1);
+    launch(k_reduce_partials, 1, 256, 0, s, ev_part_.data(), nrec, ctl_ev(), ctl_ev() + 1);
     TDMD_LAUNCH_CHECK();
     launches_ += 1;
   }
@@ -807,17 +817,14 @@ void Scheduler::enqueue_kick_drift_t(F* f, bool full, bool scale) {
   int4* q = mixed_ ? q_.data() : nullptr;
   const int ctl_dt = thermo_ ? 1 : 0;
   if (scale)
-    k_kick_drift<F, false, true><<<nb, kThreads, 0, s>>>(pos4_.data(), q, vel_.data(), f,
-                                                         types_.data(), inv_mm_.data(), n_,
-                                                         cfg_.dt, ctl_.data(), ctl_dt, box_);
+    launch(k_kick_drift<F, false, true>, nb, kThreads, 0, s, pos4_.data(), q, vel_.data(), f,
+           types_.data(), inv_mm_.data(), n_, cfg_.dt, ctl_.data(), ctl_dt, box_);
   else if (full)
-    k_kick_drift<F, true, false><<<nb, kThreads, 0, s>>>(pos4_.data(), q, vel_.data(), f,
-                                                         types_.data(), inv_mm_.data(), n_,
-                                                         cfg_.dt, ctl_.data(), ctl_dt, box_);
+    launch(k_kick_drift<F, true, false>, nb, kThreads, 0, s, pos4_.data(), q, vel_.data(), f,
+           types_.data(), inv_mm_.data(), n_, cfg_.dt, ctl_.data(), ctl_dt, box_);
   else
-    k_kick_drift<F, false, false><<<nb, kThreads, 0, s>>>(pos4_.data(), q, vel_.data(), f,
-                                                          types_.data(), inv_mm_.data(), n_,
-                                                          cfg_.dt, ctl_.data(), ctl_dt, box_);
+    launch(k_kick_drift<F, false, false>, nb, kThreads, 0, s, pos4_.data(), q, vel_.data(), f,
+           types_.data(), inv_mm_.data(), n_, cfg_.dt, ctl_.data(), ctl_dt, box_);
   TDMD_LAUNCH_CHECK();
   launches_ += 1;
 }
@@ -837,12 +844,11 @@ void Scheduler::enqueue_half_kick_t(F* f, bool ke) {
   const int nb = ceil_div(n_, kThreads);
   const int ctl_dt = thermo_ ? 1 : 0;
   if (ke)
-    k_half_kick_s<F, true><<<nb, kThreads, 0, s>>>(vel_.data(), f, types_.data(), masses_.data(), inv_mm_.data(),
-                                                   n_, cfg_.dt, ctl_.data(), ctl_dt,
-                                                   ke_part_.data());
+    launch(k_half_kick_s<F, true>, nb, kThreads, 0, s, vel_.data(), f, types_.data(),
+           masses_.data(), inv_mm_.data(), n_, cfg_.dt, ctl_.data(), ctl_dt, ke_part_.data());
   else
-    k_half_kick_s<F, false><<<nb, kThreads, 0, s>>>(vel_.data(), f, types_.data(), masses_.data(), inv_mm_.data(),
-                                                    n_, cfg_.dt, ctl_.data(), ctl_dt, nullptr);
+    launch(k_half_kick_s<F, false>, nb, kThreads, 0, s, vel_.data(), f, types_.data(),
+           masses_.data(), inv_mm_.data(), n_, cfg_.dt, ctl_.data(), ctl_dt, nullptr);
   TDMD_LAUNCH_CHECK();
   launches_ += 1;
 }
@@ -875,8 +881,8 @@ CtlParams Scheduler::ctl_params() const {
 void Scheduler::enqueue_control(int mode) {
   const CtlParams p = ctl_params();
   const int nb = ceil_div(n_, kThreads);
-  k_control<<<1, ctl_threads(nb), 0, stream_>>>(ctl_.data(), ke_part_.data(), nb, p, mode,
-                                                log_.data(), log_cap_);
+  launch(k_control, 1, ctl_threads(nb), 0, stream_, ctl_.data(), ke_part_.data(), nb, p, mode,
+         log_.data(), log_cap_);
   TDMD_LAUNCH_CHECK();
   launches_ += 1;
 }
@@ -884,8 +890,8 @@ void Scheduler::enqueue_control(int mode) {
 void Scheduler::enqueue_ke_pre() {
   cudaStream_t s = stream_;
   const int nb = ceil_div(n_, kThreads);
-  k_ke_vmax_partials<<<nb, kThreads, 0, s>>>(vel_.data(), types_.data(), masses_.data(), n_,
-                                             ke_part_.data());
+  launch(k_ke_vmax_partials, nb, kThreads, 0, s, vel_.data(), types_.data(), masses_.data(), n_,
+         ke_part_.data());
   TDMD_LAUNCH_CHECK();
   launches_ += 1;
 }
@@ -894,21 +900,21 @@ void Scheduler::enqueue_log_nve() {
   cudaStream_t s = stream_;
   const int nb = ceil_div(n_, kThreads);
   if (mixed_)
-    k_ke_integer<<<nb, kThreads, 0, s>>>(vel_.data(), f32_.data(), types_.data(), masses_.data(), inv_mm_.data(),
-                                         n_, cfg_.dt, ke_part_.data());
+    launch(k_ke_integer<float>, nb, kThreads, 0, s, vel_.data(), f32_.data(), types_.data(),
+           masses_.data(), inv_mm_.data(), n_, cfg_.dt, ke_part_.data());
   else
-    k_ke_integer<<<nb, kThreads, 0, s>>>(vel_.data(), f64_.data(), types_.data(), masses_.data(), inv_mm_.data(),
-                                         n_, cfg_.dt, ke_part_.data());
+    launch(k_ke_integer<double>, nb, kThreads, 0, s, vel_.data(), f64_.data(), types_.data(),
+           masses_.data(), inv_mm_.data(), n_, cfg_.dt, ke_part_.data());
   TDMD_LAUNCH_CHECK();
-  k_log_nve<<<1, ctl_threads(nb), 0, s>>>(ctl_.data(), ke_part_.data(), nb, log_.data(),
-                                          log_cap_);
+  launch(k_log_nve, 1, ctl_threads(nb), 0, s, ctl_.data(), ke_part_.data(), nb, log_.data(),
+         log_cap_);
   TDMD_LAUNCH_CHECK();
   launches_ += 2;
 }
 
 void Scheduler::enqueue_apply_scale() {
   const long long m = 3ll * n_;
-  k_apply_scale<<<ceil_div(m, kThreads), kThreads, 0, stream_>>>(vel_.data(), m, ctl_.data());
+  launch(k_apply_scale, ceil_div(m, kThreads), kThreads, 0, stream_, vel_.data(), m, ctl_.data());
   TDMD_LAUNCH_CHECK();
   launches_ += 1;
 }
@@ -1195,8 +1201,8 @@ void Scheduler::energies(double* pe, double* ke, double* virial6) {
   enqueue_force(true);
   profiling_ = prof;
   enqueue_ke_pre();
-  k_ke_vmax_finish<<<1, 256, 0, stream_>>>(ke_part_.data(), ceil_div(n_, kThreads),
-                                           ke_part_.data() + 2ll * ceil_div(n_, kThreads));
+  launch(k_ke_vmax_finish, 1, 256, 0, stream_, ke_part_.data(), ceil_div(n_, kThreads),
+         ke_part_.data() + 2ll * ceil_div(n_, kThreads));
   TDMD_LAUNCH_CHECK();
   double ev[7], k2[2];
   TDMD_CU(cudaMemcpyAsync(ev, ctl_ev(), sizeof(ev), cudaMemcpyDeviceToHost, stream_));
