@@ -242,9 +242,10 @@ int32_t tdmd_get_deterministic_reduce(int32_t* on);
 /* read_lammps_data, src/io/lammps_data_reader.cpp:33-204: a LAMMPS
  * `atomic` data file into a host SystemState (ids 1-based, atom with id k
  * at index k-1, velocities 0 without a Velocities section, masses
- * [ntypes+1] with 1.0 where Masses gives none, periodic box).  Parse errors
- * return TDMD_ERR_PARSE; so does an atom id outside 1..N or a Masses type
- * outside 1..ntypes (where the reference would index out of its arrays). */
+ * [ntypes+1] with 1.0 where Masses gives none, periodic box).  A file that
+ * cannot be opened returns TDMD_ERR_IO; parse errors return TDMD_ERR_PARSE;
+ * so does an atom id outside 1..N or a Masses type outside 1..ntypes (where
+ * the reference would index out of its arrays). */
 typedef struct tdmd_system tdmd_system;
 int32_t tdmd_read_lammps_data(const char* path, tdmd_system** out);
 int32_t tdmd_system_destroy(tdmd_system* s);

@@ -142,7 +142,7 @@ struct SetflReader {
 
 static void read_setfl(const std::string& path, tdmd_eam& e) {
   std::ifstream f(path);
-  if (!f.is_open()) throw Error{TDMD_ERR_PARSE, "cannot open EAM file: " + path};
+  if (!f.is_open()) throw Error{TDMD_ERR_IO, "cannot open EAM file: " + path};
   std::string line;
   e.comments.clear();
   for (int k = 0; k < 3; ++k) {

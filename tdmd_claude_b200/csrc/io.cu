@@ -62,7 +62,7 @@ bool begins(const std::string& s, const char* p) { return s.compare(0, std::strl
 
 void read_data(const std::string& path, tdmd_system& st) {
   std::ifstream in(path);
-  if (!in.is_open()) parse_fail("cannot open LAMMPS data file: " + path);
+  if (!in.is_open()) throw Error{TDMD_ERR_IO, "cannot open LAMMPS data file: " + path};
   std::string line;
   std::getline(in, line);  // title
   int64_t natoms = 0;
@@ -291,7 +291,7 @@ int32_t tdmd_read_force_dump(const char* path, int64_t* natoms, int64_t capacity
   return guarded([&] {
     TDMD_REQUIRE(path && natoms, "null argument");
     std::ifstream in(path);
-    if (!in.is_open()) parse_fail(std::string("cannot open dump file: ") + path);
+    if (!in.is_open()) throw Error{TDMD_ERR_IO, std::string("cannot open dump file: ") + path};
     std::string line;
     int64_t n = 0;
     bool atoms = false;

@@ -101,10 +101,20 @@ def test_malformed_setfl_rejected(L, contents):
     assert ei.value.code == 4
 
 
-def test_missing_setfl_file(L):
+def test_missing_files_are_io_errors(L, tmp_path):
+    """A file that cannot be opened is TDMD_ERR_IO for every reader and
+    writer (LammpsDataReader.FileNotFound, tests/unit/test_lammps_data_reader.cpp)."""
     from tdmd_claude_b200 import EamAlloy, TdmdError
-    with pytest.raises(TdmdError):
-        EamAlloy().read_setfl("/nonexistent/file.eam.alloy")
+    from tdmd_claude_b200 import io as TIO
+    from tdmd_claude_b200 import workloads as W
+    missing = str(tmp_path / "no_such_dir" / "file")
+    for call in (lambda: EamAlloy().read_setfl(missing + ".eam.alloy"),
+                 lambda: TIO.read_lammps_data(missing + ".data"),
+                 lambda: TIO.read_force_dump(missing + ".dump"),
+                 lambda: TIO.write_lammps_data(missing + ".data", W.morse_256())):
+        with pytest.raises(TdmdError) as ei:
+            call()
+        assert ei.value.code == 9 and "cannot open" in str(ei.value)
 
 
 def test_nhc_host_chain_equals_reference(L):
