@@ -163,6 +163,26 @@ def test_nve_energy_log_and_drift(cuda):
     assert abs(log[-1, 2] - ke) < 1e-9 * abs(ke)
 
 
+@pytest.mark.parametrize("precision,per_step", [("fp64", 1e-15), ("mixed", 1e-9)])
+def test_adr0007_nve_acceptance_100k(cuda, precision, per_step):
+    """DeviceNVEDrift.ADR0007AcceptanceTest100k (tests/unit/test_device_nve_drift.cu:158-257):
+    the reference's 256-atom Cu data file (perfect lattice, at rest), Morse
+    rc 6.0, skin 1.0, dt 1 fs, rebuild every 10 steps, 100 000 steps; the
+    total-energy change per step relative to E0 stays under the reference's
+    ADR-0007 targets (tests/support/precision_tolerance.hpp:70-71)."""
+    g = golden("run0_morse_256.json")
+    pos = np.array(g["positions"])
+    s = _sched_morse(pos, np.zeros_like(pos), np.array(g["masses"]), g["lo"], g["hi"],
+                     g["morse"], 1.0, dt=0.001, rebuild_every=10, precision=precision)
+    s.run_until(0)
+    pe0, ke0, _ = s.energies()
+    s.run_until(100000)
+    pe1, ke1, _ = s.energies()
+    e0, e1 = pe0 + ke0, pe1 + ke1
+    assert abs((e1 - e0) / e0) / 100000 < per_step
+    s.close()
+
+
 def test_nvt_matches_oracle_composition(cuda, oracle):
     """NHC chain 3, tau 0.1 ps at 600 K on the EAM system: trajectory equals
     the oracle composition of NoseHooverChain + VV (pipeline_scheduler order)."""
@@ -230,14 +250,26 @@ def test_graph_replay_equals_direct_launches(cuda):
     assert a.stats().graph_launches > 0 and b.stats().graph_launches == 0
 
 
-def test_deterministic_replay(cuda):
-    s1, _, _ = _eam_setup("mixed", ncell=5)
-    s2, _, _ = _eam_setup("mixed", ncell=5)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("mode", ["nve", "nvt", "nvt_adaptive_dt"])
+def test_deterministic_replay(cuda, precision, mode):
+    """EamDeterministicReplay (tests/unit/test_fast_pipeline_eam.cu) and
+    NVTThermostat.DeterministicReproducibility (test_nvt_thermostat.cu:203-250):
+    two runs of the same input are bit-identical, the NHC chain and the
+    adaptive dt included."""
+    cfg = {"nve": {}, "nvt": dict(t_target=300.0, t_period=0.1, nhc_length=3),
+           "nvt_adaptive_dt": dict(t_target=300.0, t_period=0.1, nhc_length=3,
+                                   adaptive_dt=True)}[mode]
+    s1, _, _ = _eam_setup(precision, ncell=5, **cfg)
+    s2, _, _ = _eam_setup(precision, ncell=5, **cfg)
     s1.run_until(100)
     s2.run_until(100)
     a, b = s1.download(), s2.download()
     assert np.array_equal(a.positions, b.positions)
+    assert np.array_equal(a.velocities, b.velocities)
     assert np.array_equal(a.forces, b.forces)
+    (p1, k1, w1), (p2, k2, w2) = s1.energies(), s2.energies()
+    assert p1 == p2 and k1 == k2 and np.array_equal(w1, w2)
 
 
 def test_neighbor_overflow_retry(cuda, oracle):
