@@ -185,3 +185,39 @@ def test_eam_mishin_run0_lammps(cuda, mishin_setfl, precision):
                         precision)
     tol = g["tolerance_fp64"] if precision == "fp64" else g["tolerance_mixed"]
     assert np.abs(f - np.array(g["lammps_forces"])).max() < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_stream_order_after_caller_kernels(cuda, oracle, precision):
+    """Library kernels are launched with programmatic dependent launch: on a
+    caller's stream they wait for the caller's preceding kernels.  Each round
+    the caller zeroes the position buffer, runs a 128 MiB reduction and only
+    then writes the positions, all on one stream, right before the list
+    build and the force call (a library kernel that ran early would see
+    every atom at the origin); the forces equal the oracle's every round."""
+    torch = cuda
+    from tdmd_claude_b200 import DeviceNeighborList, MorseParams, compute_morse_gpu
+    g = golden("ref_morse_256.json")
+    pos0 = np.array(g["positions"])
+    n = len(pos0)
+    box = _box(g["lo"], g["hi"])
+    _, fo, _ = oracle.morse_forces(pos0, g["lo"], g["hi"], *g["morse"], g["skin"])
+    s = torch.cuda.Stream()
+    big = torch.rand(1 << 24, device="cuda", dtype=torch.float64)
+    base = torch.tensor(pos0, device="cuda", dtype=torch.float64)
+    d = torch.empty_like(base)
+    fdt = torch.float64 if precision == "fp64" else torch.float32
+    nl = DeviceNeighborList()
+    torch.cuda.synchronize()
+    for _ in range(4):
+        with torch.cuda.stream(s):
+            f = torch.zeros((n, 3), dtype=fdt, device="cuda")
+            d.zero_()
+            zero = (big * 0.0).sum()
+            torch.add(base, zero, out=d)  # the kernel right before the library's first
+            nl.build(d, n, box, g["morse"][3], g["skin"], stream=s)
+            compute_morse_gpu(d, f, nl.d_neighbors(), nl.d_offsets(), nl.d_counts(), n, box,
+                              MorseParams.make(*g["morse"]), precision=precision, stream=s)
+        s.synchronize()
+        assert rel_rms(f.double().cpu().numpy(), fo) < (FP64_TOL if precision == "fp64"
+                                                        else MIXED_FORCE_TOL)
