@@ -7,16 +7,26 @@
 // 44-61): define TDMD_PRECISION_MIXED for `real = float` and float forces,
 // otherwise (or with TDMD_PRECISION_FP64) everything is double.
 //
-// Errors: every non-zero status becomes a tdmd::Error (std::runtime_error,
-// as src/core/error.hpp:13) carrying the status code; the reference aborts on
-// CUDA failures instead (src/core/device_buffer.cuh:16-24).
+// Core types: by default this header defines the reference's core types
+// itself (src/core/{types,box,system_state,constants,error}.hpp, same names
+// and layouts).  A caller that keeps the reference's own core headers on its
+// include path defines TDMD_B200_REFERENCE_CORE instead, and this layer uses
+// those headers' types; the reference's CPU classes (NeighborList,
+// MorsePair, EamAlloy::compute_forces, ...) then link beside it unchanged.
 //
-// Needs <cuda_runtime_api.h> for cudaStream_t only.
+// Errors: every non-zero status becomes a tdmd::StatusError carrying the
+// status code, a tdmd::Error (std::runtime_error, as src/core/error.hpp:13);
+// without TDMD_B200_REFERENCE_CORE the two names are one class.  The
+// reference aborts on CUDA failures instead (src/core/device_buffer.cuh:16-24);
+// TDMD_CUDA_CHECK here throws.
+//
+// Needs <cuda_runtime_api.h>; callers link the CUDA runtime (DeviceBuffer).
 #pragma once
 
 #include <cuda_runtime_api.h>
 
 #include <array>
+#include <cstddef>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -24,8 +34,19 @@
 
 #include "tdmd_b200.h"
 
+#if defined(TDMD_B200_REFERENCE_CORE)
+// The caller's tree supplies the reference's own core headers; this layer
+// uses those types as they are.
+#include "core/box.hpp"
+#include "core/constants.hpp"
+#include "core/error.hpp"
+#include "core/system_state.hpp"
+#include "core/types.hpp"
+#endif
+
 namespace tdmd {
 
+#if !defined(TDMD_B200_REFERENCE_CORE)
 // --- src/core/types.hpp -----------------------------------------------------
 #if defined(TDMD_PRECISION_MIXED)
 using real = float;
@@ -34,6 +55,8 @@ using real = double;
 #endif
 using i32 = std::int32_t;
 using i64 = std::int64_t;
+using u32 = std::uint32_t;
+using u64 = std::uint64_t;
 
 template <class T>
 struct Vec3T {
@@ -45,6 +68,11 @@ using Vec3D = Vec3T<double>;
 using Vec3F = Vec3T<float>;
 using Vec3 = Vec3T<real>;
 
+struct Aabb {
+  Vec3D lo;
+  Vec3D hi;
+};
+
 using pos_t = double;
 using vel_t = double;
 using accum_t = double;
@@ -53,11 +81,9 @@ using VelocityVec = Vec3D;
 #if defined(TDMD_PRECISION_MIXED)
 using force_t = float;
 using ForceVec = Vec3F;
-constexpr int32_t kForcePrecision = TDMD_MIXED;
 #else
 using force_t = double;
 using ForceVec = Vec3D;
-constexpr int32_t kForcePrecision = TDMD_FP64;
 #endif
 
 // --- src/core/constants.hpp:15,28 (metal units) -----------------------------
@@ -73,25 +99,7 @@ class Error : public std::runtime_error {
  private:
   int32_t status_;
 };
-
-namespace detail {
-inline void check(int32_t rc) {
-  if (rc != TDMD_OK) throw Error(rc, tdmd_last_error());
-}
-inline void* stream_ptr(cudaStream_t s) { return reinterpret_cast<void*>(s); }
-}  // namespace detail
-
-// --- src/core/determinism.hpp:20-24 ----------------------------------------
-// The reference selects ID-ordered energy sums at build time
-// (kDeterministicReduce); here it is a process-wide run-time switch.
-inline void set_deterministic_reduce(bool on) {
-  detail::check(tdmd_set_deterministic_reduce(on ? 1 : 0));
-}
-inline bool deterministic_reduce() {
-  int32_t on = 0;
-  detail::check(tdmd_get_deterministic_reduce(&on));
-  return on != 0;
-}
+using StatusError = Error;
 
 // --- src/core/box.hpp -------------------------------------------------------
 struct Box {
@@ -100,14 +108,6 @@ struct Box {
   std::array<bool, 3> periodic{true, true, true};
 
   Vec3D size() const noexcept { return Vec3D{hi.x - lo.x, hi.y - lo.y, hi.z - lo.z}; }
-
-  tdmd_box to_c() const noexcept {
-    tdmd_box b{};
-    b.lo[0] = lo.x; b.lo[1] = lo.y; b.lo[2] = lo.z;
-    b.hi[0] = hi.x; b.hi[1] = hi.y; b.hi[2] = hi.z;
-    for (int k = 0; k < 3; ++k) b.periodic[k] = periodic[static_cast<size_t>(k)] ? 1 : 0;
-    return b;
-  }
 };
 
 // --- src/core/system_state.hpp: the host SoA state of a simulation ----------
@@ -134,6 +134,178 @@ struct SystemState {
     ids.resize(k);
   }
 };
+#else
+// The reference's tdmd::Error (a std::runtime_error) is the base; the status
+// code of the failing call rides in this subclass.
+class StatusError : public Error {
+ public:
+  StatusError(int32_t status, const std::string& what) : Error(what), status_(status) {}
+  int32_t status() const noexcept { return status_; }
+
+ private:
+  int32_t status_;
+};
+#endif  // TDMD_B200_REFERENCE_CORE
+
+#if defined(TDMD_PRECISION_MIXED)
+constexpr int32_t kForcePrecision = TDMD_MIXED;
+#else
+constexpr int32_t kForcePrecision = TDMD_FP64;
+#endif
+
+namespace detail {
+inline void check(int32_t rc) {
+  if (rc != TDMD_OK) throw StatusError(rc, tdmd_last_error());
+}
+inline void* stream_ptr(cudaStream_t s) { return reinterpret_cast<void*>(s); }
+inline tdmd_box to_c(const Box& box) noexcept {
+  tdmd_box b{};
+  b.lo[0] = box.lo.x;
+  b.lo[1] = box.lo.y;
+  b.lo[2] = box.lo.z;
+  b.hi[0] = box.hi.x;
+  b.hi[1] = box.hi.y;
+  b.hi[2] = box.hi.z;
+  for (int k = 0; k < 3; ++k) b.periodic[k] = box.periodic[static_cast<size_t>(k)] ? 1 : 0;
+  return b;
+}
+}  // namespace detail
+
+// --- src/core/determinism.hpp:20-24 ----------------------------------------
+// The reference selects ID-ordered energy sums at build time
+// (kDeterministicReduce); here it is a process-wide run-time switch.
+inline void set_deterministic_reduce(bool on) {
+  detail::check(tdmd_set_deterministic_reduce(on ? 1 : 0));
+}
+inline bool deterministic_reduce() {
+  int32_t on = 0;
+  detail::check(tdmd_get_deterministic_reduce(&on));
+  return on != 0;
+}
+
+// --- src/core/device_buffer.cuh:16-112 ---------------------------------------
+// A CUDA call that fails throws StatusError (TDMD_ERR_CUDA, or
+// TDMD_ERR_OUT_OF_MEMORY for an allocation).
+inline void check_cuda(cudaError_t err, const char* file, int line) {
+  if (err != cudaSuccess)
+    throw StatusError(err == cudaErrorMemoryAllocation ? TDMD_ERR_OUT_OF_MEMORY : TDMD_ERR_CUDA,
+                      std::string(cudaGetErrorString(err)) + " at " + file + ":" +
+                          std::to_string(line));
+}
+#define TDMD_CUDA_CHECK(call) ::tdmd::check_cuda((call), __FILE__, __LINE__)
+
+// Device array of n elements (uninitialised), move-only; resize discards the
+// contents; copies are synchronous.
+template <typename T>
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(std::size_t n) { resize(n); }
+  ~DeviceBuffer() { release(); }
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  DeviceBuffer(DeviceBuffer&& o) noexcept : ptr_(o.ptr_), size_(o.size_) {
+    o.ptr_ = nullptr;
+    o.size_ = 0;
+  }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr_ = o.ptr_;
+      size_ = o.size_;
+      o.ptr_ = nullptr;
+      o.size_ = 0;
+    }
+    return *this;
+  }
+
+  void resize(std::size_t n) {
+    if (n == size_) return;
+    release();
+    if (n > 0) TDMD_CUDA_CHECK(cudaMalloc(reinterpret_cast<void**>(&ptr_), n * sizeof(T)));
+    size_ = n;
+  }
+  void copy_from_host(const T* src, std::size_t n, std::size_t offset = 0) {
+    in_range(n, offset);
+    if (n) TDMD_CUDA_CHECK(cudaMemcpy(ptr_ + offset, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void copy_to_host(T* dst, std::size_t n, std::size_t offset = 0) const {
+    in_range(n, offset);
+    if (n) TDMD_CUDA_CHECK(cudaMemcpy(dst, ptr_ + offset, n * sizeof(T), cudaMemcpyDeviceToHost));
+  }
+  void zero() {
+    if (size_) TDMD_CUDA_CHECK(cudaMemset(ptr_, 0, size_ * sizeof(T)));
+  }
+  T* data() noexcept { return ptr_; }
+  const T* data() const noexcept { return ptr_; }
+  std::size_t size() const noexcept { return size_; }
+
+ private:
+  void release() noexcept {
+    if (ptr_) cudaFree(ptr_);
+    ptr_ = nullptr;
+    size_ = 0;
+  }
+  void in_range(std::size_t n, std::size_t offset) const {
+    if (offset > size_ || n > size_ - offset)
+      throw StatusError(TDMD_ERR_INVALID_ARGUMENT, "DeviceBuffer copy out of range");
+  }
+
+  T* ptr_ = nullptr;
+  std::size_t size_ = 0;
+};
+
+// --- src/core/device_system_state.cuh:18-42 ----------------------------------
+// Device copy of a SystemState's per-atom arrays and per-type masses.
+struct DeviceSystemState {
+  i64 natoms{0};
+  Box box;
+  DeviceBuffer<PositionVec> positions;
+  DeviceBuffer<VelocityVec> velocities;
+  DeviceBuffer<ForceVec> forces;
+  DeviceBuffer<i32> types;
+  DeviceBuffer<i32> ids;
+  DeviceBuffer<real> masses;
+
+  void resize(i64 n, i32 ntypes = 0) {
+    natoms = n;
+    const std::size_t k = static_cast<std::size_t>(n);
+    positions.resize(k);
+    velocities.resize(k);
+    forces.resize(k);
+    types.resize(k);
+    ids.resize(k);
+    if (ntypes > 0) masses.resize(static_cast<std::size_t>(ntypes));
+  }
+  void upload(const SystemState& host) {
+    const std::size_t k = static_cast<std::size_t>(host.natoms);
+    if (positions.size() != k || masses.size() < host.masses.size())
+      resize(host.natoms, static_cast<i32>(host.masses.size()));
+    natoms = host.natoms;
+    box = host.box;
+    positions.copy_from_host(host.positions.data(), k);
+    velocities.copy_from_host(host.velocities.data(), k);
+    forces.copy_from_host(host.forces.data(), k);
+    types.copy_from_host(host.types.data(), k);
+    ids.copy_from_host(host.ids.data(), k);
+    masses.copy_from_host(host.masses.data(), host.masses.size());
+  }
+  void download(SystemState& host) const {
+    const std::size_t k = static_cast<std::size_t>(natoms);
+    host.resize(natoms);
+    host.box = box;
+    positions.copy_to_host(host.positions.data(), k);
+    velocities.copy_to_host(host.velocities.data(), k);
+    forces.copy_to_host(host.forces.data(), k);
+    types.copy_to_host(host.types.data(), k);
+    ids.copy_to_host(host.ids.data(), k);
+    if (masses.size() > 0) {
+      host.masses.resize(masses.size());
+      masses.copy_to_host(host.masses.data(), masses.size());
+    }
+  }
+  void zero_forces() { forces.zero(); }
+};
 
 // --- src/potentials -----------------------------------------------------------
 namespace potentials {
@@ -156,7 +328,7 @@ inline void compute_morse_gpu(const PositionVec* d_positions, ForceVec* d_forces
                               const i32* d_neighbors, const i32* d_offsets, const i32* d_counts,
                               i32 natoms, const Box& box, const MorseParams& params,
                               accum_t* d_energy, cudaStream_t stream = 0) {
-  const tdmd_box b = box.to_c();
+  const tdmd_box b = detail::to_c(box);
   const tdmd_morse_params p = params.to_c();
   detail::check(tdmd_morse_compute(reinterpret_cast<const double*>(d_positions), d_forces,
                                    kForcePrecision, d_neighbors, d_offsets, d_counts, natoms, &b,
@@ -217,7 +389,7 @@ class DeviceEam {
   void compute(const PositionVec* d_positions, ForceVec* d_forces, const i32* d_types,
                const i32* d_neighbors, const i32* d_offsets, const i32* d_counts, i32 natoms,
                const Box& box, accum_t* d_energy, cudaStream_t stream = 0) {
-    const tdmd_box b = box.to_c();
+    const tdmd_box b = detail::to_c(box);
     detail::check(tdmd_device_eam_compute(h_, reinterpret_cast<const double*>(d_positions),
                                           d_forces, kForcePrecision, d_types, d_neighbors,
                                           d_offsets, d_counts, natoms, &b, d_energy, nullptr,
@@ -294,7 +466,7 @@ inline std::vector<DumpAtom> read_lammps_dump(const std::string& filename) {
 // No reference counterpart (the reference only reads data files).
 inline void write_lammps_data(const SystemState& s, const std::string& path,
                               const std::string& title = "tdmd_claude_b200 data") {
-  const tdmd_box b = s.box.to_c();
+  const tdmd_box b = detail::to_c(s.box);
   std::vector<double> m(s.masses.begin(), s.masses.end());
   const int32_t nt = s.masses.empty() ? 1 : static_cast<int32_t>(s.masses.size()) - 1;
   detail::check(tdmd_write_lammps_data(
@@ -306,7 +478,7 @@ inline void write_lammps_data(const SystemState& s, const std::string& path,
 
 // tdmd_main.cpp:65-95 (the reference driver's dump writer)
 inline void write_lammps_force_dump(const SystemState& s, const std::string& path) {
-  const tdmd_box b = s.box.to_c();
+  const tdmd_box b = detail::to_c(s.box);
   detail::check(tdmd_write_force_dump(path.c_str(), s.step, s.natoms, &b, s.ids.data(),
                                       s.types.data(),
                                       reinterpret_cast<const double*>(s.positions.data()),
@@ -331,7 +503,7 @@ class DeviceCellList {
   ~DeviceCellList() { tdmd_cell_list_destroy(h_); }
 
   void build(const PositionVec* d_positions, i64 natoms, const Box& box, real r_list) {
-    const tdmd_box b = box.to_c();
+    const tdmd_box b = detail::to_c(box);
     detail::check(tdmd_cell_list_build(h_, reinterpret_cast<const double*>(d_positions), natoms,
                                        &b, r_list, nullptr));
     detail::check(tdmd_cell_list_get(h_, &atoms_, &offsets_, &counts_, &atom_cells_, nc_));
@@ -368,7 +540,7 @@ class DeviceNeighborList {
 
   void build(const PositionVec* d_positions, i64 natoms, const Box& box, real r_cut, real r_skin,
              cudaStream_t stream = 0) {
-    const tdmd_box b = box.to_c();
+    const tdmd_box b = detail::to_c(box);
     detail::check(tdmd_nlist_build(h_, reinterpret_cast<const double*>(d_positions), natoms, &b,
                                    r_cut, r_skin, detail::stream_ptr(stream)));
     int64_t total = 0;
@@ -430,7 +602,7 @@ inline const double* masses(const real* d_masses, const i32* d_types, i32 natoms
     w.d = nullptr;
     w.cap = 0;
     if (cudaMalloc(reinterpret_cast<void**>(&w.d), sizeof(double) * hd.size()) != cudaSuccess)
-      throw Error(TDMD_ERR_OUT_OF_MEMORY, "mass buffer allocation failed");
+      throw StatusError(TDMD_ERR_OUT_OF_MEMORY, "mass buffer allocation failed");
     w.cap = hd.size();
   }
   ::tdmd::detail::check(tdmd_copy(w.d, hd.data(), sizeof(double) * hd.size(), s));
@@ -453,7 +625,7 @@ inline void device_half_kick(VelocityVec* d_velocities, const ForceVec* d_forces
 }
 inline void device_drift(PositionVec* d_positions, const VelocityVec* d_velocities, i32 natoms,
                          real dt, const Box& box, cudaStream_t stream = 0) {
-  const tdmd_box b = box.to_c();
+  const tdmd_box b = detail::to_c(box);
   ::tdmd::detail::check(tdmd_vv_drift(reinterpret_cast<double*>(d_positions),
                                       reinterpret_cast<const double*>(d_velocities), natoms, dt,
                                       &b, ::tdmd::detail::stream_ptr(stream)));
@@ -462,7 +634,7 @@ inline void device_fused_half_kick_drift(VelocityVec* d_velocities, PositionVec*
                                          const ForceVec* d_forces, const i32* d_types,
                                          const real* d_masses, i32 natoms, real dt,
                                          const Box& box, cudaStream_t stream = 0) {
-  const tdmd_box b = box.to_c();
+  const tdmd_box b = detail::to_c(box);
   ::tdmd::detail::check(tdmd_vv_fused_kick_drift(
       reinterpret_cast<double*>(d_velocities), reinterpret_cast<double*>(d_positions), d_forces,
       kForcePrecision, d_types, detail_masses::masses(d_masses, d_types, natoms, stream), natoms, dt, &b, 0,
@@ -472,7 +644,7 @@ inline void device_fused_full_kick_drift(VelocityVec* d_velocities, PositionVec*
                                          const ForceVec* d_forces, const i32* d_types,
                                          const real* d_masses, i32 natoms, real dt,
                                          const Box& box, cudaStream_t stream = 0) {
-  const tdmd_box b = box.to_c();
+  const tdmd_box b = detail::to_c(box);
   ::tdmd::detail::check(tdmd_vv_fused_kick_drift(
       reinterpret_cast<double*>(d_velocities), reinterpret_cast<double*>(d_positions), d_forces,
       kForcePrecision, d_types, detail_masses::masses(d_masses, d_types, natoms, stream), natoms, dt, &b, 1,
@@ -605,7 +777,7 @@ class FastPipelineScheduler {
  public:
   FastPipelineScheduler(const Box& box, i32 natoms, const potentials::MorseParams& params,
                         const FastPipelineConfig& cfg) {
-    const tdmd_box b = box.to_c();
+    const tdmd_box b = detail::to_c(box);
     const tdmd_morse_params p = params.to_c();
     const tdmd_fast_pipeline_config c = cfg.to_c();
     ::tdmd::detail::check(tdmd_sched_create_morse(&b, natoms, &p, &c, &h_));
@@ -613,7 +785,7 @@ class FastPipelineScheduler {
   }
   FastPipelineScheduler(const Box& box, i32 natoms, const potentials::EamAlloy& eam,
                         const FastPipelineConfig& cfg) {
-    const tdmd_box b = box.to_c();
+    const tdmd_box b = detail::to_c(box);
     const tdmd_fast_pipeline_config c = cfg.to_c();
     ::tdmd::detail::check(tdmd_sched_create_eam(&b, natoms, eam.handle(), &c, &h_));
     refresh();

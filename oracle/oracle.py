@@ -65,7 +65,7 @@ def build(ref: bool | None = None) -> None:
     if ref:
         if ref_tree is None:
             raise RuntimeError("reference tree not found: set TDMD_REFERENCE_TREE")
-        targets += ["ref", "refgpu", "dropin"]
+        targets += ["ref", "refgpu", "dropin", "reftests"]
     args = [f"REF={ref_tree}"] if ref_tree else []
     jobs = str(max(1, min(8, os.cpu_count() or 1)))
     subprocess.run(["make", "-s", "-j", jobs, "-C", _HERE, *args, *targets], check=True)

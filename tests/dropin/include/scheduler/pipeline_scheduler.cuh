@@ -41,11 +41,12 @@ struct PipelineStats {
 class PipelineScheduler {
  public:
   PipelineScheduler(const Box&, i32, const potentials::MorseParams&, const PipelineConfig&) {
-    throw Error(TDMD_ERR_UNSUPPORTED, "the TD zone PipelineScheduler is not part of this library");
+    throw StatusError(TDMD_ERR_UNSUPPORTED, "the TD zone PipelineScheduler is not part of this library");
   }
   void upload(const PositionVec*, const VelocityVec*, const ForceVec*, const i32*, const i32*,
               const real*, i32) {}
   void run_until(i32) {}
+  void download(PositionVec*, VelocityVec*, ForceVec*, i32*, i32*, i32) const {}
   const PipelineStats& stats() const noexcept { return stats_; }
   const domain::ZonePartition& partition() const noexcept { return zones_; }
 
