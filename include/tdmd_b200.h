@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define TDMD_B200_ABI_VERSION 2
+#define TDMD_B200_ABI_VERSION 3
 
 typedef enum tdmd_status {
   TDMD_OK = 0,
@@ -143,6 +143,15 @@ int32_t tdmd_eam_read_setfl(const char* path, tdmd_eam** out);
 int32_t tdmd_eam_create(int32_t ntypes, int32_t nrho, double drho, int32_t nr, double dr,
                         double cutoff, const double* F, const double* rho, const double* rphi,
                         tdmd_eam** out);
+/* Same tables from the sampled functions as the reference's EamAlloy holds
+ * them after read_setfl (eam_alloy.cpp:150-189, the SplineTable values of
+ * embedding(), density() and phi()): F[ntypes*nrho], rho[ntypes*nr] and
+ * phi[npairs*nr] = phi(k*dr) itself (the setfl's r*phi over r, phi(0) = 0),
+ * pairs i<=j in setfl order.  The splines are built from these samples
+ * exactly as from read_setfl's. */
+int32_t tdmd_eam_create_sampled(int32_t ntypes, int32_t nrho, double drho, int32_t nr,
+                                double dr, double cutoff, const double* F, const double* rho,
+                                const double* phi, tdmd_eam** out);
 int32_t tdmd_eam_destroy(tdmd_eam* eam);
 /* cutoff(), ntypes(); table sizes. */
 int32_t tdmd_eam_info(const tdmd_eam* eam, int32_t* ntypes, int32_t* nrho, double* drho,

@@ -42,6 +42,7 @@
 #include "core/error.hpp"
 #include "core/system_state.hpp"
 #include "core/types.hpp"
+#include "potentials/eam_alloy.hpp"
 #endif
 
 namespace tdmd {
@@ -335,6 +336,7 @@ inline void compute_morse_gpu(const PositionVec* d_positions, ForceVec* d_forces
                                    &p, d_energy, nullptr, detail::stream_ptr(stream)));
 }
 
+#if !defined(TDMD_B200_REFERENCE_CORE)
 // eam_alloy.hpp:47-93 (tables; the CPU compute_forces stays in the reference).
 class EamAlloy {
  public:
@@ -368,6 +370,50 @@ class EamAlloy {
  private:
   tdmd_eam* h_ = nullptr;
 };
+#endif  // !TDMD_B200_REFERENCE_CORE
+
+// The library's tables of an EamAlloy: its own handle, or, with the
+// reference's EamAlloy (TDMD_B200_REFERENCE_CORE), a temporary set built from
+// that class's sampled F(rho), rho(r) and phi(r) (eam_alloy.hpp:65-73) and
+// freed once the consumer has copied it.
+class EamTables {
+ public:
+#if defined(TDMD_B200_REFERENCE_CORE)
+  explicit EamTables(const EamAlloy& eam) {
+    const auto& F = eam.embedding();
+    const auto& rho = eam.density();
+    const auto& phi = eam.phi();
+    const i32 nt = eam.ntypes();
+    const size_t npairs = static_cast<size_t>(nt) * static_cast<size_t>(nt + 1) / 2;
+    if (nt < 1 || F.size() != static_cast<size_t>(nt) || rho.size() != static_cast<size_t>(nt) ||
+        phi.size() != npairs)
+      throw StatusError(TDMD_ERR_INVALID_ARGUMENT, "EamAlloy has no tables (read_setfl first)");
+    const i32 nrho = F[0].n, nr = rho[0].n;
+    std::vector<double> f, r, p;
+    for (const auto& t : F) f.insert(f.end(), t.values.begin(), t.values.end());
+    for (const auto& t : rho) r.insert(r.end(), t.values.begin(), t.values.end());
+    for (const auto& t : phi) p.insert(p.end(), t.values.begin(), t.values.end());
+    if (f.size() != static_cast<size_t>(nt) * nrho || r.size() != static_cast<size_t>(nt) * nr ||
+        p.size() != npairs * static_cast<size_t>(nr))
+      throw StatusError(TDMD_ERR_INVALID_ARGUMENT, "EamAlloy tables of unequal lengths");
+    detail::check(tdmd_eam_create_sampled(nt, nrho, F[0].dr, nr, rho[0].dr, eam.cutoff(),
+                                          f.data(), r.data(), p.data(), &own_));
+    h_ = own_;
+  }
+#else
+  explicit EamTables(const EamAlloy& eam) : h_(eam.handle()) {}
+#endif
+  ~EamTables() {
+    if (own_) tdmd_eam_destroy(own_);
+  }
+  EamTables(const EamTables&) = delete;
+  EamTables& operator=(const EamTables&) = delete;
+  const tdmd_eam* get() const noexcept { return h_; }
+
+ private:
+  const tdmd_eam* h_ = nullptr;
+  tdmd_eam* own_ = nullptr;
+};
 
 // device_eam.cuh:26-50
 class DeviceEam {
@@ -381,7 +427,7 @@ class DeviceEam {
 
   void upload_tables(const EamAlloy& eam) {
     tdmd_device_eam* h = nullptr;
-    detail::check(tdmd_device_eam_create(eam.handle(), &h));
+    detail::check(tdmd_device_eam_create(EamTables(eam).get(), &h));
     if (h_) tdmd_device_eam_destroy(h_);
     h_ = h;
     cutoff_ = eam.cutoff();
@@ -487,7 +533,8 @@ inline void write_lammps_force_dump(const SystemState& s, const std::string& pat
 
 // No reference counterpart (the reference only reads setfl).
 inline void write_setfl(const potentials::EamAlloy& eam, const std::string& path) {
-  detail::check(tdmd_write_setfl(path.c_str(), eam.handle(), nullptr, nullptr, nullptr));
+  detail::check(tdmd_write_setfl(path.c_str(), potentials::EamTables(eam).get(), nullptr, nullptr,
+                                 nullptr));
 }
 
 }  // namespace io
@@ -787,7 +834,8 @@ class FastPipelineScheduler {
                         const FastPipelineConfig& cfg) {
     const tdmd_box b = detail::to_c(box);
     const tdmd_fast_pipeline_config c = cfg.to_c();
-    ::tdmd::detail::check(tdmd_sched_create_eam(&b, natoms, eam.handle(), &c, &h_));
+    ::tdmd::detail::check(
+        tdmd_sched_create_eam(&b, natoms, potentials::EamTables(eam).get(), &c, &h_));
     refresh();
   }
   ~FastPipelineScheduler() { tdmd_sched_destroy(h_); }

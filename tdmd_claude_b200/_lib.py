@@ -95,6 +95,7 @@ SIGNATURES = {
     "tdmd_fast_pipeline_config_default": [C.POINTER(FastPipelineConfig)],
     "tdmd_eam_read_setfl": [C.c_char_p, _pp],
     "tdmd_eam_create": [_i32, _i32, _f64, _i32, _f64, _f64, _p, _p, _p, _pp],
+    "tdmd_eam_create_sampled": [_i32, _i32, _f64, _i32, _f64, _f64, _p, _p, _p, _pp],
     "tdmd_eam_destroy": [_p],
     "tdmd_eam_info": [_p, _pi32, _pi32, _pf64, _pi32, _pf64, _pf64],
     "tdmd_set_deterministic_reduce": [_i32],

@@ -129,6 +129,16 @@ class EamAlloy:
              float(cutoff), _ptr(F), _ptr(rho), _ptr(rphi), C.byref(h))
         return cls(h)
 
+    @classmethod
+    def from_samples(cls, ntypes, nrho, drho, nr, dr, cutoff, F, rho, phi) -> "EamAlloy":
+        """Tables from phi(r) samples (the reference EamAlloy's SplineTable
+        values) instead of the setfl's r*phi(r)."""
+        F, rho, phi = _f64(F), _f64(rho), _f64(phi)
+        h = C.c_void_p()
+        call("tdmd_eam_create_sampled", int(ntypes), int(nrho), float(drho), int(nr), float(dr),
+             float(cutoff), _ptr(F), _ptr(rho), _ptr(phi), C.byref(h))
+        return cls(h)
+
     @property
     def handle(self):
         if not self._h:

@@ -29,6 +29,9 @@ struct tdmd_eam {
   std::vector<double> F;     // [ntypes][nrho] raw F(rho)
   std::vector<double> rho;   // [ntypes][nr]   raw rho(r)
   std::vector<double> rphi;  // [npairs][nr]   raw r*phi(r)
+  // [npairs][nr] phi(r) itself, when the tables were given as phi samples
+  // (empty otherwise: phi is then r*phi / r)
+  std::vector<double> phi;
   // Packed a|b|c|d coefficients per spline, each block 4*(n-1) long.
   std::vector<double> Fc, rhoc, phic;
 };

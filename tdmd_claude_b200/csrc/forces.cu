@@ -3,6 +3,7 @@
 // force entry points of the C ABI (compute_morse_gpu, DeviceEam).
 #include <cctype>
 #include <climits>
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <fstream>
@@ -59,12 +60,19 @@ void eam_build_coeffs(tdmd_eam& e) {
     build_spline(e.rho.data() + static_cast<size_t>(t) * e.nr, e.nr, e.dr,
                  e.rhoc.data() + static_cast<size_t>(t) * 4 * (e.nr - 1));
   }
-  // phi = (r*phi)/r with phi(0) = 0, eam_alloy.cpp:176-188.
+  // phi = (r*phi)/r with phi(0) = 0, eam_alloy.cpp:176-188, unless the
+  // tables came as phi samples.
   std::vector<double> phi(static_cast<size_t>(e.nr));
   for (int p = 0; p < npairs; ++p) {
-    const double* rp = e.rphi.data() + static_cast<size_t>(p) * e.nr;
-    phi[0] = 0.0;
-    for (int k = 1; k < e.nr; ++k) phi[static_cast<size_t>(k)] = rp[k] / (k * e.dr);
+    const size_t off = static_cast<size_t>(p) * e.nr;
+    if (!e.phi.empty()) {
+      std::copy(e.phi.begin() + static_cast<long>(off),
+                e.phi.begin() + static_cast<long>(off + e.nr), phi.begin());
+    } else {
+      const double* rp = e.rphi.data() + off;
+      phi[0] = 0.0;
+      for (int k = 1; k < e.nr; ++k) phi[static_cast<size_t>(k)] = rp[k] / (k * e.dr);
+    }
     build_spline(phi.data(), e.nr, e.dr, e.phic.data() + static_cast<size_t>(p) * 4 * (e.nr - 1));
   }
 }
@@ -358,6 +366,34 @@ int32_t tdmd_eam_create(int32_t ntypes, int32_t nrho, double drho, int32_t nr, d
     e->F.assign(F, F + static_cast<size_t>(ntypes) * nrho);
     e->rho.assign(rho, rho + static_cast<size_t>(ntypes) * nr);
     e->rphi.assign(rphi, rphi + static_cast<size_t>(npairs) * nr);
+    e->elements.assign(static_cast<size_t>(ntypes), "X");
+    eam_build_coeffs(*e);
+    *out = e;
+  });
+}
+
+int32_t tdmd_eam_create_sampled(int32_t ntypes, int32_t nrho, double drho, int32_t nr,
+                                double dr, double cutoff, const double* F, const double* rho,
+                                const double* phi, tdmd_eam** out) {
+  return guarded([&] {
+    TDMD_REQUIRE(out && F && rho && phi, "null argument");
+    TDMD_REQUIRE(ntypes >= 1 && ntypes <= 64, "ntypes out of range");
+    TDMD_REQUIRE(nrho >= 2 && nr >= 2 && drho > 0 && dr > 0 && cutoff > 0, "bad grid");
+    auto* e = new tdmd_eam();
+    e->ntypes = ntypes;
+    e->nrho = nrho;
+    e->nr = nr;
+    e->drho = drho;
+    e->dr = dr;
+    e->cutoff = cutoff;
+    const int npairs = ntypes * (ntypes + 1) / 2;
+    const size_t np = static_cast<size_t>(npairs) * nr;
+    e->F.assign(F, F + static_cast<size_t>(ntypes) * nrho);
+    e->rho.assign(rho, rho + static_cast<size_t>(ntypes) * nr);
+    e->phi.assign(phi, phi + np);
+    // r*phi for writing the tables out as setfl
+    e->rphi.resize(np);
+    for (size_t i = 0; i < np; ++i) e->rphi[i] = phi[i] * (static_cast<double>(i % nr) * dr);
     e->elements.assign(static_cast<size_t>(ntypes), "X");
     eam_build_coeffs(*e);
     *out = e;

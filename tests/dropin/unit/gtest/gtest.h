@@ -91,15 +91,22 @@ template <class T>
 struct Streamable<T, std::void_t<decltype(std::declval<std::ostream&>() << std::declval<const T&>())>>
     : std::true_type {};
 
-// The value in a failure message; containers print their size, other
-// values without an output operator print a placeholder.
+template <class T, class = void>
+struct HasSize : std::false_type {};
+template <class T>
+struct HasSize<T, std::void_t<decltype(std::declval<const T&>().size())>> : std::true_type {};
+
+// The value in a failure message; enums print their integer, containers
+// their size, other values without an output operator a placeholder.
 template <class T>
 std::string show(const T& v) {
   std::ostringstream s;
   s.precision(17);
-  if constexpr (Streamable<T>::value)
+  if constexpr (std::is_enum_v<T>)
+    s << static_cast<long long>(v);
+  else if constexpr (Streamable<T>::value)
     s << v;
-  else if constexpr (std::is_class_v<T> && sizeof(std::declval<const T&>().size()) > 0)
+  else if constexpr (HasSize<T>::value)
     s << "{container of " << v.size() << " elements}";
   else
     s << "{value}";

@@ -2,15 +2,16 @@
 compiled unchanged against this library and run on the GPU.
 
 `make -C oracle reftests` builds each test file twice (FP64 and mixed
-builds, as the reference builds them) plus its Morse device and cell-list
-tests with the reference's deterministic-reduction switch: the path's GPU
+builds, as the reference builds them) plus its Morse, EAM and cell-list
+device tests with the reference's deterministic-reduction switch: the path's GPU
 headers come from the include-path shim (tests/dropin/include ->
 include/tdmd_b200.hpp), the reference's core headers and CPU classes -- the
 tests' expected values -- from its own tree (TDMD_B200_REFERENCE_CORE), and
 GoogleTest's macros from tests/dropin/unit.  The binaries read their data directory from
 TDMD_TEST_DATA_DIR, filled here from committed fixtures: the reference's
-256-atom data file (tests/data/cu_fcc_256.data, from run0_morse_256.json)
-and its Mishin setfl.
+256-atom data file (tests/data/cu_fcc_256.data, from run0_morse_256.json),
+its Mishin setfl and the LAMMPS run-0 force dumps of that system
+(run0_morse_256.json, run0_eam_256.json).
 
 Expected outcome, per test: OK, except
   * FastPipelineScheduler.KernelLaunchInvariant, which pins the reference's
@@ -42,6 +43,7 @@ LAUNCH_INVARIANT = {"FastPipelineScheduler.KernelLaunchInvariant"}
 ZONE_PIPELINE = {"NVTThermostat.TemperatureConvergesToTarget",
                  "NVTThermostat.DeterministicReproducibility", "AdaptiveDt.StableNVETrajectory"}
 DETERMINISM = {"DeviceMorseDeterminism.EnergyBitIdentical",
+               "DeviceEamDeterminism.EnergyBitIdentical",
                "DeviceCellListDeterminism.TwoBuildsBitIdentical"}
 
 CASES = {
@@ -56,12 +58,19 @@ CASES = {
                                   "DeviceNeighborList.MatchesCPUHalfListPairCount"},
     "test_device_morse": {"DeviceMorse.MatchesCPUForces256Atoms",
                           "DeviceMorseDeterminism.EnergyBitIdentical"},
+    "test_device_eam": {"DeviceEam.MatchesCPUForces256Atoms",
+                        "DeviceEamDeterminism.EnergyBitIdentical"},
+    "test_device_lammps_ab": {"DeviceLammpsAB.MorseRun0ForceMatch",
+                              "DeviceLammpsAB.EamRun0ForceMatch"},
     "test_device_nve_drift": {"DeviceNVEDrift.Morse256Atoms50kSteps",
                               "DeviceNVEDrift.ADR0007AcceptanceTest100k",
                               "DeviceVelocityVerlet.FusedKickDriftMatchesUnfused"},
     "test_fast_pipeline": {"FastPipelineScheduler.NVEConservation",
                            "FastPipelineScheduler.LongNVEDrift",
                            "FastPipelineScheduler.KernelLaunchInvariant"},
+    "test_fast_pipeline_eam": {"FastPipelineSchedulerEam.EamStepMatchesDirectCompute",
+                               "FastPipelineSchedulerEam.EamNve100StepsStable",
+                               "FastPipelineSchedulerEam.EamDeterministicReplay"},
     "test_nvt_thermostat": {"NVTThermostat.TemperatureConvergesToTarget",
                             "NVTThermostat.DeviceKEMatchesHost",
                             "NVTThermostat.DeterministicReproducibility",
@@ -79,14 +88,19 @@ def data_dir(tmp_path_factory):
     from tdmd_claude_b200 import workloads as W
     d = str(tmp_path_factory.mktemp("ref_unit_data"))
     g = golden("run0_morse_256.json")
+    ge = golden("run0_eam_256.json")
     pos = np.array(g["positions"])
     n = len(pos)
-    TIO.write_lammps_data(os.path.join(d, "cu_fcc_256.data"),
-                          W.System(pos, np.zeros_like(pos), np.ones(n, np.int32),
-                                   np.arange(1, n + 1, dtype=np.int32), np.array(g["masses"]),
-                                   tuple(g["lo"]), tuple(g["hi"])))
-    setfl = golden_file(golden("run0_eam_256.json")["potential_file"], d)
+    s = W.System(pos, np.zeros_like(pos), np.ones(n, np.int32), np.arange(1, n + 1, dtype=np.int32),
+                 np.array(g["masses"]), tuple(g["lo"]), tuple(g["hi"]))
+    TIO.write_lammps_data(os.path.join(d, "cu_fcc_256.data"), s)
+    setfl = golden_file(ge["potential_file"], d)
     os.replace(setfl, os.path.join(d, "Cu_mishin1.eam.alloy"))
+    # the LAMMPS run-0 dumps of the same system (verifylab/cases/run0-force-match)
+    os.makedirs(os.path.join(d, "reference"))
+    for name, fix in (("forces_morse.dump", g), ("forces_eam.dump", ge)):
+        TIO.write_force_dump(os.path.join(d, "reference", name), s,
+                             np.array(fix["lammps_forces"]), step=0)
     return d
 
 
@@ -117,13 +131,13 @@ def test_reference_unit_tests_run_unchanged(cuda, data_dir, case, precision):
         assert "TD zone PipelineScheduler is not part of this library" in out.stdout
 
 
-@pytest.mark.parametrize("case", ["test_device_morse", "test_device_cell_list"])
+@pytest.mark.parametrize("case", ["test_device_morse", "test_device_eam", "test_device_cell_list"])
 def test_reference_determinism_tests_in_their_deterministic_build(cuda, data_dir, case):
     """The reference's determinism tests, built with its
     TDMD_DETERMINISTIC_REDUCE switch (the library's ID-ordered mode turned on
-    before main): two Morse compute calls give bit-identical energies, two
-    cell-list builds bit-identical cells; the other tests of each file still
-    pass in that build."""
+    before main): two Morse or EAM compute calls give bit-identical
+    energies, two cell-list builds bit-identical cells; the other tests of
+    each file still pass in that build."""
     out, results = _run(f"reftest_{case}_fp64_det", data_dir)
     assert set(results) == CASES[case], out.stdout[-3000:]
     assert all(v == "OK" for v in results.values()), out.stdout[-3000:]

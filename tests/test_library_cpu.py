@@ -35,7 +35,7 @@ def test_exports_every_declared_symbol(L):
     for s in syms:
         assert hasattr(L, s), s
     assert set(syms) == set(_lib.SIGNATURES), set(syms) ^ set(_lib.SIGNATURES)
-    assert L.tdmd_abi_version() == 2
+    assert L.tdmd_abi_version() == 3
 
 
 def test_config_defaults_follow_reference(L):
@@ -79,6 +79,26 @@ def test_eam_from_tables_equals_setfl(L):
     b = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
     for kind in (0, 1, 2):
         np.testing.assert_allclose(a.coeffs(kind, 0), b.coeffs(kind, 0), rtol=1e-13, atol=1e-13)
+
+
+def test_eam_from_phi_samples_equals_setfl_tables(L):
+    """tdmd_eam_create_sampled: tables given as phi(r) samples (r*phi / r,
+    phi(0) = 0, as the reference's EamAlloy stores them) build the same
+    splines as the r*phi arrays of the setfl, bit for bit (ternary: six
+    pair tables)."""
+    from tdmd_claude_b200 import EamAlloy
+    from tdmd_claude_b200 import workloads as W
+    t = W.ternary_eam_tables()
+    a = EamAlloy.from_tables(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, t.rphi)
+    rphi = np.asarray(t.rphi, np.float64).reshape(-1, t.nr)
+    r = np.arange(t.nr) * t.dr
+    phi = np.zeros_like(rphi)
+    phi[:, 1:] = rphi[:, 1:] / r[1:]
+    b = EamAlloy.from_samples(t.ntypes, t.nrho, t.drho, t.nr, t.dr, t.cutoff, t.F, t.rho, phi)
+    npairs = t.ntypes * (t.ntypes + 1) // 2
+    for kind, count in ((0, t.ntypes), (1, t.ntypes), (2, npairs)):
+        for idx in range(count):
+            assert np.array_equal(a.coeffs(kind, idx), b.coeffs(kind, idx))
 
 
 @pytest.mark.parametrize("contents", [
