@@ -1,6 +1,7 @@
 // gtest/gtest.h -- the subset of GoogleTest's test macros that the
-// reference's GPU unit tests use (TEST, EXPECT_/ASSERT_ EQ NE LT LE GT GE
-// NEAR TRUE FALSE, GTEST_SKIP, streamed messages), so those test files
+// reference's unit tests of this path use (TEST, EXPECT_/ASSERT_ EQ NE LT LE
+// GT GE NEAR TRUE FALSE THROW, EXPECT_DOUBLE_EQ / FLOAT_EQ, GTEST_SKIP,
+// streamed messages), so those test files
 // compile unchanged here without GoogleTest.  Test infrastructure only.
 //
 // Each TEST registers a function; tests/dropin/unit/gtest_main.cpp runs
@@ -11,6 +12,8 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstring>
+#include <limits>
 #include <functional>
 #include <sstream>
 #include <string>
@@ -130,6 +133,26 @@ Result near(const A& a, const B& b, const C& tol, const char* ea, const char* eb
                            "\n  right: " + show(b)};
 }
 
+// Within 4 units in the last place, GoogleTest's floating-point equality.
+template <class T>
+Result ulp_eq(T a, T b, const char* macro, const char* ea, const char* eb) {
+  static_assert(std::is_floating_point_v<T>);
+  using U = std::conditional_t<sizeof(T) == 8, long long, int>;
+  auto key = [](T x) {
+    U u;
+    std::memcpy(&u, &x, sizeof u);
+    return u < 0 ? std::numeric_limits<U>::min() - u : u;  // sign-magnitude -> ordered
+  };
+  bool ok = a == b;
+  if (!ok && !std::isnan(a) && !std::isnan(b)) {
+    const U ka = key(a), kb = key(b);
+    ok = (ka > kb ? ka - kb : kb - ka) <= 4;
+  }
+  if (ok) return Result{true, {}};
+  return Result{false, std::string(macro) + "(" + ea + ", " + eb + ")\n  left:  " + show(a) +
+                           "\n  right: " + show(b)};
+}
+
 inline Result truth(bool v, bool want, const char* macro, const char* e) {
   if (v == want) return Result{true, {}};
   return Result{false, std::string(macro) + "(" + e + ")"};
@@ -180,6 +203,27 @@ inline Result truth(bool v, bool want, const char* macro, const char* e) {
 #define EXPECT_FALSE(c) TDMD_GT_EXPECT_(::gtest_shim::truth(static_cast<bool>(c), false, "EXPECT_FALSE", #c))
 #define ASSERT_TRUE(c) TDMD_GT_ASSERT_(::gtest_shim::truth(static_cast<bool>(c), true, "ASSERT_TRUE", #c))
 #define ASSERT_FALSE(c) TDMD_GT_ASSERT_(::gtest_shim::truth(static_cast<bool>(c), false, "ASSERT_FALSE", #c))
+#define EXPECT_DOUBLE_EQ(a, b) \
+  TDMD_GT_EXPECT_(::gtest_shim::ulp_eq<double>((a), (b), "EXPECT_DOUBLE_EQ", #a, #b))
+#define EXPECT_FLOAT_EQ(a, b) \
+  TDMD_GT_EXPECT_(::gtest_shim::ulp_eq<float>((a), (b), "EXPECT_FLOAT_EQ", #a, #b))
+#define TDMD_GT_THROWS_(stmt, type, fatal_return)                                      \
+  if (const ::gtest_shim::Result tdmd_gt_r_ = [&] {                                    \
+        try {                                                                          \
+          stmt;                                                                        \
+        } catch (const type&) {                                                        \
+          return ::gtest_shim::Result{true, {}};                                       \
+        } catch (...) {                                                                \
+          return ::gtest_shim::Result{false, "EXPECT_THROW(" #stmt ", " #type           \
+                                             "): threw another type"};                 \
+        }                                                                              \
+        return ::gtest_shim::Result{false, "EXPECT_THROW(" #stmt ", " #type            \
+                                           "): did not throw"};                        \
+      }()) {                                                                           \
+  } else                                                                               \
+    fatal_return TDMD_GT_FAIL_(tdmd_gt_r_.what)
+#define EXPECT_THROW(stmt, type) TDMD_GT_THROWS_(stmt, type, )
+#define ASSERT_THROW(stmt, type) TDMD_GT_THROWS_(stmt, type, return)
 #define GTEST_SKIP() return ::gtest_shim::SkipHelper{} = ::gtest_shim::Message()
 #define FAIL() return TDMD_GT_FAIL_("FAIL()")
 #define ADD_FAILURE() TDMD_GT_FAIL_("ADD_FAILURE()")

@@ -4,7 +4,8 @@ Run where the reference tree is available ($TDMD_REFERENCE_TREE, or a
 checkout named `reference` beside this repository) after
 `make -C oracle all ref`:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py               # everything
+    python tests/golden/make_golden.py --data-files  # the copied inputs only
 
 Sources of truth, all from the reference itself:
   * two_atoms_morse.json   -- VerifyLab analytic values
@@ -20,6 +21,10 @@ Sources of truth, all from the reference itself:
                               PRB 63, 224106 (2001)), xz-compressed byte for
                               byte, so the EAM run-0 tests run where the
                               reference tree is absent
+  * 4atoms.data            -- the reference's data-reader test input
+                              (tests/data/4atoms.data), byte for byte, for
+                              its LammpsDataReader unit test run against this
+                              library's reader
   * ref_*.json             -- outputs of the reference's CPU path (compiled
                               from its sources into oracle/_ref/) on the
                               seeded synthetic inputs of tdmd_claude_b200.workloads
@@ -74,7 +79,20 @@ def read_data(path):
     return pos, vel, ty, ids, m, lo, hi
 
 
+def copy_data_files():
+    """Reference test inputs that its unit tests read, copied unchanged."""
+    for name in ("4atoms.data",):
+        with open(os.path.join(REF, "tests/data", name), "rb") as f:
+            raw = f.read()
+        with open(os.path.join(HERE, name), "wb") as f:
+            f.write(raw)
+        print("wrote", name)
+
+
 def main():
+    copy_data_files()
+    if "--data-files" in sys.argv:
+        return
     O.build(ref=True)
     R = O.ref()
     assert R is not None, "reference harness not built"

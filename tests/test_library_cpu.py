@@ -435,3 +435,20 @@ def test_native_setfl_writer_roundtrip(L, mishin_setfl, tmp_path):
             out.append((pe, f))
         assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
         _ = C
+
+
+def test_reference_data_reader_unit_test(L):
+    """The reference's own LammpsDataReader unit test
+    (tests/unit/test_lammps_data_reader.cpp: Basic4Atoms, FileNotFound),
+    compiled unchanged against this library's native reader
+    (`make -C oracle reftests`), on its 4-atom input (tests/golden/4atoms.data,
+    copied from the reference by make_golden.py)."""
+    import subprocess
+    exe = os.path.join(ROOT, "oracle", "_ref", "reftest_test_lammps_data_reader_fp64")
+    if not os.path.exists(exe):
+        pytest.skip("reference unit tests not built (make -C oracle reftests)")
+    env = dict(os.environ, TDMD_TEST_DATA_DIR=os.path.join(ROOT, "tests", "golden"))
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=120, env=env)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "[       OK ] LammpsDataReader.Basic4Atoms" in out.stdout
+    assert "[       OK ] LammpsDataReader.FileNotFound" in out.stdout
