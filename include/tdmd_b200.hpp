@@ -554,6 +554,8 @@ class DeviceCellList {
     detail::check(tdmd_cell_list_build(h_, reinterpret_cast<const double*>(d_positions), natoms,
                                        &b, r_list, nullptr));
     detail::check(tdmd_cell_list_get(h_, &atoms_, &offsets_, &counts_, &atom_cells_, nc_));
+    const Vec3D L = box.size();
+    cell_size_ = Vec3D{L.x / nc_[0], L.y / nc_[1], L.z / nc_[2]};  // cell_list.cpp:21-23
   }
   i32 ncells_x() const noexcept { return nc_[0]; }
   i32 ncells_y() const noexcept { return nc_[1]; }
@@ -563,6 +565,7 @@ class DeviceCellList {
   const i32* d_cell_counts() const noexcept { return counts_; }
   const i32* d_cell_atoms() const noexcept { return atoms_; }
   const i32* d_atom_cells() const noexcept { return atom_cells_; }
+  Vec3D cell_size() const noexcept { return cell_size_; }
 
  private:
   tdmd_cell_list* h_ = nullptr;
@@ -571,6 +574,7 @@ class DeviceCellList {
   const int32_t* counts_ = nullptr;
   const int32_t* atom_cells_ = nullptr;
   int32_t nc_[3] = {0, 0, 0};
+  Vec3D cell_size_{0, 0, 0};
 };
 
 }  // namespace domain

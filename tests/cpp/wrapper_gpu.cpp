@@ -81,6 +81,17 @@ int main(int argc, char** argv) {
   for (int i = 0; i < n; ++i)
     std::fprintf(out, "%.17g %.17g %.17g\n", static_cast<double>(forces[i].x),
                  static_cast<double>(forces[i].y), static_cast<double>(forces[i].z));
+  // cell list of the same positions at r_list = rc + skin: grid and cell size
+  try {
+    domain::DeviceCellList cl;
+    cl.build(d_pos, n, box, rc + real(0.3));
+    const Vec3D cs = cl.cell_size();
+    std::fprintf(out, "%d %d %d %.17g %.17g %.17g\n", cl.ncells_x(), cl.ncells_y(),
+                 cl.ncells_z(), cs.x, cs.y, cs.z);
+  } catch (const Error& e) {
+    std::fprintf(stderr, "error %d: %s\n", e.status(), e.what());
+    return 9;
+  }
   std::fclose(out);
   cudaFree(d_pos);
   cudaFree(d_f);

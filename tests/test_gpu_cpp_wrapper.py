@@ -19,6 +19,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 
+def rd_(precision):
+    """The mixed build's `real` is float: its dt, skin, masses and Morse
+    parameters arrive rounded to float."""
+    return (lambda x: float(np.float32(x))) if precision == "mixed" else float  # noqa: E731
+
+
 @pytest.mark.parametrize("define,precision", [("TDMD_PRECISION_FP64", "fp64"),
                                               ("TDMD_PRECISION_MIXED", "mixed")])
 def test_cpp_layer_runs_gpu_path(cuda, tmp_path, define, precision):
@@ -49,9 +55,13 @@ def test_cpp_layer_runs_gpu_path(cuda, tmp_path, define, precision):
     sched_rows = np.array([[float(x) for x in l.split()] for l in rows[:n]])
     e_cpp = float(rows[n])
     f_cpp = np.array([[float(x) for x in l.split()] for l in rows[n + 1:2 * n + 1]])
-    # the same through the Python API; the mixed build's `real` is float, so
-    # its dt, skin, masses and Morse parameters arrive rounded to float
-    rd = (lambda x: float(np.float32(x))) if precision == "mixed" else float  # noqa: E731
+    cells = rows[2 * n + 1].split()
+    L = hi - lo
+    nc = max(3, int(np.floor(L / (6.0 + rd_(precision)(0.3)))))
+    assert [int(x) for x in cells[:3]] == [nc] * 3
+    assert [float(x) for x in cells[3:]] == [L / nc] * 3
+    # the same through the Python API
+    rd = rd_(precision)
     box = Box.make((lo,) * 3, (hi,) * 3)
     mp = MorseParams.make(rd(0.3429), rd(1.3588), rd(2.866), 6.0)
     s = FastPipelineScheduler(box, n, mp, make_config(dt=rd(0.001), r_skin=rd(0.3),
