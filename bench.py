@@ -550,6 +550,47 @@ def ternary_bench(steps, warmup, flush, torch, total_steps=2000):
                         "NVT NHC-3 1000 K, adaptive dt"}
 
 
+def size_scaling_bench(steps, warmup, flush, torch, ncells=(32, 64, 128, 160)):
+    """The headline workload (Cu FCC, analytic EAM, skin 0.3, rebuild every
+    10) at 4 n^3 atoms for each n in ncells, mixed and FP64, one system per
+    GPU: atom-steps/s out of L2 (the 32^3 system's ~55 MB stays resident in
+    the 126 MB L2; 128^3 and 160^3 hold 3-8 GB) and the device memory each
+    scheduler holds."""
+    from tdmd_claude_b200 import workloads as W
+    t = W.cu_eam_tables()
+    eam = make_eam(t)
+    hbm, _ = measured_peaks()
+    rl = t.cutoff + SKIN
+    K = fcc_neighbors(3.615, rl)
+    out = {}
+    for nc in ncells:
+        sysm = W.fcc_system(nc, 3.615, 300.0, 4321 + nc)
+        row = {"atoms": sysm.n}
+        for prec in ("mixed", "fp64"):
+            torch.cuda.synchronize()
+            free0, _ = torch.cuda.mem_get_info()
+            s = make_sched(sysm, eam, prec)
+            s.run_until(0)
+            torch.cuda.synchronize()
+            free1, _ = torch.cuda.mem_get_info()
+            ms, _, _, _ = timed_windows(s, steps, warmup, flush, torch, None)
+            st = s.stats()
+            s.close()
+            value = sysm.n * WINDOW * steps / (ms * 1e-3)
+            row[prec] = {"value": value, "ms_per_window": ms / steps,
+                         "device_bytes": int(free0 - free1),
+                         "launch_shapes": stats_shapes(st),
+                         "path_roofline": path_roofline(
+                             value, "eam", prec, K,
+                             cell_occupancy(sysm.n, sysm.hi[0] - sysm.lo[0], rl), hbm)}
+        row["mixed_over_fp64"] = row["mixed"]["value"] / row["fp64"]["value"]
+        out[f"{nc}^3"] = row
+        del sysm
+    return {"unit": "atom-steps/s", "sizes": out,
+            "workload": "Cu FCC n^3 cells, analytic EAM, NVE, skin 0.3, rebuild every 10; "
+                        "L2 flushed (256 MiB write) before every window"}
+
+
 def fit_bench(torch, adam_steps=200, nsnap=64, continue_morse=True):
     """Force matching: nsnap snapshots of a 10^3-cell Cu FCC (4,000 atoms)
     FP64 NVE run at 1200 K (one every 100 steps, config-1 EAM); targets from
@@ -827,6 +868,8 @@ def main():
                     help="skip the 4M-atom ternary NVT + adaptive-dt figure")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-replica (512 Morse systems) figure")
+    ap.add_argument("--no-sizes", action="store_true",
+                    help="skip the single-system size sweep (131 k to 16.4 M atoms)")
     ap.add_argument("--drift-steps", type=int, default=50000,
                     help="NVE steps for the energy-drift figure (0 = skip)")
     args = ap.parse_args()
@@ -836,7 +879,7 @@ def main():
         # N replicas: the headline, e2e and the sharded batch figure; the
         # single-GPU extras (drift, force matching, 4 M-atom ternary) are not
         # repeated per rank.
-        args.no_fit = args.no_ternary = True
+        args.no_fit = args.no_ternary = args.no_sizes = True
         args.drift_steps = 0
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -961,6 +1004,8 @@ def main():
     small = None if args.no_batch else morse256_bench(torch)
     ternary = None if args.no_ternary else ternary_bench(max(3, args.steps // 3), 3, flush,
                                                            torch)
+    sizes = None if args.no_sizes else size_scaling_bench(max(3, args.steps // 5), 3, flush,
+                                                          torch)
 
     hbm, peak_kind = measured_peaks()
     occ = cell_occupancy(sysm.n, sysm.hi[0] - sysm.lo[0], eam.cutoff() + SKIN)
@@ -1051,6 +1096,7 @@ def main():
                 "batched_replicas": batch,
                 "batched_eam_131k_x8": beam,
                 "ternary_4m_nvt_adaptive": ternary,
+                "single_system_sizes": sizes,
                 "morse_256_nve_1000": small,
                 "force_matching": fitfig,
                 "wall_s_timed_region": wall_mixed,
