@@ -283,7 +283,8 @@ class Batch {
   void kick_drift(bool full);
   void half_kick();
   void enqueue_step(const BatchStep& st);
-  void run_segment(const std::vector<BatchStep>& seg, bool finalize);
+  void run_segment(const std::vector<BatchStep>& seg, bool finalize, bool prologue);
+  void enqueue_prologue();
   void initial_forces();
   void grow_capacity(int max_count);
   void reduce_energies(double* out);
@@ -671,13 +672,31 @@ void Batch::enqueue_step(const BatchStep& st) {
   force(st.fuse_next, st.log_e);
 }
 
-void Batch::run_segment(const std::vector<BatchStep>& seg, bool finalize) {
+// A window's first segment starts with the snapshot for an overflow retry
+// (positions, fixed point, velocities; forces are recomputed from the
+// restored positions) and the reset of the overflow flags, captured with its
+// steps so that a window is one submission.
+void Batch::enqueue_prologue() {
+  const size_t n = static_cast<size_t>(n_);
+  cudaStream_t s = stream_;
+  TDMD_CU(cudaMemcpyAsync(snap_pos4_.data(), pos4_.data(), n * sizeof(double4),
+                          cudaMemcpyDeviceToDevice, s));
+  TDMD_CU(cudaMemcpyAsync(snap_vel_.data(), vel_.data(), 3 * n * sizeof(double),
+                          cudaMemcpyDeviceToDevice, s));
+  if (mixed_)
+    TDMD_CU(cudaMemcpyAsync(snap_q_.data(), q_.data(), n * sizeof(int4),
+                            cudaMemcpyDeviceToDevice, s));
+  TDMD_CU(cudaMemsetAsync(status_.data(), 0, sizeof(int) * 4, s));
+}
+
+void Batch::run_segment(const std::vector<BatchStep>& seg, bool finalize, bool prologue) {
   std::vector<int> key;
-  key.reserve(seg.size() + 1);
+  key.reserve(seg.size() + 2);
   for (const auto& st : seg)
     key.push_back((st.first ? 1 : 0) | (st.rebuild ? 2 : 0) | (st.kd_fused ? 4 : 0) |
                   (st.fuse_next ? 8 : 0) | (st.log_e ? 16 : 0));
   key.push_back(finalize ? 1 : 0);
+  key.push_back(prologue ? 1 : 0);
   const long long l0 = launches_;
   // the window's closing half kick, then (logged windows) the per-replica
   // energies of the integer-time state
@@ -687,6 +706,7 @@ void Batch::run_segment(const std::vector<BatchStep>& seg, bool finalize) {
     if (!seg.empty() && seg.back().log_e) rep_energy();
   };
   if (!cfg_.use_graphs) {
+    if (prologue) enqueue_prologue();
     for (const auto& st : seg) enqueue_step(st);
     close();
     return;
@@ -704,6 +724,7 @@ void Batch::run_segment(const std::vector<BatchStep>& seg, bool finalize) {
     cudaGraph_t g = nullptr;
     TDMD_CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     try {
+      if (prologue) enqueue_prologue();
       for (const auto& st : seg) enqueue_step(st);
       close();
     } catch (...) {
@@ -827,22 +848,12 @@ void Batch::run_until(int target) {
   const size_t n = static_cast<size_t>(n_);
   cudaStream_t s = stream_;
   const int step0 = step_, since0 = since_rebuild_;
+  // snapshot buffers sized outside any stream capture
+  snap_pos4_.reserve(n);
+  snap_vel_.reserve(3 * n);
+  if (mixed_) snap_q_.reserve(n);
   for (int attempt = 0;; ++attempt) {
     TDMD_CU(cudaEventRecord(win_ev_[0], s));
-    // Snapshot for an overflow retry (positions, fixed point, velocities;
-    // forces are recomputed from the restored positions).
-    snap_pos4_.reserve(n);
-    snap_vel_.reserve(3 * n);
-    TDMD_CU(cudaMemcpyAsync(snap_pos4_.data(), pos4_.data(), n * sizeof(double4),
-                            cudaMemcpyDeviceToDevice, s));
-    TDMD_CU(cudaMemcpyAsync(snap_vel_.data(), vel_.data(), 3 * n * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-    if (mixed_) {
-      snap_q_.reserve(n);
-      TDMD_CU(cudaMemcpyAsync(snap_q_.data(), q_.data(), n * sizeof(int4),
-                              cudaMemcpyDeviceToDevice, s));
-    }
-    TDMD_CU(cudaMemsetAsync(status_.data(), 0, sizeof(int) * 4, s));
     std::vector<BatchStep> plan;
     int since = since_rebuild_;
     // energy log of windows whose last step is a multiple of energy_every
@@ -869,7 +880,7 @@ void Batch::run_until(int target) {
       while (b < plan.size() && !plan[b].rebuild && b - a < 64) ++b;
       run_segment(std::vector<BatchStep>(plan.begin() + static_cast<long>(a),
                                          plan.begin() + static_cast<long>(b)),
-                  b == plan.size());
+                  b == plan.size(), a == 0);
       a = b;
     }
     ticks_ += static_cast<long long>(plan.size());

@@ -134,9 +134,14 @@ class Scheduler {
   void enqueue_apply_scale();
   void enqueue_step(const StepPlan& st);
   void enqueue_finalize();
-  void run_segment(const std::vector<StepPlan>& seg, bool finalize);
+  // prologue bits of a window's first segment (captured with its steps)
+  static constexpr int kPrologueSnapshot = 1;     // state copy for an overflow retry
+  static constexpr int kPrologueResetStatus = 2;  // zero the overflow flags
+  void run_segment(const std::vector<StepPlan>& seg, bool finalize, int prologue);
+  void enqueue_prologue(int prologue);
   std::vector<StepPlan> plan_steps(int target, int* since_out) const;
-  void snapshot();
+  void reserve_snapshot();
+  void enqueue_snapshot();
   void restore();
   void clear_graphs();
   void prof_begin(int cat);
@@ -220,8 +225,7 @@ class Scheduler {
   // Snapshot for the overflow retry.
   DevArray<double4> snap_pos4_;
   DevArray<int4> snap_q_;
-  DevArray<double> snap_vel_, snap_f64_;
-  DevArray<float> snap_f32_;
+  DevArray<double> snap_vel_;
 
   cudaStream_t stream_ = nullptr;
   std::map<std::vector<int>, GraphEntry> graphs_;

@@ -955,15 +955,17 @@ void Scheduler::clear_graphs() {
   graph_lru_.clear();
 }
 
-void Scheduler::run_segment(const std::vector<StepPlan>& seg, bool finalize) {
+void Scheduler::run_segment(const std::vector<StepPlan>& seg, bool finalize, int prologue) {
   std::vector<int> key;
-  key.reserve(seg.size() + 1);
+  key.reserve(seg.size() + 2);
   for (const auto& st : seg)
     key.push_back((st.first ? 1 : 0) | (st.rebuild ? 2 : 0) | (st.ev ? 4 : 0) | (st.last ? 8 : 0) |
                   (st.kd_fused ? 16 : 0) | (st.fuse_next ? 32 : 0));
   key.push_back(finalize ? 1 : 0);
+  key.push_back(prologue);
   const long long l0 = launches_;
   if (!cfg_.use_graphs || profiling_) {
+    enqueue_prologue(prologue);
     for (const auto& st : seg) enqueue_step(st);
     if (finalize) enqueue_finalize();
     return;
@@ -981,6 +983,7 @@ void Scheduler::run_segment(const std::vector<StepPlan>& seg, bool finalize) {
     cudaGraph_t g = nullptr;
     TDMD_CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     try {
+      enqueue_prologue(prologue);
       for (const auto& st : seg) enqueue_step(st);
       if (finalize) enqueue_finalize();
     } catch (...) {
@@ -1072,28 +1075,34 @@ void Scheduler::initial_forces(bool defer_check) {
   profiling_ = prof;
 }
 
-void Scheduler::snapshot() {
-  cudaStream_t s = stream_;
+// State a window may have to rewind to (neighbor capacity overflow):
+// positions, their fixed-point records, velocities and the control block.
+// The forces are not kept: a retry recomputes them from the restored
+// positions.  Sized outside any stream capture (allocation is not capturable).
+void Scheduler::reserve_snapshot() {
   const size_t n = static_cast<size_t>(n_);
   snap_pos4_.reserve(n);
   snap_vel_.reserve(3 * n);
+  if (mixed_) snap_q_.reserve(n);
+}
+
+void Scheduler::enqueue_snapshot() {
+  cudaStream_t s = stream_;
+  const size_t n = static_cast<size_t>(n_);
   TDMD_CU(cudaMemcpyAsync(snap_pos4_.data(), pos4_.data(), n * sizeof(double4),
                           cudaMemcpyDeviceToDevice, s));
   TDMD_CU(cudaMemcpyAsync(snap_vel_.data(), vel_.data(), 3 * n * sizeof(double),
                           cudaMemcpyDeviceToDevice, s));
-  if (mixed_) {
-    snap_q_.reserve(n);
-    snap_f32_.reserve(3 * n);
+  if (mixed_)
     TDMD_CU(cudaMemcpyAsync(snap_q_.data(), q_.data(), n * sizeof(int4), cudaMemcpyDeviceToDevice, s));
-    TDMD_CU(cudaMemcpyAsync(snap_f32_.data(), f32_.data(), 3 * n * sizeof(float),
-                            cudaMemcpyDeviceToDevice, s));
-  } else {
-    snap_f64_.reserve(3 * n);
-    TDMD_CU(cudaMemcpyAsync(snap_f64_.data(), f64_.data(), 3 * n * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-  }
   TDMD_CU(cudaMemcpyAsync(snap_ctl_.data(), ctl_.data(), sizeof(SchedCtl),
                           cudaMemcpyDeviceToDevice, s));
+}
+
+void Scheduler::enqueue_prologue(int prologue) {
+  if (prologue & kPrologueSnapshot) enqueue_snapshot();
+  if (prologue & kPrologueResetStatus)
+    TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, stream_));
 }
 
 void Scheduler::restore() {
@@ -1103,14 +1112,8 @@ void Scheduler::restore() {
                           cudaMemcpyDeviceToDevice, s));
   TDMD_CU(cudaMemcpyAsync(vel_.data(), snap_vel_.data(), 3 * n * sizeof(double),
                           cudaMemcpyDeviceToDevice, s));
-  if (mixed_) {
+  if (mixed_)
     TDMD_CU(cudaMemcpyAsync(q_.data(), snap_q_.data(), n * sizeof(int4), cudaMemcpyDeviceToDevice, s));
-    TDMD_CU(cudaMemcpyAsync(f32_.data(), snap_f32_.data(), 3 * n * sizeof(float),
-                            cudaMemcpyDeviceToDevice, s));
-  } else {
-    TDMD_CU(cudaMemcpyAsync(f64_.data(), snap_f64_.data(), 3 * n * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-  }
   TDMD_CU(cudaMemcpyAsync(ctl_.data(), snap_ctl_.data(), sizeof(SchedCtl),
                           cudaMemcpyDeviceToDevice, s));
 }
@@ -1132,12 +1135,14 @@ void Scheduler::run_until(int target) {
     return;
   }
   const int step0 = step_, since0 = since_rebuild_;
+  reserve_snapshot();
   for (int attempt = 0;; ++attempt) {
     TDMD_CU(cudaEventRecord(win_ev_[0], stream_));
-    snapshot();
-    // a pending first-list overflow flag stays set for this window's check
-    if (attempt > 0 || !init_check_pending_)
-      TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, stream_));
+    // The snapshot and the flag reset go into the first segment's graph: one
+    // submission per window.  A pending first-list overflow flag stays set
+    // for this window's check.
+    const int prologue = kPrologueSnapshot |
+                         ((attempt > 0 || !init_check_pending_) ? kPrologueResetStatus : 0);
     int since_end = 0;
     const std::vector<StepPlan> plan = plan_steps(target, &since_end);
     // Segments start at each rebuild step; at most 64 steps each.
@@ -1147,7 +1152,7 @@ void Scheduler::run_until(int target) {
       while (b < plan.size() && !plan[b].rebuild && b - a < 64) ++b;
       const std::vector<StepPlan> seg(plan.begin() + static_cast<long>(a),
                                       plan.begin() + static_cast<long>(b));
-      run_segment(seg, b == plan.size());
+      run_segment(seg, b == plan.size(), a == 0 ? prologue : 0);
       a = b;
     }
     ticks_ += static_cast<long long>(plan.size());
