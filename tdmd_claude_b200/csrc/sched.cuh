@@ -141,7 +141,6 @@ class Scheduler {
   void enqueue_prologue(int prologue);
   std::vector<StepPlan> plan_steps(int target, int* since_out) const;
   void reserve_snapshot();
-  void enqueue_snapshot();
   void restore();
   void clear_graphs();
   void prof_begin(int cat);

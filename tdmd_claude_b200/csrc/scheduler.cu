@@ -131,6 +131,33 @@ __global__ void k_scatter_positions(const double4* __restrict__ pos4, const int*
   x[3 * k + 2] = p.z;
 }
 
+// A window's prologue in one launch: the state an overflow retry rewinds to
+// (positions, fixed-point records when q is non-null, velocities, the
+// control block) copied aside, then -- with reset -- the overflow flags of
+// the live control block zeroed (after the copy, by the same thread).
+__global__ void __launch_bounds__(kThreads) k_window_prologue(
+    const double4* __restrict__ pos4, double4* __restrict__ snap_pos4,
+    const int4* __restrict__ q, int4* __restrict__ snap_q, const double* __restrict__ vel,
+    double* __restrict__ snap_vel, int n, SchedCtl* __restrict__ ctl,
+    SchedCtl* __restrict__ snap_ctl, int reset) {
+  dependent_launch_prologue();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    snap_pos4[i] = pos4[i];
+    if (q) snap_q[i] = q[i];
+    const long long k = 3ll * i;
+    snap_vel[k] = vel[k];
+    snap_vel[k + 1] = vel[k + 1];
+    snap_vel[k + 2] = vel[k + 2];
+  }
+  if (i == 0) {
+    *snap_ctl = *ctl;
+    if (reset) {
+      for (int c = 0; c < 4; ++c) ctl->status[c] = 0;
+    }
+  }
+}
+
 // Kick (half or full dt, optionally after the pending NHC scale) + drift +
 // single-image wrap + fixed-point refresh.  fused_kick_drift_kernel,
 // device_velocity_verlet.cu:88-130.  dt comes from the control block when
@@ -1086,23 +1113,17 @@ void Scheduler::reserve_snapshot() {
   if (mixed_) snap_q_.reserve(n);
 }
 
-void Scheduler::enqueue_snapshot() {
-  cudaStream_t s = stream_;
-  const size_t n = static_cast<size_t>(n_);
-  TDMD_CU(cudaMemcpyAsync(snap_pos4_.data(), pos4_.data(), n * sizeof(double4),
-                          cudaMemcpyDeviceToDevice, s));
-  TDMD_CU(cudaMemcpyAsync(snap_vel_.data(), vel_.data(), 3 * n * sizeof(double),
-                          cudaMemcpyDeviceToDevice, s));
-  if (mixed_)
-    TDMD_CU(cudaMemcpyAsync(snap_q_.data(), q_.data(), n * sizeof(int4), cudaMemcpyDeviceToDevice, s));
-  TDMD_CU(cudaMemcpyAsync(snap_ctl_.data(), ctl_.data(), sizeof(SchedCtl),
-                          cudaMemcpyDeviceToDevice, s));
-}
-
 void Scheduler::enqueue_prologue(int prologue) {
-  if (prologue & kPrologueSnapshot) enqueue_snapshot();
-  if (prologue & kPrologueResetStatus)
+  if (prologue & kPrologueSnapshot) {
+    launch(k_window_prologue, ceil_div(n_, kThreads), kThreads, 0, stream_, pos4_.data(),
+           snap_pos4_.data(), mixed_ ? q_.data() : nullptr, mixed_ ? snap_q_.data() : nullptr,
+           vel_.data(), snap_vel_.data(), n_, ctl_.data(), snap_ctl_.data(),
+           (prologue & kPrologueResetStatus) ? 1 : 0);
+    TDMD_LAUNCH_CHECK();
+    launches_ += 1;
+  } else if (prologue & kPrologueResetStatus) {
     TDMD_CU(cudaMemsetAsync(ctl_status(), 0, sizeof(int) * 4, stream_));
+  }
 }
 
 void Scheduler::restore() {

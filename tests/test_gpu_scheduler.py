@@ -225,15 +225,16 @@ def test_adaptive_dt_matches_oracle(cuda, oracle):
 
 
 def test_kernel_launch_accounting(cuda):
-    """Morse NVE, one window without rebuild: 1 (initial force) + 2 per step
-    + 1 closing half kick, plus the initial list build: 3 kernels (the
-    upload already binned the atoms into the cell order, so the cell list
-    is an identity fill; then the row-sizing count pass and the fill)."""
+    """Morse NVE, one window without rebuild: 1 (initial force) + 1 window
+    prologue (the state copy an overflow retry rewinds to) + 2 per step + 1
+    closing half kick, plus the initial list build: 3 kernels (the upload
+    already binned the atoms into the cell order, so the cell list is an
+    identity fill; then the row-sizing count pass and the fill)."""
     pos, vel, masses, lo, hi, morse, skin = _c0()
     s = _sched_morse(pos, vel, masses, lo, hi, morse, skin, use_graphs=False)
     s.run_until(5)
     st = s.stats()
-    assert st.kernel_launches == 3 + 1 + 2 * 5 + 1
+    assert st.kernel_launches == 3 + 1 + 1 + 2 * 5 + 1
     assert st.ticks == 5 and st.rebuilds == 1
 
 
