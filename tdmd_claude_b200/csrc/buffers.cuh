@@ -71,10 +71,10 @@ struct CellListDev {
   long long natoms = 0;
 };
 
-// Exclusive scan of in[0..n) into out[0..n); *total (device, nullable) gets
-// the sum.  Multi-block, fixed order.
+// Exclusive scan of in[0..n) into out[0..n) (and out2, when non-null);
+// *total (device, nullable) gets the sum.  Fixed order.
 void device_exclusive_scan(const int* in, int* out, long long n, int* total, DevArray<int>& tmp,
-                           cudaStream_t stream);
+                           cudaStream_t stream, int* out2 = nullptr);
 // Kernels one device_exclusive_scan of n items launches (1 or 3).
 int device_scan_launches(long long n);
 

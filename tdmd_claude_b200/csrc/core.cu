@@ -165,7 +165,8 @@ __global__ void k_scan_single(const int* __restrict__ in, int* __restrict__ out,
 // warps_before(k, t) + lanes_before(k, t).  out may alias in.
 constexpr int kScanWide = 16;
 __global__ void __launch_bounds__(kScanThreads) k_scan_wide(const int* __restrict__ in,
-                                                            int* __restrict__ out, int n,
+                                                            int* __restrict__ out,
+                                                            int* __restrict__ out2, int n,
                                                             int* __restrict__ total_out) {
   dependent_launch_prologue();
   __shared__ int wsum[kScanWide][kScanThreads / 32];  // row k: per-warp totals -> prefixes
@@ -217,7 +218,11 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_wide(const int* __restric
 #pragma unroll
   for (int k = 0; k < kScanWide; ++k) {
     const int i = k * kScanThreads + t;
-    if (i < n) out[i] = rsum[k] + wsum[k][warp] + incl[k] - v[k];
+    if (i < n) {
+      const int e = rsum[k] + wsum[k][warp] + incl[k] - v[k];
+      out[i] = e;
+      if (out2) out2[i] = e;
+    }
   }
   if (t == 0 && total_out) *total_out = rsum[kScanWide];
 }
@@ -253,15 +258,20 @@ int device_scan_launches(long long n) {
 }
 
 void device_exclusive_scan(const int* in, int* out, long long n, int* total, DevArray<int>& tmp,
-                           cudaStream_t stream) {
+                           cudaStream_t stream, int* out2) {
   if (n <= 0) {
     if (total) TDMD_CU(cudaMemsetAsync(total, 0, sizeof(int), stream));
     return;
   }
   const long long nblocks = (n + kScanTile - 1) / kScanTile;
   if (n <= static_cast<long long>(kScanThreads) * kScanWide) {
-    launch(k_scan_wide, 1, kScanThreads, 0, stream, in, out, static_cast<int>(n), total);
+    launch(k_scan_wide, 1, kScanThreads, 0, stream, in, out, out2, static_cast<int>(n), total);
     TDMD_LAUNCH_CHECK();
+    return;
+  }
+  if (out2) {  // the tiled scans write one output; copy it after them
+    device_exclusive_scan(in, out, n, total, tmp, stream, nullptr);
+    TDMD_CU(cudaMemcpyAsync(out2, out, sizeof(int) * n, cudaMemcpyDeviceToDevice, stream));
     return;
   }
   // Up to kScanSingleTiles tiles one block walking the tiles beats three

@@ -612,10 +612,9 @@ void build_cell_list(CellListDev& cl, const void* d_pos, PosLayout layout, long 
     launch(k_bin_atoms<LoadD4>, nb, 256, 0, stream, LoadD4{static_cast<const double4*>(d_pos)},
            static_cast<int>(n), box, cl.atom_cell.data(), cl.cell_count.data());
   TDMD_LAUNCH_CHECK();
+  // the scatter's cursors start as a copy of the cell starts
   device_exclusive_scan(cl.cell_count.data(), cl.cell_start.data(), ncells, nullptr, cl.scan_tmp,
-                        stream);
-  TDMD_CU(cudaMemcpyAsync(cl.cursor.data(), cl.cell_start.data(), sizeof(int) * ncells,
-                          cudaMemcpyDeviceToDevice, stream));
+                        stream, cl.cursor.data());
   launch(k_scatter_atoms, nb, 256, 0, stream, cl.atom_cell.data(), static_cast<int>(n),
          cl.cursor.data(), cl.cell_atoms.data());
   TDMD_LAUNCH_CHECK();
@@ -658,9 +657,7 @@ void build_cell_list_batch(CellListDev& cl, const double4* pos, const int* rep,
          cl.atom_cell.data(), cl.cell_count.data());
   TDMD_LAUNCH_CHECK();
   device_exclusive_scan(cl.cell_count.data(), cl.cell_start.data(), ncells_total, nullptr,
-                        cl.scan_tmp, stream);
-  TDMD_CU(cudaMemcpyAsync(cl.cursor.data(), cl.cell_start.data(), sizeof(int) * ncells_total,
-                          cudaMemcpyDeviceToDevice, stream));
+                        cl.scan_tmp, stream, cl.cursor.data());
   launch(k_scatter_atoms, nb, 256, 0, stream, cl.atom_cell.data(), static_cast<int>(n),
          cl.cursor.data(), cl.cell_atoms.data());
   TDMD_LAUNCH_CHECK();
