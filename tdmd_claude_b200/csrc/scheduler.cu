@@ -72,14 +72,6 @@ struct F3 {
   float x, y, z;
 };
 
-// dst[i] = src[idx[i]]
-template <class T>
-__global__ void k_gather(const T* __restrict__ src, const int* __restrict__ idx, int n,
-                         T* __restrict__ dst) {
-  dependent_launch_prologue();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) dst[i] = src[idx[i]];
-}
 
 // The whole per-atom state into the cell order in one pass: dst[i] =
 // src[idx[i]] for positions, velocities, types, ids, fixed-point records
