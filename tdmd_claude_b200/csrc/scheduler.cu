@@ -72,7 +72,6 @@ struct F3 {
   float x, y, z;
 };
 
-
 // The whole per-atom state into the cell order in one pass: dst[i] =
 // src[idx[i]] for positions, velocities, types, ids, fixed-point records
 // (nullable) and forces.
