@@ -613,3 +613,32 @@ def test_arbitrary_atom_order(cuda, oracle, precision):
     L = np.array(sysm.hi) - np.array(sysm.lo)
     tol = 1e-10 if precision == "fp64" else 5e-4
     assert np.abs(_wrap_diff(st.positions, r["pos"], L)).max() < tol
+
+
+def test_launches_without_programmatic_dependent_launch_agree(cuda, tmp_path):
+    """TDMD_PDL=0 (read at the library's first launch) turns off the
+    programmatic-serialization attribute: a mixed EAM run in a process with
+    it off gives the same bits as one with it on."""
+    import os
+    import subprocess
+    import sys
+    script = tmp_path / "run.py"
+    script.write_text(
+        "import sys, numpy as np\n"
+        f"sys.path.insert(0, {os.path.dirname(os.path.abspath(__file__))!r})\n"
+        f"sys.path.insert(0, {os.path.dirname(os.path.dirname(os.path.abspath(__file__)))!r})\n"
+        "from test_gpu_scheduler import _eam_setup\n"
+        "s, _, _ = _eam_setup('mixed', ncell=5)\n"
+        "s.run_until(37)\n"
+        "st = s.download()\n"
+        "np.save(sys.argv[1], np.concatenate([st.positions.ravel(), st.velocities.ravel(),\n"
+        "                                     st.forces.astype(np.float64).ravel()]))\n")
+    out = {}
+    for flag in ("0", "1"):
+        path = str(tmp_path / f"pdl{flag}.npy")
+        env = dict(os.environ, TDMD_PDL=flag)
+        r = subprocess.run([sys.executable, str(script), path], capture_output=True, text=True,
+                           timeout=600, env=env)
+        assert r.returncode == 0, r.stderr
+        out[flag] = np.load(path)
+    assert np.array_equal(out["0"], out["1"])
