@@ -37,7 +37,9 @@
 namespace tdmd_b200 {
 namespace {
 
-constexpr int kMaxBlocks = 16384;
+// Force blocks at the atom limit with the default 8 lanes per atom.
+constexpr int kMaxBlocks =
+    static_cast<int>(static_cast<long long>(TDMD_MORSE_NOALLOC_MAX_ATOMS) * 8 / kForceThreads);
 constexpr int kMaxDevices = 64;
 
 // One lane per atom fits at the atom limit, so halving the lanes always
