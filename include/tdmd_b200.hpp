@@ -25,9 +25,13 @@
 
 #include <cuda_runtime_api.h>
 
+#include <algorithm>
 #include <array>
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <limits>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -42,6 +46,7 @@
 #include "core/error.hpp"
 #include "core/system_state.hpp"
 #include "core/types.hpp"
+#include "domain/zone_partition.hpp"
 #include "potentials/eam_alloy.hpp"
 #endif
 
@@ -889,6 +894,196 @@ class FastPipelineScheduler {
   i32 step_ = 0;
   PotentialKind kind_ = PotentialKind::Morse;
   real cutoff_ = 0;
+};
+
+}  // namespace scheduler
+
+#if !defined(TDMD_B200_REFERENCE_CORE)
+// --- src/scheduler/zone.hpp, src/domain/zone_partition.hpp (single rank) ----
+namespace scheduler {
+enum class ZoneState : std::uint8_t {
+  Free = 0,
+  Receiving = 1,
+  Received = 2,
+  Ready = 3,
+  Computing = 4,
+  Done = 5,
+  Sending = 6,
+};
+
+struct Zone {
+  i32 id{-1};
+  std::array<i32, 3> lattice_index{0, 0, 0};
+  Aabb bbox{};
+  i32 atom_offset{0};
+  i32 natoms_in_zone{0};
+  i32 time_step{0};
+  ZoneState state{ZoneState::Free};
+  i32 owner_rank{-1};
+};
+}  // namespace scheduler
+
+namespace domain {
+// Slabs of the box along x (zone_partition.cpp:12-40): n zones of width
+// L_x / n, n = max(3, floor(L_x / r_cut)) unless given; a zone's neighbors
+// are the zones within r_list of it, periodic in x.
+class ZonePartition {
+ public:
+  void build(const Box& box, real r_cut, i32 n_zones = 0) {
+    const Vec3D size = box.size();
+    lo_x_ = box.lo.x;
+    if (n_zones <= 0) n_zones = std::max(3, static_cast<i32>(std::floor(size.x / r_cut)));
+    if (n_zones < 3) throw StatusError(TDMD_ERR_INVALID_ARGUMENT, "need at least 3 zones");
+    width_ = size.x / n_zones;
+    zones_.assign(static_cast<size_t>(n_zones), scheduler::Zone{});
+    for (i32 i = 0; i < n_zones; ++i) {
+      scheduler::Zone& z = zones_[static_cast<size_t>(i)];
+      z.id = i;
+      z.lattice_index = {i, 0, 0};
+      z.bbox.lo = Vec3D{box.lo.x + i * width_, box.lo.y, box.lo.z};
+      z.bbox.hi = Vec3D{box.lo.x + (i + 1) * width_, box.hi.y, box.hi.z};
+      z.owner_rank = 0;
+    }
+    neighbors_.assign(static_cast<size_t>(n_zones), {});
+  }
+  void build_zone_neighbors(real r_list) {
+    const i32 n = n_zones();
+    const i32 reach = std::min(n / 2, static_cast<i32>(std::ceil(r_list / width_)));
+    for (i32 i = 0; i < n; ++i) {
+      std::vector<i32>& nb = neighbors_[static_cast<size_t>(i)];
+      nb.clear();
+      for (i32 d = -reach; d <= reach; ++d) {
+        const i32 j = ((i + d) % n + n) % n;
+        if (std::find(nb.begin(), nb.end(), j) == nb.end()) nb.push_back(j);
+      }
+      std::sort(nb.begin(), nb.end());
+    }
+  }
+  i32 n_zones() const noexcept { return static_cast<i32>(zones_.size()); }
+  const std::vector<scheduler::Zone>& zones() const noexcept { return zones_; }
+  std::vector<scheduler::Zone>& zones() noexcept { return zones_; }
+  i32 zone_of(real x) const noexcept {
+    i32 z = static_cast<i32>((x - lo_x_) / width_);
+    return z < 0 ? 0 : (z >= n_zones() ? n_zones() - 1 : z);
+  }
+  const std::vector<i32>& zone_neighbors(i32 z) const {
+    return neighbors_[static_cast<size_t>(z)];
+  }
+
+ private:
+  double lo_x_ = 0.0;
+  double width_ = 1.0;
+  std::vector<scheduler::Zone> zones_;
+  std::vector<std::vector<i32>> neighbors_;
+};
+}  // namespace domain
+#endif  // !TDMD_B200_REFERENCE_CORE
+
+namespace scheduler {
+
+// --- src/scheduler/pipeline_scheduler.cuh:18-44 -----------------------------
+struct PipelineConfig {
+  real dt{real{0.001}};
+  real r_skin{real{1.0}};
+  i32 n_zones{0};      // 0: max(3, floor(L_x / rc))
+  i32 n_streams{4};    // accepted; one stream here
+  i32 rebuild_every{10};
+  bool deterministic{false};  // accepted; every run here is deterministic
+  real t_target{0};    // > 0: NVT (Nose-Hoover chain)
+  real t_period{real{0.1}};
+  i32 nhc_length{3};
+  bool adaptive_dt{false};
+  real dt_max{real{0.002}};
+  real dt_min{real{0.0001}};
+  real c2{real{0.05}};
+};
+
+struct PipelineStats {
+  i64 kernel_launches{0};
+  i64 dep_check_calls{0};
+  i64 dep_check_failures{0};
+  i64 ticks{0};
+};
+
+// The reference's TD zone pipeline (pipeline_scheduler.cu:93-290) with its
+// API and physics -- one velocity-Verlet step per zone step, NVT as the
+// NHC half step around each step, adaptive dt from v_max -- run as whole-
+// system windows on the library's scheduler: on one GPU the zones gain
+// nothing from being stepped apart (the reference's own deterministic mode
+// equals the plain sequential loop), so all zones advance together.  The
+// partition is built as the reference builds it and reported (zone time
+// steps follow the run); no zone waits on another, so no dependency checks
+// are counted.
+class PipelineScheduler {
+ public:
+  PipelineScheduler(const Box& box, i32 natoms, const potentials::MorseParams& params,
+                    const PipelineConfig& cfg) {
+    partition_.build(box, params.rc, cfg.n_zones);
+    partition_.build_zone_neighbors(params.rc + cfg.r_skin);
+    FastPipelineConfig f{};
+    f.dt = cfg.dt;
+    f.r_skin = cfg.r_skin;
+    f.rebuild_every = cfg.rebuild_every;
+    f.t_target = cfg.t_target;
+    f.t_period = cfg.t_period;
+    f.nhc_length = cfg.nhc_length;
+    f.adaptive_dt = cfg.adaptive_dt;
+    f.dt_min = cfg.dt_min;
+    f.dt_max = cfg.dt_max;
+    f.c2 = cfg.c2;
+    sched_ = std::make_unique<FastPipelineScheduler>(box, natoms, params, f);
+    natoms_ = natoms;
+  }
+
+  void upload(const PositionVec* positions, const VelocityVec* velocities, const ForceVec* forces,
+              const i32* types, const i32* ids, const real* masses, i32 n_masses) {
+    sched_->upload(positions, velocities, forces, types, ids, masses, n_masses);
+    // zone populations as the reference's assign_atoms groups them
+    const i32 nz = partition_.n_zones();
+    std::vector<i32> count(static_cast<size_t>(nz), 0);
+    for (i32 i = 0; i < natoms_; ++i)
+      ++count[static_cast<size_t>(
+          partition_.zone_of(static_cast<real>(positions[static_cast<size_t>(i)].x)))];
+    i32 off = 0;
+    for (i32 z = 0; z < nz; ++z) {
+      Zone& zone = partition_.zones()[static_cast<size_t>(z)];
+      zone.atom_offset = off;
+      zone.natoms_in_zone = count[static_cast<size_t>(z)];
+      off += zone.natoms_in_zone;
+    }
+    set_zones(0);
+  }
+  void run_until(i32 target_step) {
+    sched_->run_until(target_step);
+    set_zones(sched_->current_step());
+    const FastPipelineStats& f = sched_->stats();
+    stats_.kernel_launches = f.kernel_launches;
+    stats_.ticks = f.ticks;
+  }
+  void download(PositionVec* positions, VelocityVec* velocities, ForceVec* forces, i32* types,
+                i32* ids, i32 natoms) const {
+    sched_->download(positions, velocities, forces, types, ids, natoms);
+  }
+  const domain::ZonePartition& partition() const noexcept { return partition_; }
+  const PipelineStats& stats() const noexcept { return stats_; }
+  i32 min_time_step() const noexcept {
+    i32 m = std::numeric_limits<i32>::max();
+    for (const Zone& z : partition_.zones()) m = std::min(m, z.time_step);
+    return m;
+  }
+
+ private:
+  void set_zones(i32 step) {
+    for (Zone& z : partition_.zones()) {
+      z.time_step = step;
+      z.state = ZoneState::Ready;
+    }
+  }
+
+  domain::ZonePartition partition_;
+  std::unique_ptr<FastPipelineScheduler> sched_;
+  PipelineStats stats_{};
+  i32 natoms_ = 0;
 };
 
 }  // namespace scheduler

@@ -7,11 +7,11 @@ where the reference tree is present (the binaries in oracle/_ref travel
 with the tree).
 
 The driver reads a LAMMPS data file (tdmd::io::read_lammps_data),
-initialises velocities, builds a FastPipelineScheduler (Morse or EAM),
-runs warm-up and measured run_until windows and prints JSON with the
-scheduler's counters; the test checks that JSON against the same run made
-through this library's Python API: atoms, steps, ticks and kernel launches
-of the measured region."""
+initialises velocities, builds a FastPipelineScheduler (Morse or EAM) or
+its default TD zone PipelineScheduler, runs warm-up and measured run_until
+windows and prints JSON with the scheduler's counters; the test checks that
+JSON against the same run made through this library's Python API: atoms,
+steps, ticks and kernel launches of the measured region."""
 from __future__ import annotations
 
 import json
@@ -76,17 +76,25 @@ def test_reference_driver_runs_unchanged(cuda, tmp_path, mishin_setfl, precision
     assert d["kernel_launches_total"] == launches
 
 
-def test_reference_driver_reports_out_of_scope_scheduler(cuda, tmp_path):
-    """The driver's default TD zone scheduler is not part of this library:
-    the shim's PipelineScheduler throws tdmd::Error, so the driver ends
-    with an uncaught exception instead of running something else."""
+def test_reference_driver_default_zone_scheduler(cuda, tmp_path):
+    """The driver's default scheduler, the TD zone PipelineScheduler, runs
+    on this library's whole-system path: the reference's zone count for the
+    box (max(3, floor(L_x / rc))), the measured steps, no zone dependency
+    checks (all zones step together)."""
     from tdmd_claude_b200 import io as TIO
     from tdmd_claude_b200 import workloads as W
-    sysm = W.fcc_system(4, 3.615, 300.0, seed=3)
-    data = str(tmp_path / "c0.data")
+    sysm = W.fcc_system(10, 3.615, 300.0, seed=3)
+    data = str(tmp_path / "fcc4000.data")
     TIO.write_lammps_data(data, sysm)
-    r = subprocess.run([_exe("fp64"), "--data", data, "--steps", "5", "--warmup", "0"],
-                       capture_output=True, text=True, timeout=120)
-    assert r.returncode != 0
-    assert "not part of this library" in r.stderr
-    _ = np
+    out = str(tmp_path / "bench.json")
+    r = subprocess.run([_exe("fp64"), "--data", data, "--steps", str(STEPS), "--warmup",
+                        str(WARMUP), "--skin", str(SKIN), "--output", out],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    with open(out) as f:
+        d = json.load(f)
+    L = sysm.hi[0] - sysm.lo[0]
+    assert d["n_zones"] == max(3, int(np.floor(L / 6.0)))
+    assert d["n_atoms"] == sysm.n and d["n_steps"] == STEPS
+    assert d["dep_check_calls"] == 0 and d["dep_check_failures"] == 0
+    assert d["timesteps_per_s"] > 0

@@ -17,11 +17,14 @@ Expected outcome, per test: OK, except
   * FastPipelineScheduler.KernelLaunchInvariant, which pins the reference's
     own launch count (1 + 2 per step + 1; this library's FastPipelineScheduler
     counts its cell-list and list-build launches too);
-  * the NVTThermostat / AdaptiveDt tests that drive the TD zone
-    PipelineScheduler (outside this library: its constructor throws
-    TDMD_ERR_UNSUPPORTED);
   * the determinism tests, skipped unless built with the reference's
-    TDMD_DETERMINISTIC_REDUCE switch (mapped here onto the run-time switch).
+    TDMD_DETERMINISTIC_REDUCE switch (mapped here onto the run-time switch);
+  * PipelineScheduler.DeterministicMatchesM3, which the reference itself
+    skips in its mixed build.
+The TD zone PipelineScheduler tests (test_pipeline_scheduler.cu and the
+NVT / adaptive-dt ones) run on the C++ layer's PipelineScheduler, which
+steps all zones together on the whole-system path; the deterministic one
+compares it with the reference's own sequential CPU loop.
 """
 from __future__ import annotations
 
@@ -40,8 +43,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 LAUNCH_INVARIANT = {"FastPipelineScheduler.KernelLaunchInvariant"}
-ZONE_PIPELINE = {"NVTThermostat.TemperatureConvergesToTarget",
-                 "NVTThermostat.DeterministicReproducibility", "AdaptiveDt.StableNVETrajectory"}
+SKIPPED_IN_MIXED = {"PipelineScheduler.DeterministicMatchesM3"}
 DETERMINISM = {"DeviceMorseDeterminism.EnergyBitIdentical",
                "DeviceEamDeterminism.EnergyBitIdentical",
                "DeviceCellListDeterminism.TwoBuildsBitIdentical"}
@@ -77,6 +79,9 @@ CASES = {
                             "AdaptiveDt.DeviceVmaxMatchesHost", "AdaptiveDt.StableNVETrajectory"},
     "test_sum_order_sensitivity": {"SumOrderSensitivity.MorseEnergyBounded",
                                    "SumOrderSensitivity.EamEnergyBounded"},
+    "test_pipeline_scheduler": {"PipelineScheduler.DeterministicMatchesM3",
+                                "PipelineScheduler.PipelineNVEConservation",
+                                "PipelineScheduler.ZoneTimeStepsAdvance"},
 }
 
 LINE = re.compile(r"^\[\s+(OK|FAILED|SKIPPED)\s+\] (\S+)$", re.M)
@@ -120,15 +125,13 @@ def test_reference_unit_tests_run_unchanged(cuda, data_dir, case, precision):
     out, results = _run(f"reftest_{case}_{precision}", data_dir)
     assert set(results) == CASES[case], out.stdout[-3000:]
     for name, status in results.items():
-        if name in LAUNCH_INVARIANT or name in ZONE_PIPELINE:
+        if name in LAUNCH_INVARIANT:
             want = "FAILED"
-        elif name in DETERMINISM:
+        elif name in DETERMINISM or (precision == "mixed" and name in SKIPPED_IN_MIXED):
             want = "SKIPPED"
         else:
             want = "OK"
         assert status == want, f"{name}: {status}\n{out.stdout[-3000:]}"
-    for name in ZONE_PIPELINE & set(results):
-        assert "TD zone PipelineScheduler is not part of this library" in out.stdout
 
 
 @pytest.mark.parametrize("case", ["test_device_morse", "test_device_eam", "test_device_cell_list"])
