@@ -911,6 +911,21 @@ enum class ZoneState : std::uint8_t {
   Sending = 6,
 };
 
+// The zone life cycle (zone.hpp:22-40): Free -> Receiving -> Received ->
+// Ready -> Computing -> Done -> Sending -> Free.
+constexpr bool is_legal_transition(ZoneState from, ZoneState to) noexcept {
+  switch (from) {
+    case ZoneState::Free: return to == ZoneState::Receiving;
+    case ZoneState::Receiving: return to == ZoneState::Received;
+    case ZoneState::Received: return to == ZoneState::Ready;
+    case ZoneState::Ready: return to == ZoneState::Computing;
+    case ZoneState::Computing: return to == ZoneState::Done;
+    case ZoneState::Done: return to == ZoneState::Sending;
+    case ZoneState::Sending: return to == ZoneState::Free;
+  }
+  return false;
+}
+
 struct Zone {
   i32 id{-1};
   std::array<i32, 3> lattice_index{0, 0, 0};
@@ -920,6 +935,15 @@ struct Zone {
   i32 time_step{0};
   ZoneState state{ZoneState::Free};
   i32 owner_rank{-1};
+
+  // A step of the life cycle; reaching Done completes a time step.  An
+  // illegal one throws (the reference asserts).
+  void transition_to(ZoneState next) {
+    if (!is_legal_transition(state, next))
+      throw StatusError(TDMD_ERR_STATE, "illegal zone transition");
+    state = next;
+    if (next == ZoneState::Done) ++time_step;
+  }
 };
 }  // namespace scheduler
 
@@ -969,8 +993,39 @@ class ZonePartition {
   const std::vector<i32>& zone_neighbors(i32 z) const {
     return neighbors_[static_cast<size_t>(z)];
   }
+  // Groups the host arrays by zone, in input order within a zone (a
+  // counting sort on x), and records each zone's offset and count.
+  void assign_atoms(PositionVec* positions, VelocityVec* velocities, ForceVec* forces, i32* types,
+                    i32* ids, i64 natoms) {
+    const size_t n = static_cast<size_t>(natoms), nz = static_cast<size_t>(n_zones());
+    std::vector<i32> zone(n), count(nz, 0), offset(nz, 0), perm(n);
+    for (size_t i = 0; i < n; ++i) {
+      zone[i] = zone_of(static_cast<real>(positions[i].x));
+      ++count[static_cast<size_t>(zone[i])];
+    }
+    for (size_t z = 1; z < nz; ++z) offset[z] = offset[z - 1] + count[z - 1];
+    std::vector<i32> next(offset);
+    for (size_t i = 0; i < n; ++i)
+      perm[static_cast<size_t>(next[static_cast<size_t>(zone[i])]++)] = static_cast<i32>(i);
+    permute(positions, perm);
+    permute(velocities, perm);
+    permute(forces, perm);
+    permute(types, perm);
+    permute(ids, perm);
+    for (size_t z = 0; z < nz; ++z) {
+      zones_[z].atom_offset = offset[z];
+      zones_[z].natoms_in_zone = count[z];
+    }
+  }
 
  private:
+  template <class T>
+  static void permute(T* a, const std::vector<i32>& perm) {
+    std::vector<T> tmp(perm.size());
+    for (size_t i = 0; i < perm.size(); ++i) tmp[i] = a[static_cast<size_t>(perm[i])];
+    std::copy(tmp.begin(), tmp.end(), a);
+  }
+
   double lo_x_ = 0.0;
   double width_ = 1.0;
   std::vector<scheduler::Zone> zones_;

@@ -452,3 +452,35 @@ def test_reference_data_reader_unit_test(L):
     assert out.returncode == 0, out.stdout + out.stderr
     assert "[       OK ] LammpsDataReader.Basic4Atoms" in out.stdout
     assert "[       OK ] LammpsDataReader.FileNotFound" in out.stdout
+
+
+@pytest.mark.parametrize("name,tests", [
+    ("test_zone_partition", ("ZonePartition.EveryAtomInExactlyOneZone",
+                             "ZonePartition.AtomsInCorrectZone", "ZonePartition.ZoneNeighbors")),
+    ("test_zone_state_machine", ("ZoneStateMachine.LegalTransitions",
+                                 "ZoneStateMachine.IllegalTransitions",
+                                 "ZoneStateMachine.TimeStepMonotonicity")),
+])
+def test_reference_zone_unit_tests(L, tmp_path, name, tests):
+    """The reference's zone tests (tests/unit/test_zone_partition.cpp,
+    test_zone_state_machine.cpp) compiled unchanged against the C++ layer's
+    own single-rank zone types (`make -C oracle reftests`), on the
+    reference's 256-atom data file (from the run0_morse_256.json fixture)."""
+    import subprocess
+    from tdmd_claude_b200 import io as TIO
+    from tdmd_claude_b200 import workloads as W
+    exe = os.path.join(ROOT, "oracle", "_ref", f"reftest_{name}_own")
+    if not os.path.exists(exe):
+        pytest.skip("reference unit tests not built (make -C oracle reftests)")
+    g = golden("run0_morse_256.json")
+    pos = np.array(g["positions"])
+    n = len(pos)
+    TIO.write_lammps_data(str(tmp_path / "cu_fcc_256.data"),
+                          W.System(pos, np.zeros_like(pos), np.ones(n, np.int32),
+                                   np.arange(1, n + 1, dtype=np.int32), np.array(g["masses"]),
+                                   tuple(g["lo"]), tuple(g["hi"])))
+    env = dict(os.environ, TDMD_TEST_DATA_DIR=str(tmp_path))
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=120, env=env)
+    assert out.returncode == 0, out.stdout + out.stderr
+    for t in tests:
+        assert f"[       OK ] {t}" in out.stdout
