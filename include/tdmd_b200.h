@@ -208,6 +208,21 @@ int32_t tdmd_morse_compute(const double* d_positions, void* d_forces, int32_t pr
                            const tdmd_morse_params* params, double* d_energy, double* d_virial,
                            void* stream);
 
+/* compute_morse_gpu_zone, src/potentials/device_morse_zone.cuh:13-23 (the
+ * TD zone pipeline's force call): Morse forces of atoms
+ * [first_atom, first_atom + atom_count) only, from the global positions and
+ * the global neighbor list (dense CSR; neighbor indices are global).  Forces
+ * are ADDED to d_forces[first_atom ..] (the reference's zone kernel
+ * accumulates; zero the range first for the zone's forces); d_energy /
+ * d_virial (nullable) are added to with the range's potential energy and
+ * virial, reduced in a fixed order.  The ID-ordered energy mode does not
+ * apply to this call. */
+int32_t tdmd_morse_compute_zone(const double* d_positions, void* d_forces, int32_t precision,
+                                const int32_t* d_neighbors, const int32_t* d_offsets,
+                                const int32_t* d_counts, int32_t first_atom, int32_t atom_count,
+                                const tdmd_box* box, const tdmd_morse_params* params,
+                                double* d_energy, double* d_virial, void* stream);
+
 /* No counterpart in the reference.  Same arguments and results as
  * tdmd_morse_compute, but it allocates no device memory: the per-block
  * energy/virial partials live in a fixed 1 MiB scratch array compiled into

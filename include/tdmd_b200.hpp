@@ -341,6 +341,22 @@ inline void compute_morse_gpu(const PositionVec* d_positions, ForceVec* d_forces
                                    &p, d_energy, nullptr, detail::stream_ptr(stream)));
 }
 
+// device_morse_zone.cuh:13-23: forces of atoms [first_atom, first_atom +
+// atom_count) ADDED to d_forces (zero the zone first), from the global
+// positions and list; *d_energy accumulated.
+inline void compute_morse_gpu_zone(const PositionVec* d_positions, ForceVec* d_forces,
+                                   const i32* d_neighbors, const i32* d_offsets,
+                                   const i32* d_counts, i32 first_atom, i32 atom_count,
+                                   const Box& box, const MorseParams& params, accum_t* d_energy,
+                                   cudaStream_t stream) {
+  const tdmd_box b = detail::to_c(box);
+  const tdmd_morse_params p = params.to_c();
+  detail::check(tdmd_morse_compute_zone(reinterpret_cast<const double*>(d_positions), d_forces,
+                                        kForcePrecision, d_neighbors, d_offsets, d_counts,
+                                        first_atom, atom_count, &b, &p, d_energy, nullptr,
+                                        detail::stream_ptr(stream)));
+}
+
 #if !defined(TDMD_B200_REFERENCE_CORE)
 // eam_alloy.hpp:47-93 (tables; the CPU compute_forces stays in the reference).
 class EamAlloy {
@@ -709,6 +725,24 @@ inline void device_fused_full_kick_drift(VelocityVec* d_velocities, PositionVec*
 inline void device_zero_forces(ForceVec* d_forces, i32 natoms, cudaStream_t stream = 0) {
   ::tdmd::detail::check(
       tdmd_vv_zero_forces(d_forces, kForcePrecision, natoms, ::tdmd::detail::stream_ptr(stream)));
+}
+
+// device_velocity_verlet_zone.cuh:12-29: the same kernels on atoms
+// [first_atom, first_atom + atom_count) of the arrays.
+inline void device_half_kick_zone(VelocityVec* d_velocities, const ForceVec* d_forces,
+                                  const i32* d_types, const real* d_masses, i32 first_atom,
+                                  i32 atom_count, real dt, cudaStream_t stream) {
+  device_half_kick(d_velocities + first_atom, d_forces + first_atom, d_types + first_atom,
+                   d_masses, atom_count, dt, stream);
+}
+inline void device_drift_zone(PositionVec* d_positions, const VelocityVec* d_velocities,
+                              i32 first_atom, i32 atom_count, real dt, const Box& box,
+                              cudaStream_t stream) {
+  device_drift(d_positions + first_atom, d_velocities + first_atom, atom_count, dt, box, stream);
+}
+inline void device_zero_forces_zone(ForceVec* d_forces, i32 first_atom, i32 atom_count,
+                                    cudaStream_t stream) {
+  device_zero_forces(d_forces + first_atom, atom_count, stream);
 }
 
 // device_nose_hoover.cuh:26-88

@@ -118,6 +118,8 @@ SIGNATURES = {
     "tdmd_nlist_get": [_p, _pp, _pp, _pp, _pi32, C.POINTER(C.c_int64)],
     "tdmd_morse_compute": [_p, _p, _i32, _p, _p, _p, _i32, C.POINTER(Box),
                            C.POINTER(MorseParams), _p, _p, _p],
+    "tdmd_morse_compute_zone": [_p, _p, _i32, _p, _p, _p, _i32, _i32, C.POINTER(Box),
+                                C.POINTER(MorseParams), _p, _p, _p],
     "tdmd_morse_compute_noalloc": [_p, _p, _i32, _p, _p, _p, _i32, C.POINTER(Box),
                                    C.POINTER(MorseParams), _p, _p, _p],
     "tdmd_device_eam_create": [_p, _pp],

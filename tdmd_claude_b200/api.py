@@ -560,6 +560,17 @@ def compute_morse_gpu(d_positions, d_forces, d_neighbors, d_offsets, d_counts, n
          _ptr(d_virial), _stream(stream))
 
 
+def compute_morse_gpu_zone(d_positions, d_forces, d_neighbors, d_offsets, d_counts, first_atom,
+                           atom_count, box: Box, params: MorseParams, d_energy=None, d_virial=None,
+                           precision="fp64", stream=None):
+    """compute_morse_gpu_zone (device_morse_zone.cuh:13-23): forces of atoms
+    [first_atom, first_atom + atom_count) ADDED to d_forces, energy added."""
+    call("tdmd_morse_compute_zone", _ptr(d_positions), _ptr(d_forces), _prec(precision),
+         C.c_void_p(int(d_neighbors)) if d_neighbors else None, C.c_void_p(int(d_offsets)),
+         C.c_void_p(int(d_counts)), int(first_atom), int(atom_count), C.byref(box),
+         C.byref(params), _ptr(d_energy), _ptr(d_virial), _stream(stream))
+
+
 class DeviceEam:
     """DeviceEam (src/potentials/device_eam.cuh:26)."""
 

@@ -474,6 +474,45 @@ int32_t tdmd_morse_compute(const double* d_positions, void* d_forces, int32_t pr
   });
 }
 
+int32_t tdmd_morse_compute_zone(const double* d_positions, void* d_forces, int32_t precision,
+                                const int32_t* d_neighbors, const int32_t* d_offsets,
+                                const int32_t* d_counts, int32_t first_atom, int32_t atom_count,
+                                const tdmd_box* box, const tdmd_morse_params* params,
+                                double* d_energy, double* d_virial, void* stream) {
+  return guarded([&] {
+    TDMD_REQUIRE(box && params, "null box or params");
+    TDMD_REQUIRE(first_atom >= 0 && atom_count >= 0, "first_atom and atom_count must be >= 0");
+    if (atom_count == 0) return;
+    TDMD_REQUIRE(d_positions && d_forces && d_offsets && d_counts, "null device array");
+    cudaStream_t s = as_stream(stream);
+    const bool ev = d_energy || d_virial;
+    const DevBox b = make_devbox(*box, 0.0);
+    // the range's rows: offsets and counts shifted, neighbor indices global
+    const NbrView nl = make_view(d_neighbors, d_offsets + first_atom, d_counts + first_atom);
+    const int lpa = default_lpa(atom_count);
+    const int nblk = force_blocks(atom_count, lpa);
+    Partials part(ev ? nblk : 0, s);
+    if (precision == TDMD_FP64) {
+      GeoAoS64 g{d_positions, {b.L[0], b.L[1], b.L[2]}, {b.halfL[0], b.halfL[1], b.halfL[2]},
+                 {b.periodic[0], b.periodic[1], b.periodic[2]}};
+      MorseP<double> mp{params->d, params->alpha, params->r0, params->rc_sq, params->r0};
+      launch_morse_zone(g, first_atom, nl, atom_count, mp, static_cast<double*>(d_forces), ev,
+                        part.p, lpa, s);
+    } else {
+      TDMD_REQUIRE(precision == TDMD_MIXED, "unknown precision");
+      const GeoAoS32 g = make_geo_aos32(d_positions, b);
+      MorseP<float> mp{float(params->d), float(params->alpha), float(params->r0),
+                       float(params->rc_sq), params->r0};
+      launch_morse_zone(g, first_atom, nl, atom_count, mp, static_cast<float*>(d_forces), ev,
+                        part.p, lpa, s);
+    }
+    if (ev) {
+      launch(k_reduce_partials, 1, 256, 0, s, part.p, nblk, d_energy, d_virial);
+      TDMD_LAUNCH_CHECK();
+    }
+  });
+}
+
 int32_t tdmd_device_eam_create(const tdmd_eam* eam, tdmd_device_eam** out) {
   return guarded([&] {
     TDMD_REQUIRE(eam && out, "null argument");

@@ -373,6 +373,28 @@ struct ForceOut {
   }
 };
 
+// Accumulating force output (the per-zone form: a zone's forces are added to
+// what the caller zeroed, compute_morse_gpu_zone, device_morse_zone.cu).
+template <class F>
+struct ForceAdd {
+  F* f;
+  __device__ __forceinline__ void store(int i, double x, double y, double z) const {
+    f[3ll * i] += static_cast<F>(x);
+    f[3ll * i + 1] += static_cast<F>(y);
+    f[3ll * i + 2] += static_cast<F>(z);
+  }
+};
+
+// A geometry whose own atoms start at `first` of the position array; the
+// neighbors j of a row stay global indices.  A kernel over atoms
+// [first, first + n) then reads its rows, counts and outputs through views
+// shifted by first.
+template <class G>
+struct GeoShift : G {
+  int first;
+  __device__ __forceinline__ typename G::Own own(int i) const { return G::own(first + i); }
+};
+
 // Per-block FP64 energy/virial partials (thread 0 writes 8 doubles).
 __device__ __forceinline__ void write_ev_partials(double e, const double (&w)[6],
                                                   double* __restrict__ partials) {
@@ -411,9 +433,9 @@ struct MorseP {
 
 // EV: 0 forces only; 1 also energy + virial into per-block partials and,
 // where pe_atom is given, per-atom energies; 2 forces + per-atom energies.
-template <class Geo, int LPA, int U, int EV, bool VEC, class F>
+template <class Geo, int LPA, int U, int EV, bool VEC, class F, class Out = ForceOut<F>>
 __global__ void __launch_bounds__(256) k_morse(Geo g, NbrView nl, int n,
-                                               MorseP<typename Geo::T> mp, ForceOut<F> out,
+                                               MorseP<typename Geo::T> mp, Out out,
                                                double* __restrict__ partials,
                                                double* __restrict__ pe_atom) {
   dependent_launch_prologue();

@@ -87,6 +87,28 @@ void launch_morse(const Geo& g, const NbrView& nl, int n, const MorseP<typename 
   TDMD_LAUNCH_CHECK();
 }
 
+// Morse forces of atoms [first, first + n) ADDED to forces[first ..], the
+// neighbor j of a row read at its global index (the per-zone call).  nl's
+// row offsets and counts are those of the range (shifted by the caller);
+// dense CSR rows only, U = kU.
+template <class Geo, class F>
+void launch_morse_zone(const Geo& g, int first, const NbrView& nl, int n,
+                       const MorseP<typename Geo::T>& mp, F* forces, bool ev, double* partials,
+                       int lpa, cudaStream_t s) {
+  const int nblk = force_blocks(n, lpa);
+  const GeoShift<Geo> gs{g, first};
+  const ForceAdd<F> out{forces + 3ll * first};
+  TDMD_LPA_DISPATCH(lpa, {
+    if (ev)
+      launch(k_morse<GeoShift<Geo>, L, kU, 1, false, F, ForceAdd<F>>, nblk, kForceThreads, 0, s,
+             gs, nl, n, mp, out, partials, nullptr);
+    else
+      launch(k_morse<GeoShift<Geo>, L, kU, 0, false, F, ForceAdd<F>>, nblk, kForceThreads, 0, s,
+             gs, nl, n, mp, out, nullptr, nullptr);
+  });
+  TDMD_LAUNCH_CHECK();
+}
+
 // Density + embedding pass.  gout (fixed-point geometries only) receives
 // the force pass's {q, F'} gather records; e_out (nullable) each atom's
 // embedding energy F(rho_i).

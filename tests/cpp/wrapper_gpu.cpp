@@ -6,6 +6,8 @@
 // (17 significant digits), then the free-function energy and forces.
 #include <cuda_runtime_api.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <vector>
 
@@ -91,6 +93,55 @@ int main(int argc, char** argv) {
   } catch (const Error& e) {
     std::fprintf(stderr, "error %d: %s\n", e.status(), e.what());
     return 9;
+  }
+  // the zone calls of the TD pipeline on the same list: two zones' forces
+  // added into zeroed forces equal the whole-system forces; a zone half kick
+  // moves only its zone
+  try {
+    ForceVec* d_fz = nullptr;
+    VelocityVec* d_v = nullptr;
+    i32* d_t = nullptr;
+    real* d_m = nullptr;
+    accum_t* d_ez = nullptr;
+    cudaMalloc(reinterpret_cast<void**>(&d_fz), sizeof(ForceVec) * n);
+    cudaMalloc(reinterpret_cast<void**>(&d_v), sizeof(VelocityVec) * n);
+    cudaMalloc(reinterpret_cast<void**>(&d_t), sizeof(i32) * n);
+    cudaMalloc(reinterpret_cast<void**>(&d_m), sizeof(real) * masses.size());
+    cudaMalloc(reinterpret_cast<void**>(&d_ez), sizeof(accum_t));
+    cudaMemset(d_ez, 0, sizeof(accum_t));
+    cudaMemset(d_v, 0, sizeof(VelocityVec) * n);
+    cudaMemcpy(d_t, types.data(), sizeof(i32) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_m, masses.data(), sizeof(real) * masses.size(), cudaMemcpyHostToDevice);
+    neighbors::DeviceNeighborList nl;
+    nl.build(d_pos, n, box, rc, real(0.3));
+    const i32 half = n / 2;
+    integrator::device_zero_forces_zone(d_fz, 0, half, nullptr);
+    integrator::device_zero_forces_zone(d_fz, half, n - half, nullptr);
+    potentials::compute_morse_gpu_zone(d_pos, d_fz, nl.d_neighbors(), nl.d_offsets(),
+                                       nl.d_counts(), 0, half, box, mp, d_ez, nullptr);
+    potentials::compute_morse_gpu_zone(d_pos, d_fz, nl.d_neighbors(), nl.d_offsets(),
+                                       nl.d_counts(), half, n - half, box, mp, d_ez, nullptr);
+    integrator::device_half_kick_zone(d_v, d_fz, d_t, d_m, half, n - half, real(0.001), nullptr);
+    std::vector<ForceVec> fz(static_cast<size_t>(n));
+    std::vector<VelocityVec> vz(static_cast<size_t>(n));
+    accum_t ez = 0;
+    cudaMemcpy(fz.data(), d_fz, sizeof(ForceVec) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(vz.data(), d_v, sizeof(VelocityVec) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(&ez, d_ez, sizeof(ez), cudaMemcpyDeviceToHost);
+    double df = 0, vlo = 0, vhi = 0;
+    for (int i = 0; i < n; ++i) {
+      df = std::max(df, std::abs(static_cast<double>(fz[i].x) - static_cast<double>(forces[i].x)));
+      (i < half ? vlo : vhi) += std::abs(vz[i].x) + std::abs(vz[i].y) + std::abs(vz[i].z);
+    }
+    std::fprintf(out, "%.17g %.17g %.17g %.17g\n", ez, df, vlo, vhi);
+    cudaFree(d_fz);
+    cudaFree(d_v);
+    cudaFree(d_t);
+    cudaFree(d_m);
+    cudaFree(d_ez);
+  } catch (const Error& e) {
+    std::fprintf(stderr, "error %d: %s\n", e.status(), e.what());
+    return 10;
   }
   std::fclose(out);
   cudaFree(d_pos);

@@ -56,6 +56,12 @@ def test_cpp_layer_runs_gpu_path(cuda, tmp_path, define, precision):
     e_cpp = float(rows[n])
     f_cpp = np.array([[float(x) for x in l.split()] for l in rows[n + 1:2 * n + 1]])
     cells = rows[2 * n + 1].split()
+    # zone calls: two zones = the whole system; the zone kick moved its zone only
+    ez, dfz, vlo, vhi = (float(x) for x in rows[2 * n + 2].split())
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert abs(ez - e_cpp) <= tol * abs(e_cpp)
+    assert dfz <= tol * np.abs(f_cpp).max()
+    assert vlo == 0.0 and vhi > 0.0
     L = hi - lo
     nc = max(3, int(np.floor(L / (6.0 + rd_(precision)(0.3)))))
     assert [int(x) for x in cells[:3]] == [nc] * 3
