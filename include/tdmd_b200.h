@@ -430,9 +430,12 @@ int32_t tdmd_sched_atom_order(const tdmd_sched* s, const int32_t** d_order);
 int32_t tdmd_sched_neighbor_list(const tdmd_sched* s, int32_t* counts, int32_t* neighbors,
                                  int64_t capacity, int64_t* total);
 /* Per-kernel timing (no reference counterpart; the reference profiles only
- * from outside with nsys/ncu).  While on, windows run without graph replay
- * and CUDA events on the scheduler's stream bracket each phase; averages in
- * ms per launch for the phases {kick+drift, neighbor rebuild, EAM density,
+ * from outside with nsys/ncu).  While on, CUDA events bracket each phase:
+ * windows replay graphs of their own whose event-record nodes surround each
+ * phase (their kernels launch without programmatic serialization, so each
+ * phase is timed alone), or, with use_graphs off, events recorded on the
+ * scheduler's stream.  Results are those of an untimed run.  Averages in ms
+ * per launch for the phases {kick+drift, neighbor rebuild, EAM density,
  * force, other} go to avg_ms[0..4], launch counts to counts[0..4]. */
 int32_t tdmd_sched_set_profiling(tdmd_sched* s, int32_t on);
 int32_t tdmd_sched_kernel_times(const tdmd_sched* s, double* avg_ms, int64_t* counts,

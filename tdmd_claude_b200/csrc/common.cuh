@@ -221,6 +221,9 @@ __device__ __forceinline__ void dependent_launch_prologue() { grid_dependency_wa
 // Whether launch() sets the programmatic-serialization attribute (environment
 // TDMD_PDL=0 turns it off; read once per process).
 bool programmatic_launch();
+// Turns the attribute off for this host thread's launches while set (a
+// profiling capture: event nodes sit between its kernels).
+void suppress_programmatic_launch(bool off);
 
 template <class... P, class... A>
 void launch(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,

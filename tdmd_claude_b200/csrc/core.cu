@@ -39,13 +39,19 @@ int sm_count() {
   return v;
 }
 
+namespace {
+thread_local bool t_pdl_suppressed = false;
+}
+
 bool programmatic_launch() {
   static const bool on = [] {
     const char* v = std::getenv("TDMD_PDL");
     return !(v && v[0] == '0');
   }();
-  return on;
+  return on && !t_pdl_suppressed;
 }
+
+void suppress_programmatic_launch(bool off) { t_pdl_suppressed = off; }
 
 DevBox make_devbox(const tdmd_box& b, double r_list) {
   DevBox d{};

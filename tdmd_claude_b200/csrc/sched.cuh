@@ -57,9 +57,18 @@ enum ProfCat : int {
   kProfCount = 5
 };
 
+// A phase's timing events: category, start, end.
+struct ProfEvents {
+  int cat;
+  cudaEvent_t a, b;
+};
+
 struct GraphEntry {
   cudaGraphExec_t exec = nullptr;
   long long kernels = 0;
+  // profiling graphs: the event-record nodes captured around each phase,
+  // recorded again by every replay (owned by the entry)
+  std::vector<ProfEvents> prof;
 };
 
 class Scheduler {
@@ -148,7 +157,7 @@ class Scheduler {
   void prof_collect();
   // bin + scan + scatter + sort
   int cell_list_kernels() const { return 3 + device_scan_launches(cl_.ncells); }
-  void reorder_by_cell();
+  void reorder_by_cell(cudaEvent_t side_done = nullptr);
   // Keyed cell list of the current positions; returns the kernels launched.
   int build_cells();
   int* ctl_status() const {
@@ -207,6 +216,14 @@ class Scheduler {
   DevArray<int> cellmax_;
   int* h_cellmax_ = nullptr;
   int max_cell_ = 0;
+  // Upload: velocities, ids and forces come in on a side stream while the
+  // positions are binned on stream_ (joined before the cell-order gather);
+  // the small per-type and control copies go from a pinned block, so they
+  // never hold the host back behind the stream.
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t up_ev_[2] = {nullptr, nullptr};
+  unsigned char* h_stage_ = nullptr;
+  size_t h_stage_cap_ = 0;
 
   // Neighbor list: padded rows of cap_ entries.
   CellListDev cl_;
@@ -234,6 +251,12 @@ class Scheduler {
   double last_window_ms_ = 0.0;
   bool profiling_ = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending_;
+  // events of replayed profiling graphs awaiting this window's collection,
+  // the capture in progress (nullable), and events of evicted graphs freed at
+  // the next collection
+  std::vector<ProfEvents> prof_graph_pending_;
+  std::vector<ProfEvents>* prof_sink_ = nullptr;
+  std::vector<ProfEvents> prof_retired_;
   std::vector<cudaEvent_t> prof_pool_;
   cudaEvent_t prof_open_ = nullptr;
   double prof_ms_[kProfCount] = {0, 0, 0, 0, 0};

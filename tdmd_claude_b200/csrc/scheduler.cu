@@ -438,15 +438,30 @@ Scheduler::Scheduler(const tdmd_box& box, int natoms, const tdmd_fast_pipeline_c
   nvt_ = cfg.t_target > 0.0 && cfg.nhc_length > 0;
   thermo_ = nvt_ || cfg.adaptive_dt != 0;
   TDMD_CU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  TDMD_CU(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
   TDMD_CU(cudaEventCreate(&win_ev_[0]));
   TDMD_CU(cudaEventCreate(&win_ev_[1]));
+  TDMD_CU(cudaEventCreateWithFlags(&up_ev_[0], cudaEventDisableTiming));
+  TDMD_CU(cudaEventCreateWithFlags(&up_ev_[1], cudaEventDisableTiming));
   ctl_.reserve(1);
   snap_ctl_.reserve(1);
 }
 
 Scheduler::~Scheduler() {
   clear_graphs();
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (const ProfEvents& pe : prof_retired_) {
+    cudaEventDestroy(pe.a);
+    cudaEventDestroy(pe.b);
+  }
   if (h_cellmax_) cudaFreeHost(h_cellmax_);
+  if (side_) {
+    cudaStreamSynchronize(side_);
+    cudaStreamDestroy(side_);
+  }
+  if (h_stage_) cudaFreeHost(h_stage_);
+  for (auto e : up_ev_)
+    if (e) cudaEventDestroy(e);
   for (auto& pe : prof_pending_) {
     cudaEventDestroy(pe.second.first);
     cudaEventDestroy(pe.second.second);
@@ -514,42 +529,61 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
   n_types_ = n_types;
   uploaded_ = false;
   cells_from_upload_ = false;
+  // Masses, kick factors and the control block through the pinned block
+  // (the previous upload's copies from it finished at its synchronisation).
+  const size_t stage_bytes = 2 * sizeof(double) * static_cast<size_t>(n_types) + sizeof(SchedCtl);
+  if (h_stage_cap_ < stage_bytes) {
+    if (h_stage_) cudaFreeHost(h_stage_);
+    h_stage_ = nullptr;
+    h_stage_cap_ = 0;
+    TDMD_CU(cudaMallocHost(reinterpret_cast<void**>(&h_stage_), stage_bytes));
+    h_stage_cap_ = stage_bytes;
+  }
+  double* h_masses = reinterpret_cast<double*>(h_stage_);
+  double* h_inv = h_masses + n_types;
+  SchedCtl* h_ctl = reinterpret_cast<SchedCtl*>(h_inv + n_types);
   if (n_ > 0) {
-    TDMD_CU(cudaMemcpyAsync(stage_.data(), x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
-    TDMD_CU(cudaMemcpyAsync(vel_.data(), v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    // stream_: types and positions, then packing and the cell list; side_
+    // (after stream_'s earlier work): velocities, ids, forces.
+    TDMD_CU(cudaEventRecord(up_ev_[0], s));
+    TDMD_CU(cudaStreamWaitEvent(side_, up_ev_[0], 0));
     TDMD_CU(cudaMemcpyAsync(types_.data(), types, n * sizeof(int), cudaMemcpyHostToDevice, s));
+    TDMD_CU(cudaMemcpyAsync(stage_.data(), x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    TDMD_CU(cudaMemcpyAsync(vel_.data(), v, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
+                            side_));
     if (ids)
-      TDMD_CU(cudaMemcpyAsync(ids_.data(), ids, n * sizeof(int), cudaMemcpyHostToDevice, s));
+      TDMD_CU(cudaMemcpyAsync(ids_.data(), ids, n * sizeof(int), cudaMemcpyHostToDevice, side_));
     else
-      TDMD_CU(cudaMemsetAsync(ids_.data(), 0, n * sizeof(int), s));
+      TDMD_CU(cudaMemsetAsync(ids_.data(), 0, n * sizeof(int), side_));
     const size_t fb = 3 * n * (mixed_ ? sizeof(float) : sizeof(double));
     void* fd = mixed_ ? static_cast<void*>(f32_.data()) : static_cast<void*>(f64_.data());
     if (f)
-      TDMD_CU(cudaMemcpyAsync(fd, f, fb, cudaMemcpyHostToDevice, s));
+      TDMD_CU(cudaMemcpyAsync(fd, f, fb, cudaMemcpyHostToDevice, side_));
     else
-      TDMD_CU(cudaMemsetAsync(fd, 0, fb, s));
+      TDMD_CU(cudaMemsetAsync(fd, 0, fb, side_));
+    TDMD_CU(cudaEventRecord(up_ev_[1], side_));
     launch(k_pack_positions, ceil_div(n_, kThreads), kThreads, 0, s, stage_.data(), types_.data(),
            n_, box_, pos4_.data(), mixed_ ? q_.data() : nullptr);
     TDMD_LAUNCH_CHECK();
-    reorder_by_cell();
+    reorder_by_cell(up_ev_[1]);
   }
-  TDMD_CU(cudaMemcpyAsync(masses_.data(), masses, sizeof(double) * n_types,
+  std::copy(masses, masses + n_types, h_masses);
+  TDMD_CU(cudaMemcpyAsync(masses_.data(), h_masses, sizeof(double) * n_types,
                           cudaMemcpyHostToDevice, s));
   // Kick factor per unit dt, 1/(m mvv2e) -- the reference divides per atom
   // (device_velocity_verlet.cu:100-102); one host division per type here.
-  std::vector<double> inv(static_cast<size_t>(n_types), 0.0);
-  for (int t = 0; t < n_types; ++t)
-    inv[static_cast<size_t>(t)] = masses[t] > 0.0 ? 1.0 / (masses[t] * kMvv2e) : 0.0;
+  for (int t = 0; t < n_types; ++t) h_inv[t] = masses[t] > 0.0 ? 1.0 / (masses[t] * kMvv2e) : 0.0;
   inv_mm_.reserve(static_cast<size_t>(n_types));
-  TDMD_CU(cudaMemcpyAsync(inv_mm_.data(), inv.data(), sizeof(double) * n_types,
+  TDMD_CU(cudaMemcpyAsync(inv_mm_.data(), h_inv, sizeof(double) * n_types,
                           cudaMemcpyHostToDevice, s));
   // Control block: dt, unit scale, fresh chain.
-  SchedCtl h{};
-  h.dt = cfg_.dt;
-  h.scale = 1.0;
+  *h_ctl = SchedCtl{};
+  h_ctl->dt = cfg_.dt;
+  h_ctl->scale = 1.0;
   if (nvt_)
-    nhc_init(h.eta, h.eta_v, h.eta_m, cfg_.nhc_length, cfg_.t_target, cfg_.t_period, 3 * n_ - 3);
-  TDMD_CU(cudaMemcpyAsync(ctl_.data(), &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    nhc_init(h_ctl->eta, h_ctl->eta_v, h_ctl->eta_m, cfg_.nhc_length, cfg_.t_target,
+             cfg_.t_period, 3 * n_ - 3);
+  TDMD_CU(cudaMemcpyAsync(ctl_.data(), h_ctl, sizeof(SchedCtl), cudaMemcpyHostToDevice, s));
   // Scratch sized for the chosen lanes-per-atom.
   // Energy partials sized for the widest lanes-per-atom the autotuner tries.
   const int nblk_force = force_blocks(n_ > 0 ? n_ : 1, 32);
@@ -584,8 +618,9 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
 }
 
 // Permutes the uploaded state into the cell order of its positions:
-// order_ = the cell list's atoms (index order within each cell).
-void Scheduler::reorder_by_cell() {
+// order_ = the cell list's atoms (index order within each cell).  side_done
+// (nullable): the event after which the rest of the state is on the device.
+void Scheduler::reorder_by_cell(cudaEvent_t side_done) {
   cudaStream_t s = stream_;
   const size_t n = static_cast<size_t>(n_);
   build_cell_list(cl_, pos4_.data(), PosLayout::D4, n_, box_, s);
@@ -598,6 +633,7 @@ void Scheduler::reorder_by_cell() {
   TDMD_CU(cudaMemcpyAsync(order_.data(), cl_.cell_atoms.data(), n * sizeof(int),
                           cudaMemcpyDeviceToDevice, s));
   // Gather into the second set of buffers, then swap them in.
+  if (side_done) TDMD_CU(cudaStreamWaitEvent(s, side_done, 0));
   pos4_alt_.reserve(n);
   vel_alt_.reserve(3 * n);
   types_alt_.reserve(n);
@@ -968,6 +1004,7 @@ void Scheduler::enqueue_finalize() {
 void Scheduler::clear_graphs() {
   for (auto& kv : graphs_) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (const ProfEvents& pe : kv.second.prof) prof_retired_.push_back(pe);
   }
   graphs_.clear();
   graph_lru_.clear();
@@ -981,8 +1018,9 @@ void Scheduler::run_segment(const std::vector<StepPlan>& seg, bool finalize, int
                   (st.kd_fused ? 16 : 0) | (st.fuse_next ? 32 : 0));
   key.push_back(finalize ? 1 : 0);
   key.push_back(prologue);
+  key.push_back(profiling_ ? 1 : 0);
   const long long l0 = launches_;
-  if (!cfg_.use_graphs || profiling_) {
+  if (!cfg_.use_graphs) {
     enqueue_prologue(prologue);
     for (const auto& st : seg) enqueue_step(st);
     if (finalize) enqueue_finalize();
@@ -994,23 +1032,35 @@ void Scheduler::run_segment(const std::vector<StepPlan>& seg, bool finalize, int
       auto old = graphs_.find(graph_lru_.back());
       if (old != graphs_.end()) {
         cudaGraphExecDestroy(old->second.exec);
+        for (const ProfEvents& pe : old->second.prof) prof_retired_.push_back(pe);
         graphs_.erase(old);
       }
       graph_lru_.pop_back();
     }
     cudaGraph_t g = nullptr;
+    GraphEntry ge{};
+    // Profiling graphs carry event-record nodes around each phase and plain
+    // edges between kernels (no programmatic launch inside them).
+    if (profiling_) {
+      prof_sink_ = &ge.prof;
+      suppress_programmatic_launch(true);
+    }
     TDMD_CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     try {
       enqueue_prologue(prologue);
       for (const auto& st : seg) enqueue_step(st);
       if (finalize) enqueue_finalize();
     } catch (...) {
+      prof_sink_ = nullptr;
+      suppress_programmatic_launch(false);
       cudaStreamEndCapture(stream_, &g);
       if (g) cudaGraphDestroy(g);
+      for (const ProfEvents& pe : ge.prof) prof_retired_.push_back(pe);
       throw;
     }
+    prof_sink_ = nullptr;
+    suppress_programmatic_launch(false);
     TDMD_CU(cudaStreamEndCapture(stream_, &g));
-    GraphEntry ge{};
     ge.kernels = launches_ - l0;
     const cudaError_t ie = cudaGraphInstantiate(&ge.exec, g, 0);
     cudaGraphDestroy(g);
@@ -1025,6 +1075,7 @@ void Scheduler::run_segment(const std::vector<StepPlan>& seg, bool finalize, int
   TDMD_CU(cudaGraphLaunch(it->second.exec, stream_));
   launches_ += it->second.kernels;
   ++graph_launches_;
+  for (const ProfEvents& pe : it->second.prof) prof_graph_pending_.push_back(pe);
 }
 
 // ----- run_until --------------------------------------------------------------
@@ -1349,6 +1400,11 @@ void Scheduler::set_profiling(bool on) {
 
 void Scheduler::prof_begin(int /*cat*/) {
   if (!profiling_) return;
+  if (prof_sink_) {  // capturing: an event-record node the graph owns
+    TDMD_CU(cudaEventCreate(&prof_open_));
+    TDMD_CU(cudaEventRecordWithFlags(prof_open_, stream_, cudaEventRecordExternal));
+    return;
+  }
   if (prof_pool_.empty()) {
     cudaEvent_t e;
     TDMD_CU(cudaEventCreate(&e));
@@ -1361,6 +1417,14 @@ void Scheduler::prof_begin(int /*cat*/) {
 
 void Scheduler::prof_end(int cat) {
   if (!profiling_ || !prof_open_) return;
+  if (prof_sink_) {
+    cudaEvent_t e;
+    TDMD_CU(cudaEventCreate(&e));
+    TDMD_CU(cudaEventRecordWithFlags(e, stream_, cudaEventRecordExternal));
+    prof_sink_->push_back({cat, prof_open_, e});
+    prof_open_ = nullptr;
+    return;
+  }
   cudaEvent_t e;
   if (prof_pool_.empty()) {
     TDMD_CU(cudaEventCreate(&e));
@@ -1384,6 +1448,19 @@ void Scheduler::prof_collect() {
     prof_pool_.push_back(pe.second.second);
   }
   prof_pending_.clear();
+  for (const ProfEvents& pe : prof_graph_pending_) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pe.a, pe.b) == cudaSuccess) {
+      prof_ms_[pe.cat] += ms;
+      prof_n_[pe.cat] += 1;
+    }
+  }
+  prof_graph_pending_.clear();
+  for (const ProfEvents& pe : prof_retired_) {
+    cudaEventDestroy(pe.a);
+    cudaEventDestroy(pe.b);
+  }
+  prof_retired_.clear();
 }
 
 void Scheduler::kernel_times(double* avg_ms, long long* counts, int ncat) const {

@@ -642,3 +642,37 @@ def test_launches_without_programmatic_dependent_launch_agree(cuda, tmp_path):
         assert r.returncode == 0, r.stderr
         out[flag] = np.load(path)
     assert np.array_equal(out["0"], out["1"])
+
+
+@pytest.mark.parametrize("use_graphs", [True, False])
+def test_phase_timing_inside_replayed_windows(cuda, use_graphs):
+    """Per-phase timing (tdmd_sched_set_profiling): with graphs, the windows
+    replay graphs of their own whose event-record nodes bracket each phase;
+    every phase of every step is counted, the phases add up to about the
+    window, and the trajectory is that of an untimed run bit for bit."""
+    # one fixed launch shape (the autotuner's timed choice could differ)
+    a, _, _ = _eam_setup("mixed", ncell=10, use_graphs=use_graphs, lanes_per_atom=4)
+    b, _, _ = _eam_setup("mixed", ncell=10, use_graphs=use_graphs, lanes_per_atom=4)
+    for s in (a, b):
+        s.run_until(10)
+    a.set_profiling(True)
+    win = []
+    for w in range(2, 5):
+        a.run_until(10 * w)
+        win.append(a.last_window_ms())
+    kt = a.kernel_times()
+    a.set_profiling(False)
+    for w in range(2, 5):  # the same windows (a window fuses its inner kicks)
+        b.run_until(10 * w)
+    assert kt["force"][1] == 30 and kt["density"][1] == 30  # 3 windows x 10 steps
+    assert kt["rebuild"][1] == 3
+    assert all(ms > 0 for ms, n in kt.values() if n > 0)
+    phases = sum(ms * n for ms, n in kt.values())
+    assert 0.5 * sum(win) < phases < 1.05 * sum(win)
+    sa, sb = a.download(), b.download()
+    assert np.array_equal(sa.positions, sb.positions)
+    assert np.array_equal(sa.forces, sb.forces)
+    # back to the plain graphs: still the same bits
+    a.run_until(50)
+    b.run_until(50)
+    assert np.array_equal(a.download().velocities, b.download().velocities)
