@@ -510,6 +510,52 @@ def morse256_bench(torch, nsteps=1000):
     return out
 
 
+def td_ring_bench(torch, ncell=32, steps=30):
+    """The TD zone ring (DistributedPipelineScheduler) on one rank: 32^3 Cu
+    FCC (131 072 atoms), Morse rc 6.0, skin 0.3, 300 K, FP64, windows of 10
+    steps, host wall clock around synchronised run_until calls (its steps are
+    orchestrated from the host: one kick-drift, one force call per zone and
+    one closing kick per step); beside it the library's FastPipelineScheduler
+    on the same system and schedule, device time.  Both the same state at the
+    end (max position difference reported)."""
+    from tdmd_claude_b200 import Box, FastPipelineScheduler, MorseParams, make_config
+    from tdmd_claude_b200 import workloads as W
+    from tdmd_claude_b200.distributed import DistributedConfig, DistributedPipelineScheduler
+    sysm = W.fcc_system(ncell, 3.615, 300.0, 4321)
+    box, mp_ = Box.make(sysm.lo, sysm.hi), MorseParams.make(*W.MORSE_CU)
+    ring = DistributedPipelineScheduler(box, sysm.n, mp_, DistributedConfig(
+        dt=DT, r_skin=SKIN, rebuild_every=WINDOW))
+    ring.upload(sysm.positions, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+    ring.run_until(WINDOW)                   # warm-up window
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ring.run_until(WINDOW + steps)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    fast = FastPipelineScheduler(box, sysm.n, mp_, make_config(
+        dt=DT, r_skin=SKIN, rebuild_every=WINDOW, precision="fp64"))
+    fast.upload(sysm.positions, sysm.velocities, None, sysm.types, sysm.ids, sysm.masses)
+    fast.run_until(WINDOW)
+    ms = 0.0
+    for w in range(steps // WINDOW):
+        fast.run_until(WINDOW * (w + 2))
+        ms += fast.last_window_ms()
+    p, _, _, _, ids = ring.download()
+    q = fast.download().positions
+    L = np.array(sysm.hi) - np.array(sysm.lo)
+    d = p[np.argsort(ids)] - q
+    d -= np.round(d / L) * L
+    fast.close()
+    return {"workload": f"Cu FCC {ncell}^3 cells = {sysm.n} atoms, Morse rc 6.0, skin 0.3, "
+                        "300 K, FP64, rebuild every 10",
+            "ranks": 1, "zones": ring.partition().n_zones,
+            "value": sysm.n * steps / wall, "unit": "atom-steps/s",
+            "ms_per_step": 1e3 * wall / steps, "timing": "host wall clock",
+            "fast_pipeline_value": sysm.n * steps / (ms * 1e-3),
+            "max_abs_position_diff_vs_fast_pipeline": float(np.abs(d).max()),
+            "note": "one rank; the ring exchange (NCCL) is unmeasured on one GPU"}
+
+
 def ternary_bench(steps, warmup, flush, torch, total_steps=2000):
     """Equiatomic random ternary FCC alloy, 100^3 cells = 4,000,000 atoms
     (a = 3.56 A), per-species analytic EAM, mixed precision, NVT
@@ -1013,6 +1059,7 @@ def main():
             beam["nve_drift"] = dr
     fitfig = None if args.no_fit else fit_bench(torch)
     small = None if args.no_batch else morse256_bench(torch)
+    ring = None if (args.no_batch or world > 1) else td_ring_bench(torch)
     ternary = None if args.no_ternary else ternary_bench(max(3, args.steps // 3), 3, flush,
                                                            torch)
     sizes = None if args.no_sizes else size_scaling_bench(max(3, args.steps // 5), 3, flush,
@@ -1109,6 +1156,7 @@ def main():
                 "ternary_4m_nvt_adaptive": ternary,
                 "single_system_sizes": sizes,
                 "morse_256_nve_1000": small,
+                "td_ring_morse_131k": ring,
                 "force_matching": fitfig,
                 "wall_s_timed_region": wall_mixed,
                 "reference_gpu_same_run": ref_gpu,

@@ -46,8 +46,10 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+import ctypes as C
+
 from . import api
-from ._lib import Box, MorseParams
+from ._lib import Box, MorseParams, check, lib
 
 
 # --------------------------------------------------------------------------
@@ -362,6 +364,8 @@ class DistributedPipelineScheduler:
         self.part.build_zone_neighbors(r_list)
         self.span = self.part.span(r_list)
         self.plan = ring_plan(self.part, self._rank, self._size, self.span)
+        self._ghosts = self.part.ghost_zones(self._rank)
+        self._zone_calls = None
         self.stats_ = DistributedStats()
         self.dev = torch.device("cuda", torch.cuda.current_device())
         self.s = _State()
@@ -508,6 +512,23 @@ class DistributedPipelineScheduler:
                 setattr(self.s, name, getattr(self.s, name).index_select(0, p).contiguous())
             self.stats_.rezones += 1
         self.nlist.build(self.s.pos, self.natoms, self.box, self.params.rc, self.cfg.r_skin)
+        self._zone_calls = self._prepare_zone_calls()
+
+    def _prepare_zone_calls(self):
+        """The argument lists of the local zones' force calls, fixed until
+        the next rebuild (list and state arrays are not reallocated between
+        rebuilds)."""
+        nb, off, cnt = self.nlist._get()[:3]
+        fn = lib().tdmd_morse_compute_zone
+        head = (C.c_void_p(self.s.pos.data_ptr()), C.c_void_p(self.s.forces.data_ptr()),
+                api._prec(self.cfg.precision), C.c_void_p(nb), C.c_void_p(off), C.c_void_p(cnt))
+        tail = (C.byref(self.box), C.byref(self.params), None, None, None)
+        calls = []
+        for z in range(*self.plan.local):
+            zn = self.part.zones[z]
+            if zn.natoms_in_zone:
+                calls.append(head + (zn.atom_offset, zn.natoms_in_zone) + tail)
+        return fn, calls
 
     def _local_forces(self):
         """One zone call per local zone (launch_zone_step's force call,
@@ -515,13 +536,11 @@ class DistributedPipelineScheduler:
         own atom count, the same for every rank count."""
         a, b = self._local()
         api.device_zero_forces(self.s.forces[a:b], b - a)
-        nb, off, cnt = self.nlist.d_neighbors(), self.nlist.d_offsets(), self.nlist.d_counts()
-        for z in range(*self.plan.local):
-            zn = self.part.zones[z]
-            if zn.natoms_in_zone:
-                api.compute_morse_gpu_zone(self.s.pos, self.s.forces, nb, off, cnt,
-                                           zn.atom_offset, zn.natoms_in_zone, self.box,
-                                           self.params, precision=self.cfg.precision)
+        fn, calls = self._zone_calls
+        for args in calls:
+            rc = fn(*args)
+            if rc != 0:
+                check(rc)
 
     def _check_deps(self, ghost_ts):
         """I-2 (pipeline_scheduler.cu:93-121): each local zone's ghosts are
@@ -600,7 +619,7 @@ class DistributedPipelineScheduler:
             z0, z1 = self.plan.local
             for z in range(z0, z1):
                 self.part.zones[z].time_step = self._step
-            for z in self.part.ghost_zones(self._rank):
+            for z in self._ghosts:
                 self.part.zones[z].time_step = self._step
             self.stats_.kernel_launches += z1 - z0
             self.stats_.ticks += 1

@@ -164,12 +164,12 @@ def _run(world, rank, case, out):
                exchanges=st.exchanges, ticks=st.ticks, mgts=s.min_global_time_step(),
                fails=st.dep_check_failures)
     if out is not None:
-        np.savez(os.path.join(out, f"r{rank}.npz"), **res)
+        np.savez(out, **res)
     torch.cuda.synchronize()
     return res
 
 
-def _rank_main(rank, world, port, case, out):
+def _rank_main(rank, world, port, cases, out):
     import torch
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -178,7 +178,8 @@ def _rank_main(rank, world, port, case, out):
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=120))
     try:
-        _run(world, rank, case, out)
+        for k, case in enumerate(cases):
+            _run(world, rank, case, os.path.join(out, f"c{k}_r{rank}.npz"))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -193,29 +194,31 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}c-{c[2]}-{'nvt' if c[3] else 'nve'}")
 @pytest.mark.parametrize("world", [2, 3])
-def test_ranks_give_the_one_rank_bits(cuda, tmp_path, case, world):
+def test_ranks_give_the_one_rank_bits(cuda, tmp_path, world):
+    """Every case of CASES (FP64 / mixed NVE, FP64 NVT, a 3-zone system) run
+    by `world` processes: each rank's final state is the one-rank state."""
     import torch.multiprocessing as mp
-    from tdmd_claude_b200.distributed import ZonePartition
     from tdmd_claude_b200 import Box
-    pos, _, _, lo, hi = _system(case[0], case[1], 5)
-    zp = ZonePartition()
-    zp.build(Box.make(lo, hi), MORSE[3])
-    assert zp.n_zones >= world
-    one = _run(1, 0, case, None)
-    mp.spawn(_rank_main, args=(world, _free_port(), case, str(tmp_path)), nprocs=world,
+    from tdmd_claude_b200.distributed import ZonePartition
+    mp.spawn(_rank_main, args=(world, _free_port(), CASES, str(tmp_path)), nprocs=world,
              join=True)
-    for r in range(world):
-        got = np.load(tmp_path / f"r{r}.npz")
-        for k in ("pos", "vel", "frc", "ids"):
-            assert np.array_equal(got[k], one[k]), (r, k)
-        assert got["pe"] == one["pe"] and got["ke"] == one["ke"]
-        assert int(got["exchanges"]) == case[4] and int(got["ticks"]) == case[4]
-        assert int(got["mgts"]) == case[4] and int(got["fails"]) == 0
-        assert int(got["rezones"]) == one["rezones"]
-    if case[0] == 8:
-        assert one["rezones"] > 0  # atoms crossed zone slabs: zones re-assigned
+    for k, case in enumerate(CASES):
+        pos, _, _, lo, hi = _system(case[0], case[1], 5)
+        zp = ZonePartition()
+        zp.build(Box.make(lo, hi), MORSE[3])
+        assert zp.n_zones >= world
+        one = _run(1, 0, case, None)
+        for r in range(world):
+            got = np.load(tmp_path / f"c{k}_r{r}.npz")
+            for key in ("pos", "vel", "frc", "ids"):
+                assert np.array_equal(got[key], one[key]), (case, r, key)
+            assert got["pe"] == one["pe"] and got["ke"] == one["ke"]
+            assert int(got["exchanges"]) == case[4] and int(got["ticks"]) == case[4]
+            assert int(got["mgts"]) == case[4] and int(got["fails"]) == 0
+            assert int(got["rezones"]) == one["rezones"]
+        if case[0] == 8:
+            assert one["rezones"] > 0  # atoms crossed zone slabs: zones re-assigned
 
 
 def _reference_tests_main(rank, world, port, out):
