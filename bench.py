@@ -1087,8 +1087,8 @@ def main():
 
     # e2e: every rank times its own steps; the job's time is the slowest rank's
     from tdmd_claude_b200.replicas import max_over_ranks
-    e2e_steps = max(3, args.steps // 3)
-    e2e_wall, h2d, d2h = e2e_windows(sysm, eam, e2e_steps, 2, torch, dist)
+    e2e_steps = max(3, args.steps)
+    e2e_wall, h2d, d2h = e2e_windows(sysm, eam, e2e_steps, max(3, args.warmup), torch, dist)
     e2e_wall = max_over_ranks(e2e_wall, dist, "cuda")
     e2e_value = world * sysm.n * WINDOW * e2e_steps / e2e_wall
 
@@ -1176,7 +1176,8 @@ def main():
             "kernel_ms": {"mixed": kt, "fp64": kt64,
                           "density_bytes_per_launch": dens_bytes},
             "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "timing": "wall clock per step"},
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                    "timing": "wall clock over the steps (barriers on both sides)"},
             "gpu_launches": launches,
             "clocks": clk,
             "cpu_baseline": cpu,
