@@ -35,6 +35,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "integrate.cuh"
 #include "replicas.cuh"
@@ -206,6 +208,48 @@ struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
 };
 
+// FP64 pair from a gather record: the neighbor's F'(rho) rides along.
+struct PairDF {
+  double dx, dy, dz, r2;
+  double fw;
+};
+
+// FP64, scheduler gather records double4 {x, y, z, F'(rho)} written by the
+// density pass: the force pass reads a neighbor's position and F' with one
+// 32-byte load instead of a position record plus a separate F' gather.
+struct GeoD4F {
+  using T = double;
+  static constexpr bool kRecords = false;
+  using Own = double3;
+  using Pair = PairDF;
+  const double4* p;
+  double L[3], halfL[3];
+  int per[3];
+  __device__ __forceinline__ Own own(int i) const {
+    const double4 a = ld_d4(p + i);
+    return make_double3(a.x, a.y, a.z);
+  }
+  __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
+    const double4 q = ld_d4(p + j);
+    pr.dx = min_image1(o.x - q.x, L[0], halfL[0], per[0]);
+    pr.dy = min_image1(o.y - q.y, L[1], halfL[1], per[1]);
+    pr.dz = min_image1(o.z - q.z, L[2], halfL[2], per[2]);
+    pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
+    pr.fw = q.w;
+  }
+  __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
+                                         double& rd) const {
+    r = sqrt(pr.r2);
+    rinv = 1.0 / r;
+    rd = r;
+  }
+  __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
+  // F'(rho_j) of a pair's record
+  __device__ __forceinline__ double gather_fp(const Pair& pr, int /*tmask*/) const {
+    return pr.fw;
+  }
+};
+
 struct GeoAoS64 {  // FP64, reference Vec3D AoS
   using T = double;
   static constexpr bool kRecords = false;
@@ -301,6 +345,10 @@ struct GeoQ {
     radius_q(pr.r2, pr.res, r, rinv, rd);
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
+  // F'(rho_j) of a gather record: the 4th word's float bits, type bits cleared
+  __device__ __forceinline__ float gather_fp(const Pair& pr, int tmask) const {
+    return __int_as_float(pr.w & ~tmask);
+  }
 };
 
 __host__ inline GeoQ make_geoq(const int4* q, const DevBox& b) {
@@ -644,7 +692,8 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
                                                      double* __restrict__ fpd_out,
                                                      int4* __restrict__ gout,
                                                      double* __restrict__ partials,
-                                                     double* __restrict__ e_out) {
+                                                     double* __restrict__ e_out,
+                                                     double4* __restrict__ gout64) {
   dependent_launch_prologue();
   using T = typename Geo::T;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -704,6 +753,9 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
     if (rho_out) rho_out[i] = rh;
     if (fpd_out) fpd_out[i] = dF;
     if (e_out) e_out[i] = Fi;
+    if constexpr (std::is_same_v<Geo, GeoD4>) {
+      if (gout64) gout64[i] = make_double4(o.x, o.y, o.z, dF);
+    }
     if constexpr (Geo::kRecords) {
       if (gout) {
         int4 rec = g.record(o);
@@ -818,7 +870,7 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
           const int idx = spline_at(r, rd, e.dr, e.inv_dr, e.nr, e.dr_d, sx);
           const int j = jj[u];
           int tj = 0;
-          if constexpr (MULTI && FPG)
+          if constexpr (MULTI && FPG && Geo::kRecords)
             tj = packed ? (pr[u].w & tmask) : __ldg(types + j) - 1;
           else if constexpr (MULTI)
             tj = __ldg(types + j) - 1;
@@ -835,7 +887,7 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
           if (MULTI && tj != ti) dri = dspl_der(ldv4<T>(rowp + ti), sx);
           T fpj;
           if constexpr (FPG) {
-            fpj = __int_as_float(pr[u].w & ~tmask);
+            fpj = g.gather_fp(pr[u], tmask);
           } else {
             fpj = static_cast<T>(__ldg(fp + j));
           }

@@ -110,21 +110,23 @@ void launch_morse_zone(const Geo& g, int first, const NbrView& nl, int n,
 }
 
 // Density + embedding pass.  gout (fixed-point geometries only) receives
-// the force pass's {q, F'} gather records; e_out (nullable) each atom's
-// embedding energy F(rho_i).
+// the force pass's {q, F'} gather records, gout64 (GeoD4 only) its FP64
+// records {x, y, z, F'}; e_out (nullable) each atom's embedding energy
+// F(rho_i).
 template <class Geo, class FP>
 void launch_eam_density(const Geo& g, const NbrView& nl, int n,
                         const EamDev<typename Geo::T>& e, const int* types, FP* fp,
                         double* rho_out, double* fpd_out, int4* gout, bool ev, double* partials,
-                        Tune tn, cudaStream_t s, double* e_out = nullptr) {
+                        Tune tn, cudaStream_t s, double* e_out = nullptr,
+                        double4* gout64 = nullptr) {
   const int nblk = force_blocks(n, tn.lpa);
   TDMD_MULTI_DISPATCH(types != nullptr, TDMD_VEC_DISPATCH(vec_rows(nl), TDMD_TUNE_DISPATCH(tn, {
     if (ev)
       launch(k_eam_density<Geo, L, U, true, V, M, FP>, nblk, kForceThreads, 0, s, g, nl, n, e,
-             types, fp, rho_out, fpd_out, gout, partials, e_out);
+             types, fp, rho_out, fpd_out, gout, partials, e_out, gout64);
     else
       launch(k_eam_density<Geo, L, U, false, V, M, FP>, nblk, kForceThreads, 0, s, g, nl, n, e,
-             types, fp, rho_out, fpd_out, gout, nullptr, e_out);
+             types, fp, rho_out, fpd_out, gout, nullptr, e_out, gout64);
   })));
   TDMD_LAUNCH_CHECK();
 }

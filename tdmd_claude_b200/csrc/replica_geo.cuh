@@ -60,6 +60,10 @@ struct GeoQB {
     radius_q(pr.r2, pr.res, r, rinv, rd);
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return pr.r2 * rsqrtf(pr.r2); }
+  // F'(rho_j) of a gather record: the 4th word's float bits, type bits cleared
+  __device__ __forceinline__ float gather_fp(const Pair& pr, int tmask) const {
+    return __int_as_float(pr.w & ~tmask);
+  }
 };
 
 // FP64: double4 positions, per-replica minimum image.

@@ -202,6 +202,7 @@ class Scheduler {
   DevArray<double> masses_;
   DevArray<double> inv_mm_;  // 1 / (m mvv2e) per type: the kick factor per unit dt
   DevArray<int4> g_;         // mixed EAM: {qx, qy, qz, bits(F'(rho))} per atom
+  DevArray<double4> g64_;    // FP64 EAM: {x, y, z, F'(rho)} per atom
   mutable DevArray<double> stage_;
   // Atoms are held in the cell order of the uploaded positions (neighbors of
   // an atom then sit at nearby indices, whatever order the caller used);

@@ -594,7 +594,7 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
     if (mixed_)
       fp32_.reserve(n), g_.reserve(n);
     else
-      fp64_.reserve(n);
+      fp64_.reserve(n), g64_.reserve(n);
   }
   if (cfg_.energy_every > 0) {
     log_cap_ = cfg_.energy_log_capacity > 0 ? cfg_.energy_log_capacity : 1024;
@@ -834,18 +834,24 @@ void Scheduler::enqueue_force(bool ev, bool kd, int parts) {
         prof_end(kProfForce);
       }
     } else {
+      // Density reads the position records and writes {x, y, z, F'} gather
+      // records; the force pass gathers those.
       GeoD4 g{pos4_.data(), {box_.L[0], box_.L[1], box_.L[2]},
               {box_.halfL[0], box_.halfL[1], box_.halfL[2]},
               {box_.periodic[0], box_.periodic[1], box_.periodic[2]}};
+      GeoD4F gg{g64_.data(), {box_.L[0], box_.L[1], box_.L[2]},
+                {box_.halfL[0], box_.halfL[1], box_.halfL[2]},
+                {box_.periodic[0], box_.periodic[1], box_.periodic[2]}};
       if (parts & kPassDensity) {
         prof_begin(kProfDensity);
         launch_eam_density<GeoD4, double>(g, nl, n_, eam_->d64, types, fp64_.data(), nullptr,
-                                          nullptr, nullptr, ev, part, td, s);
+                                          nullptr, nullptr, ev, part, td, s, nullptr,
+                                          g64_.data());
         prof_end(kProfDensity);
       }
       if (parts & kPassForce) {
         prof_begin(kProfForce);
-        launch_eam_force<GeoD4, false, double, double>(g, nl, n_, eam_->d64, types,
+        launch_eam_force<GeoD4F, true, double, double>(gg, nl, n_, eam_->d64, types,
                                                        fp64_.data(), f64_.data(), ev, part2, tf,
                                                        s);
         prof_end(kProfForce);
