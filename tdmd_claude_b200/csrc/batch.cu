@@ -302,6 +302,7 @@ class Batch {
   DevArray<float> fp32_;
   DevArray<double> fp64_, rho_;
   DevArray<int4> g_;                   // mixed EAM gather records {q, bits(F')}
+  DevArray<double4> g64_;              // FP64 EAM gather records {x, y, z, F'}
   std::vector<RepDesc> hreps_;
   int ncells_ = 0;
   int lpa_ = 0;
@@ -482,7 +483,7 @@ void Batch::upload(const double* x, const double* v, const int* types, const dou
     if (mixed_)
       fp32_.reserve(nn), g_.reserve(nn);
     else
-      fp64_.reserve(nn);
+      fp64_.reserve(nn), g64_.reserve(nn);
   }
   pos4_.reserve(nn);
   vel_.reserve(3 * nn);
@@ -574,7 +575,7 @@ void Batch::force(bool kd, bool pea, int parts) {
   const int n = static_cast<int>(n_);
   const Tune td{lpa_d_, nu_d_}, tf{lpa_, nu_};
   const bool dens = parts & kPassDensity, pair = parts & kPassForce;
-  TDMD_REQUIRE(!kd || (eam_ && mixed_), "fused kick-drift needs the mixed EAM batch");
+  TDMD_REQUIRE(!kd || eam_, "fused kick-drift needs the EAM batch");
   if (eam_) {
     // Density + embedding, then forces, over all replicas at once (the
     // single scheduler's passes on the batched geometries).
@@ -596,15 +597,20 @@ void Batch::force(bool kd, bool pea, int parts) {
                                                     kd ? &kdr : nullptr,
                                                     pea ? pe_atom_.data() : nullptr);
     } else {
+      // FP64: the density pass writes {x, y, z, F'} gather records, which the
+      // force pass reads (so it may also kick and drift, like the mixed pass)
       const GeoD4B g{pos4_.data(), rep_.data(), imgs_.data()};
+      const GeoD4BF gg{g64_.data(), rep_.data(), imgs_.data()};
       if (dens)
         launch_eam_density<GeoD4B, double>(g, nl, n, eam_->d64, types, fp64_.data(), nullptr,
                                            nullptr, nullptr, false, nullptr, td, s,
-                                           pea ? pe_atom_.data() : nullptr);
+                                           pea ? pe_atom_.data() : nullptr, g64_.data());
+      const KickDrift kdr{pos4_.data(), nullptr, vel_.data(), types_.data(), inv_mm_.data(),
+                          cfg_.dt, nullptr, DevBox{}, rep_.data(), reps_.data()};
       if (pair)
-        launch_eam_force<GeoD4B, false, double, double>(g, nl, n, eam_->d64, types,
+        launch_eam_force<GeoD4BF, true, double, double>(gg, nl, n, eam_->d64, types,
                                                         fp64_.data(), f64_.data(), pea, nullptr,
-                                                        tf, s, nullptr,
+                                                        tf, s, kd ? &kdr : nullptr,
                                                         pea ? pe_atom_.data() : nullptr);
     }
     launches_ += (dens ? 1 : 0) + (pair ? 1 : 0);
@@ -867,9 +873,10 @@ void Batch::run_until(int target) {
       b.rebuild = since >= cfg_.rebuild_every;
       if (b.rebuild) since = 0;
       ++since;
-      // mixed EAM: every force pass but the window's last also kicks and
-      // drifts for the next step (energies are logged after the window)
-      b.fuse_next = eam_ && mixed_ && st + 1 < target;
+      // EAM (both precisions): every force pass but the window's last also
+      // kicks and drifts for the next step (energies are logged after the
+      // window)
+      b.fuse_next = eam_ && st + 1 < target;
       b.kd_fused = !plan.empty() && plan.back().fuse_next;
       b.log_e = log_now && st + 1 == target;
       plan.push_back(b);

@@ -179,8 +179,16 @@ __device__ __forceinline__ void radius_f(float r2, double r2d, float& r, float& 
        static_cast<double>(static_cast<float>(fma(-static_cast<double>(r), r, r2d)) * 0.5f * rinv);
 }
 
+// Geometries whose density pass may write FP64 gather records {x, y, z, F'}
+// (their own atom's position as x, y, z members) declare kD4Out.
+template <class G, class = void>
+struct has_d4out : std::false_type {};
+template <class G>
+struct has_d4out<G, std::void_t<decltype(G::kD4Out)>> : std::bool_constant<G::kD4Out> {};
+
 struct GeoD4 {  // FP64, scheduler layout double4 {x,y,z,type}
   using T = double;
+  static constexpr bool kD4Out = true;
   static constexpr bool kRecords = false;  // no fixed-point gather records
   using Own = double3;
   using Pair = PairD;
@@ -753,7 +761,7 @@ __global__ void __launch_bounds__(256) k_eam_density(Geo g, NbrView nl, int n,
     if (rho_out) rho_out[i] = rh;
     if (fpd_out) fpd_out[i] = dF;
     if (e_out) e_out[i] = Fi;
-    if constexpr (std::is_same_v<Geo, GeoD4>) {
+    if constexpr (has_d4out<Geo>::value) {
       if (gout64) gout64[i] = make_double4(o.x, o.y, o.z, dF);
     }
     if constexpr (Geo::kRecords) {
@@ -793,8 +801,10 @@ struct KickDrift {
   const RepDesc* reps;
 };
 
-__device__ __forceinline__ void kick_drift_atom(const KickDrift& k, int i, float fx, float fy,
-                                                float fz) {
+// FT: the force type (float: mixed, also refreshes the fixed-point record;
+// double: FP64, which keeps no fixed-point copy).
+template <class FT>
+__device__ __forceinline__ void kick_drift_atom(const KickDrift& k, int i, FT fx, FT fy, FT fz) {
   const DevBox& b = k.reps ? k.reps[__ldg(k.rep + i)].box : k.b;
   const int t = __ldg(k.types + i);
   const double factor = k.dt * __ldg(k.inv_mm + t);
@@ -810,8 +820,9 @@ __device__ __forceinline__ void kick_drift_atom(const KickDrift& k, int i, float
   k.v[3ll * i + 1] = vy;
   k.v[3ll * i + 2] = vz;
   k.pos4[i] = p;
-  k.q[i] = make_int4(encode_q(p.x, b.qlo[0], b.qinv[0]), encode_q(p.y, b.qlo[1], b.qinv[1]),
-                     encode_q(p.z, b.qlo[2], b.qinv[2]), t);
+  if constexpr (sizeof(FT) == sizeof(float))
+    k.q[i] = make_int4(encode_q(p.x, b.qlo[0], b.qinv[0]), encode_q(p.y, b.qlo[1], b.qinv[1]),
+                       encode_q(p.z, b.qlo[2], b.qinv[2]), t);
 }
 
 // Pass 3: f_ij = -(phi' + fp_i rho'_tj + fp_j rho'_ti)/r * (r_i - r_j).
@@ -912,9 +923,9 @@ __global__ void __launch_bounds__(256) k_eam_force(Geo g, NbrView nl, int n,
   if (active && sub == 0) {
     out.store(i, fx.value(), fy.value(), fz.value());
     if constexpr (KD) {
-      static_assert(FPG && sizeof(F) == sizeof(float), "fused kick-drift: mixed gather pass");
-      kick_drift_atom(kd, i, static_cast<float>(fx.value()), static_cast<float>(fy.value()),
-                      static_cast<float>(fz.value()));
+      static_assert(FPG, "fused kick-drift: a force pass that reads gather records");
+      kick_drift_atom(kd, i, static_cast<F>(fx.value()), static_cast<F>(fy.value()),
+                      static_cast<F>(fz.value()));
     }
   }
   if (KD && kd.step && blockIdx.x == 0 && threadIdx.x == 0) *kd.step += 1;

@@ -110,7 +110,7 @@ void launch_morse_zone(const Geo& g, int first, const NbrView& nl, int n,
 }
 
 // Density + embedding pass.  gout (fixed-point geometries only) receives
-// the force pass's {q, F'} gather records, gout64 (GeoD4 only) its FP64
+// the force pass's {q, F'} gather records, gout64 (GeoD4 / GeoD4B) its FP64
 // records {x, y, z, F'}; e_out (nullable) each atom's embedding energy
 // F(rho_i).
 template <class Geo, class FP>
@@ -132,8 +132,9 @@ void launch_eam_density(const Geo& g, const NbrView& nl, int n,
 }
 
 // Force pass.  FPG: the geometry reads gather records that carry F'(rho).
-// kd (nullable; FPG with float forces only): also apply the next step's
-// kick + drift to each atom after its force.  With ev: per-block partials
+// kd (nullable; FPG only -- the pass then never reads the positions it
+// updates): also apply the next step's kick + drift to each atom after its
+// force.  With ev: per-block partials
 // (nullable) and per-atom energies added to pe_atom (nullable; holds
 // F(rho_i) from the density pass).
 template <class Geo, bool FPG, class FP, class F>
@@ -149,7 +150,7 @@ void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typen
     else if (ev)
       launch(k_eam_force<Geo, L, U, 1, FPG, V, M, FP, F>, nblk, kForceThreads, 0, s, g, nl, n, e,
              types, fp, ForceOut<F>{forces}, partials, KickDrift{}, pe_atom);
-    else if constexpr (FPG && sizeof(F) == sizeof(float)) {
+    else if constexpr (FPG) {
       if (kd)
         launch(k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F, true>, nblk, kForceThreads, 0, s, g, nl,
                n, e, types, fp, ForceOut<F>{forces}, nullptr, *kd, nullptr);
@@ -157,7 +158,7 @@ void launch_eam_force(const Geo& g, const NbrView& nl, int n, const EamDev<typen
         launch(k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F>, nblk, kForceThreads, 0, s, g, nl, n, e,
                types, fp, ForceOut<F>{forces}, nullptr, KickDrift{}, nullptr);
     } else {
-      TDMD_REQUIRE(kd == nullptr, "fused kick-drift needs the mixed gather-record pass");
+      TDMD_REQUIRE(kd == nullptr, "fused kick-drift needs a gather-record force pass");
       launch(k_eam_force<Geo, L, U, 0, FPG, V, M, FP, F>, nblk, kForceThreads, 0, s, g, nl, n, e,
              types, fp, ForceOut<F>{forces}, nullptr, KickDrift{}, nullptr);
     }

@@ -69,6 +69,7 @@ struct GeoQB {
 // FP64: double4 positions, per-replica minimum image.
 struct GeoD4B {
   using T = double;
+  static constexpr bool kD4Out = true;  // the density pass may write {x, y, z, F'} records
   struct Own {
     double x, y, z;
     double L0, L1, L2, h0, h1, h2;
@@ -115,6 +116,40 @@ struct GeoD4B {
     rd = r;
   }
   __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
+};
+
+// FP64 gather records {x, y, z, F'(rho)} of a batch (written by the
+// density pass), per-replica minimum image: the force pass reads a
+// neighbor's position and F' with one 32-byte load.
+struct GeoD4BF {
+  using T = double;
+  using Own = GeoD4B::Own;
+  using Pair = PairDF;
+  static constexpr bool kRecords = false;
+  const double4* p;
+  const int* rep;
+  const RepImg* img;
+  __device__ __forceinline__ Own own(int i) const {
+    return GeoD4B{p, rep, img}.own(i);
+  }
+  __device__ __forceinline__ void pair(const Own& o, int j, Pair& pr) const {
+    const double4 q = ld_d4(p + j);
+    pr.dx = min_image1(o.x - q.x, o.L0, o.h0, o.p0);
+    pr.dy = min_image1(o.y - q.y, o.L1, o.h1, o.p1);
+    pr.dz = min_image1(o.z - q.z, o.L2, o.h2, o.p2);
+    pr.r2 = pr.dx * pr.dx + pr.dy * pr.dy + pr.dz * pr.dz;
+    pr.fw = q.w;
+  }
+  __device__ __forceinline__ void radius(const Own&, const Pair& pr, T& r, T& rinv,
+                                         double& rd) const {
+    r = sqrt(pr.r2);
+    rinv = 1.0 / r;
+    rd = r;
+  }
+  __device__ __forceinline__ T radius_fast(const Pair& pr) const { return sqrt(pr.r2); }
+  __device__ __forceinline__ double gather_fp(const Pair& pr, int /*tmask*/) const {
+    return pr.fw;
+  }
 };
 
 __host__ inline RepImg rep_img(const DevBox& b) {

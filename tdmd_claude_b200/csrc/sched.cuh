@@ -129,7 +129,9 @@ class Scheduler {
   // parts: which EAM passes (density, pair force); Morse has one pass.
   static constexpr int kPassDensity = 1, kPassForce = 2, kPassBoth = 3;
   void enqueue_force(bool ev, bool kd = false, int parts = kPassBoth);
-  bool can_fuse_kick() const { return mixed_ && kind_ == TDMD_POT_EAM && !thermo_; }
+  // The EAM force passes of both precisions read gather records, never the
+  // positions, so they can carry the next step's kick + drift (NVE only).
+  bool can_fuse_kick() const { return kind_ == TDMD_POT_EAM && !thermo_; }
   template <class F>
   void enqueue_kick_drift_t(F* f, bool full, bool scale);
   void enqueue_kick_drift(bool full, bool scale);

@@ -787,7 +787,7 @@ void Scheduler::enqueue_rebuild() {
 
 // ----- forces ---------------------------------------------------------------
 void Scheduler::enqueue_force(bool ev, bool kd, int parts) {
-  TDMD_REQUIRE(!kd || can_fuse_kick(), "fused kick-drift needs the mixed EAM NVE path");
+  TDMD_REQUIRE(!kd || can_fuse_kick(), "fused kick-drift needs the EAM NVE path");
   cudaStream_t s = stream_;
   const NbrView nl{nbr_.data(), nullptr, cnt_.data(), cap_};
   const int nblk = force_blocks(n_, lpa_);       // pair-force pass records
@@ -849,11 +849,16 @@ void Scheduler::enqueue_force(bool ev, bool kd, int parts) {
                                           g64_.data());
         prof_end(kProfDensity);
       }
+      const KickDrift kdr{pos4_.data(), nullptr, vel_.data(), types_.data(), inv_mm_.data(),
+                          cfg_.dt,
+                          reinterpret_cast<long long*>(reinterpret_cast<char*>(ctl_.data()) +
+                                                       offsetof(SchedCtl, step)),
+                          box_, nullptr, nullptr};
       if (parts & kPassForce) {
         prof_begin(kProfForce);
         launch_eam_force<GeoD4F, true, double, double>(gg, nl, n_, eam_->d64, types,
                                                        fp64_.data(), f64_.data(), ev, part2, tf,
-                                                       s);
+                                                       s, kd ? &kdr : nullptr);
         prof_end(kProfForce);
       }
     }

@@ -513,15 +513,17 @@ def test_neighbor_batch_sizes(cuda, precision):
     s.close()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("use_graphs", [True, False])
-def test_mixed_eam_fused_kick_equals_unfused(cuda, use_graphs):
-    """Mixed EAM NVE fuses the next step's kick + drift into the force pass
-    except on energy-log steps.  Logging every step (nothing fused) and
-    logging never (all but window-end steps fused) give bit-identical
-    trajectories; a log every 5 steps carries the right step numbers."""
+def test_mixed_eam_fused_kick_equals_unfused(cuda, use_graphs, precision):
+    """EAM NVE (both precisions) fuses the next step's kick + drift into the
+    force pass except on energy-log steps.  Logging every step (nothing
+    fused) and logging never (all but window-end steps fused) give
+    bit-identical trajectories; a log every 5 steps carries the right step
+    numbers."""
     runs = []
     for every in (0, 1, 5):
-        s, sysm, _ = _eam_setup("mixed", ncell=5, lanes_per_atom=4, use_graphs=use_graphs,
+        s, sysm, _ = _eam_setup(precision, ncell=5, lanes_per_atom=4, use_graphs=use_graphs,
                                 energy_every=every, energy_log_capacity=64)
         for t in (7, 20, 33):
             s.run_until(t)
