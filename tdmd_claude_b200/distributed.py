@@ -41,12 +41,11 @@ library's FastPipelineScheduler).
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 from dataclasses import dataclass, field
 
 import numpy as np
-
-import ctypes as C
 
 from . import api
 from ._lib import Box, MorseParams, check, lib
