@@ -136,10 +136,13 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _system(ncell, temp, seed):
+def _system(ncell, temp, seed, vac=0.0):
+    """ncell^3 FCC Cu; vac > 0 lengthens the box along x by that much
+    vacuum (a periodic slab)."""
     from tdmd_claude_b200 import workloads as W
     s = W.fcc_system(ncell, 3.615, temp, seed=seed)
-    return s.positions, s.velocities, s.masses, s.lo, s.hi
+    hi = (s.hi[0] + vac, s.hi[1], s.hi[2])
+    return s.positions, s.velocities, s.masses, s.lo, hi
 
 
 MORSE = (0.3429, 1.3588, 2.866, 6.0)
@@ -149,8 +152,8 @@ def _run(world, rank, case, out):
     import torch
     from tdmd_claude_b200 import Box, MorseParams
     from tdmd_claude_b200.distributed import DistributedConfig, DistributedPipelineScheduler
-    ncell, temp, precision, nvt, steps = case
-    pos, vel, masses, lo, hi = _system(ncell, temp, 5)
+    ncell, temp, precision, nvt, steps, vac = case
+    pos, vel, masses, lo, hi = _system(ncell, temp, 5, vac)
     cfg = DistributedConfig(dt=0.001, r_skin=0.3, rebuild_every=10, precision=precision,
                             t_target=temp if nvt else 0.0)
     s = DistributedPipelineScheduler(Box.make(lo, hi), len(pos), MorseParams.make(*MORSE), cfg)
@@ -186,25 +189,29 @@ def _rank_main(rank, world, port, cases, out):
 
 
 CASES = [
-    # ncell, T, precision, NVT, steps
-    (8, 900.0, "fp64", False, 60),
-    (8, 900.0, "mixed", False, 60),
-    (8, 600.0, "fp64", True, 40),
-    (6, 900.0, "fp64", False, 30),   # 3 zones: the reference test's layout
+    # ncell, T, precision, NVT, steps, vacuum along x
+    (8, 900.0, "fp64", False, 60, 0.0),
+    (8, 900.0, "mixed", False, 60, 0.0),
+    (8, 600.0, "fp64", True, 40, 0.0),
+    (6, 900.0, "fp64", False, 30, 0.0),   # 3 zones: the reference test's layout
+    # a slab: 8 zones of 6.26 A, the last three empty -- with 3 ranks the
+    # last rank owns no atom and sends and receives empty runs
+    (8, 900.0, "fp64", False, 30, 21.16),
 ]
 
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_ranks_give_the_one_rank_bits(cuda, tmp_path, world):
-    """Every case of CASES (FP64 / mixed NVE, FP64 NVT, a 3-zone system) run
-    by `world` processes: each rank's final state is the one-rank state."""
+    """Every case of CASES (FP64 / mixed NVE, FP64 NVT, a 3-zone system, a
+    slab with empty zones) run by `world` processes: each rank's final state
+    is the one-rank state."""
     import torch.multiprocessing as mp
     from tdmd_claude_b200 import Box
     from tdmd_claude_b200.distributed import ZonePartition
     mp.spawn(_rank_main, args=(world, _free_port(), CASES, str(tmp_path)), nprocs=world,
              join=True)
     for k, case in enumerate(CASES):
-        pos, _, _, lo, hi = _system(case[0], case[1], 5)
+        pos, _, _, lo, hi = _system(case[0], case[1], 5, case[5])
         zp = ZonePartition()
         zp.build(Box.make(lo, hi), MORSE[3])
         assert zp.n_zones >= world
@@ -217,8 +224,11 @@ def test_ranks_give_the_one_rank_bits(cuda, tmp_path, world):
             assert int(got["exchanges"]) == case[4] and int(got["ticks"]) == case[4]
             assert int(got["mgts"]) == case[4] and int(got["fails"]) == 0
             assert int(got["rezones"]) == one["rezones"]
-        if case[0] == 8:
+        if case[0] == 8 and case[5] == 0.0:
             assert one["rezones"] > 0  # atoms crossed zone slabs: zones re-assigned
+        if case[5] > 0.0:
+            counts = np.bincount(zp.zone_of(pos[:, 0]), minlength=zp.n_zones)
+            assert zp.n_zones == 8 and (counts[5:] == 0).all() and (counts[:5] > 0).all()
 
 
 def _reference_tests_main(rank, world, port, out):
