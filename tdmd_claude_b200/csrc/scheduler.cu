@@ -544,11 +544,13 @@ void Scheduler::upload(const double* x, const double* v, const void* f, const in
   SchedCtl* h_ctl = reinterpret_cast<SchedCtl*>(h_inv + n_types);
   if (n_ > 0) {
     // stream_: types and positions, then packing and the cell list; side_
-    // (after stream_'s earlier work): velocities, ids, forces.
-    TDMD_CU(cudaEventRecord(up_ev_[0], s));
-    TDMD_CU(cudaStreamWaitEvent(side_, up_ev_[0], 0));
+    // (after stream_'s earlier work and those two copies, so that the
+    // positions do not share the bus with the rest): velocities, ids,
+    // forces, while the positions are binned.
     TDMD_CU(cudaMemcpyAsync(types_.data(), types, n * sizeof(int), cudaMemcpyHostToDevice, s));
     TDMD_CU(cudaMemcpyAsync(stage_.data(), x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    TDMD_CU(cudaEventRecord(up_ev_[0], s));
+    TDMD_CU(cudaStreamWaitEvent(side_, up_ev_[0], 0));
     TDMD_CU(cudaMemcpyAsync(vel_.data(), v, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
                             side_));
     if (ids)
